@@ -1,0 +1,346 @@
+/*
+ * CPU oracle: C/OpenMP restatement of DFTBaby's Fortran kernels on the
+ * LR-TD-DFTB path.  TEST INFRASTRUCTURE ONLY -- used by tests/, the smoke
+ * check and bench.py's CPU baseline; never by the product path.
+ *
+ * Restated from (file:line inside the DFTBaby project):
+ *   splev_uniform / fpbspl  DFTB/extensions/splines.f90:25-92, 118-148
+ *   directional_cosines     DFTB/extensions/slako.f90:31-70
+ *   H0andS                  DFTB/extensions/slako.f90:77-231
+ *   DipoleMatrix            DFTB/extensions/slako.f90:238-394
+ *   SK rules (s,p subset)   DFTB/extensions/slako_transformations_lmax2.f90
+ *                           DFTB/extensions/slako_transformations_dipole_lmax2.f90
+ *   trans_charges           DFTB/extensions/tddftb.f90:12-112
+ *   monopoles               DFTB/extensions/mulliken.f90:11-66
+ *
+ * Array layouts are C row-major.  Symmetric matrices (S, H0, P) are Norb x Norb.
+ * The dipole matrix is returned as three planes D[c][mu][nu], c = x,y,z.
+ * Transition charges are q[A][p][q] (A = atom index first), i.e. numpy arrays
+ * of the reference's logical shape (Nat, n1, n2).
+ *
+ * The Slater-Koster angular rules are written in tensor form (see sk_rule and
+ * sk_dipole_rule); tests/golden/sk_rules.npz pins them against the reference's
+ * own per-case rule table.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ---- B-splines ------------------------------------------------------- */
+
+/* De Boor-Cox recurrence for the k+1 non-zero B-splines at x, knot interval l
+ * (1-based, as in the Fortran).  splines.f90:118-148 */
+static void fpbspl(const double *t, int k, double x, int l, double *h)
+{
+    double hh[5];
+    h[0] = 1.0;
+    for (int j = 1; j <= k; ++j) {
+        for (int i = 1; i <= j; ++i) hh[i - 1] = h[i - 1];
+        h[0] = 0.0;
+        for (int i = 1; i <= j; ++i) {
+            int li = l + i, lj = li - j;
+            double f = hh[i - 1] / (t[li - 1] - t[lj - 1]);
+            h[i - 1] = h[i - 1] + f * (t[li - 1] - x);
+            h[i] = f * (x - t[lj - 1]);
+        }
+    }
+}
+
+/* Bug-compatible evaluation of a spline with uniformly spaced interior knots.
+ * splines.f90:25-92.  The interval index is l = INT((x - t(1))/dt) + 1 with
+ * dt = t(k+3) - t(k+2); for not-a-knot knots from splrep this selects the
+ * piece two knots to the left of the containing interval, and arguments at or
+ * beyond t(n-k) are clamped there.  A coefficient index below 1 (reachable
+ * only for x < 3*dt, i.e. nuclei closer than ~0.12 bohr) reads outside the
+ * array in the reference; it contributes zero here. */
+double oracle_splev_uniform(const double *t, int n, const double *c, int k, double x)
+{
+    int k1 = k + 1, nk1 = n - k1;
+    double tb = t[k1 - 1], te = t[nk1];
+    double arg;
+    int l;
+    if (x <= tb) {
+        arg = tb;
+        l = k1;
+    } else if (x >= te) {
+        arg = te;
+        l = nk1;
+    } else {
+        arg = x;
+        double dt = t[k1 + 1] - t[k1];
+        l = (int)((x - t[0]) / dt) + 1;
+    }
+    if (l < k) l = k1;
+    double h[6];
+    fpbspl(t, k, arg, l, h);
+    double sp = 0.0;
+    int ll = l - k1;
+    for (int j = 1; j <= k1; ++j) {
+        ++ll;
+        if (ll >= 1) sp += c[ll - 1] * h[j - 1];
+    }
+    return sp;
+}
+
+/* ---- Slater-Koster angular rules ------------------------------------- */
+
+/* real spherical harmonic index m -> Cartesian axis (m=-1: y, 0: z, 1: x) */
+static inline int axis_of_m(int m) { return m == -1 ? 1 : (m == 0 ? 2 : 0); }
+
+/* S or H0 element between orbital (l1,m1) on centre 1 and (l2,m2) on centre 2,
+ * e = unit vector from centre 1 to centre 2, V = SK integrals of the pair
+ * (table index as in the reference: 0 ss-sigma, 2 sp-sigma, 4 ps-sigma,
+ * 5 pp-pi, 6 pp-sigma).  Equivalent to slako_transformations_lmax2.f90 for l<=1. */
+double oracle_sk_rule(int l1, int m1, int l2, int m2, const double *e, const double *V)
+{
+    if (l1 == 0 && l2 == 0) return V[0];
+    if (l1 == 0 && l2 == 1) return e[axis_of_m(m2)] * V[2];
+    if (l1 == 1 && l2 == 0) return e[axis_of_m(m1)] * V[4];
+    int a = axis_of_m(m1), b = axis_of_m(m2);
+    return (a == b ? V[5] : 0.0) + e[a] * e[b] * (V[6] - V[5]);
+}
+
+/* Dipole element <l1 m1| r_c |l2 m2> (c: 0=x,1=y,2=z) with dipole SK integrals
+ * D (indices 1,3,4 for s-s/s-p; 6,13 for p-s; 7,8,14 for p-p).  Equivalent to
+ * slako_transformations_dipole_lmax2.f90 for l<=1. */
+double oracle_sk_dipole_rule(int l1, int m1, int c, int l2, int m2, const double *e, const double *D)
+{
+    if (l1 == 0 && l2 == 0) return e[c] * D[3];
+    if (l1 == 0 && l2 == 1) {
+        int b = axis_of_m(m2);
+        return (c == b ? D[1] : 0.0) + e[c] * e[b] * (D[4] - D[1]);
+    }
+    if (l1 == 1 && l2 == 0) {
+        int b = axis_of_m(m1);
+        return (c == b ? D[6] : 0.0) + e[c] * e[b] * (D[13] - D[6]);
+    }
+    int a = axis_of_m(m1), b = axis_of_m(m2);
+    double r = e[a] * e[c] * e[b] * (D[14] - D[7] - 2.0 * D[8]);
+    if (a == c) r += e[b] * D[7];
+    if (c == b) r += e[a] * D[8];
+    if (a == b) r += e[c] * D[8];
+    return r;
+}
+
+/* ---- geometry ---------------------------------------------------------- */
+
+/* r(i,j) and unit vectors from atom j to atom i; z=1 on the diagonal.
+ * slako.f90:31-70.  r,x,y,z are Nat x Nat row-major with [i][j]. */
+void oracle_directional_cosines(int nat, const double *pos, double *r, double *x, double *y, double *z)
+{
+#pragma omp parallel for
+    for (int j = 0; j < nat; ++j)
+        for (int i = 0; i < nat; ++i) {
+            double xc = pos[3 * i] - pos[3 * j];
+            double yc = pos[3 * i + 1] - pos[3 * j + 1];
+            double zc = pos[3 * i + 2] - pos[3 * j + 2];
+            double rr = sqrt(xc * xc + yc * yc + zc * zc);
+            size_t o = (size_t)i * nat + j;
+            r[o] = rr;
+            if (rr > 0.0) {
+                x[o] = xc / rr;
+                y[o] = yc / rr;
+                z[o] = zc / rr;
+            } else {
+                x[o] = 0.0;
+                y[o] = 0.0;
+                z[o] = 1.0;
+            }
+        }
+}
+
+/* direction and distance from atom i (orbital mu) to atom j (orbital nu):
+ * the reference reads r(j,i), x(j,i), ... = (pos_j - pos_i)/r */
+static void pair_geometry(const double *pos, int i, int j, double *rij, double *e)
+{
+    double xc = pos[3 * j] - pos[3 * i];
+    double yc = pos[3 * j + 1] - pos[3 * i + 1];
+    double zc = pos[3 * j + 2] - pos[3 * i + 2];
+    double rr = sqrt(xc * xc + yc * yc + zc * zc);
+    *rij = rr;
+    if (rr > 0.0) {
+        e[0] = xc / rr;
+        e[1] = yc / rr;
+        e[2] = zc / rr;
+    } else {
+        e[0] = 0.0;
+        e[1] = 0.0;
+        e[2] = 1.0;
+    }
+}
+
+/* ---- H0 and S ---------------------------------------------------------- */
+
+/* slako.f90:77-231.  Orbital tables ind/typ/ls/ms have length norb, typ are
+ * atom types 0..ntype-1, mprox is Nat x Nat (1 = interacting), tables are
+ * [npair][nsk][npts].  S and H0 (norb x norb) are fully overwritten. */
+void oracle_h0_and_s(int norb, int nat, const int *ind, const int *typ, const int *ls, const int *ms,
+                     const double *pos, const int *mprox, const double *orben, int deg,
+                     const int *tab_filled, const double *S_knots, const double *S_coefs,
+                     const double *H_knots, const double *H_coefs, int npair, int nsk, int npts,
+                     double *S, double *H0)
+{
+    (void)npair;
+    memset(S, 0, sizeof(double) * (size_t)norb * norb);
+    memset(H0, 0, sizeof(double) * (size_t)norb * norb);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int nu = 0; nu < norb; ++nu) {
+        double Si[16], Hi[16];
+        int j = ind[nu], typj = typ[nu], l2 = ls[nu], m2 = ms[nu];
+        for (int mu = nu; mu < norb; ++mu) {
+            int i = ind[mu], typi = typ[mu], l1 = ls[mu], m1 = ms[mu];
+            if (mprox[(size_t)i * nat + j] == 0) continue;
+            size_t o = (size_t)mu * norb + nu;
+            if (mu == nu) {
+                S[o] = 1.0;
+                H0[o] = orben[mu];
+                continue;
+            }
+            double rij, e[3];
+            pair_geometry(pos, i, j, &rij, e);
+            if (i != j) {
+                int tmin = typi < typj ? typi : typj, tmax = typi < typj ? typj : typi;
+                int ipair = tmax * (tmax + 1) / 2 + tmin;
+                for (int tab = 0; tab < nsk; ++tab) {
+                    if (tab_filled[ipair * nsk + tab] == 1) {
+                        size_t b = ((size_t)ipair * nsk + tab) * npts;
+                        Si[tab] = oracle_splev_uniform(S_knots + b, npts, S_coefs + b, deg, rij);
+                        Hi[tab] = oracle_splev_uniform(H_knots + b, npts, H_coefs + b, deg, rij);
+                    } else {
+                        Si[tab] = 0.0;
+                        Hi[tab] = 0.0;
+                    }
+                }
+            }
+            if (typi <= typj) {
+                if (i == j) {
+                    S[o] = 0.0;
+                    H0[o] = 0.0;
+                } else {
+                    S[o] = oracle_sk_rule(l1, m1, l2, m2, e, Si);
+                    H0[o] = oracle_sk_rule(l1, m1, l2, m2, e, Hi);
+                }
+            } else {
+                double me[3] = {-e[0], -e[1], -e[2]};
+                S[o] = oracle_sk_rule(l2, m2, l1, m1, me, Si);
+                H0[o] = oracle_sk_rule(l2, m2, l1, m1, me, Hi);
+            }
+        }
+    }
+    for (int nu = 0; nu < norb; ++nu)
+        for (int mu = 0; mu < nu; ++mu) {
+            S[(size_t)mu * norb + nu] = S[(size_t)nu * norb + mu];
+            H0[(size_t)mu * norb + nu] = H0[(size_t)nu * norb + mu];
+        }
+}
+
+/* ---- dipole matrix ----------------------------------------------------- */
+
+/* slako.f90:238-394.  D receives three planes [3][norb][norb]. */
+void oracle_dipole_matrix(int norb, int nat, const int *ind, const int *typ, const int *ls, const int *ms,
+                          const double *pos, const int *mprox, const double *S, int deg,
+                          const int *tab_filled_D, const double *D_knots, const double *D_coefs,
+                          int npair, int nskd, int npts, double *D)
+{
+    (void)npair;
+    size_t plane = (size_t)norb * norb;
+    memset(D, 0, sizeof(double) * 3 * plane);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int nu = 0; nu < norb; ++nu) {
+        double Di[32];
+        int j = ind[nu], typj = typ[nu], l2 = ls[nu], m2 = ms[nu];
+        for (int mu = nu; mu < norb; ++mu) {
+            int i = ind[mu], typi = typ[mu], l1 = ls[mu], m1 = ms[mu];
+            if (mprox[(size_t)i * nat + j] == 0) continue;
+            double rij, e[3];
+            pair_geometry(pos, i, j, &rij, e);
+            int tmin = typi < typj ? typi : typj, tmax = typi < typj ? typj : typi;
+            int ipair = tmax * (tmax + 1) / 2 + tmin;
+            for (int tab = 0; tab < nskd; ++tab) {
+                if (tab_filled_D[ipair * nskd + tab] == 1) {
+                    size_t b = ((size_t)ipair * nskd + tab) * npts;
+                    Di[tab] = oracle_splev_uniform(D_knots + b, npts, D_coefs + b, deg, rij);
+                } else {
+                    Di[tab] = 0.0;
+                }
+            }
+            size_t o = (size_t)mu * norb + nu;
+            double s = S[o];
+            /* mr = +1 (x), -1 (y), 0 (z) in the reference; planes are x,y,z */
+            if (typi <= typj) {
+                for (int c = 0; c < 3; ++c)
+                    D[c * plane + o] = oracle_sk_dipole_rule(l1, m1, c, l2, m2, e, Di) + pos[3 * j + c] * s;
+            } else {
+                double me[3] = {-e[0], -e[1], -e[2]};
+                for (int c = 0; c < 3; ++c)
+                    D[c * plane + o] = oracle_sk_dipole_rule(l2, m2, c, l1, m1, me, Di) + pos[3 * i + c] * s;
+            }
+        }
+    }
+    for (int c = 0; c < 3; ++c)
+        for (int nu = 0; nu < norb; ++nu)
+            for (int mu = 0; mu < nu; ++mu)
+                D[c * plane + (size_t)mu * norb + nu] = D[c * plane + (size_t)nu * norb + mu];
+}
+
+/* ---- transition charges ------------------------------------------------ */
+
+/* q^{pq}_A = 1/2 sum_{mu in A} (C_mu,p (SC)_mu,q + C_mu,q (SC)_mu,p).
+ * tddftb.f90:12-112.  orbs_occ is norb x nocc row-major (column i = MO i),
+ * orbs_virt norb x nvirt, S norb x norb.  Outputs q_oo[Nat][nocc][nocc],
+ * q_ov[Nat][nocc][nvirt], q_vv[Nat][nvirt][nvirt]; any may be NULL. */
+void oracle_trans_charges(int norb, int nat, int nocc, int nvirt, const double *orbs_occ,
+                          const double *orbs_virt, const double *S, const int *orbs_per_atom,
+                          double *q_oo, double *q_ov, double *q_vv)
+{
+    double *sco = (double *)calloc((size_t)norb * nocc, sizeof(double));
+    double *scv = (double *)calloc((size_t)norb * nvirt, sizeof(double));
+#pragma omp parallel for
+    for (int mu = 0; mu < norb; ++mu)
+        for (int nu = 0; nu < norb; ++nu) {
+            double s = S[(size_t)mu * norb + nu];
+            for (int i = 0; i < nocc; ++i) sco[(size_t)mu * nocc + i] += s * orbs_occ[(size_t)nu * nocc + i];
+            for (int a = 0; a < nvirt; ++a) scv[(size_t)mu * nvirt + a] += s * orbs_virt[(size_t)nu * nvirt + a];
+        }
+    int *first = (int *)malloc(sizeof(int) * (nat + 1));
+    first[0] = 0;
+    for (int A = 0; A < nat; ++A) first[A + 1] = first[A] + orbs_per_atom[A];
+#define QBLOCK(OUT, C1, SC1, N1, C2, SC2, N2)                                                  \
+    if (OUT) {                                                                                 \
+        _Pragma("omp parallel for") for (int p = 0; p < N1; ++p) for (int q = 0; q < N2; ++q) \
+            for (int A = 0; A < nat; ++A) {                                                    \
+                double acc = 0.0;                                                              \
+                for (int mu = first[A]; mu < first[A + 1]; ++mu)                               \
+                    acc += C1[(size_t)mu * N1 + p] * SC2[(size_t)mu * N2 + q] +                \
+                           C2[(size_t)mu * N2 + q] * SC1[(size_t)mu * N1 + p];                 \
+                OUT[((size_t)A * N1 + p) * N2 + q] = 0.5 * acc;                                \
+            }                                                                                  \
+    }
+    QBLOCK(q_oo, orbs_occ, sco, nocc, orbs_occ, sco, nocc)
+    QBLOCK(q_ov, orbs_occ, sco, nocc, orbs_virt, scv, nvirt)
+    QBLOCK(q_vv, orbs_virt, scv, nvirt, orbs_virt, scv, nvirt)
+#undef QBLOCK
+    free(first);
+    free(sco);
+    free(scv);
+}
+
+/* ---- Mulliken monopoles ------------------------------------------------ */
+
+/* q_A = sum_{mu in A} sum_nu P S, dq_A = sum (P - P0) S.  mulliken.f90:11-66 */
+void oracle_monopoles(int norb, int nat, const double *P, const double *P0, const double *S,
+                      const int *orbs_per_atom, double *q, double *dq)
+{
+    int mu = 0;
+    for (int A = 0; A < nat; ++A) {
+        double qa = 0.0, dqa = 0.0;
+        for (int k = 0; k < orbs_per_atom[A]; ++k, ++mu)
+            for (int nu = 0; nu < norb; ++nu) {
+                size_t o = (size_t)mu * norb + nu;
+                qa += P[o] * S[o];
+                dqa += (P[o] - P0[o]) * S[o];
+            }
+        q[A] = qa;
+        dq[A] = dqa;
+    }
+}

@@ -1,0 +1,230 @@
+"""Generate the golden fixtures in tests/golden/ from DFTBaby's own code.
+
+DFTBaby is Python 2 code, so its pure-numpy modules on the LR-TD-DFTB path are
+loaded through a mechanical py2->py3 shim (print statements become calls,
+``iteritems``/``xrange``/``has_key`` are renamed; nothing else changes) into a
+throw-away package under a temporary directory.  Modules run this way:
+
+* ``DFTB/Solver.py``            Casida, HermitianDavidson, nonHermitianDavidson, _ApBv, _AmBv
+* ``DFTB/GammaApproximation.py`` gaussian_decay, GammaGaussian, GammaGaussianLC, GammaMatrix
+* ``DFTB/ConvAcceleration.py``   DIIS_80
+
+The Slater-Koster angular rules (``DFTB/extensions/slako_transformations_lmax2.f90``
+and ``..._dipole_lmax2.f90``) are Fortran ``SELECT CASE`` tables whose
+right-hand sides are also valid Python expressions; they are evaluated here for
+random directions and table values.
+
+Inputs of the solver fixtures (transition charges, gamma matrices, orbital
+energy differences) come from a small seeded polyene; they are stored in the
+fixtures next to the reference outputs, so the tests feed identical inputs to
+the code under test.
+
+Usage::
+
+    python tests/golden/make_golden.py /path/to/DFTBaby
+"""
+import io
+import os
+import re
+import shutil
+import sys
+import tempfile
+import tokenize
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+def py2to3(src):
+    """Mechanical conversion of print statements and renamed dict/range methods."""
+    src = src.replace(".iteritems()", ".items()").replace("xrange(", "range(")
+    src = re.sub(r"\.has_key\(", ".__contains__(", src)
+    toks = list(tokenize.generate_tokens(io.StringIO(src).readline))
+    edits = []
+    for k, t in enumerate(toks):
+        if t.type != tokenize.NAME or t.string != "print":
+            continue
+        j = k - 1
+        while j >= 0 and toks[j].type in (tokenize.NL, tokenize.COMMENT):
+            j -= 1
+        if j >= 0 and toks[j].type not in (tokenize.NEWLINE, tokenize.INDENT, tokenize.DEDENT) \
+                and toks[j].string != ":":
+            continue
+        m = k + 1
+        while toks[m].type not in (tokenize.NEWLINE, tokenize.ENDMARKER):
+            m += 1
+        e = m - 1
+        while toks[e].type in (tokenize.COMMENT, tokenize.NL):
+            e -= 1
+        if e == k:
+            edits.append((t.start, t.end, "print()"))
+        elif toks[e].string == ",":
+            edits.append((toks[e].start, toks[e].end, ', end=" ")'))
+            edits.append((t.start, t.end, "print("))
+        else:
+            edits.append((toks[e].end, toks[e].end, ")"))
+            edits.append((t.start, t.end, "print("))
+    lines = src.splitlines(keepends=True)
+    for (r0, c0), (r1, c1), text in sorted(edits, key=lambda x: (x[0], x[1]), reverse=True):
+        assert r0 == r1
+        ln = lines[r0 - 1]
+        lines[r0 - 1] = ln[:c0] + text + ln[c1:]
+    return "".join(lines)
+
+
+def load_reference_modules(ref_root):
+    """Build a temporary ``DFTB`` package holding shimmed copies of the needed modules."""
+    tmp = tempfile.mkdtemp(prefix="dftbaby_ref_")
+    pkg = os.path.join(tmp, "DFTB")
+    os.makedirs(os.path.join(pkg, "extensions"))
+    open(os.path.join(pkg, "__init__.py"), "w").close()
+    open(os.path.join(pkg, "extensions", "__init__.py"), "w").write("tddftb = None\n")
+    open(os.path.join(pkg, "Timer.py"), "w").write(
+        "class _T:\n    def timer(self, f):\n        return f\nGlobalTimer = _T()\n")
+    open(os.path.join(pkg, "AtomicData.py"), "w").write("atom_names = ['h','he','li','be','b','c']\n")
+    for name in ("Solver", "GammaApproximation", "ConvAcceleration"):
+        src = open(os.path.join(ref_root, "DFTB", name + ".py")).read()
+        open(os.path.join(pkg, name + ".py"), "w").write(py2to3(src))
+    sys.path.insert(0, tmp)
+    import importlib
+    mods = {n: importlib.import_module("DFTB." + n) for n in ("Solver", "GammaApproximation", "ConvAcceleration")}
+    return tmp, mods
+
+
+def sk_rule_cases(ref_root):
+    """Parse the reference's SK rule tables: {(l1,m1,l2,m2): expr} and {(l1,m1,mr,l2,m2): expr}."""
+    ext = os.path.join(ref_root, "DFTB", "extensions")
+    pat = re.compile(r"CASE \((\d+)\)\s*\n\s*! \(([^)]*)\)\s*\n\s*res = ([^\n]*)")
+    sh = {}
+    for _, tup, expr in pat.findall(open(os.path.join(ext, "slako_transformations_lmax2.f90")).read()):
+        key = tuple(int(v) for v in tup.split(","))
+        if key[0] <= 1 and key[2] <= 1:
+            sh[key] = expr
+    dip = {}
+    for _, tup, expr in pat.findall(open(os.path.join(ext, "slako_transformations_dipole_lmax2.f90")).read()):
+        key = tuple(int(v) for v in tup.split(","))
+        if key[0] <= 1 and key[3] <= 1:
+            dip[key] = expr
+    return sh, dip
+
+
+def make_sk_rules(ref_root, rng):
+    sh, dip = sk_rule_cases(ref_root)
+    ndir = 16
+    e = rng.normal(size=(ndir, 3))
+    e /= np.linalg.norm(e, axis=1)[:, None]
+    V = rng.normal(size=(ndir, 7))
+    Dt = rng.normal(size=(ndir, 15))
+    sh_keys = np.array(sorted(sh), dtype=np.int64)
+    dip_keys = np.array(sorted(dip), dtype=np.int64)
+    sh_val = np.zeros((ndir, len(sh_keys)))
+    dip_val = np.zeros((ndir, len(dip_keys)))
+    for n in range(ndir):
+        env = dict(x=e[n, 0], y=e[n, 1], z=e[n, 2], sqrt3=np.sqrt(3.0))
+        env["SorH"] = lambda k, n=n: V[n, k - 1]
+        env["Dip"] = lambda k, n=n: Dt[n, k - 1]
+        for c, key in enumerate(sh_keys):
+            sh_val[n, c] = eval(sh[tuple(key)], env)
+        for c, key in enumerate(dip_keys):
+            dip_val[n, c] = eval(dip[tuple(key)], env)
+    np.savez_compressed(os.path.join(HERE, "sk_rules.npz"), e=e, V=V, D=Dt, sh_keys=sh_keys, sh_val=sh_val,
+                        dip_keys=dip_keys, dip_val=dip_val)
+
+
+def make_gamma(mods, rng):
+    GA = mods["GammaApproximation"]
+    from dftbaby_b200 import geometry
+    al = geometry.polyene(6, sigma=0.05, seed=3)
+    hub = {1: (13.5984 - 0.75419) / 27.211396132, 6: (11.2603 - 1.262119) / 27.211396132}
+    valorbs = {1: [(0, 0, 0)], 6: [(1, 0, 0), (1, 1, -1), (1, 1, 0), (1, 1, 1)]}
+    sig = GA.gaussian_decay(hub, valorbs, 3.03, 1, verbose=0)
+    pos = np.array([p for _, p in al])
+    R = pos[:, None] - pos[None]
+    dist = np.sqrt(np.sum(R * R, axis=-1))
+    nat = len(al)
+    dirs = np.zeros((nat, nat, 3))
+    off = dist > 0
+    dirs[off] = R[off] / dist[off][:, None]
+    g = GA.GammaMatrix(GA.GammaGaussian(sig)).gamma_atomwise(al, dist)[0]
+    glr, _, Glr, _ = GA.GammaMatrix(GA.GammaGaussianLC(sig, 3.03)).gamma_AOwise(al, valorbs, dist, dirs)
+    np.savez_compressed(os.path.join(HERE, "gamma.npz"), Z=np.array([z for z, _ in al]), pos=pos,
+                        sigma_H=sig[1], sigma_C=sig[6], gamma=g, gamma_lr=glr, G_lr=Glr)
+
+
+def make_diis(mods, rng):
+    CA = mods["ConvAcceleration"]
+    n = 12
+    A = rng.normal(size=(n, n)) * 0.15
+    b = rng.normal(size=n)
+    x = np.zeros(n)
+    mixer = CA.DIIS_80(5)
+    xs_in, xs_out, rel = [], [], []
+    for it in range(25):
+        x_new = np.dot(A, x) + b
+        xs_in.append(x_new.copy())
+        x = mixer.next_approximation(x_new.copy())
+        xs_out.append(np.array(x, dtype=float).copy())
+        rel.append(mixer.relative_change())
+    np.savez_compressed(os.path.join(HERE, "diis.npz"), A=A, b=b, xs_in=np.array(xs_in),
+                        xs_out=np.array(xs_out), rel=np.array(rel))
+
+
+def make_solvers(mods, rng):
+    """Reference solvers on transition charges of a seeded C10H12 (lc on)."""
+    SV = mods["Solver"]
+    sys.path.insert(0, REPO)
+    from dftbaby_b200 import geometry
+    from oracle import dftb_oracle as O
+    al = geometry.polyene(10, sigma=0.02, seed=0)
+    td = O.LR_TDDFTB(al, long_range_correction=1)
+    td.setGeometry(al)
+    td.dftb2.getEnergy()
+    td.setActiveOrbitals(None, None)
+    d = td.dftb2
+    co, cv = d.orbs[:, td.active_occupied_orbs], d.orbs[:, td.active_virtual_orbs]
+    q_oo, q_ov, q_vv = O.trans_charges(co, cv, d.S, d.orbsPerAtom)
+    no, nv = td.nocc, td.nvirt
+    orbe = d.orbe
+    omega = orbe[td.active_virtual_orbs][None, :] - orbe[td.active_occupied_orbs][:, None]
+    df = np.full((no, nv), 2.0)
+    shift = np.zeros((no, nv))
+    g, glr = d.gamma, d.gamma_lr
+    out = dict(q_oo=q_oo, q_ov=q_ov, q_vv=q_vv, omega=omega, gamma=g, gamma_lr=glr)
+    for tag, gl in (("lc", glr), ("nolc", 0.0 * glr)):
+        Om, C, XmY, XpY = SV.Casida(g, gl, q_oo, q_vv, q_ov, omega, shift, df, no, nv)
+        out["casida_%s_Omega" % tag] = Om
+        out["casida_%s_XmY" % tag] = XmY[:8]
+        out["casida_%s_XpY" % tag] = XpY[:8]
+    Oia = np.zeros((no, nv))
+    Om, C, XmY, XpY = SV.HermitianDavidson(g, q_ov, omega, shift, no, nv, None, None, Oia, nstates=6, ifact=1,
+                                           conv=1.0e-9, maxiter=100, L2_thresh=0.0, verbose=0)
+    out.update(herm_Omega=Om, herm_C=C, herm_XmY=XmY, herm_XpY=XpY)
+    Om, C, XmY, XpY = SV.nonHermitianDavidson(g, glr, q_oo, q_vv, q_ov, omega, no, nv, None, None, None,
+                                              nstates=6, ifact=1, conv=1.0e-9, maxiter=100, verbose=0, lc=1)
+    out.update(nonherm_Omega=Om, nonherm_C=C, nonherm_XmY=XmY, nonherm_XpY=XpY)
+    vs = rng.normal(size=(no, nv, 3))
+    out["vs"] = vs
+    out["ApBv"] = SV._ApBv(g, glr, q_oo, q_ov, q_vv, omega, vs, 1)
+    out["AmBv"] = SV._AmBv(g, glr, q_oo, q_ov, q_vv, omega, vs, 1)
+    np.savez_compressed(os.path.join(HERE, "solvers_c10h12.npz"), **out)
+
+
+def main(ref_root):
+    sys.path.insert(0, REPO)
+    rng = np.random.default_rng(20261203)
+    tmp, mods = load_reference_modules(ref_root)
+    try:
+        make_sk_rules(ref_root, rng)
+        make_gamma(mods, rng)
+        make_diis(mods, rng)
+        make_solvers(mods, rng)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
