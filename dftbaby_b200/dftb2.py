@@ -1,0 +1,395 @@
+"""Ground-state SCC-DFTB on the GPU behind DFTBaby's ``DFTB2`` interface.
+
+Mirrors ``class DFTB2`` (DFTB/DFTB2.py:61-2514) for the options on the
+LR-TD-DFTB path: same constructor keywords and defaults, ``setGeometry``,
+``getEnergy``, ``runSCC`` and the accessors LR_TDDFTB reads
+(DFTB2.py:2405-2454).  Geometry-dependent matrices (directional cosines, S, H0,
+dipoles, gamma, gamma^lr) and the per-iteration Hamiltonian and Mulliken
+charges run in the CUDA kernels of ``libdftbaby_b200``; dense products and the
+generalised eigenproblem use the CUDA libraries through torch on the same
+stream.
+
+Every array attribute (``S``, ``H0``, ``P``, ``orbs``, ``orbe``, ``dq``,
+``gamma``, ...) is a float64 CUDA tensor; accessors return these tensors.
+"""
+import numpy as np
+import torch
+
+from . import native
+from .exceptions import SCFChargeInconsistency, SCFNotConverged
+from .params import Parametrization
+
+
+class DIIS_80:
+    """Pulay density mixing with DFTBaby's bookkeeping (ConvAcceleration.py:27-143).
+
+    Trial vectors and their differences are kept on the device; the small DIIS
+    system is solved on the host.
+    """
+
+    def __init__(self, m=5, relchange_start=0.5):
+        self.m = m
+        self.relchange_start = relchange_start
+        self.reset()
+
+    def reset(self):
+        self.trial, self.resid, self.start_flag = [], [], False
+
+    def _add(self, p):
+        self.trial.append(p)
+        if len(self.trial) >= 2:
+            self.resid.append(self.trial[-1] - self.trial[-2])
+        if len(self.trial) > self.m:
+            self.trial.pop(0)
+            self.resid.pop(0)
+
+    def next_approximation(self, P):
+        flat = P.reshape(-1).clone()
+        self._add(flat)
+        if self.start_flag:
+            n = len(self.resid)
+            R = torch.stack(self.resid[:n])
+            gram = (R @ R.T).cpu().numpy()
+            A = np.zeros((n + 1, n + 1))
+            A[:n, :n] = gram
+            A[:n, n] = A[n, :n] = -1.0
+            b = np.zeros(n + 1)
+            b[-1] = -1.0
+            c = np.linalg.solve(A, b)
+            assert abs(np.sum(c[:-1]) - 1.0) < 1.0e-10
+            p = torch.zeros_like(self.trial[0])
+            for i in range(n):
+                p += float(c[i]) * self.trial[i]
+            self.trial[-1] = p
+            self.resid[-1] = p - self.trial[-2]
+            return p.reshape(P.shape)
+        if len(self.trial) > 3:
+            rel = (torch.linalg.norm(self.resid[-1]) / torch.linalg.norm(self.trial[-1])).item()
+            if rel < self.relchange_start:
+                self.start_flag = True
+        return P
+
+    def relative_change(self):
+        """Device scalar: mean relative change over the last two steps."""
+        if len(self.resid) == 0:
+            return None
+        navg = min(len(self.resid), 2)
+        ch = 0.0
+        for i in range(1, navg + 1):
+            ch = ch + torch.linalg.norm(self.resid[-i]) / torch.linalg.norm(self.trial[-i])
+        return ch / navg
+
+
+class DFTB2(object):
+    """SCC-DFTB ground state (DFTB/DFTB2.py) on one CUDA device, FP64."""
+
+    def __init__(self, atomlist, parameter_set="homegrown", missing_reppots="dummy", verbose=0,
+                 distance_cutoff=30.0, long_range_correction=1, long_range_radius=3.03, long_range_T=1.0,
+                 long_range_switching="erf", lc_implementation=None, hubbard_scaling=1.0, hubbard_override=None,
+                 fluctuation_functions="Gaussian", nr_unpaired_electrons=0, use_symmetry=0, device=None, **opts):
+        if parameter_set != "homegrown":
+            raise ValueError("only the 'homegrown' parameter set is carried")
+        if fluctuation_functions != "Gaussian":
+            raise ValueError("only Gaussian charge fluctuations are implemented")
+        if lc_implementation not in (None,):
+            raise ValueError("only the default lc implementation is implemented")
+        if long_range_switching != "erf":
+            raise ValueError("only erf switching is implemented")
+        if nr_unpaired_electrons != 0:
+            raise ValueError("open-shell singlets are not implemented")
+        self.parameter_set = parameter_set
+        self.verbose = verbose
+        self.distance_cutoff = distance_cutoff
+        self.long_range_correction = long_range_correction
+        self.long_range_radius = long_range_radius
+        self.nr_unpaired_electrons = 0
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device()
+                                                                                   if torch.cuda.is_available() else 0)
+        native.load()
+        self.par = Parametrization([Z for Z, _ in atomlist], hubbard_scaling, hubbard_override)
+        self.valorbs = self.par.valorbs
+        self.hubbard_U = self.par.hubbard_U
+        self.ne_val = self.par.ne_val
+        self.workspace = native.Workspace(self.device)
+
+    # ------------------------------------------------------------ geometry
+    def setGeometry(self, atomlist, charge=0.0, keep_charge=False, update_symmetry=True):
+        """DFTB2.setGeometry (DFTB2.py:443-505)."""
+        new_types = set(int(Z) for Z, _ in atomlist) - set(self.par.atomtypes)
+        if new_types:
+            raise ValueError("atom types %s were not present when the object was built" % sorted(new_types))
+        self.atomlist = [(int(Z), tuple(float(c) for c in pos)) for Z, pos in atomlist]
+        self.orbsPerAtom = [len(self.valorbs[Z]) for Z, _ in self.atomlist]
+        self.q0 = [self.ne_val[Z] for Z, _ in self.atomlist]
+        self.dim = int(sum(self.orbsPerAtom))
+        self.orbitals_on_atom = []
+        off = 0
+        for n in self.orbsPerAtom:
+            self.orbitals_on_atom.append(list(range(off, off + n)))
+            off += n
+        if not (keep_charge and hasattr(self, "charge")):
+            self.charge = charge
+            self.Nelec_val = sum(self.q0) - charge
+        dev = self.device
+        ind, typ, ls, ms, orben, occ0 = [], [], [], [], [], []
+        for i, (Z, _) in enumerate(self.atomlist):
+            for k, (n, l, m) in enumerate(self.valorbs[Z]):
+                ind.append(i)
+                typ.append(self.par.atom_type[Z])
+                ls.append(l)
+                ms.append(m)
+                orben.append(self.par.orbital_energies[Z][(n, l)])
+                occ0.append(self.par.valorbs_occupation[Z][k])
+        if max(ls) > 1:
+            raise ValueError("orbitals with l > 1 are not supported by the SK kernels")
+        i32 = lambda a: torch.tensor(a, dtype=torch.int32, device=dev)
+        f64 = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+        self._ind, self._typ, self._ls, self._ms = i32(ind), i32(typ), i32(ls), i32(ms)
+        self._orben = f64(orben)
+        self._p0diag = f64(occ0)
+        self._opa = i32(self.orbsPerAtom)
+        self.pos = f64([p for _, p in self.atomlist]).reshape(-1, 3).contiguous()
+        self._sigma = f64([self.par.sigmas[Z] for Z, _ in self.atomlist])
+        self._U = f64([self.hubbard_U[Z] for Z, _ in self.atomlist])
+
+    def getGeometry(self):
+        return self.atomlist
+
+    def getValorbs(self):
+        return self.valorbs
+
+    def _geometry_matrices(self):
+        """Distances, proximity, S, H0, D, gamma, gamma^lr, G_lr on the device."""
+        nat, norb, dev = len(self.atomlist), self.dim, self.device
+        st = native.stream()
+        P = native.ptr
+        r = torch.empty((nat, nat), dtype=torch.float64, device=dev)
+        x, y, z = torch.empty_like(r), torch.empty_like(r), torch.empty_like(r)
+        native.call("dftb_directional_cosines", nat, P(self.pos), P(r), P(x), P(y), P(z), st)
+        self.distances = r
+        mprox = (r < self.distance_cutoff).to(torch.int32)
+        mprox.fill_diagonal_(1)
+        self.Mproximity = mprox
+        t = self.par.device_tables(dev)
+        p = self.par
+        self.S = torch.empty((norb, norb), dtype=torch.float64, device=dev)
+        self.H0 = torch.empty_like(self.S)
+        native.call("dftb_h0_and_s", norb, nat, P(self._ind), P(self._typ), P(self._ls), P(self._ms), P(r), P(x),
+                    P(y), P(z), P(mprox), P(self._orben), p.deg, P(t["tab_filled_SH0"]), P(t["S_knots"]),
+                    P(t["S_coefs"]), P(t["H_knots"]), P(t["H_coefs"]), p.npair, p.nsk, p.npts, P(self.S),
+                    P(self.H0), st)
+        self.D3 = torch.empty((3, norb, norb), dtype=torch.float64, device=dev)
+        native.call("dftb_dipole_matrix", norb, nat, P(self._ind), P(self._typ), P(self._ls), P(self._ms), P(r),
+                    P(x), P(y), P(z), P(self.pos), P(mprox), P(self.S), p.deg, P(t["tab_filled_D"]),
+                    P(t["D_knots"]), P(t["D_coefs"]), p.npair, p.nskd, p.npts, P(self.D3), st)
+        self.gamma = torch.empty((nat, nat), dtype=torch.float64, device=dev)
+        lc = self.long_range_correction == 1
+        self.gamma_lr = torch.empty_like(self.gamma) if lc else None
+        native.call("dftb_gamma_matrices", nat, P(r), P(self._sigma), float(self.long_range_radius), P(self.gamma),
+                    P(self.gamma_lr), st)
+        if lc:
+            self.G_lr = torch.empty((norb, norb), dtype=torch.float64, device=dev)
+            native.call("dftb_ao_expand", norb, nat, P(self._ind), P(self.gamma_lr), P(self.G_lr), st)
+        # Gaussian overlap for the Lambda diagnostic (DFTB2.py:1287-1317)
+        sig = 1.329 / np.sqrt(8.0 * np.log(2.0)) / self._U
+        sAB = sig[:, None] ** 2 + sig[None, :] ** 2
+        self.gaussOmega = 1.0 / torch.pow(2.0 * np.pi * sAB, 1.5) * torch.exp(-0.5 / sAB * r * r)
+        # S^(-1/2)-type transform for the generalised eigenproblem: S = L L^T
+        L = torch.linalg.cholesky(self.S)
+        eye = torch.eye(norb, dtype=torch.float64, device=dev)
+        self._Linv = torch.linalg.solve_triangular(L, eye, upper=False)
+
+    @property
+    def D(self):
+        """Dipole matrix in DFTBaby's (norb, norb, 3) layout (a view)."""
+        return self.D3.permute(1, 2, 0)
+
+    def density_matrix_ref(self):
+        self.P0 = torch.diag(self._p0diag)
+        return self.P0
+
+    # ------------------------------------------------------------ SCC pieces
+    def lc_exact_exchange(self):
+        """H^x = -1/8 [ (G o SdP) S + G o (SdP S) + S (dP o G) S + S (dP S o G) ]
+        with dP = P - P0 (DFTB2.py:1239-1266); S and dP are symmetric, so the
+        fourth term is the transpose of the first."""
+        dP = self.P - self.P0
+        S, G = self.S, self.G_lr
+        A1 = S @ dP
+        t1 = (G * A1) @ S
+        Hx = t1 + t1.T
+        Hx += G * (A1 @ S)
+        Hx += S @ (dP * G) @ S
+        return Hx * (-1.0 / 8.0)
+
+    def lc_exchange_energy(self):
+        dP = self.P - self.P0
+        S, G = self.S, self.G_lr
+        A1 = S @ dP
+        E = torch.sum((A1 @ S) * dP * G) + torch.sum(A1 * A1.T * G)
+        return -E / 8.0
+
+    def getEnergies(self):
+        """E_bs, E_coulomb, E_elec, E_nuc, E_tot (DFTB2.py:2235-2276); repulsive
+        potentials are not part of this path, E_nuc = 0."""
+        self.E_bs = torch.sum(self.P * self.H0).item()
+        self.E_coulomb = 0.5 * torch.dot(self.dq, self.gamma @ self.dq).item()
+        self.E_elec = self.E_bs + self.E_coulomb
+        if self.long_range_correction == 1:
+            self.E_HF_x = self.lc_exchange_energy().item()
+            self.E_elec += self.E_HF_x
+        self.E_nuc = 0.0
+        self.E_tot = self.E_elec + self.E_nuc
+        return self.E_bs, self.E_coulomb, self.E_elec, self.E_nuc, self.E_tot
+
+    def getEnergy(self, **scf_opts):
+        """DFTB2.getEnergy (DFTB2.py:2278-2338)."""
+        self._geometry_matrices()
+        self.runSCC(**scf_opts)
+        return self.getEnergies()[-1]
+
+    def _occupation(self, orbe):
+        """fermi_occupation_T0 (DFTB2.py:2594-2610) on the device."""
+        f = torch.zeros_like(orbe)
+        order = torch.argsort(orbe, stable=True)
+        nel = self.Nelec_val
+        nfull = int(nel // 2)
+        f[order[:nfull]] = 2.0
+        rem = nel - 2.0 * nfull
+        if rem > 0.0:
+            f[order[nfull]] = rem
+        return f
+
+    def runSCC(self, maxiter=1000, scf_conv=1.0e-10, start_from_previous=1, mixing_threshold=1.0e-3,
+               density_mixer="default", fock_interpolator=None, level_shift=0.1, HOMO_LUMO_tol=0.05,
+               linear_mixing_coefficient=0.33):
+        """Self-consistent charges (DFTB2.runSCC, DFTB2.py:940-1160), T = 0."""
+        if fock_interpolator is not None:
+            raise ValueError("Fock interpolation is not implemented")
+        if isinstance(density_mixer, str) and density_mixer == "default":
+            density_mixer = DIIS_80(5)
+        elif isinstance(density_mixer, str):
+            raise ValueError("density_mixer must be a DIIS_80 instance or None")
+        nat, norb, dev = len(self.atomlist), self.dim, self.device
+        st, P = native.stream(), native.ptr
+        if not hasattr(self, "dq") or start_from_previous == 0 or self.dq.numel() != nat:
+            self.dq = torch.zeros(nat, dtype=torch.float64, device=dev)
+        if density_mixer is not None:
+            density_mixer.reset()
+        self.density_matrix_ref()
+        if not hasattr(self, "P") or start_from_previous == 0 or self.P.shape[0] != norb:
+            self.P = self.P0.clone()
+        P_last = self.P
+        converged = shift_flag = mixing_flag = False
+        if not hasattr(self, "relative_change"):
+            self.relative_change = 0.0
+        have_orbe = hasattr(self, "orbe") and self.orbe.numel() == norb and hasattr(self, "HLgap")
+        estat = torch.empty(nat, dtype=torch.float64, device=dev)
+        H = torch.empty((norb, norb), dtype=torch.float64, device=dev)
+        q = torch.empty(nat, dtype=torch.float64, device=dev)
+        dq = torch.empty(nat, dtype=torch.float64, device=dev)
+        nfull = int(self.Nelec_val // 2)
+        HOMO = nfull - 1 if self.Nelec_val - 2 * nfull == 0 else nfull
+        for self.i in range(maxiter):
+            native.call("dftb_scc_hamiltonian", norb, nat, P(self._ind), P(self.H0), P(self.S), P(self.gamma),
+                        P(self.dq), P(estat), P(H), st)
+            Hk = H
+            if self.long_range_correction == 1:
+                Hk = H + self.lc_exact_exchange()
+            b = level_shift
+            if have_orbe and self.HLgap < HOMO_LUMO_tol and not mixing_flag:
+                shift_flag = True
+            if shift_flag and b > 0.0:
+                if self.relative_change < 1.0e5 * scf_conv:
+                    b *= 0.5
+                if self.relative_change < 1.0e3 * scf_conv:
+                    b = 0.0
+            if shift_flag and b > 0.0:
+                # level shift of the virtual block in the basis of the last MOs (DFTB2.py:1059-1081)
+                B = self.orbs
+                Hm = B.T @ Hk @ B
+                virt = torch.nonzero(self.f == 0.0).flatten()
+                Hm[virt, virt] += b
+                self.orbe, Cp = torch.linalg.eigh(Hm)
+                self.orbs = B @ Cp
+            else:
+                Hp = self._Linv @ Hk @ self._Linv.T
+                self.orbe, Cp = torch.linalg.eigh(Hp)
+                self.orbs = self._Linv.T @ Cp
+            have_orbe = True
+            self.f = self._occupation(self.orbe)
+            occ = self.f > 0.0
+            Cocc = self.orbs[:, occ]
+            Pnew = (Cocc * self.f[occ]) @ Cocc.T
+            if density_mixer is not None and not converged and mixing_flag:
+                Pnew = density_mixer.next_approximation(Pnew)
+            elif not converged:
+                a = linear_mixing_coefficient
+                nP = a * Pnew + (1.0 - a) * P_last
+                nP = nP * (torch.sum(Pnew * self.S) / torch.sum(nP * self.S))
+                Pnew = nP
+            self.P = Pnew
+            native.call("dftb_monopoles", norb, nat, P(self.P), P(self.P0), P(self.S), P(self._opa), P(q), P(dq), st)
+            self.q, self.dq = q.clone(), dq.clone()
+            if not converged and density_mixer is not None and mixing_flag:
+                rel = density_mixer.relative_change()
+                rel = torch.ones((), dtype=torch.float64, device=dev) if rel is None else rel
+            elif not converged:
+                rel = torch.linalg.norm(P_last - self.P) / torch.linalg.norm(self.P)
+            else:
+                rel = torch.tensor(self.relative_change, dtype=torch.float64, device=dev)
+            gap = self.orbe[HOMO + 1] - self.orbe[HOMO] if HOMO + 1 < norb else torch.zeros((), device=dev,
+                                                                                           dtype=torch.float64)
+            host = torch.stack([rel.reshape(()), self.dq.sum(), gap.reshape(())]).cpu().numpy()
+            self.relative_change, sum_dq, self.HLgap = float(host[0]), float(host[1]), float(host[2])
+            if abs(sum_dq + self.charge) > 1.0e-5:
+                raise SCFChargeInconsistency("Mulliken charges do not add up to total charge, sum dq = %s" % -sum_dq)
+            if converged:
+                break
+            if self.relative_change < scf_conv:
+                converged = True
+            if self.relative_change < mixing_threshold and not mixing_flag and density_mixer is not None:
+                mixing_flag = True
+            P_last = self.P
+        else:
+            raise SCFNotConverged("SCF calculation did not converge after %s iterations!!!" % (self.i + 1))
+        self.scc_iterations = self.i + 1
+
+    # ------------------------------------------------------------ accessors
+    def getOverlapMatrix(self):
+        return self.S
+
+    def getKSCoefficients(self):
+        return self.orbs
+
+    def getKSEnergies(self):
+        return self.orbe
+
+    def getOccupation(self):
+        return self.f
+
+    def getFrontierOrbitals(self):
+        f = self.f.cpu().numpy()
+        return int(np.where(f > 0.0)[0][-1]), int(np.where(f == 0.0)[0][0])
+
+    def getHOMO_LUMO_gap(self):
+        HOMO, LUMO = self.getFrontierOrbitals()
+        return float(self.orbe[LUMO] - self.orbe[HOMO])
+
+    def getGamma(self):
+        return self.gamma
+
+    def getGamma_lr(self):
+        return self.gamma_lr
+
+    def getDensityMatrix(self):
+        return self.P
+
+    def getDipoleMatrix(self):
+        return self.D
+
+    def getPartialCharges(self):
+        return self.dq
+
+    def getGaussianOverlap(self):
+        return self.gaussOmega

@@ -1,0 +1,321 @@
+"""Linear-response TD-DFTB on the GPU behind DFTBaby's ``LR_TDDFTB`` interface.
+
+Mirrors ``class LR_TDDFTB`` (DFTB/LR_TDDFTB.py:29-1151) for the excited-state
+solve: ``LR_TDDFTB(atomlist, **dftb2_opts)``, ``setGeometry``,
+``getEnergies(...) -> (Omega, oscillator_strength)`` with the reference's
+keywords and defaults, the attributes callers read (``Omega``, ``Cij``,
+``XmY``, ``XpY``, ``oscillator_strength``, ``Lambda2``, ``omega``, ``nocc``,
+``nvirt``, ``active_occupied_orbs``, ``active_virtual_orbs``) and the accessors
+``getXY``, ``getExcEnergies``, ``getTransitionCharges``, ``getActiveOrbitals``.
+
+``Omega`` and ``oscillator_strength`` are returned as numpy arrays (as the
+reference returns them); vectors (``XmY``, ``XpY``, ``Cij``) and transition
+charges stay on the device as float64 torch tensors.
+
+The (A+B).v / (A-B).v products with the long-range correction use the
+AO-factorised form of the exchange terms: with C the MO coefficients,
+S~ = S C and Gamma_{mu nu} = gamma^lr_{A(mu) B(nu)},
+    K1 v = 1/4 sum_{x,y} cbar_o(x)^T (Gamma o M_xy) cbar_v(y)
+    K2 v = 1/4 sum_{x,y} cbar_o(y)^T (Gamma o M_xy)^T cbar_v(x),
+    M_xy = X_o V Y_v^T,  x, y in {C, S~},  cbar(C) = S~, cbar(S~) = C,
+which is the transition-charge form of Solver._ApBv/_AmBv
+(DFTB/Solver.py:583-635) with q^{pq}_A = 1/2 sum_{mu in A} (C_mu,p S~_mu,q +
+C_mu,q S~_mu,p) substituted -- exact algebra, without materialising q_oo and
+q_vv.  The Coulomb term uses q_ov and the native product kernels.
+"""
+import numpy as np
+import torch
+
+from . import native
+from .dftb2 import DFTB2
+from .exceptions import ExcitedStatesError
+from .solver import hermitian_davidson, nonhermitian_davidson
+
+
+class ExchangeAO:
+    """(A+B).V and (A-B).V for column blocks, exchange in AO-factorised form."""
+
+    def __init__(self, gamma, G_lr, q_ov, omega_flat, Co, Cv, S, nat, nocc, nvirt, workspace, lc=1,
+                 max_bytes=8 << 30):
+        self.gamma, self.G, self.q_ov, self.omega = gamma, G_lr, q_ov, omega_flat
+        self.nat, self.nocc, self.nvirt, self.lc = nat, nocc, nvirt, lc
+        self.ws = workspace
+        if lc:
+            So, Sv = S @ Co, S @ Cv
+            self.Xo = torch.stack([Co, So])            # x = C, S~
+            self.Yv = torch.stack([Cv, Sv])            # y = C, S~
+            self.Xo_bar = torch.stack([So, Co])        # complements
+            self.Yv_bar = torch.stack([Sv, Cv])
+            norb = Co.shape[0]
+            self.chunk = max(1, int(max_bytes // (8 * 6 * norb * norb)))
+        self.products_applied = 0
+
+    def coulomb(self, V):
+        """u = omega v + 4 q^T gamma q v (native kernels)."""
+        nov, m = V.shape
+        V = V.contiguous()
+        U = torch.empty_like(V)
+        ws = self.ws.get(native.load().dftb_hermitian_rv_workspace_size(self.nat, m))
+        native.call("dftb_apbv", self.nat, self.nocc, self.nvirt, m, 0, native.ptr(self.gamma), None,
+                    None, native.ptr(self.q_ov), None, native.ptr(self.omega), native.ptr(V), native.ptr(U),
+                    native.ptr(ws), ws.numel(), native.stream())
+        return U
+
+    def exchange(self, V):
+        """K1.V and K2.V, each (nov, m)."""
+        nov, m = V.shape
+        no, nv = self.nocc, self.nvirt
+        K1 = torch.empty_like(V)
+        K2 = torch.empty_like(V)
+        for c0 in range(0, m, self.chunk):
+            c1 = min(m, c0 + self.chunk)
+            Vb = V[:, c0:c1].T.reshape(c1 - c0, no, nv)
+            W = torch.matmul(Vb[:, None], self.Yv.transpose(1, 2)[None])      # (b, y, no, norb)
+            M = torch.matmul(self.Xo[None, :, None], W[:, None])               # (b, x, y, norb, norb)
+            M.mul_(self.G)
+            P1 = torch.matmul(M, self.Yv_bar[None, None])                      # (b, x, y, norb, nv)
+            k1 = torch.matmul(self.Xo_bar.transpose(1, 2)[None], P1.sum(dim=2)).sum(dim=1)  # (b, no, nv)
+            P2 = torch.matmul(M.transpose(-1, -2), self.Yv_bar[None, :, None])       # (b, x, y, norb, nv)
+            k2 = torch.matmul(self.Xo_bar.transpose(1, 2)[None], P2.sum(dim=1)).sum(dim=1)  # (b, no, nv)
+            K1[:, c0:c1] = 0.25 * k1.reshape(c1 - c0, -1).T
+            K2[:, c0:c1] = 0.25 * k2.reshape(c1 - c0, -1).T
+            del W, M, P1, P2
+        return K1, K2
+
+    def __call__(self, V):
+        self.products_applied += V.shape[1]
+        coul = self.coulomb(V)
+        omv = self.omega[:, None] * V
+        if not self.lc:
+            return coul, omv
+        K1, K2 = self.exchange(V)
+        return coul - K1 - K2, omv + K2 - K1
+
+
+class LR_TDDFTB:
+    XpY = None
+    XmY = None
+    Omega = None
+
+    def __init__(self, atomlist, **opts):
+        self.dftb2 = DFTB2(atomlist, **opts)
+
+    def setGeometry(self, atomlist, **opts):
+        self.dftb2.setGeometry(atomlist, **opts)
+
+    # ------------------------------------------------------------ active space
+    def setActiveOrbitals(self, nr_active_occ=None, nr_active_virt=None):
+        """LR_TDDFTB.setActiveOrbitals (LR_TDDFTB.py:167-188)."""
+        f = self.dftb2.getOccupation().cpu().numpy()
+        orbe = self.dftb2.getKSEnergies().cpu().numpy()
+        self.occupied_orbs = np.where(f > 0.1)[0]
+        self.virtual_orbs = np.where(f <= 0.1)[0]
+        self.active_occupied_orbs = self.occupied_orbs[np.argsort(orbe[self.occupied_orbs])[::-1][:nr_active_occ][::-1]]
+        self.active_virtual_orbs = self.virtual_orbs[np.argsort(orbe[self.virtual_orbs])[:nr_active_virt]]
+        self.nocc = len(self.active_occupied_orbs)
+        self.nvirt = len(self.active_virtual_orbs)
+
+    def getActiveOrbitals(self):
+        return self.active_occupied_orbs, self.active_virtual_orbs
+
+    def setMultiplicity(self, multiplicity):
+        assert multiplicity in ["S", "T"], "multiplicity has to be either 'S' for Singlet or 'T' for Triplet"
+        self.multiplicity = multiplicity
+
+    # ------------------------------------------------------------ transition charges
+    def _active_coefficients(self):
+        d = self.dftb2
+        dev = d.device
+        occ = torch.as_tensor(self.active_occupied_orbs, device=dev)
+        virt = torch.as_tensor(self.active_virtual_orbs, device=dev)
+        Co = d.orbs[:, occ].contiguous()
+        Cv = d.orbs[:, virt].contiguous()
+        return Co, Cv
+
+    def _trans_charges(self, which=("ov",)):
+        """tddftb.trans_charges (tddftb.f90:12-112) through the native kernel."""
+        d = self.dftb2
+        nat, norb, no, nv = len(d.atomlist), d.dim, self.nocc, self.nvirt
+        Co, Cv = self._active_coefficients()
+        dev = d.device
+        out = {}
+        for key, shape in (("oo", (nat, no, no)), ("ov", (nat, no, nv)), ("vv", (nat, nv, nv))):
+            out[key] = torch.empty(shape, dtype=torch.float64, device=dev) if key in which else None
+        L = native.load()
+        ws = d.workspace.get(L.dftb_trans_charges_workspace_size(norb, no, nv))
+        native.call("dftb_trans_charges", norb, nat, no, nv, native.ptr(Co), native.ptr(Cv), native.ptr(d.S),
+                    native.ptr(d._opa), native.ptr(out["oo"]), native.ptr(out["ov"]), native.ptr(out["vv"]),
+                    native.ptr(ws), ws.numel(), native.stream())
+        return out["oo"], out["ov"], out["vv"]
+
+    def getTransitionCharges(self):
+        """(q_oo, q_vv, q_ov) as in LR_TDDFTB.getTransitionCharges (LR_TDDFTB.py:376-377)."""
+        if getattr(self, "qtrans_oo", None) is None or getattr(self, "qtrans_vv", None) is None:
+            self.qtrans_oo, self.qtrans_ov, self.qtrans_vv = self._trans_charges(("oo", "ov", "vv"))
+        return self.qtrans_oo, self.qtrans_vv, self.qtrans_ov
+
+    def _Lambda2_calcOia(self):
+        """O_ia of the Lambda diagnostic (LR_TDDFTB.py:538-560) from the diagonal charges."""
+        d = self.dftb2
+        nat, norb, no, nv = len(d.atomlist), d.dim, self.nocc, self.nvirt
+        Co, Cv = self._active_coefficients()
+        qii = torch.empty((nat, no), dtype=torch.float64, device=d.device)
+        qaa = torch.empty((nat, nv), dtype=torch.float64, device=d.device)
+        L = native.load()
+        ws = d.workspace.get(L.dftb_trans_charges_workspace_size(norb, no, nv))
+        native.call("dftb_trans_charges_diag", norb, nat, no, nv, native.ptr(Co), native.ptr(Cv), native.ptr(d.S),
+                    native.ptr(d._opa), native.ptr(qii), native.ptr(qaa), native.ptr(ws), ws.numel(),
+                    native.stream())
+        G = d.gaussOmega
+        Gqi, Gqa = G @ qii, G @ qaa
+        Oii = torch.sum(qii * Gqi, dim=0)
+        Oaa = torch.sum(qaa * Gqa, dim=0)
+        self.Oia = (qii.T @ Gqa) / torch.sqrt(Oii[:, None] * Oaa[None, :])
+
+    # ------------------------------------------------------------ solve
+    def getEnergies(self, nr_active_occ=None, nr_active_virt=None, select_lm=None, oszis="Dipoles",
+                    response_method="Casida", multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5,
+                    diag_maxiter=50, diag_check=0, diag_L2threshold=0.0, diag_selected_irreps=None,
+                    ct_correction=0, stability=0, **scf_opts):
+        """LR_TDDFTB.getEnergies (LR_TDDFTB.py:37-114); returns (Omega, f) in Hartree."""
+        if select_lm is not None:
+            raise ValueError("select_lm is not implemented")
+        if response_method != "Casida":
+            raise ValueError("only response_method='Casida' is implemented")
+        if ct_correction or stability:
+            raise ValueError("ct_correction and stability analysis are not implemented")
+        d = self.dftb2
+        self.en0 = d.getEnergy(**scf_opts)
+        self.setActiveOrbitals(nr_active_occ, nr_active_virt)
+        self.setMultiplicity(multiplicity)
+        self.nstates = nstates
+        if nstates is not None:
+            assert nstates > 0, "nstates==0, no excited states can be calculated!"
+        self._solve_lr_equations(multiplicity=multiplicity, nstates=nstates, diag_ifact=diag_ifact,
+                                 diag_conv=diag_conv, diag_maxiter=diag_maxiter, diag_check=diag_check,
+                                 diag_L2threshold=diag_L2threshold)
+        if oszis == "Dipoles":
+            self._TransitionDipoles()
+        else:
+            self._TransitionDipolesMulliken()
+        self.getOscillatorStrengths()
+        self.Lambda2 = torch.sum(self.Cij ** 2 * self.Oia[None], dim=(1, 2))
+        return self.Omega, self.oscillator_strength
+
+    def _solve_lr_equations(self, multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5, diag_maxiter=50,
+                            diag_check=0, diag_L2threshold=0.0):
+        """LR_TDDFTB._solve_lr_equations (LR_TDDFTB.py:403-527)."""
+        d = self.dftb2
+        dev = d.device
+        self.qtrans_oo = self.qtrans_vv = None
+        _, self.qtrans_ov, _ = self._trans_charges(("ov",))
+        self._Lambda2_calcOia()
+        orbe = d.orbe
+        occ = torch.as_tensor(self.active_occupied_orbs, device=dev)
+        virt = torch.as_tensor(self.active_virtual_orbs, device=dev)
+        self.omega = (orbe[virt][None, :] - orbe[occ][:, None]).contiguous()
+        lc = d.long_range_correction == 1
+        self.stats = {}
+        XmY0 = XpY0 = Om0 = None
+        if torch.is_tensor(self.XpY) and self.XpY.shape == (nstates or -1, self.nocc, self.nvirt):
+            XmY0, XpY0, Om0 = self.XmY, self.XpY, self._Omega_dev
+        if nstates is None:
+            Om, C, XmY, XpY = self._casida(multiplicity)
+        elif not lc:
+            ws_holder = d.workspace
+
+            def rv(V):
+                nov, m = V.shape
+                V = V.contiguous()
+                U = torch.empty_like(V)
+                ws = ws_holder.get(native.load().dftb_hermitian_rv_workspace_size(len(d.atomlist), m))
+                native.call("dftb_hermitian_rv", len(d.atomlist), self.nocc, self.nvirt, m, native.ptr(d.gamma),
+                            native.ptr(self.qtrans_ov), native.ptr(self.omega), native.ptr(V), native.ptr(U),
+                            native.ptr(ws), ws.numel(), native.stream())
+                return U
+
+            Om, C, XmY, XpY = hermitian_davidson(rv, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
+                                                 maxiter=diag_maxiter, XpYguess=XpY0, Oia=self.Oia,
+                                                 L2_thresh=diag_L2threshold, stats=self.stats)
+        else:
+            Co, Cv = self._active_coefficients()
+            prod = ExchangeAO(d.gamma, d.G_lr, self.qtrans_ov, self.omega.reshape(-1), Co, Cv, d.S,
+                              len(d.atomlist), self.nocc, self.nvirt, d.workspace, lc=1)
+            Om, C, XmY, XpY = nonhermitian_davidson(prod, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
+                                                    maxiter=diag_maxiter, XmYguess=XmY0, XpYguess=XpY0,
+                                                    w_guess=Om0, stats=self.stats)
+            self.stats["products"] = prod.products_applied
+        self._Omega_dev = Om
+        self.Omega = Om.cpu().numpy()
+        self.Cij, self.XmY, self.XpY = C, XmY, XpY
+        if diag_check == 1 and nstates is not None:
+            Om_full, _, XmY_full, XpY_full = self._casida(multiplicity)
+            err = np.sum(np.abs(self.Omega - Om_full[:nstates].cpu().numpy()))
+            if err >= 1.0e-10:
+                raise ExcitedStatesError("eigenvalues differ, err = %s" % err)
+
+    def _casida(self, multiplicity):
+        """Full diagonalisation, Solver.Casida (Solver.py:98-181), on the device."""
+        q_oo, q_vv, q_ov = self.getTransitionCharges()
+        d = self.dftb2
+        no, nv = self.nocc, self.nvirt
+        n = no * nv
+        g = d.gamma
+        glr = d.gamma_lr if d.long_range_correction == 1 else torch.zeros_like(g)
+        KA = -torch.einsum("Aij,AB,Bab->iajb", q_oo, glr, q_vv).reshape(n, n)
+        KB = -torch.einsum("Aib,AB,Bja->iajb", q_ov, glr, q_ov).reshape(n, n)
+        if multiplicity == "S":
+            Ks = 2.0 * torch.einsum("Aia,AB,Bjb->iajb", q_ov, g, q_ov).reshape(n, n)
+            KA, KB = KA + Ks, KB + Ks
+        om = self.omega.reshape(-1)
+        dfh = torch.ones_like(om)  # df/2 = 1 for a closed shell
+        A = torch.diag(dfh * om) + dfh[:, None] * KA * dfh[None, :]
+        B = dfh[:, None] * KB * dfh[None, :]
+        AmB = A - B
+        offdiag = torch.linalg.norm(AmB - torch.diag(torch.diag(AmB))).item()
+        if offdiag < 1.0e-10:
+            sq = torch.diag(torch.sqrt(torch.diag(AmB)))
+        else:
+            lam, V = torch.linalg.eigh(0.5 * (AmB + AmB.T))
+            sq = (V * torch.sqrt(lam)) @ V.T
+        R = sq @ (A + B) @ sq
+        if torch.linalg.norm(R - R.T).item() >= 1.0e-10:
+            raise ExcitedStatesError("TD-DFTB matrix not hermitian")
+        O2, F = torch.linalg.eigh(R)
+        Om = torch.sqrt(O2)
+        XpY = (sq @ F) / torch.sqrt(Om)
+        XmY = ((A + B) @ XpY) / Om
+        C = torch.linalg.solve(sq, XpY * torch.sqrt(Om))
+        shape = (n, no, nv)
+        return Om, C.T.reshape(shape), XmY.T.reshape(shape), XpY.T.reshape(shape)
+
+    # ------------------------------------------------------------ properties
+    def _TransitionDipoles(self):
+        """LR_TDDFTB._TransitionDipoles (LR_TDDFTB.py:574-592), restricted to the active block."""
+        d = self.dftb2
+        Co, Cv = self._active_coefficients()
+        t = torch.matmul(Co.T[None], torch.matmul(d.D3, Cv[None]))  # (3, no, nv)
+        tdip = torch.einsum("kia,cia->ck", self.Cij, t)
+        self.tdip_ov = t
+        self.tdipX, self.tdipY, self.tdipZ = tdip[0], tdip[1], tdip[2]
+
+    def _TransitionDipolesMulliken(self):
+        d = self.dftb2
+        tdm = torch.einsum("Aia,kia->Ak", self.qtrans_ov, self.Cij)
+        fvec = d.pos.T @ tdm
+        self.tdipX, self.tdipY, self.tdipZ = fvec[0], fvec[1], fvec[2]
+
+    def getOscillatorStrengths(self):
+        """f = 2/3 Omega |t|^2 for singlets, 0 for triplets (LR_TDDFTB.py:698-705)."""
+        if self.multiplicity == "S":
+            t2 = self.tdipX ** 2 + self.tdipY ** 2 + self.tdipZ ** 2
+            self.oscillator_strength = (2.0 / 3.0 * torch.as_tensor(self.Omega, device=t2.device) * t2).cpu().numpy()
+        else:
+            self.oscillator_strength = 0.0 * self.Omega
+        return self.oscillator_strength
+
+    def getExcEnergies(self):
+        return self.Omega
+
+    def getXY(self):
+        return self.XmY, self.XpY

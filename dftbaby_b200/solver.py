@@ -1,0 +1,238 @@
+"""Davidson-type solvers for the TD-DFTB eigenproblem on the GPU (FP64).
+
+``hermitian_davidson`` follows Solver.HermitianDavidson (DFTB/Solver.py:404-578)
+and ``nonhermitian_davidson`` follows the Stratmann-Scuseria-Frisch solver
+Solver.nonHermitianDavidson (DFTB/Solver.py:637-917): same initial vectors,
+same subspace matrices, convergence tests, residual selection, preconditioner
+and error checks.  Two deliberate, result-preserving differences:
+
+* products of the matrix with expansion vectors are kept: each new vector is
+  multiplied once and residuals use (A.b) Tb instead of re-multiplying
+  A (b Tb) (the products are linear);
+* new vectors are orthonormalised against the current (orthonormal) basis by
+  block Gram-Schmidt with re-orthogonalisation instead of re-factorising the
+  whole basis by QR; both produce the same subspace.
+
+Vectors live as (nov, ncol) column blocks (the (nocc, nvirt, nvec) layout of
+the reference flattened).  Residual updates and preconditioning run in the
+CUDA kernels of libdftbaby_b200; subspace matrices and the small eigenproblems
+are FP64 on the device.
+"""
+import numpy as np
+import torch
+
+from . import native
+from .exceptions import ExcitedStatesError, ExcitedStatesNotConverged
+
+
+def initial_expansion_vectors(omega_flat, lmax):
+    """Unit vectors on the lmax lowest omega_ia (Solver.py:232-251)."""
+    order = np.argsort(omega_flat.detach().cpu().numpy())[:lmax]
+    bs = torch.zeros((omega_flat.numel(), lmax), dtype=torch.float64, device=omega_flat.device)
+    bs[torch.as_tensor(order, device=omega_flat.device), torch.arange(lmax, device=omega_flat.device)] = 1.0
+    return bs
+
+
+def orthonormalize_new(bs, Q):
+    """Orthonormalise the columns of Q against bs and among themselves (CGS2 + QR)."""
+    if bs is not None and bs.shape[1] > 0:
+        for _ in range(2):
+            Q = Q - bs @ (bs.T @ Q)
+    Q, _ = torch.linalg.qr(Q, mode="reduced")
+    if bs is not None and bs.shape[1] > 0:
+        Q = Q - bs @ (bs.T @ Q)
+        Q, _ = torch.linalg.qr(Q, mode="reduced")
+    return Q
+
+
+def _residuals(AV, X, lam):
+    nov, k = X.shape
+    W = torch.empty((nov, k), dtype=torch.float64, device=X.device)
+    norms = torch.empty(k, dtype=torch.float64, device=X.device)
+    AV = AV.contiguous()
+    X = X.contiguous()
+    lam = lam.contiguous()
+    native.call("dftb_davidson_residual", nov, k, native.ptr(AV), AV.shape[1], native.ptr(X), X.shape[1],
+                native.ptr(lam), native.ptr(W), k, native.ptr(norms), native.stream())
+    return W, norms
+
+
+def _precondition(W, src, state, w, omega_flat):
+    nov = W.shape[0]
+    nnew = len(src)
+    Q = torch.empty((nov, nnew), dtype=torch.float64, device=W.device)
+    if nnew == 0:
+        return Q
+    dev = W.device
+    src_t = torch.tensor(src, dtype=torch.int32, device=dev)
+    st_t = torch.tensor(state, dtype=torch.int32, device=dev)
+    W = W.contiguous()
+    w = w.contiguous()
+    native.call("dftb_davidson_precondition", nov, nnew, native.ptr(W), W.shape[1], native.ptr(src_t),
+                native.ptr(st_t), native.ptr(w), native.ptr(omega_flat), native.ptr(Q), nnew, native.stream())
+    return Q
+
+
+def hermitian_davidson(rv, omega, nstates, ifact=1, conv=1.0e-14, maxiter=10, XpYguess=None, Oia=None,
+                       L2_thresh=0.0, stats=None):
+    """Lowest nstates of R T = Omega^2 T, R = (A-B)^1/2 (A+B) (A-B)^1/2.
+
+    rv(V) returns R.V for a (nov, ncol) block.  Returns Omega (k), C, XmY, XpY
+    as (k, nocc, nvirt) device tensors.
+    """
+    nocc, nvirt = omega.shape
+    om = omega.reshape(-1).contiguous()
+    kmax = nocc * nvirt
+    lmax = min(ifact * nstates, kmax)
+    k = nstates
+    omega_sq = torch.sqrt(om)
+    if XpYguess is None:
+        bs = initial_expansion_vectors(om, lmax)
+    else:
+        bs = (XpYguess[:lmax].reshape(lmax, -1).T / omega_sq[:, None]).contiguous()
+        bs = bs / torch.linalg.norm(bs, dim=0)
+    AB = rv(bs)
+    l = lmax
+    for it in range(maxiter):
+        Hb = bs.T @ AB
+        w2, Tb = torch.linalg.eigh(Hb)
+        if L2_thresh > 0.0 and Oia is not None:
+            T_all = bs @ Tb
+            L2 = torch.sum(T_all * T_all * Oia.reshape(-1, 1), dim=0).cpu().numpy()
+            order = np.concatenate([np.where(L2 > L2_thresh)[0], np.where(L2 <= L2_thresh)[0]])
+            order_t = torch.as_tensor(order, device=om.device)
+            w2, Tb = w2[order_t], Tb[:, order_t]
+        w = torch.sqrt(w2)
+        Tk = Tb[:, :k]
+        X = bs @ Tk
+        W, norms_t = _residuals(AB @ Tk, X, w2[:k])
+        norms = norms_t.cpu().numpy()
+        if stats is not None:
+            stats.setdefault("residual_norms", []).append(norms.copy())
+        if (norms < conv).all():
+            break
+        dkmax = min(kmax - l, k)
+        eps = 0.01 * conv
+        src = [n for n in range(dkmax) if norms[n] > eps]
+        Q = _precondition(W, src, src, w, om)
+        Q = orthonormalize_new(bs, Q)
+        bs = torch.cat([bs, Q], dim=1)
+        AB = torch.cat([AB, rv(Q)], dim=1)
+        l = bs.shape[1]
+    else:
+        raise ExcitedStatesNotConverged(
+            "Davidson-like diagonalization for Hermitian eigenvalue problem did not converge after %s iterations "
+            "(threshold: %e) !!!" % (it + 1, conv))
+    if stats is not None:
+        stats["iterations"] = it + 1
+        stats["subspace"] = l
+    Omega = w[:k]
+    T = X  # (nov, k)
+    XpY = omega_sq[:, None] / torch.sqrt(Omega)[None, :] * T
+    XmY = torch.sqrt(Omega)[None, :] / omega_sq[:, None] * T
+    shape = (k, nocc, nvirt)
+    return Omega, T.T.reshape(shape), XmY.T.reshape(shape), XpY.T.reshape(shape)
+
+
+def _sqrtm_spd(M):
+    """Principal square root of the symmetric positive definite subspace matrix."""
+    lam, V = torch.linalg.eigh(0.5 * (M + M.T))
+    if bool((lam <= 0.0).any()):
+        raise ExcitedStatesError("(A-B) projected onto the expansion space is not positive definite")
+    return (V * torch.sqrt(lam)) @ V.T
+
+
+def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxiter=10, XmYguess=None,
+                          XpYguess=None, w_guess=None, stats=None):
+    """Lowest nstates of the non-Hermitian TD-DFTB problem (Stratmann-Scuseria-Frisch).
+
+    products(V) returns ((A+B).V, (A-B).V) for a (nov, ncol) block.
+    Returns Omega (k), C, XmY, XpY as (k, nocc, nvirt) device tensors.
+    """
+    nocc, nvirt = omega.shape
+    om = omega.reshape(-1).contiguous()
+    kmax = nocc * nvirt
+    k = nstates
+    dev = om.device
+    if XpYguess is None:
+        lmax = min(ifact * nstates, kmax)
+        bs = initial_expansion_vectors(om, lmax)
+    else:
+        lmaxp = nstates
+        lmaxm = min(nstates, kmax - nstates)
+        lmax = lmaxp + lmaxm
+        cols = torch.cat([XmYguess.reshape(nstates, -1), XpYguess.reshape(nstates, -1)[:lmaxm]], dim=0).T
+        bs = (cols / torch.linalg.norm(cols, dim=0)).contiguous()
+    AP, AM = products(bs)
+    l = lmax
+    for it in range(maxiter):
+        if XpYguess is None or it > 0:
+            Mp = bs.T @ AP
+            Mm = bs.T @ AM
+            Mmsq = _sqrtm_spd(Mm)
+            Mh = Mmsq @ Mp @ Mmsq
+            if torch.sum(torch.abs(Mh - Mh.T)).item() > 1.0e-10:
+                raise ExcitedStatesError("Mh is not hermitian!")
+            w2, Tb = torch.linalg.eigh(Mh)
+            w = torch.sqrt(w2)
+            Rb = (Mmsq @ Tb) / torch.sqrt(w)
+            Lb = (Mp @ Rb) / w
+            err = torch.sum(torch.abs(Lb.T @ Rb - torch.eye(len(w), dtype=torch.float64, device=dev))).item()
+            if err > 1.0e-3:
+                raise ExcitedStatesError("(X+Y) and (X-Y) vectors not orthonormal! error = %s" % err)
+            Rk, Lk = bs @ Rb[:, :k], bs @ Lb[:, :k]
+            ApR, AmL = AP @ Rb[:, :k], AM @ Lb[:, :k]
+        else:
+            Rk = XpYguess.reshape(nstates, -1).T.contiguous()
+            Lk = XmYguess.reshape(nstates, -1).T.contiguous()
+            w = torch.as_tensor(np.asarray(w_guess), dtype=torch.float64, device=dev) if not torch.is_tensor(
+                w_guess) else w_guess.to(dev)
+            ApR, _ = products(Rk)
+            _, AmL = products(Lk)
+        WL, nL = _residuals(ApR, Lk, w[:k])
+        WR, nR = _residuals(AmL, Rk, w[:k])
+        host = torch.stack([nL, nR]).cpu().numpy()
+        normsL, normsR = host[0], host[1]
+        norms = normsL + normsR
+        if stats is not None:
+            stats.setdefault("residual_norms", []).append(norms.copy())
+        if (norms < conv).all() and it > 0:
+            break
+        dkmax = min(kmax - l, 2 * k)
+        eps = 0.01 * conv
+        ncL, ncR = int(np.sum(normsL > eps)), int(np.sum(normsR > eps))
+        dkR = min(int(np.ceil(dkmax / 2.0)), ncL)
+        dkL = min(dkmax - dkR, ncR)
+        dk = dkR + dkL
+        src, state = [], []
+        for n in range(k):
+            if len(src) == dk:
+                break
+            if normsL[n] > eps:
+                src.append(n)
+                state.append(n)
+        for n in range(k):
+            if len(src) == dk:
+                break
+            if normsR[n] > eps:
+                src.append(k + n)
+                state.append(n)
+        assert len(src) == dk
+        Q = _precondition(torch.cat([WL, WR], dim=1), src, state, w, om)
+        Q = orthonormalize_new(bs, Q)
+        ap, am = products(Q)
+        bs = torch.cat([bs, Q], dim=1)
+        AP = torch.cat([AP, ap], dim=1)
+        AM = torch.cat([AM, am], dim=1)
+        l = bs.shape[1]
+    else:
+        raise ExcitedStatesNotConverged(
+            "Davidson-like diagonalization for non-Hermitian eigenvalue problem did not converge after %s "
+            "iterations (threshold: %e) !!!" % (it + 1, conv))
+    if stats is not None:
+        stats["iterations"] = it + 1
+        stats["subspace"] = l
+    Omega = w[:k]
+    C = bs @ Tb[:, :k]
+    shape = (k, nocc, nvirt)
+    return Omega, C.T.reshape(shape), Lk.T.reshape(shape), Rk.T.reshape(shape)

@@ -1,0 +1,180 @@
+/*
+ * dftbaby_b200 -- C ABI of the B200 (sm_100a) LR-TD-DFTB kernels.
+ *
+ * Conventions for every entry point:
+ *   - array arguments are DEVICE pointers to row-major FP64 (int32 for index
+ *     tables) memory owned by the caller; sizes are passed explicitly;
+ *   - logical shapes follow the DFTBaby arrays they replace (e.g. q_ov has
+ *     shape (Nat, nocc, nvirt), expansion vectors (nocc, nvirt, nvec));
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream); work is
+ *     enqueued asynchronously, nothing synchronises;
+ *   - the return value is a status code (DFTB_OK or a negative DFTB_ERR_*);
+ *     no entry point allocates device memory -- where scratch space is needed
+ *     the caller passes a workspace whose size the *_workspace_size query
+ *     returns.
+ *
+ * Each function cites the DFTBaby interface it replaces (file:line inside the
+ * DFTBaby project).
+ */
+#ifndef DFTBABY_B200_H
+#define DFTBABY_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DFTB_OK 0
+#define DFTB_ERR_BAD_SIZE -1    /* a size argument is out of range            */
+#define DFTB_ERR_NULL -2        /* a required pointer is NULL                 */
+#define DFTB_ERR_CUDA -3        /* a CUDA launch or runtime call failed       */
+#define DFTB_ERR_WORKSPACE -4   /* the workspace is smaller than required     */
+#define DFTB_ERR_UNSUPPORTED -5 /* angular momentum or table layout not handled */
+
+/* Library version and the CUDA error string of the last failing call on this
+ * host thread (empty if none). */
+const char *dftb_version(void);
+const char *dftb_last_error(void);
+
+/* Distances and directional cosines between all atoms.
+ * Replaces slako.directional_cosines (DFTB/extensions/slako.f90:31-70):
+ * r[i][j] = |R_i - R_j|, (x,y,z)[i][j] = (R_i - R_j)/r, and (0,0,1) when r = 0.
+ * pos: (nat, 3). r, x, y, z: (nat, nat). */
+int dftb_directional_cosines(int nat, const double *pos, double *r, double *x, double *y, double *z,
+                             void *stream);
+
+/* Slater-Koster overlap S and reference Hamiltonian H0.
+ * Replaces slako.h0ands (DFTB/extensions/slako.f90:77-231), including the
+ * B-spline evaluation of splines.f90:25-92 with its interval selection and its
+ * clamp at the last knot.
+ *   ind, typ, ls, ms : (norb) atom index, atom type, l, m of every orbital;
+ *                      the orbitals of one atom are contiguous and atoms are
+ *                      in increasing order;
+ *   r, x, y, z       : (nat, nat) from dftb_directional_cosines;
+ *   mprox            : (nat, nat) int, 1 where the atoms interact;
+ *   orben            : (norb) on-site energies;
+ *   tab_filled       : (npair, nsk) int; knots/coefs: (npair, nsk, npts);
+ *   S, H0            : (norb, norb) outputs, every element written.
+ * Only s and p orbitals (l <= 1) are implemented: elements that involve an
+ * orbital with l > 1 are written as NaN. */
+int dftb_h0_and_s(int norb, int nat, const int *ind, const int *typ, const int *ls, const int *ms,
+                  const double *r, const double *x, const double *y, const double *z, const int *mprox,
+                  const double *orben, int deg, const int *tab_filled, const double *S_knots,
+                  const double *S_coefs, const double *H_knots, const double *H_coefs, int npair, int nsk,
+                  int npts, double *S, double *H0, void *stream);
+
+/* Dipole matrix D[c][mu][nu] = <mu| r_c |nu>, c = x, y, z (three planes).
+ * Replaces slako.dipolematrix (DFTB/extensions/slako.f90:238-394); the
+ * reference returns it as (norb, norb, 3) after rollaxis
+ * (DFTB/SKMatrixElements.py:355-356).
+ *   pos : (nat, 3); S: (norb, norb) from dftb_h0_and_s; D: (3, norb, norb). */
+int dftb_dipole_matrix(int norb, int nat, const int *ind, const int *typ, const int *ls, const int *ms,
+                       const double *r, const double *x, const double *y, const double *z, const double *pos,
+                       const int *mprox, const double *S, int deg, const int *tab_filled_D,
+                       const double *D_knots, const double *D_coefs, int npair, int nskd, int npts, double *D,
+                       void *stream);
+
+/* Gaussian gamma matrices.
+ * Replaces GammaMatrix.gamma_atomwise with GammaGaussian / GammaGaussianLC
+ * (DFTB/GammaApproximation.py:122-151, 210-243, 388-405):
+ *   gamma[A][B]    = erf(R/sqrt(2(sA^2+sB^2)))/R,            gamma[A][A] = 1/(sqrt(pi) sA)
+ *   gamma_lr[A][B] = erf(R/sqrt(2(sA^2+sB^2+Rlr^2/2)))/R,   gamma_lr[A][A] = 1/sqrt(pi(sA^2+Rlr^2/4))
+ * sigma: (nat) Gaussian widths; r: (nat, nat).  gamma_lr may be NULL. */
+int dftb_gamma_matrices(int nat, const double *r, const double *sigma, double r_lr, double *gamma,
+                        double *gamma_lr, void *stream);
+
+/* AO expansion G[mu][nu] = g[atom(mu)][atom(nu)] (gamma_AOwise's g0_AO,
+ * DFTB/GammaApproximation.py:406-447, without the unused gradient array). */
+int dftb_ao_expand(int norb, int nat, const int *ind, const double *g, double *G, void *stream);
+
+/* SCC Hamiltonian H = H0 + 1/2 S o (e_mu + e_nu), e = gamma . dq per atom.
+ * Replaces DFTB2._construct_h1 / _coulomb_hamiltonian and the sum
+ * H = H0 + Hcoul (DFTB/DFTB2.py:668-717, 1023).
+ * estat: (nat) output, the electrostatic potential gamma . dq. */
+int dftb_scc_hamiltonian(int norb, int nat, const int *ind, const double *H0, const double *S,
+                         const double *gamma, const double *dq, double *estat, double *H, void *stream);
+
+/* Mulliken monopoles q_A = sum_{mu in A} sum_nu P S, dq_A = sum (P - P0) S.
+ * Replaces mulliken.monopoles (DFTB/extensions/mulliken.f90:11-66).
+ * P, P0, S: (norb, norb); orbs_per_atom: (nat); q, dq: (nat). */
+int dftb_monopoles(int norb, int nat, const double *P, const double *P0, const double *S,
+                   const int *orbs_per_atom, double *q, double *dq, void *stream);
+
+/* Mulliken transition charges
+ *   q^{pq}_A = 1/2 sum_{mu in A} (C_mu,p (S C)_mu,q + C_mu,q (S C)_mu,p)
+ * for the occupied-occupied, occupied-virtual and virtual-virtual blocks.
+ * Replaces tddftb.trans_charges (DFTB/extensions/tddftb.f90:12-112).
+ *   orbs_occ: (norb, nocc), orbs_virt: (norb, nvirt), S: (norb, norb);
+ *   q_oo: (nat, nocc, nocc), q_ov: (nat, nocc, nvirt), q_vv: (nat, nvirt, nvirt);
+ *   any of the three outputs may be NULL to skip it;
+ *   work: at least dftb_trans_charges_workspace_size() bytes. */
+size_t dftb_trans_charges_workspace_size(int norb, int nocc, int nvirt);
+int dftb_trans_charges(int norb, int nat, int nocc, int nvirt, const double *orbs_occ, const double *orbs_virt,
+                       const double *S, const int *orbs_per_atom, double *q_oo, double *q_ov, double *q_vv,
+                       void *work, size_t work_bytes, void *stream);
+
+/* Diagonal transition charges q^{ii}_A and q^{aa}_A (the inputs of the
+ * Lambda-2 diagnostic, DFTB/LR_TDDFTB.py:538-560), without the full blocks.
+ *   q_ii: (nat, nocc), q_aa: (nat, nvirt); work as for dftb_trans_charges. */
+int dftb_trans_charges_diag(int norb, int nat, int nocc, int nvirt, const double *orbs_occ,
+                            const double *orbs_virt, const double *S, const int *orbs_per_atom, double *q_ii,
+                            double *q_aa, void *work, size_t work_bytes, void *stream);
+
+/* Hermitian TD-DFTB product for the singlet problem without long-range
+ * correction, applied to nvec vectors at once:
+ *   u = omega^2 o v + 4 sqrt(omega) o (q^T gamma q (sqrt(omega) o v))
+ * Replaces Rv() inside Solver.HermitianDavidson (DFTB/Solver.py:431-444).
+ *   gamma: (nat, nat); q_ov: (nat, nocc, nvirt); omega: (nocc, nvirt);
+ *   vs, us: (nocc, nvirt, nvec); work: dftb_hermitian_rv_workspace_size(). */
+size_t dftb_hermitian_rv_workspace_size(int nat, int nvec);
+int dftb_hermitian_rv(int nat, int nocc, int nvirt, int nvec, const double *gamma, const double *q_ov,
+                      const double *omega, const double *vs, double *us, void *work, size_t work_bytes,
+                      void *stream);
+
+/* (A+B).v and (A-B).v for nvec vectors, singlets, in the transition-charge
+ * form of the reference:
+ *   (A+B)v = omega v + 4 q_ov^T g q_ov v - K1 v - K2 v,   (A-B)v = omega v + K2 v - K1 v,
+ *   K1 v = sum q_oo g_lr q_vv v   ((ij|ab) exchange),  K2 v = sum q_ov g_lr q_ov v  ((ib|ja) exchange);
+ * with lc = 0 the exchange terms are skipped.
+ * Replaces tddftb.apbv / tddftb.ambv (DFTB/extensions/tddftb.f90:114-287) and
+ * Solver._ApBv / _AmBv (DFTB/Solver.py:583-635).
+ *   g, g_lr: (nat, nat); q_oo, q_ov, q_vv as for dftb_trans_charges;
+ *   omega: (nocc, nvirt); vs, us: (nocc, nvirt, nvec);
+ *   work: dftb_apbv_workspace_size() bytes with lc = 1, and
+ *   dftb_hermitian_rv_workspace_size() bytes with lc = 0. */
+size_t dftb_apbv_workspace_size(int nat, int nocc, int nvirt, int nvec);
+int dftb_apbv(int nat, int nocc, int nvirt, int nvec, int lc, const double *g, const double *g_lr,
+              const double *q_oo, const double *q_ov, const double *q_vv, const double *omega, const double *vs,
+              double *us, void *work, size_t work_bytes, void *stream);
+int dftb_ambv(int nat, int nocc, int nvirt, int nvec, int lc, const double *g, const double *g_lr,
+              const double *q_oo, const double *q_ov, const double *q_vv, const double *omega, const double *vs,
+              double *us, void *work, size_t work_bytes, void *stream);
+
+/* Davidson correction vectors: for c in [0, nnew),
+ *   Q[:, c] = W[:, src[c]] / (w[state[c]] - omega),  where |w - omega| < 1e-6
+ *   is replaced by 1e-6 * omega.
+ * Replaces the preconditioning loops of Solver.HermitianDavidson and
+ * Solver.nonHermitianDavidson (DFTB/Solver.py:530-539, 852-882).
+ *   W: (nov, ldw) residual columns, omega: (nov), w: eigenvalue per state,
+ *   src, state: (nnew) int32 column / state indices, Q: (nov, ldq). */
+int dftb_davidson_precondition(int nov, int nnew, const double *W, int ldw, const int *src, const int *state,
+                               const double *w, const double *omega, double *Q, int ldq, void *stream);
+
+/* Residual update W[:, c] = AV[:, c] - lam[c] * X[:, c] for c < ncol and the
+ * column norms |W[:, c]| (Solver.py:505-509, 823-832).
+ *   AV, X, W: (nov, ld*) column blocks; lam: (ncol); norms: (ncol) output. */
+int dftb_davidson_residual(int nov, int ncol, const double *AV, int ldav, const double *X, int ldx,
+                           const double *lam, double *W, int ldw, double *norms, void *stream);
+
+/* General FP64 product C = alpha * op(A) . op(B) + beta * C on row-major
+ * matrices (op = transpose when trans != 0), the contraction engine behind the
+ * entry points above, exported for the host-side solver. */
+int dftb_dgemm(int transa, int transb, int m, int n, int k, double alpha, const double *A, int lda,
+               const double *B, int ldb, double beta, double *C, int ldc, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DFTBABY_B200_H */
