@@ -1,0 +1,323 @@
+"""Benchmark: converged excited states per second for LR-TD-DFTB on B200.
+
+Default workload (N=1): lc-TD-DFTB on a hydrogen-terminated hexagonal
+graphene flake with armchair edges, C1014H90 (1104 atoms, 4146 orbitals;
+C-C 1.42 A, C-H 1.09 A, seeded sigma = 0.01 A jitter), active window
+1225 x 1225 occupied x virtual (1,500,625 pairs), lowest 30 singlets,
+Davidson residual 1e-6, SCC to 1e-10.  (The zigzag-edged flake of the same
+size, C864H72, has a singlet-unstable long-range-corrected ground state --
+(A-B) is not positive definite -- so neither this solver nor DFTBaby's can
+converge its excited states.)
+One step = one complete solve of a freshly jittered geometry (new seed per
+step and rank): SK matrices, gamma, SCC, transition charges, Davidson,
+transition dipoles and oscillator strengths.  Inputs are synthetic.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload armchair7|zigzag8|polyene20]
+
+With torchrun each rank solves its own geometries (independent replicas, weak
+scaling); the step time is the maximum over ranks.  ``--impl reference`` times
+the CPU restatement of DFTBaby's algorithm (oracle/) on the host cores with a
+bounded, extrapolated sample and prints the same metric.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "converged excited states/s vs plain FP64 GPU path at ≤1 meV, ≤1e-4 f error"
+UNIT = "states/s"
+
+WORKLOADS = {
+    # name: (builder args, lc, LR options)
+    "armchair7": dict(kind="armchair", n=7, sigma=0.01, lc=1,
+                      opts=dict(nstates=30, nr_active_occ=1225, nr_active_virt=1225, diag_conv=1.0e-6,
+                                diag_maxiter=100)),
+    "zigzag8": dict(kind="flake", n=8, sigma=0.01, lc=1,
+                    opts=dict(nstates=30, nr_active_occ=300, nr_active_virt=300, diag_conv=1.0e-6,
+                              diag_maxiter=100)),
+    "polyene20": dict(kind="polyene", n=20, sigma=0.02, lc=0,
+                      opts=dict(nstates=10, diag_conv=1.0e-6, diag_maxiter=100)),
+}
+
+
+def build_geometry(w, seed):
+    from dftbaby_b200 import geometry
+    if w["kind"] == "flake":
+        return geometry.hexagonal_flake(w["n"], sigma=w["sigma"], seed=seed)
+    if w["kind"] == "armchair":
+        return geometry.armchair_flake(w["n"], sigma=w["sigma"], seed=seed)
+    return geometry.polyene(w["n"], sigma=w["sigma"], seed=seed)
+
+
+def workload_config(name, w, n_gpus):
+    from dftbaby_b200 import geometry
+    al = build_geometry(w, 0)
+    nat = len(al)
+    norb = sum(1 if z == 1 else 4 for z, _ in al)
+    o = w["opts"]
+    no = o.get("nr_active_occ") or None
+    cfg = {"workload": "%s %s lc-TD-DFTB" % (name, geometry.formula(al)) if w["lc"] else
+           "%s %s TD-DFTB" % (name, geometry.formula(al)),
+           "atoms": nat, "orbitals": norb, "long_range_correction": w["lc"], "nstates": o["nstates"],
+           "active_window": [o.get("nr_active_occ"), o.get("nr_active_virt")],
+           "davidson_residual": o["diag_conv"], "scf_conv": 1e-10, "precision": "fp64",
+           "geometry": "seeded jitter per step and rank",
+           "l2": "working set (q_ov %s GB) larger than L2; no flush needed" % (
+               round(8.0 * nat * (no or norb // 2) ** 2 / 1e9, 2) if no else "n/a"),
+           "parallelism": "replicas x%d" % n_gpus}
+    return cfg
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def run_reference(args, rank, world):
+    """CPU arm: the oracle restatement of DFTBaby's algorithm on the host cores."""
+    if rank != 0:
+        return
+    from oracle import cpu_baseline as CB
+    w = WORKLOADS[args.workload]
+    cfg = workload_config(args.workload, w, 1)
+    totals, samples = [], []
+    for step in range(args.warmup + args.steps):
+        al = build_geometry(w, 1000 + step)
+        if w["lc"]:
+            r = CB.flake_lc_sample(al, window=w["opts"]["nr_active_occ"], nstates=w["opts"]["nstates"])
+            t, desc = r["extrapolated_total_s"], r["sample"]
+        else:
+            t, _ = CB.small_full_run(al, w["lc"], w["opts"]["nstates"], w["opts"]["diag_conv"])
+            desc = "full oracle solve"
+        if step >= args.warmup:
+            totals.append(t)
+            samples.append(desc)
+    T = sum(totals) / len(totals)
+    value = w["opts"]["nstates"] / T
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": T * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS",
+                                                                                        os.cpu_count())),
+                             "kind": "port", "sample": samples[0]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_entry(args):
+    from oracle import cpu_baseline as CB
+    w = WORKLOADS[args.workload]
+    al = build_geometry(w, 999)
+    if w["lc"]:
+        r = CB.flake_lc_sample(al, window=w["opts"]["nr_active_occ"], nstates=w["opts"]["nstates"])
+        return {"value": w["opts"]["nstates"] / r["extrapolated_total_s"], "unit": UNIT, "cores": r["threads"],
+                "kind": "port", "sample": r["sample"] + " (timed %.1f s)" % r["sample_wall_s"]}
+    t, _ = CB.small_full_run(al, w["lc"], w["opts"]["nstates"], w["opts"]["diag_conv"])
+    return {"value": w["opts"]["nstates"] / t, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS",
+                                                                                       os.cpu_count())),
+            "kind": "port", "sample": "one full oracle solve"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--workload", default="armchair7", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    from dftbaby_b200 import LR_TDDFTB, native
+    native.load()
+    w = WORKLOADS[args.workload]
+    opts = w["opts"]
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def solve(seed, timed_entries=False):
+        al = build_geometry(w, seed)
+        td = LR_TDDFTB(al, long_range_correction=w["lc"])
+        td.setGeometry(al)
+        Om, f = td.getEnergies(**opts)
+        return td, Om, f
+
+    for s in range(args.warmup):
+        solve(10_000 + s * world + rank)
+    barrier()
+    # ---- device-timed region (inputs resident: geometry and tables uploaded before each solve's timer)
+    native.counters.reset()
+    native.counters.time_entries(["dftb_apbv", "dftb_trans_charges", "dftb_h0_and_s", "dftb_dipole_matrix"])
+    sampler = ClockSampler(local)
+    sampler.start()
+    stream = torch.cuda.current_stream()
+    dev_ms = 0.0
+    phases = {}
+    stats = []
+    for s in range(args.steps):
+        al = build_geometry(w, 20_000 + s * world + rank)
+        td = LR_TDDFTB(al, long_range_correction=w["lc"])
+        td.setGeometry(al)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        td.getEnergies(**opts)
+        e1.record(stream)
+        e1.synchronize()
+        dev_ms += e0.elapsed_time(e1)
+        for k, v in td.phase_ms().items():
+            phases[k] = phases.get(k, 0.0) + v
+        stats.append({"scc_iterations": td.dftb2.scc_iterations, "davidson_iterations": td.stats.get("iterations"),
+                      "subspace": td.stats.get("subspace")})
+    barrier()
+    clocks = sampler.stop()
+    launches = native.counters.launches
+    # kernel timings for the roofline
+    entry_ms = {n: native.counters.elapsed_ms(n) for n in native.counters.timed}
+    native.counters.timed = None
+    t_dev = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
+    ms_per_step = t_dev.item() / args.steps
+    value = world * opts["nstates"] / (ms_per_step / 1e3)
+
+    # ---- end to end through the public API: host atomlist in, numpy (Omega, f) out
+    barrier()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for s in range(0 if args.no_e2e else args.steps):
+        al = build_geometry(w, 30_000 + s * world + rank)
+        td = LR_TDDFTB(al, long_range_correction=w["lc"])
+        td.setGeometry(al)
+        Om, f = td.getEnergies(**opts)
+        h2d = 8 * 3 * len(al) + 4 * 6 * td.dftb2.dim + 8 * sum(v.numel() for v in td.dftb2.par.device_tables(
+            td.dftb2.device).values())
+        d2h = Om.nbytes + f.nbytes
+    torch.cuda.synchronize()
+    e2e_s = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
+    e2e_value = None if args.no_e2e else world * opts["nstates"] * args.steps / e2e_s.item()
+
+    # ---- roofline of the dominant native kernel group
+    peak, peak_kind = measured_peaks()
+    nat = len(build_geometry(w, 0))
+    no = opts.get("nr_active_occ") or td.nocc
+    nv = opts.get("nr_active_virt") or td.nvirt
+    totals = {n: sum(v) for n, v in entry_ms.items() if v}
+    dom = max(totals, key=totals.get) if totals else None
+    roof = None
+    if dom == "dftb_apbv":
+        # Coulomb product u = omega v + 4 q^T gamma q v: q_ov (nat x nov) is streamed twice
+        ms = statistics.mean(entry_ms[dom])
+        nvec = statistics.mean([c for c in [2 * opts["nstates"]]])
+        algo = 2 * 8.0 * nat * no * nv + 2 * 8.0 * no * nv * nvec
+        roof = {"kernel": "dftb_apbv (Coulomb product, 3 launches)", "bound": "hbm", "achieved": algo / ms / 1e6,
+                "peak": peak, "unit": "GB/s", "frac": algo / ms / 1e6 / peak, "traffic": None,
+                "algorithmic_bytes_per_launch": algo, "ms_per_launch": ms, "peak_source": peak_kind}
+    elif dom == "dftb_trans_charges":
+        ms = statistics.mean(entry_ms[dom])
+        algo = 8.0 * nat * no * nv + 8.0 * td.dftb2.dim * (no + nv) * 2
+        roof = {"kernel": "dftb_trans_charges (q_ov)", "bound": "hbm", "achieved": algo / ms / 1e6, "peak": peak,
+                "unit": "GB/s", "frac": algo / ms / 1e6 / peak, "traffic": None,
+                "algorithmic_bytes_per_launch": algo, "ms_per_launch": ms, "peak_source": peak_kind}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometries)",
+            "config": workload_config(args.workload, w, world),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": launches, "clocks": clocks, "roofline": roof,
+            "phases_ms_per_step": {k: v / args.steps for k, v in phases.items()},
+            "native_ms_per_step": {k: v / args.steps for k, v in totals.items()},
+            "solver": stats[-1] if stats else None}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_entry(args)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

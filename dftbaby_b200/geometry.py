@@ -103,6 +103,25 @@ def hexagonal_flake(n, sigma=0.0, seed=0, cc=1.42, ch=1.09):
     return _to_atomlist(C, _terminate(C, cc, ch), sigma, seed)
 
 
+def armchair_flake(n, sigma=0.0, seed=0, cc=1.42, ch=1.09):
+    """Armchair-edged hexagonal flake: hexagons whose centres lie inside a
+    hexagon whose edge normals are the lattice directions (edges along the
+    armchair directions 30, 90, 150 degrees); n sets the size."""
+    w = np.sqrt(3.0) * cc
+    a1 = np.array([w, 0.0])
+    a2 = np.array([w / 2.0, 1.5 * cc])
+    dirs = [np.array([np.cos(np.deg2rad(60.0 * k)), np.sin(np.deg2rad(60.0 * k))]) for k in range(6)]
+    R = 1.5 * w * n + 1e-6
+    centers = []
+    for i in range(-3 * n, 3 * n + 1):
+        for j in range(-3 * n, 3 * n + 1):
+            c = i * a1 + j * a2
+            if max(np.dot(c, d) for d in dirs) <= R:
+                centers.append(tuple(c))
+    C = _honeycomb(centers, cc)
+    return _to_atomlist(C, _terminate(C, cc, ch), sigma, seed)
+
+
 def formula(atomlist):
     nc = sum(1 for Z, _ in atomlist if Z == 6)
     nh = sum(1 for Z, _ in atomlist if Z == 1)

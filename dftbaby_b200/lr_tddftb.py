@@ -185,7 +185,11 @@ class LR_TDDFTB:
         if ct_correction or stability:
             raise ValueError("ct_correction and stability analysis are not implemented")
         d = self.dftb2
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record()
         self.en0 = d.getEnergy(**scf_opts)
+        ev[1].record()
+        self._phase_events = ev
         self.setActiveOrbitals(nr_active_occ, nr_active_virt)
         self.setMultiplicity(multiplicity)
         self.nstates = nstates
@@ -194,13 +198,23 @@ class LR_TDDFTB:
         self._solve_lr_equations(multiplicity=multiplicity, nstates=nstates, diag_ifact=diag_ifact,
                                  diag_conv=diag_conv, diag_maxiter=diag_maxiter, diag_check=diag_check,
                                  diag_L2threshold=diag_L2threshold)
+        ev[2].record()
         if oszis == "Dipoles":
             self._TransitionDipoles()
         else:
             self._TransitionDipolesMulliken()
         self.getOscillatorStrengths()
         self.Lambda2 = torch.sum(self.Cij ** 2 * self.Oia[None], dim=(1, 2))
+        ev[3].record()
         return self.Omega, self.oscillator_strength
+
+    def phase_ms(self):
+        """Device time (ms) of the last getEnergies: ground state (SK, gamma, SCC),
+        excited states (transition charges, Davidson), properties (dipoles, f)."""
+        ev = self._phase_events
+        ev[3].synchronize()
+        return {"ground_state": ev[0].elapsed_time(ev[1]), "excited_states": ev[1].elapsed_time(ev[2]),
+                "properties": ev[2].elapsed_time(ev[3])}
 
     def _solve_lr_equations(self, multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5, diag_maxiter=50,
                             diag_check=0, diag_L2threshold=0.0):

@@ -95,9 +95,49 @@ def check(rc, what):
         raise NativeError("%s failed (%s): %s" % (what, _ERRORS.get(rc, rc), msg))
 
 
+# kernels launched per entry point (dgemm-backed entry points launch several)
+KERNELS_PER_CALL = {
+    "dftb_directional_cosines": 1, "dftb_h0_and_s": 1, "dftb_dipole_matrix": 1, "dftb_gamma_matrices": 1,
+    "dftb_ao_expand": 1, "dftb_scc_hamiltonian": 2, "dftb_monopoles": 1, "dftb_trans_charges": 6,
+    "dftb_trans_charges_diag": 5, "dftb_hermitian_rv": 3, "dftb_apbv": 3, "dftb_ambv": 1,
+    "dftb_davidson_precondition": 1, "dftb_davidson_residual": 2, "dftb_dgemm": 1,
+}
+
+
+class Counters:
+    """Launch counts and optional CUDA-event timing of native entry points."""
+
+    def __init__(self):
+        self.reset()
+
+    def reset(self):
+        self.launches = 0
+        self.calls = {}
+        self.timed = None  # name -> list of (start_event, end_event)
+
+    def time_entries(self, names):
+        self.timed = {n: [] for n in names}
+
+    def elapsed_ms(self, name):
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in (self.timed or {}).get(name, [])]
+
+
+counters = Counters()
+
+
 def call(name, *args):
     L = load()
+    ev = None
+    if counters.timed is not None and name in counters.timed:
+        ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        ev[0].record()
     check(getattr(L, name)(*args), name)
+    if ev is not None:
+        ev[1].record()
+        counters.timed[name].append(ev)
+    counters.launches += KERNELS_PER_CALL.get(name, 1)
+    counters.calls[name] = counters.calls.get(name, 0) + 1
 
 
 class Workspace:
