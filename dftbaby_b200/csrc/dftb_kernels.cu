@@ -10,6 +10,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
+
 #include "dftbaby_b200.h"
 
 namespace {
@@ -1083,3 +1085,100 @@ int dftb_dgemm(int transa, int transb, int m, int n, int k, double alpha, const 
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Allocation-free variant of dftb_trans_charges.
+//
+// Some callers cannot allocate device memory at the point where they need the
+// transition charges: applications that reserve the GPU's memory up front in
+// their own pool and forbid any further cudaMalloc, or language bindings that
+// only receive device pointers from their host program and have no allocator
+// of their own.  dftb_trans_charges wants a caller-provided workspace; this
+// variant instead keeps its scratch (S.C for both orbital blocks and the
+// per-atom orbital offsets) in a fixed file-scope device array.
+//
+// The array exists once per GPU that loads this library and stays resident
+// until the process exits.  On the host its name is only a stand-in symbol,
+// so its device address is looked up with cudaGetSymbolAddress, once per
+// device, the first time the entry point runs with that device current (the
+// first call should therefore come before any stream capture).  All calls on
+// one device share the array: calls that can run at the same time on the GPU
+// (unordered streams, concurrent host threads) race on it and must be
+// serialised by the caller.  Every call rewrites the parts of the scratch it
+// reads, so nothing has to be cleared between calls.
+// ============================================================================
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // 8 MiB per device
+static __device__ __align__(256) unsigned char g_tc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+void *g_tc_scratch_addr[kMaxDevices] = {nullptr};
+std::mutex g_tc_scratch_mutex;
+
+int tc_scratch_address(void **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        snprintf(g_last_error, sizeof(g_last_error), "trans_charges_noalloc: cudaGetDevice: %s",
+                 cudaGetErrorString(e));
+        return DFTB_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= kMaxDevices) return fail(DFTB_ERR_BAD_SIZE, "trans_charges_noalloc: device index");
+    std::lock_guard<std::mutex> lock(g_tc_scratch_mutex);
+    if (!g_tc_scratch_addr[dev]) {
+        void *ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_tc_scratch);
+        if (e != cudaSuccess || !ptr) {
+            snprintf(g_last_error, sizeof(g_last_error), "trans_charges_noalloc: cudaGetSymbolAddress: %s",
+                     cudaGetErrorString(e));
+            return DFTB_ERR_CUDA;
+        }
+        g_tc_scratch_addr[dev] = ptr;
+    }
+    *out = g_tc_scratch_addr[dev];
+    return DFTB_OK;
+}
+
+}  // namespace
+
+extern "C" size_t dftb_trans_charges_noalloc_max_bytes(void) { return kNoAllocScratchBytes; }
+
+extern "C" int dftb_trans_charges_noalloc(int norb, int nat, int nocc, int nvirt, const double *co, const double *cv,
+                                          const double *Sm, const int *opa, double *q_oo, double *q_ov,
+                                          double *q_vv, void *stream) {
+    if (norb <= 0 || nat <= 0 || nocc < 0 || nvirt < 0 || nat > norb)
+        return fail(DFTB_ERR_BAD_SIZE, "trans_charges_noalloc: sizes");
+    const size_t need = dftb_trans_charges_workspace_size(norb, nocc, nvirt);
+    if (need > kNoAllocScratchBytes) {
+        snprintf(g_last_error, sizeof(g_last_error),
+                 "trans_charges_noalloc: needs %zu bytes of scratch, the static array holds %zu "
+                 "(use dftb_trans_charges with a workspace)",
+                 need, kNoAllocScratchBytes);
+        return DFTB_ERR_WORKSPACE;
+    }
+    void *scratch = nullptr;
+    int rc = tc_scratch_address(&scratch);
+    if (rc) return rc;
+    cudaStream_t st = S(stream);
+    double *sco, *scv;
+    int *first;
+    rc = trans_charges_common(norb, nat, nocc, nvirt, co, cv, Sm, opa, scratch, kNoAllocScratchBytes, st, &sco, &scv,
+                              &first);
+    if (rc) return rc;
+    struct Blk {
+        double *out;
+        const double *c1, *s1, *c2, *s2;
+        int n1, n2;
+    } blks[3] = {{q_oo, co, sco, co, sco, nocc, nocc},
+                 {q_ov, co, sco, cv, scv, nocc, nvirt},
+                 {q_vv, cv, scv, cv, scv, nvirt, nvirt}};
+    for (auto &b : blks) {
+        if (!b.out || b.n1 == 0 || b.n2 == 0) continue;
+        if (nat > 65535) return fail(DFTB_ERR_BAD_SIZE, "trans_charges_noalloc: nat > 65535");
+        dim3 grid(cdiv(b.n2, 32), cdiv(b.n1, 32), nat);
+        tc_kernel<<<grid, dim3(32, 8), 0, st>>>(b.n1, b.n2, first, b.c1, b.s1, b.c2, b.s2, b.out);
+        if ((rc = check_launch("tc_kernel (noalloc)"))) return rc;
+    }
+    return DFTB_OK;
+}

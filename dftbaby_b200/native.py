@@ -13,6 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libdftbaby_b200.so")
 
 DFTB_OK = 0
+DFTB_ERR_WORKSPACE = -4
 _ERRORS = {-1: "bad size", -2: "null pointer", -3: "CUDA error", -4: "workspace too small", -5: "unsupported"}
 
 
@@ -46,6 +47,8 @@ _SIGNATURES = {
     "dftb_trans_charges_workspace_size": (_Z, [_I, _I, _I]),
     "dftb_trans_charges": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _Z, _P]),
     "dftb_trans_charges_diag": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _Z, _P]),
+    "dftb_trans_charges_noalloc_max_bytes": (_Z, []),
+    "dftb_trans_charges_noalloc": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
     "dftb_hermitian_rv_workspace_size": (_Z, [_I, _I]),
     "dftb_hermitian_rv": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _Z, _P]),
     "dftb_apbv_workspace_size": (_Z, [_I, _I, _I, _I]),
@@ -99,7 +102,7 @@ def check(rc, what):
 KERNELS_PER_CALL = {
     "dftb_directional_cosines": 1, "dftb_h0_and_s": 1, "dftb_dipole_matrix": 1, "dftb_gamma_matrices": 1,
     "dftb_ao_expand": 1, "dftb_scc_hamiltonian": 2, "dftb_monopoles": 1, "dftb_trans_charges": 6,
-    "dftb_trans_charges_diag": 5, "dftb_hermitian_rv": 3, "dftb_apbv": 3, "dftb_ambv": 1,
+    "dftb_trans_charges_diag": 5, "dftb_trans_charges_noalloc": 6, "dftb_hermitian_rv": 3, "dftb_apbv": 3, "dftb_ambv": 1,
     "dftb_davidson_precondition": 1, "dftb_davidson_residual": 2, "dftb_dgemm": 1,
 }
 

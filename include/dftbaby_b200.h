@@ -114,6 +114,25 @@ int dftb_trans_charges(int norb, int nat, int nocc, int nvirt, const double *orb
                        const double *S, const int *orbs_per_atom, double *q_oo, double *q_ov, double *q_vv,
                        void *work, size_t work_bytes, void *stream);
 
+/* Allocation-free variant of dftb_trans_charges (no counterpart in DFTBaby).
+ * For callers that cannot allocate device memory where they need the charges:
+ * hosts that reserve the GPU's memory up front in their own pool and forbid
+ * further cudaMalloc, or bindings that only receive device pointers.  Same
+ * arguments and results as dftb_trans_charges, without the workspace: the
+ * scratch (S.C of both orbital blocks and per-atom orbital offsets) lives in a
+ * fixed 8 MiB device array that each GPU loading the library holds until the
+ * process exits.  Requests needing more than dftb_trans_charges_noalloc_max_bytes()
+ * of scratch (dftb_trans_charges_workspace_size() > 8 MiB) return
+ * DFTB_ERR_WORKSPACE and launch nothing.  The first call on a device looks up
+ * the array's address for that device (cudaGetSymbolAddress), so make it
+ * before any stream capture.  All calls on one device share the array: calls
+ * that may run concurrently on the GPU race and must be serialised.  No
+ * device memory is allocated or freed. */
+size_t dftb_trans_charges_noalloc_max_bytes(void);
+int dftb_trans_charges_noalloc(int norb, int nat, int nocc, int nvirt, const double *orbs_occ,
+                               const double *orbs_virt, const double *S, const int *orbs_per_atom, double *q_oo,
+                               double *q_ov, double *q_vv, void *stream);
+
 /* Diagonal transition charges q^{ii}_A and q^{aa}_A (the inputs of the
  * Lambda-2 diagnostic, DFTB/LR_TDDFTB.py:538-560), without the full blocks.
  *   q_ii: (nat, nocc), q_aa: (nat, nvirt); work as for dftb_trans_charges. */
