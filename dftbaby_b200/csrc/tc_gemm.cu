@@ -1,0 +1,427 @@
+// Split-precision BF16 GEMM on the 5th-generation tensor cores (tcgen05) of B200.
+//
+//   C(m, n) = alpha * sum_s sum_k A_s(m, k) B_s(n, k)          (FP32 accumulation in TMEM)
+//
+// with up to three (A_s, B_s) operand pairs ("segments") that share M, N, K.
+// Splitting an FP32 operand X into BF16 parts X = X_hi + X_lo and summing the
+// segments (A_hi,B_hi), (A_hi,B_lo), (A_lo,B_hi) reproduces the FP32 product to
+// ~2^-16 relative error at three BF16 tensor-core passes.
+//
+// Operands are K-major row-major BF16 matrices (A: M x K, B: N x K, leading
+// dimensions multiples of 8 elements, 16-byte aligned base).  The epilogue can
+//   * multiply elementwise by an FP32 matrix G (the AO-expanded gamma^lr),
+//   * store FP32 C,
+//   * store the result as a BF16 hi/lo pair, row-major and/or transposed
+//     (the transposed store is coalesced across a warp).
+//
+// Structure per CTA (128 threads, one 128x128 output tile):
+//   warp 0 lane 0 : TMA producer, 4-stage ring of 128x64 A and B tiles
+//                   (128-byte swizzle), mbarrier::complete_tx completion;
+//   warp 1 lane 0 : issues tcgen05.mma (M=128, N=128, K=16 per instruction)
+//                   into a 128-column TMEM accumulator; tcgen05.commit frees
+//                   ring slots and finally signals the epilogue;
+//   warps 0..3    : epilogue, tcgen05.ld 32x32b of their 32 TMEM lanes.
+// Every mbarrier wait is bounded; on timeout the kernel records an error
+// code, stops issuing work, drains the copies it started and releases TMEM.
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+
+#include "dftbaby_b200.h"
+
+namespace tcg {
+
+constexpr int BM = 128, BN = 128, BK = 64, STAGES = 4;
+constexpr int TILE_A_BYTES = BM * BK * 2;  // 16 KiB
+constexpr int TILE_B_BYTES = BN * BK * 2;  // 16 KiB
+constexpr int STAGE_BYTES = TILE_A_BYTES + TILE_B_BYTES;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /* alignment slack */ + 256 /* barriers */;
+constexpr unsigned long long kSpinLimit = 1ull << 24;  // bounded waits (well above any legitimate wait)
+
+struct Maps {
+    CUtensorMap a[3];
+    CUtensorMap b[3];
+};
+
+struct Params {
+    int M, N, K, nseg;
+    float alpha;
+    const float *G;
+    long long ldg;
+    float *C;
+    long long ldc;
+    __nv_bfloat16 *Ohi, *Olo;  // row-major hi/lo output (ld = ldo)
+    long long ldo;
+    __nv_bfloat16 *Thi, *Tlo;  // transposed hi/lo output: T(n, m) (ld = ldt)
+    long long ldt;
+    int *err;  // device error word (0 = ok)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// bounded parity wait; returns false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (unsigned long long it = 0; it < kSpinLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], "
+        "[%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major operand, 128-byte swizzle, rows of 128 B,
+// 8-row core-matrix groups 1024 B apart (SBO), version 1 (sm_100).
+__device__ __forceinline__ uint64_t smem_desc_k128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFF) >> 4);      // start address
+    d |= (uint64_t)1 << 16;                        // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;              // stride byte offset
+    d |= (uint64_t)1 << 46;                        // descriptor version
+    d |= (uint64_t)2 << 61;                        // SWIZZLE_128B
+    return d;
+}
+
+// instruction descriptor: D = F32, A = B = BF16, both K-major, M = 128, N = 128
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                            ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_c, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_c),
+        "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Maps maps, const Params p) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    uint64_t *done = empty + STAGES;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int kblocks = (p.K + BK - 1) / BK;
+    const int total = kblocks * p.nseg;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncwarp();
+    if (warp == 0) {
+        // allocate 128 TMEM columns (128 lanes x 128 FP32 accumulators)
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(128));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer
+        int issued = 0;
+        for (int it = 0; it < total; ++it) {
+            const int s = it % STAGES;
+            if (it >= STAGES) {
+                if (!mbar_wait(&empty[s], ((it / STAGES) - 1) & 1)) {
+                    atomicExch(p.err, 1);
+                    *(volatile int *)abort_flag = 1;
+                    break;
+                }
+            }
+            if (*(volatile int *)abort_flag) break;
+            const int seg = it / kblocks, kb = it % kblocks;
+            uint8_t *sa = smem + s * STAGE_BYTES;
+            uint8_t *sb = sa + TILE_A_BYTES;
+            mbar_expect_tx(&full[s], STAGE_BYTES);
+            tma_load_2d(sa, &maps.a[seg], &full[s], kb * BK, m0);
+            tma_load_2d(sb, &maps.b[seg], &full[s], kb * BK, n0);
+            ++issued;
+        }
+        // drain: wait (bounded) until every copy that was started has landed
+        for (int it = max(0, issued - STAGES); it < issued; ++it) mbar_wait(&full[it % STAGES], (it / STAGES) & 1);
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer
+        int consumed = 0;
+        for (int it = 0; it < total; ++it) {
+            const int s = it % STAGES;
+            if (!mbar_wait(&full[s], (it / STAGES) & 1)) {
+                atomicExch(p.err, 2);
+                *(volatile int *)abort_flag = 1;
+                break;
+            }
+            if (*(volatile int *)abort_flag) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
+            const uint32_t sb = sa + TILE_A_BYTES;
+#pragma unroll
+            for (int k = 0; k < BK / 16; ++k) {
+                // advance 16 BF16 = 32 bytes along K inside the 128-byte swizzle atom
+                umma_bf16(tmem, smem_desc_k128(sa + k * 32), smem_desc_k128(sb + k * 32), (it > 0 || k > 0) ? 1u : 0u);
+            }
+            umma_commit(&empty[s]);  // slot s may be refilled once these MMAs have read it
+            ++consumed;
+        }
+        umma_commit(done);  // all issued MMAs complete -> epilogue
+        (void)consumed;
+    }
+    // ---------------- epilogue (all 4 warps)
+    __syncwarp();
+    const bool ok = mbar_wait(done, 0);
+    if (!ok && threadIdx.x == 0) atomicExch(p.err, 3);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const bool live = ok && !*(volatile int *)abort_flag;
+    const int row = m0 + warp * 32 + lane;  // TMEM lane = tile row
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+        if (!live) continue;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int col = n0 + c0 + j;
+            float x = p.alpha * v[j];
+            if (row < p.M && col < p.N) {
+                if (p.G) x *= p.G[(long long)row * p.ldg + col];
+                if (p.C) p.C[(long long)row * p.ldc + col] = x;
+                const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+                const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+                if (p.Ohi) {
+                    p.Ohi[(long long)row * p.ldo + col] = hi;
+                    p.Olo[(long long)row * p.ldo + col] = lo;
+                }
+                if (p.Thi) {
+                    p.Thi[(long long)col * p.ldt + row] = hi;  // coalesced across the warp (consecutive rows)
+                    p.Tlo[(long long)col * p.ldt + row] = lo;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+    }
+}
+
+// FP32 -> BF16 hi/lo split, with zero padding of the columns [cols, ld)
+__global__ void split_kernel(int rows, int cols, const float *X, long long ldx, int transpose, __nv_bfloat16 *hi,
+                             __nv_bfloat16 *lo, long long ld) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long outr = transpose ? cols : rows;
+    if (idx >= outr * ld) return;
+    const long long r = idx / ld, c = idx % ld;
+    float x = 0.0f;
+    const long long inr = transpose ? c : r, inc = transpose ? r : c;
+    if (c < (transpose ? rows : cols)) x = X[inr * ldx + inc];
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    hi[idx] = h;
+    lo[idx] = __float2bfloat16_rn(x - __bfloat162float(h));
+}
+
+__global__ void split64_kernel(int rows, int cols, const double *X, long long ldx, int transpose, __nv_bfloat16 *hi,
+                               __nv_bfloat16 *lo, long long ld, double scale) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long outr = transpose ? cols : rows;
+    if (idx >= outr * ld) return;
+    const long long r = idx / ld, c = idx % ld;
+    double x = 0.0;
+    const long long inr = transpose ? c : r, inc = transpose ? r : c;
+    if (c < (transpose ? rows : cols)) x = scale * X[inr * ldx + inc];
+    const float xf = (float)x;
+    const __nv_bfloat16 h = __float2bfloat16_rn(xf);
+    hi[idx] = h;
+    lo[idx] = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
+}
+
+// ---------------------------------------------------------------------------- host side
+thread_local char g_err[256] = "";
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::mutex g_mutex;
+int *g_errword[64] = {nullptr};
+
+int get_encode() {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (g_encode) return 0;
+    cudaDriverEntryPointQueryResult q;
+    void *fn = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+        snprintf(g_err, sizeof(g_err), "cuTensorMapEncodeTiled unavailable");
+        return -1;
+    }
+    g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    return 0;
+}
+
+int make_map(CUtensorMap *map, const void *base, int rows, int cols, long long ld) {
+    // 2D BF16 tensor: innermost dimension = columns (K), box 64 x 128, 128-byte swizzle, zero fill
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
+    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        snprintf(g_err, sizeof(g_err), "cuTensorMapEncodeTiled failed (%d): rows %d cols %d ld %lld", (int)r, rows,
+                 cols, ld);
+        return -1;
+    }
+    return 0;
+}
+
+}  // namespace tcg
+
+extern "C" {
+
+const char *dftb_tc_last_error(void) { return tcg::g_err; }
+
+int dftb_bf16x3_gemm(int M, int N, int K, int nseg, const void *const *A, int lda, const void *const *B, int ldb,
+                     float alpha, const float *G, int ldg, float *C, int ldc, void *Ohi, void *Olo, int ldo, void *Thi,
+                     void *Tlo, int ldt, int *err, void *stream) {
+    using namespace tcg;
+    if (M <= 0 || N <= 0 || K <= 0 || nseg < 1 || nseg > 3) return DFTB_ERR_BAD_SIZE;
+    if (lda % 8 || ldb % 8 || lda < K || ldb < K) {
+        snprintf(g_err, sizeof(g_err), "bf16x3_gemm: lda/ldb must be multiples of 8 and >= K");
+        return DFTB_ERR_BAD_SIZE;
+    }
+    if (!A || !B || !err) return DFTB_ERR_NULL;
+    if ((Ohi && (!Olo || ldo < N)) || (Thi && (!Tlo || ldt < M)) || (C && ldc < N) || (G && ldg < N))
+        return DFTB_ERR_BAD_SIZE;
+    if (get_encode()) return DFTB_ERR_CUDA;
+    Maps maps;
+    memset(&maps, 0, sizeof(maps));
+    for (int s = 0; s < nseg; ++s) {
+        if (!A[s] || !B[s]) return DFTB_ERR_NULL;
+        if ((reinterpret_cast<uintptr_t>(A[s]) & 15) || (reinterpret_cast<uintptr_t>(B[s]) & 15)) {
+            snprintf(g_err, sizeof(g_err), "bf16x3_gemm: operands must be 16-byte aligned");
+            return DFTB_ERR_BAD_SIZE;
+        }
+        if (make_map(&maps.a[s], A[s], M, K, lda) || make_map(&maps.b[s], B[s], N, K, ldb)) return DFTB_ERR_CUDA;
+    }
+    Params p;
+    p.M = M;
+    p.N = N;
+    p.K = K;
+    p.nseg = nseg;
+    p.alpha = alpha;
+    p.G = G;
+    p.ldg = ldg;
+    p.C = C;
+    p.ldc = ldc;
+    p.Ohi = reinterpret_cast<__nv_bfloat16 *>(Ohi);
+    p.Olo = reinterpret_cast<__nv_bfloat16 *>(Olo);
+    p.ldo = ldo;
+    p.Thi = reinterpret_cast<__nv_bfloat16 *>(Thi);
+    p.Tlo = reinterpret_cast<__nv_bfloat16 *>(Tlo);
+    p.ldt = ldt;
+    p.err = err;
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        if (cudaFuncSetAttribute(gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) !=
+            cudaSuccess) {
+            snprintf(g_err, sizeof(g_err), "bf16x3_gemm: cannot reserve %d bytes of shared memory", SMEM_BYTES);
+            return DFTB_ERR_CUDA;
+        }
+        attr_set[dev] = true;
+    }
+    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+    if (grid.y > 65535u) return DFTB_ERR_BAD_SIZE;
+    gemm_kernel<<<grid, 128, SMEM_BYTES, reinterpret_cast<cudaStream_t>(stream)>>>(maps, p);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        snprintf(g_err, sizeof(g_err), "gemm_kernel: %s", cudaGetErrorString(e));
+        return DFTB_ERR_CUDA;
+    }
+    return DFTB_OK;
+}
+
+int dftb_split_bf16(int rows, int cols, const float *X, int ldx, int transpose, void *hi, void *lo, int ld,
+                    void *stream) {
+    using namespace tcg;
+    if (rows <= 0 || cols <= 0 || ld < (transpose ? rows : cols)) return DFTB_ERR_BAD_SIZE;
+    if (!X || !hi || !lo) return DFTB_ERR_NULL;
+    const long long n = (long long)(transpose ? cols : rows) * ld;
+    split_kernel<<<(unsigned)((n + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        rows, cols, X, ldx, transpose, reinterpret_cast<__nv_bfloat16 *>(hi), reinterpret_cast<__nv_bfloat16 *>(lo),
+        ld);
+    return cudaGetLastError() == cudaSuccess ? DFTB_OK : DFTB_ERR_CUDA;
+}
+
+int dftb_split_bf16_f64(int rows, int cols, const double *X, int ldx, int transpose, double scale, void *hi, void *lo,
+                        int ld, void *stream) {
+    using namespace tcg;
+    if (rows <= 0 || cols <= 0 || ld < (transpose ? rows : cols)) return DFTB_ERR_BAD_SIZE;
+    if (!X || !hi || !lo) return DFTB_ERR_NULL;
+    const long long n = (long long)(transpose ? cols : rows) * ld;
+    split64_kernel<<<(unsigned)((n + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        rows, cols, X, ldx, transpose, reinterpret_cast<__nv_bfloat16 *>(hi), reinterpret_cast<__nv_bfloat16 *>(lo),
+        ld, scale);
+    return cudaGetLastError() == cudaSuccess ? DFTB_OK : DFTB_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -7,8 +7,9 @@ same subspace matrices, convergence tests, residual selection, preconditioner
 and error checks.  Two deliberate, result-preserving differences:
 
 * products of the matrix with expansion vectors are kept: each new vector is
-  multiplied once and residuals use (A.b) Tb instead of re-multiplying
-  A (b Tb) (the products are linear);
+  multiplied once, residuals use (A.b) Tb instead of re-multiplying
+  A (b Tb) (the products are linear), and the projected matrices b^T A b
+  are extended by the new rows and columns instead of being recomputed;
 * new vectors are orthonormalised against the current (orthonormal) basis by
   block Gram-Schmidt with re-orthogonalisation instead of re-factorising the
   whole basis by QR; both produce the same subspace.
@@ -43,6 +44,60 @@ def orthonormalize_new(bs, Q):
         Q = Q - bs @ (bs.T @ Q)
         Q, _ = torch.linalg.qr(Q, mode="reduced")
     return Q
+
+
+class Basis:
+    """Expansion vectors and their products in preallocated column blocks.
+
+    Columns are appended in place (capacity grows geometrically) and the
+    projected matrices b^T (A b) are extended by the new rows and columns only.
+    """
+
+    def __init__(self, nov, nprod, device, capacity=64):
+        self.nov, self.nprod, self.device = nov, nprod, device
+        self.l = 0
+        self.cap = 0
+        self.V = None
+        self.P = [None] * nprod
+        self.M = [torch.zeros((0, 0), dtype=torch.float64, device=device) for _ in range(nprod)]
+        self._grow(capacity)
+
+    def _grow(self, need):
+        cap = max(need, 2 * self.cap, 16)
+        def grow(old):
+            new = torch.empty((self.nov, cap), dtype=torch.float64, device=self.device)
+            if old is not None and self.l > 0:
+                new[:, :self.l] = old[:, :self.l]
+            return new
+        self.V = grow(self.V)
+        self.P = [grow(p) for p in self.P]
+        self.cap = cap
+
+    def append(self, Q, prods):
+        dk = Q.shape[1]
+        if self.l + dk > self.cap:
+            self._grow(self.l + dk)
+        l0, l1 = self.l, self.l + dk
+        self.V[:, l0:l1] = Q
+        for i, pr in enumerate(prods):
+            self.P[i][:, l0:l1] = pr
+        # extend the projected matrices: [[M, V0^T P_new], [Q^T P0, Q^T P_new]]
+        V = self.V[:, :l1]
+        for i in range(self.nprod):
+            Pn = self.P[i][:, l0:l1]
+            M = torch.empty((l1, l1), dtype=torch.float64, device=self.device)
+            M[:l0, :l0] = self.M[i]
+            M[:, l0:l1] = V.T @ Pn
+            M[l0:l1, :l0] = Q.T @ self.P[i][:, :l0]
+            self.M[i] = M
+        self.l = l1
+
+    @property
+    def bs(self):
+        return self.V[:, :self.l]
+
+    def prod(self, i):
+        return self.P[i][:, :self.l]
 
 
 def _residuals(AV, X, lam):
@@ -87,14 +142,16 @@ def hermitian_davidson(rv, omega, nstates, ifact=1, conv=1.0e-14, maxiter=10, Xp
     k = nstates
     omega_sq = torch.sqrt(om)
     if XpYguess is None:
-        bs = initial_expansion_vectors(om, lmax)
+        b0 = initial_expansion_vectors(om, lmax)
     else:
-        bs = (XpYguess[:lmax].reshape(lmax, -1).T / omega_sq[:, None]).contiguous()
-        bs = bs / torch.linalg.norm(bs, dim=0)
-    AB = rv(bs)
+        b0 = (XpYguess[:lmax].reshape(lmax, -1).T / omega_sq[:, None]).contiguous()
+        b0 = b0 / torch.linalg.norm(b0, dim=0)
+    B = Basis(om.numel(), 1, om.device, capacity=lmax + 4 * k)
+    B.append(b0, [rv(b0)])
     l = lmax
     for it in range(maxiter):
-        Hb = bs.T @ AB
+        bs, AB = B.bs, B.prod(0)
+        Hb = B.M[0]
         w2, Tb = torch.linalg.eigh(Hb)
         if L2_thresh > 0.0 and Oia is not None:
             T_all = bs @ Tb
@@ -116,9 +173,8 @@ def hermitian_davidson(rv, omega, nstates, ifact=1, conv=1.0e-14, maxiter=10, Xp
         src = [n for n in range(dkmax) if norms[n] > eps]
         Q = _precondition(W, src, src, w, om)
         Q = orthonormalize_new(bs, Q)
-        bs = torch.cat([bs, Q], dim=1)
-        AB = torch.cat([AB, rv(Q)], dim=1)
-        l = bs.shape[1]
+        B.append(Q, [rv(Q)])
+        l = B.l
     else:
         raise ExcitedStatesNotConverged(
             "Davidson-like diagonalization for Hermitian eigenvalue problem did not converge after %s iterations "
@@ -163,12 +219,14 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
         lmax = lmaxp + lmaxm
         cols = torch.cat([XmYguess.reshape(nstates, -1), XpYguess.reshape(nstates, -1)[:lmaxm]], dim=0).T
         bs = (cols / torch.linalg.norm(cols, dim=0)).contiguous()
-    AP, AM = products(bs)
+    B = Basis(om.numel(), 2, dev, capacity=lmax + 8 * k)
+    B.append(bs, list(products(bs)))
     l = lmax
     for it in range(maxiter):
+        bs, AP, AM = B.bs, B.prod(0), B.prod(1)
         if XpYguess is None or it > 0:
-            Mp = bs.T @ AP
-            Mm = bs.T @ AM
+            Mp = B.M[0]
+            Mm = B.M[1]
             Mmsq = _sqrtm_spd(Mm)
             Mh = Mmsq @ Mp @ Mmsq
             if torch.sum(torch.abs(Mh - Mh.T)).item() > 1.0e-10:
@@ -220,11 +278,8 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
         assert len(src) == dk
         Q = _precondition(torch.cat([WL, WR], dim=1), src, state, w, om)
         Q = orthonormalize_new(bs, Q)
-        ap, am = products(Q)
-        bs = torch.cat([bs, Q], dim=1)
-        AP = torch.cat([AP, ap], dim=1)
-        AM = torch.cat([AM, am], dim=1)
-        l = bs.shape[1]
+        B.append(Q, list(products(Q)))
+        l = B.l
     else:
         raise ExcitedStatesNotConverged(
             "Davidson-like diagonalization for non-Hermitian eigenvalue problem did not converge after %s "

@@ -186,6 +186,28 @@ int dftb_davidson_precondition(int nov, int nnew, const double *W, int ldw, cons
 int dftb_davidson_residual(int nov, int ncol, const double *AV, int ldav, const double *X, int ldx,
                            const double *lam, double *W, int ldw, double *norms, void *stream);
 
+/* Split-precision BF16 product on the tcgen05 tensor cores (no counterpart in
+ * DFTBaby; it carries the mixed-precision form of the long-range exchange
+ * contractions of Solver._ApBv/_AmBv, DFTB/Solver.py:583-635):
+ *   C(m, n) = alpha * sum_{s < nseg} sum_k A_s(m, k) B_s(n, k),  FP32 accumulation,
+ * A_s: (M, K) and B_s: (N, K) K-major BF16, leading dimensions multiples of 8
+ * elements, bases 16-byte aligned (A and B are host arrays of nseg device
+ * pointers, nseg <= 3).  With X = X_hi + X_lo the three segments
+ * (A_hi,B_hi), (A_hi,B_lo), (A_lo,B_hi) give ~2^-16 relative accuracy.
+ * Epilogue: optional elementwise factor G (FP32, ldg), FP32 output C (ldc),
+ * BF16 hi/lo outputs row-major (Ohi/Olo, ldo) and/or transposed (Thi/Tlo, ldt).
+ * err: device int set non-zero if an internal wait timed out. */
+int dftb_bf16x3_gemm(int M, int N, int K, int nseg, const void *const *A, int lda, const void *const *B, int ldb,
+                     float alpha, const float *G, int ldg, float *C, int ldc, void *Ohi, void *Olo, int ldo,
+                     void *Thi, void *Tlo, int ldt, int *err, void *stream);
+/* X (rows x cols, FP32 or FP64, optionally transposed and scaled) -> BF16
+ * hi/lo pair with leading dimension ld; columns beyond the matrix are zeroed. */
+int dftb_split_bf16(int rows, int cols, const float *X, int ldx, int transpose, void *hi, void *lo, int ld,
+                    void *stream);
+int dftb_split_bf16_f64(int rows, int cols, const double *X, int ldx, int transpose, double scale, void *hi,
+                        void *lo, int ld, void *stream);
+const char *dftb_tc_last_error(void);
+
 /* General FP64 product C = alpha * op(A) . op(B) + beta * C on row-major
  * matrices (op = transpose when trans != 0), the contraction engine behind the
  * entry points above, exported for the host-side solver. */

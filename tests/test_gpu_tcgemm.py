@@ -1,0 +1,54 @@
+"""The tcgen05 split-precision BF16 GEMM against FP64 products."""
+import numpy as np
+import pytest
+import torch
+
+from dftbaby_b200 import native, tcgemm
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (300, 200, 150), (1000, 513, 777), (257, 1030, 2049)])
+def test_gemm_bf16_and_split_accuracy(M, N, K):
+    native.load()
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device="cpu").manual_seed(M + N + K)
+    A = torch.randn(M, K, generator=g, dtype=torch.float64).to(dev)
+    B = torch.randn(N, K, generator=g, dtype=torch.float64).to(dev)
+    ref = A @ B.T
+    scale = ref.abs().max().item()
+    pa, pb = tcgemm.split(A), tcgemm.split(B)
+    C1 = torch.empty((M, N), dtype=torch.float32, device=dev)
+    tcgemm.gemm(pa, pb, K=K, refine=False, out=C1)
+    C3 = torch.empty((M, N), dtype=torch.float32, device=dev)
+    tcgemm.gemm(pa, pb, K=K, refine=True, out=C3)
+    torch.cuda.synchronize()
+    tcgemm.check_errors(dev)
+    e1 = (C1.double() - ref).abs().max().item() / scale
+    e3 = (C3.double() - ref).abs().max().item() / scale
+    assert e1 < 2e-2, e1
+    assert e3 < 5e-5, e3
+
+
+def test_gemm_epilogue_hadamard_and_pair_outputs():
+    native.load()
+    dev = torch.device("cuda", 0)
+    M, N, K = 390, 270, 130
+    g = torch.Generator(device="cpu").manual_seed(1)
+    A = torch.randn(M, K, generator=g, dtype=torch.float64).to(dev)
+    B = torch.randn(N, K, generator=g, dtype=torch.float64).to(dev)
+    G = torch.rand(M, N, generator=g, dtype=torch.float32).to(dev)
+    ref = (A @ B.T) * G.double() * 0.5
+    pa, pb = tcgemm.split(A), tcgemm.split(B)
+    C = torch.empty((M, N), dtype=torch.float32, device=dev)
+    O = tcgemm.Pair(M, N, dev)
+    T = tcgemm.Pair(N, M, dev)
+    tcgemm.gemm(pa, pb, K=K, alpha=0.5, G=G, out=C, out_pair=O, out_pair_t=T)
+    torch.cuda.synchronize()
+    tcgemm.check_errors(dev)
+    scale = ref.abs().max().item()
+    assert (C.double() - ref).abs().max().item() / scale < 5e-5
+    rec = O.hi[:, :N].double() + O.lo[:, :N].double()
+    assert (rec - C.double()).abs().max().item() / scale < 1e-5
+    rect = T.hi[:, :M].double() + T.lo[:, :M].double()
+    assert (rect - C.double().T).abs().max().item() / scale < 1e-5
