@@ -57,7 +57,7 @@ def build_geometry(w, seed):
     return geometry.polyene(w["n"], sigma=w["sigma"], seed=seed)
 
 
-def workload_config(name, w, n_gpus):
+def workload_config(name, w, n_gpus, precision="fp64"):
     from dftbaby_b200 import geometry
     al = build_geometry(w, 0)
     nat = len(al)
@@ -68,7 +68,10 @@ def workload_config(name, w, n_gpus):
            "%s %s TD-DFTB" % (name, geometry.formula(al)),
            "atoms": nat, "orbitals": norb, "long_range_correction": w["lc"], "nstates": o["nstates"],
            "active_window": [o.get("nr_active_occ"), o.get("nr_active_virt")],
-           "davidson_residual": o["diag_conv"], "scf_conv": 1e-10, "precision": "fp64",
+           "davidson_residual": o["diag_conv"], "scf_conv": 1e-10,
+           "precision": ("mixed: exchange on tensor cores (bf16x3, f32 accumulate); Coulomb, SCC, subspace "
+                         "eigenproblems f64; accuracy vs the plain f64 path reported per run")
+           if precision == "mixed" and w["lc"] else "fp64",
            "geometry": "seeded jitter per step and rank",
            "l2": "working set (q_ov %s GB) larger than L2; no flush needed" % (
                round(8.0 * nat * (no or norb // 2) ** 2 / 1e9, 2) if no else "n/a"),
@@ -126,6 +129,18 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def cluster_df(Om_ref, f_ref, f_test, tol):
+    """max |sum f_test - sum f_ref| over clusters of reference states closer than tol."""
+    worst, i, n = 0.0, 0, len(Om_ref)
+    while i < n:
+        j = i + 1
+        while j < n and Om_ref[j] - Om_ref[j - 1] < tol:
+            j += 1
+        worst = max(worst, abs(float(sum(f_test[i:j]) - sum(f_ref[i:j]))))
+        i = j
+    return worst
 
 
 def measured_peaks():
@@ -190,6 +205,9 @@ def main():
     ap.add_argument("--workload", default="armchair7", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="mixed: tensor-core exchange + FP64 refinement (default); fp64: the plain path")
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison solve")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -208,7 +226,10 @@ def main():
     from dftbaby_b200 import LR_TDDFTB, native
     native.load()
     w = WORKLOADS[args.workload]
-    opts = w["opts"]
+    opts = dict(w["opts"])
+    if args.precision == "mixed" and w["lc"]:
+        opts.update(precision="mixed", refine_fp64=False)
+    mixed = opts.get("precision") == "mixed"
 
     def barrier():
         if world > 1:
@@ -227,13 +248,15 @@ def main():
     barrier()
     # ---- device-timed region (inputs resident: geometry and tables uploaded before each solve's timer)
     native.counters.reset()
-    native.counters.time_entries(["dftb_apbv", "dftb_trans_charges", "dftb_h0_and_s", "dftb_dipole_matrix"])
+    native.counters.time_entries(["dftb_apbv", "dftb_trans_charges", "dftb_h0_and_s", "dftb_dipole_matrix",
+                                  "dftb_bf16x3_gemm"])
     sampler = ClockSampler(local)
     sampler.start()
     stream = torch.cuda.current_stream()
     dev_ms = 0.0
     phases = {}
     stats = []
+    last = None
     for s in range(args.steps):
         al = build_geometry(w, 20_000 + s * world + rank)
         td = LR_TDDFTB(al, long_range_correction=w["lc"])
@@ -241,20 +264,43 @@ def main():
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        td.getEnergies(**opts)
+        Om_t, f_t = td.getEnergies(**opts)
+        last = (al, Om_t, f_t)
         e1.record(stream)
         e1.synchronize()
         dev_ms += e0.elapsed_time(e1)
         for k, v in td.phase_ms().items():
             phases[k] = phases.get(k, 0.0) + v
         stats.append({"scc_iterations": td.dftb2.scc_iterations, "davidson_iterations": td.stats.get("iterations"),
-                      "subspace": td.stats.get("subspace")})
+                      "subspace": td.stats.get("subspace"), "fp64_products": td.stats.get("products"),
+                      "mixed": td.stats.get("mixed"), "mixed_products": td.stats.get("mixed_products")})
     barrier()
     clocks = sampler.stop()
     launches = native.counters.launches
     # kernel timings for the roofline
     entry_ms = {n: native.counters.elapsed_ms(n) for n in native.counters.timed}
+    entry_flops = dict(native.counters.flops)
     native.counters.timed = None
+    native.counters.flops = {}
+    # ---- the plain FP64 path on the same geometry (comparison and accuracy)
+    plain = None
+    if mixed and not args.no_compare:
+        al, Om_t, f_t = last
+        td = LR_TDDFTB(al, long_range_correction=w["lc"])
+        td.setGeometry(al)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        Om_p, f_p = td.getEnergies(**w["opts"])
+        e1.record(stream)
+        e1.synchronize()
+        pms = e0.elapsed_time(e1)
+        plain = {"value": opts["nstates"] / (pms / 1e3), "ms_per_step": pms,
+                 "max_dOmega_meV": float(abs(Om_t - Om_p).max() * 27211.396132),
+                 "max_df_per_state": float(abs(f_t - f_p).max()),
+                 "max_df": cluster_df(Om_p, f_p, f_t, 1.0e-3 / 27.211396132),
+                 "f_comparison": "sums over clusters of states closer than 1 meV (near-degenerate pairs mix "
+                                 "freely inside such clusters)"}
     t_dev = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
@@ -287,7 +333,20 @@ def main():
     totals = {n: sum(v) for n, v in entry_ms.items() if v}
     dom = max(totals, key=totals.get) if totals else None
     roof = None
-    if dom == "dftb_apbv":
+    if dom == "dftb_bf16x3_gemm":
+        import json as _j
+        pk = _j.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+        tpeak = pk.get("bf16_tflops_sustained", 1400.0)
+        fl = sum(entry_flops.get(dom, []))
+        ms = totals[dom]
+        nl = len(entry_ms[dom])
+        roof = {"kernel": "tcg::gemm_kernel (tcgen05 BF16, split-precision segments)", "bound": "tensor",
+                "achieved": fl / (ms / 1e3) / 1e12, "peak": tpeak, "unit": "TFLOP/s",
+                "frac": fl / (ms / 1e3) / 1e12 / tpeak, "traffic": None, "launches": nl,
+                "algorithmic_flops_per_launch": fl / nl, "ms_per_launch": ms / nl,
+                "peak_source": "measured (bf16 sustained)" if pk else "fallback"}
+    elif dom == "dftb_apbv":
         # Coulomb product u = omega v + 4 q^T gamma q v: q_ov (nat x nov) is streamed twice
         ms = statistics.mean(entry_ms[dom])
         nvec = statistics.mean([c for c in [2 * opts["nstates"]]])
@@ -303,13 +362,15 @@ def main():
                 "algorithmic_bytes_per_launch": algo, "ms_per_launch": ms, "peak_source": peak_kind}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometries)",
-            "config": workload_config(args.workload, w, world),
+            "vs_baseline": None, "dtype": "f64 + bf16x3 exchange" if mixed else "f64",
+            "data": "synthetic (seeded geometries)",
+            "config": workload_config(args.workload, w, world, "mixed" if mixed else "fp64"),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches, "clocks": clocks, "roofline": roof,
             "phases_ms_per_step": {k: v / args.steps for k, v in phases.items()},
             "native_ms_per_step": {k: v / args.steps for k, v in totals.items()},
-            "solver": stats[-1] if stats else None}
+            "solver": stats[-1] if stats else None, "plain_fp64": plain,
+            "speedup_vs_plain_fp64": (plain["ms_per_step"] / ms_per_step) if plain else None}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_entry(args)
     if world > 1:

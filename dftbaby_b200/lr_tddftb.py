@@ -92,6 +92,79 @@ class ExchangeAO:
         return coul - K1 - K2, omv + K2 - K1
 
 
+class ExchangeMixed(ExchangeAO):
+    """(A+B).V and (A-B).V with the exchange contractions on the tensor cores.
+
+    Same AO-factorised algebra as ExchangeAO, evaluated per column with six
+    split-precision BF16 GEMMs (three BF16 passes each, FP32 accumulation,
+    ~2^-16 relative accuracy; tcgemm.py):
+        W^T  = [C_v; S~_v] v^T                        (2 Norb x nocc)
+        N_xy = Gamma o (X_o W_y), stored and transposed (fused epilogue)
+        P1^T = Ybar^T N,  P2^T = Ybar^T N^T            (K = 2 Norb)
+        K1^T = P1^T Xbar_o / 4,  K2^T = P2^T Xbar_o / 4
+    with Ybar = [S~_v; C_v] and Xbar = [S~_o; C_o].  The Coulomb term stays
+    FP64 (native q_ov products).
+    """
+
+    def __init__(self, gamma, G_lr, q_ov, omega_flat, Co, Cv, S, nat, nocc, nvirt, workspace, lc=1):
+        from . import tcgemm as T
+        super().__init__(gamma, G_lr, q_ov, omega_flat, Co, Cv, S, nat, nocc, nvirt, workspace, lc=lc,
+                         max_bytes=1)
+        self.T = T
+        dev = Co.device
+        norb = Co.shape[0]
+        self.norb = norb
+        So, Sv = S @ Co, S @ Cv
+        self.YV = T.split(torch.cat([Cv, Sv], dim=0))                      # (2 Norb, nv), K = nv
+        self.XO = T.split(torch.cat([Co, So], dim=0))                      # (2 Norb, no), K = no
+        self.YbarT = T.split(torch.cat([Sv, Cv], dim=0), transpose=True)   # (nv, 2 Norb), K = 2 Norb
+        self.XbarT = T.split(torch.cat([So, Co], dim=0), transpose=True)   # (no, 2 Norb), K = 2 Norb
+        self.G2 = torch.cat([G_lr, G_lr], dim=0).to(torch.float32).contiguous()  # (2 Norb, Norb)
+        self.W = T.Pair(2 * norb, nocc, dev)
+        self.NN = T.Pair(2 * norb, 2 * norb, dev)
+        self.NT = T.Pair(2 * norb, 2 * norb, dev)
+        self.P1 = T.Pair(nvirt, 2 * norb, dev)
+        self.P2 = T.Pair(nvirt, 2 * norb, dev)
+        self.K1t = torch.empty((nvirt, nocc), dtype=torch.float32, device=dev)
+        self.K2t = torch.empty((nvirt, nocc), dtype=torch.float32, device=dev)
+        self.Vp = T.Pair(nocc, nvirt, dev)
+        # views for the per-y blocks (y = C, S~)
+        self.Wy, self.outN, self.outT = [], [], []
+        for y in range(2):
+            w = T.Pair.__new__(T.Pair)
+            w.rows, w.cols, w.ld = norb, nocc, self.W.ld
+            w.hi, w.lo = self.W.hi[y * norb:(y + 1) * norb], self.W.lo[y * norb:(y + 1) * norb]
+            self.Wy.append(w)
+            o = T.Pair.__new__(T.Pair)
+            o.rows, o.cols, o.ld = 2 * norb, norb, self.NN.ld
+            o.hi, o.lo = self.NN.hi[:, y * norb:], self.NN.lo[:, y * norb:]
+            self.outN.append(o)
+            t = T.Pair.__new__(T.Pair)
+            t.rows, t.cols, t.ld = norb, 2 * norb, self.NT.ld
+            t.hi, t.lo = self.NT.hi[y * norb:], self.NT.lo[y * norb:]
+            self.outT.append(t)
+
+    def exchange(self, V):
+        T = self.T
+        nov, m = V.shape
+        no, nv, norb = self.nocc, self.nvirt, self.norb
+        K1 = torch.empty_like(V)
+        K2 = torch.empty_like(V)
+        Vt = V.T.contiguous()  # one contiguous (nocc, nvirt) block per column
+        for c in range(m):
+            T.split(Vt[c].reshape(no, nv), out=self.Vp)
+            T.gemm(self.YV, self.Vp, K=nv, out_pair=self.W)
+            for y in range(2):
+                T.gemm(self.XO, self.Wy[y], K=no, G=self.G2, out_pair=self.outN[y], out_pair_t=self.outT[y])
+            T.gemm(self.YbarT, self.NN, K=2 * norb, out_pair=self.P1)
+            T.gemm(self.YbarT, self.NT, K=2 * norb, out_pair=self.P2)
+            T.gemm(self.P1, self.XbarT, K=2 * norb, alpha=0.25, out=self.K1t)
+            T.gemm(self.P2, self.XbarT, K=2 * norb, alpha=0.25, out=self.K2t)
+            K1[:, c] = self.K1t.T.reshape(-1).double()
+            K2[:, c] = self.K2t.T.reshape(-1).double()
+        return K1, K2
+
+
 class LR_TDDFTB:
     XpY = None
     XmY = None
@@ -176,8 +249,14 @@ class LR_TDDFTB:
     def getEnergies(self, nr_active_occ=None, nr_active_virt=None, select_lm=None, oszis="Dipoles",
                     response_method="Casida", multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5,
                     diag_maxiter=50, diag_check=0, diag_L2threshold=0.0, diag_selected_irreps=None,
-                    ct_correction=0, stability=0, **scf_opts):
-        """LR_TDDFTB.getEnergies (LR_TDDFTB.py:37-114); returns (Omega, f) in Hartree."""
+                    ct_correction=0, stability=0, precision="fp64", refine_fp64=True, **scf_opts):
+        """LR_TDDFTB.getEnergies (LR_TDDFTB.py:37-114); returns (Omega, f) in Hartree.
+
+        precision="mixed" (not in DFTBaby) evaluates the long-range exchange of
+        the Davidson products with split-precision BF16 tensor-core GEMMs; with
+        refine_fp64 the mixed result then seeds the FP64 solver, whose residual
+        test (diag_conv) decides convergence as in the plain path.
+        """
         if select_lm is not None:
             raise ValueError("select_lm is not implemented")
         if response_method != "Casida":
@@ -197,7 +276,7 @@ class LR_TDDFTB:
             assert nstates > 0, "nstates==0, no excited states can be calculated!"
         self._solve_lr_equations(multiplicity=multiplicity, nstates=nstates, diag_ifact=diag_ifact,
                                  diag_conv=diag_conv, diag_maxiter=diag_maxiter, diag_check=diag_check,
-                                 diag_L2threshold=diag_L2threshold)
+                                 diag_L2threshold=diag_L2threshold, precision=precision, refine_fp64=refine_fp64)
         ev[2].record()
         if oszis == "Dipoles":
             self._TransitionDipoles()
@@ -217,7 +296,7 @@ class LR_TDDFTB:
                 "properties": ev[2].elapsed_time(ev[3])}
 
     def _solve_lr_equations(self, multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5, diag_maxiter=50,
-                            diag_check=0, diag_L2threshold=0.0):
+                            diag_check=0, diag_L2threshold=0.0, precision="fp64", refine_fp64=True):
         """LR_TDDFTB._solve_lr_equations (LR_TDDFTB.py:403-527)."""
         d = self.dftb2
         dev = d.device
@@ -255,9 +334,25 @@ class LR_TDDFTB:
             Co, Cv = self._active_coefficients()
             prod = ExchangeAO(d.gamma, d.G_lr, self.qtrans_ov, self.omega.reshape(-1), Co, Cv, d.S,
                               len(d.atomlist), self.nocc, self.nvirt, d.workspace, lc=1)
-            Om, C, XmY, XpY = nonhermitian_davidson(prod, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
-                                                    maxiter=diag_maxiter, XmYguess=XmY0, XpYguess=XpY0,
-                                                    w_guess=Om0, stats=self.stats)
+            if precision == "mixed":
+                from . import tcgemm
+                mixed = ExchangeMixed(d.gamma, d.G_lr, self.qtrans_ov, self.omega.reshape(-1), Co, Cv, d.S,
+                                      len(d.atomlist), self.nocc, self.nvirt, d.workspace, lc=1)
+                mstats = {}
+                Om, C, XmY, XpY = nonhermitian_davidson(mixed, self.omega, nstates, ifact=diag_ifact,
+                                                        conv=diag_conv, maxiter=diag_maxiter, XmYguess=XmY0,
+                                                        XpYguess=XpY0, w_guess=Om0, stats=mstats, symmetrize=True)
+                tcgemm.check_errors(dev)
+                self.stats["mixed"] = {k: v for k, v in mstats.items() if k != "residual_norms"}
+                self.stats["mixed_products"] = mixed.products_applied
+                XmY0, XpY0, Om0, C0 = XmY, XpY, Om, C
+                del mixed
+            if precision != "mixed" or refine_fp64:
+                Om, C, XmY, XpY = nonhermitian_davidson(prod, self.omega, nstates, ifact=diag_ifact,
+                                                        conv=diag_conv, maxiter=diag_maxiter, XmYguess=XmY0,
+                                                        XpYguess=XpY0, w_guess=Om0, stats=self.stats,
+                                                        accept_guess=(precision == "mixed"),
+                                                        Cguess=C0 if precision == "mixed" else None)
             self.stats["products"] = prod.products_applied
         self._Omega_dev = Om
         self.Omega = Om.cpu().numpy()

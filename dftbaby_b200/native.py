@@ -122,6 +122,7 @@ class Counters:
         self.launches = 0
         self.calls = {}
         self.timed = None  # name -> list of (start_event, end_event)
+        self.flops = {}  # name -> list of algorithmic FLOPs per timed launch
 
     def time_entries(self, names):
         self.timed = {n: [] for n in names}

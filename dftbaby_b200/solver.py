@@ -199,11 +199,21 @@ def _sqrtm_spd(M):
 
 
 def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxiter=10, XmYguess=None,
-                          XpYguess=None, w_guess=None, stats=None):
+                          XpYguess=None, w_guess=None, stats=None, symmetrize=False, accept_guess=False,
+                          Cguess=None):
     """Lowest nstates of the non-Hermitian TD-DFTB problem (Stratmann-Scuseria-Frisch).
 
     products(V) returns ((A+B).V, (A-B).V) for a (nov, ncol) block.
     Returns Omega (k), C, XmY, XpY as (k, nocc, nvirt) device tensors.
+    With symmetrize=True (products evaluated in reduced precision) the
+    projected matrices are symmetrised, since A+B and A-B are symmetric and
+    only rounding breaks the symmetry; the FP64 path keeps DFTBaby's check.
+    With a guess (XmYguess, XpYguess, w_guess), iteration 0 tests the guess
+    itself as DFTBaby does (Solver.py:707-748); accept_guess=True lets a guess
+    whose residuals already meet conv end the solve there (refinement stage;
+    Cguess then supplies the C vectors, which iteration 0 does not form).
+    The guess block is orthonormalised before use -- DFTBaby orthonormalises
+    the whole basis by QR at the end of iteration 0, which spans the same space.
     """
     nocc, nvirt = omega.shape
     om = omega.reshape(-1).contiguous()
@@ -218,7 +228,8 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
         lmaxm = min(nstates, kmax - nstates)
         lmax = lmaxp + lmaxm
         cols = torch.cat([XmYguess.reshape(nstates, -1), XpYguess.reshape(nstates, -1)[:lmaxm]], dim=0).T
-        bs = (cols / torch.linalg.norm(cols, dim=0)).contiguous()
+        bs, _ = torch.linalg.qr(cols / torch.linalg.norm(cols, dim=0), mode="reduced")
+        bs = bs.contiguous()
     B = Basis(om.numel(), 2, dev, capacity=lmax + 8 * k)
     B.append(bs, list(products(bs)))
     l = lmax
@@ -227,6 +238,9 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
         if XpYguess is None or it > 0:
             Mp = B.M[0]
             Mm = B.M[1]
+            if symmetrize:
+                Mp = 0.5 * (Mp + Mp.T)
+                Mm = 0.5 * (Mm + Mm.T)
             Mmsq = _sqrtm_spd(Mm)
             Mh = Mmsq @ Mp @ Mmsq
             if torch.sum(torch.abs(Mh - Mh.T)).item() > 1.0e-10:
@@ -245,8 +259,10 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
             Lk = XmYguess.reshape(nstates, -1).T.contiguous()
             w = torch.as_tensor(np.asarray(w_guess), dtype=torch.float64, device=dev) if not torch.is_tensor(
                 w_guess) else w_guess.to(dev)
-            ApR, _ = products(Rk)
-            _, AmL = products(Lk)
+            # R and L lie in the span of the orthonormal guess block: their
+            # products follow from the cached ones by linearity
+            ApR = B.prod(0) @ (B.bs.T @ Rk)
+            AmL = B.prod(1) @ (B.bs.T @ Lk)
         WL, nL = _residuals(ApR, Lk, w[:k])
         WR, nR = _residuals(AmL, Rk, w[:k])
         host = torch.stack([nL, nR]).cpu().numpy()
@@ -254,7 +270,7 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
         norms = normsL + normsR
         if stats is not None:
             stats.setdefault("residual_norms", []).append(norms.copy())
-        if (norms < conv).all() and it > 0:
+        if (norms < conv).all() and (it > 0 or accept_guess):
             break
         dkmax = min(kmax - l, 2 * k)
         eps = 0.01 * conv
@@ -288,6 +304,11 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
         stats["iterations"] = it + 1
         stats["subspace"] = l
     Omega = w[:k]
-    C = bs @ Tb[:, :k]
+    if XpYguess is not None and it == 0:
+        if Cguess is None:
+            raise ExcitedStatesError("a guess was accepted without its C vectors")
+        C = Cguess.reshape(k, -1).T
+    else:
+        C = bs @ Tb[:, :k]
     shape = (k, nocc, nvirt)
     return Omega, C.T.reshape(shape), Lk.T.reshape(shape), Rk.T.reshape(shape)

@@ -95,6 +95,10 @@ def gemm(A, B, K=None, refine=True, alpha=1.0, G=None, out=None, out_pair=None, 
     lda, ldb = segments[0][0].stride(0), segments[0][1].stride(0)
     err = _errword(A.hi.device)
     P = native.ptr
+    timed = native.counters.timed is not None and "dftb_bf16x3_gemm" in native.counters.timed
+    if timed:
+        ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        ev[0].record()
     rc = L.dftb_bf16x3_gemm(M, N, K, nseg, Aptrs, lda, Bptrs, ldb, float(alpha), P(G), G.stride(0) if G is not None
                             else 0, P(out), out.stride(0) if out is not None else 0,
                             P(out_pair.hi) if out_pair else None, P(out_pair.lo) if out_pair else None,
@@ -103,6 +107,10 @@ def gemm(A, B, K=None, refine=True, alpha=1.0, G=None, out=None, out_pair=None, 
                             native.stream())
     if rc != 0:
         raise native.NativeError("bf16x3 gemm failed (%d): %s" % (rc, L.dftb_tc_last_error().decode()))
+    if timed:
+        ev[1].record()
+        native.counters.timed["dftb_bf16x3_gemm"].append(ev)
+        native.counters.flops.setdefault("dftb_bf16x3_gemm", []).append(2.0 * M * N * K * nseg)
     native.counters.launches += 1
     native.counters.calls["dftb_bf16x3_gemm"] = native.counters.calls.get("dftb_bf16x3_gemm", 0) + 1
 

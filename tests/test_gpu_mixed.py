@@ -1,0 +1,64 @@
+"""Mixed-precision (tensor-core) exchange against the FP64 path."""
+import numpy as np
+import pytest
+import torch
+
+from dftbaby_b200 import geometry, native
+
+pytestmark = pytest.mark.gpu
+
+HARTREE_TO_EV = 27.211396132
+
+
+def _setup(al):
+    from dftbaby_b200 import LR_TDDFTB
+    td = LR_TDDFTB(al, long_range_correction=1)
+    td.setGeometry(al)
+    td.dftb2.getEnergy()
+    td.setActiveOrbitals(None, None)
+    _, td.qtrans_ov, _ = td._trans_charges(("ov",))
+    d = td.dftb2
+    occ = torch.as_tensor(td.active_occupied_orbs, device=d.device)
+    virt = torch.as_tensor(td.active_virtual_orbs, device=d.device)
+    omega = (d.orbe[virt][None, :] - d.orbe[occ][:, None]).contiguous()
+    return td, omega
+
+
+def test_mixed_exchange_products_match_fp64():
+    from dftbaby_b200.lr_tddftb import ExchangeAO, ExchangeMixed
+    native.load()
+    al = geometry.polyene(20, sigma=0.02, seed=3)
+    td, omega = _setup(al)
+    d = td.dftb2
+    Co, Cv = td._active_coefficients()
+    args = (d.gamma, d.G_lr, td.qtrans_ov, omega.reshape(-1), Co, Cv, d.S, len(al), td.nocc, td.nvirt, d.workspace)
+    ref = ExchangeAO(*args, lc=1)
+    mix = ExchangeMixed(*args, lc=1)
+    g = torch.Generator(device="cpu").manual_seed(0)
+    V = torch.randn(td.nocc * td.nvirt, 5, generator=g, dtype=torch.float64).to(d.device)
+    K1r, K2r = ref.exchange(V)
+    K1m, K2m = mix.exchange(V)
+    for a, b in ((K1m, K1r), (K2m, K2r)):
+        rel = (a - b).abs().max().item() / b.abs().max().item()
+        assert rel < 2e-4, rel
+
+
+def test_mixed_solve_within_1meV_and_refined_solve_matches_fp64():
+    from dftbaby_b200 import LR_TDDFTB
+    native.load()
+    al = geometry.polyene(16, sigma=0.02, seed=5)
+    opts = dict(nstates=8, diag_conv=1e-6, diag_maxiter=100)
+    res = {}
+    for tag, kw in (("fp64", {}), ("mixed", dict(precision="mixed", refine_fp64=False)),
+                    ("refined", dict(precision="mixed", refine_fp64=True))):
+        td = LR_TDDFTB(al, long_range_correction=1)
+        td.setGeometry(al)
+        res[tag] = td.getEnergies(**opts, **kw)
+    (O64, f64), (Om, fm), (Or, fr) = res["fp64"], res["mixed"], res["refined"]
+    assert np.abs(Om - O64).max() * HARTREE_TO_EV < 1e-3
+    assert np.abs(fm - f64).max() < 1e-4
+    # the refined solve meets the FP64 residual test: energies agree with the
+    # plain FP64 path to far below the Davidson tolerance.  (Its f comes from
+    # C = b.Tb of the short refinement subspace, which the non-Hermitian
+    # solver does not converge, so f is not compared for it.)
+    assert np.abs(Or - O64).max() * HARTREE_TO_EV < 1e-6
