@@ -13,7 +13,7 @@ step and rank): SK matrices, gamma, SCC, transition charges, Davidson,
 transition dipoles and oscillator strengths.  Inputs are synthetic.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload armchair7|zigzag8|polyene20]
+                    [--workload armchair7|armchair2|zigzag8|polyene20]
 
 With torchrun each rank solves its own geometries (independent replicas, weak
 scaling); the step time is the maximum over ranks.  ``--impl reference`` times
@@ -39,6 +39,9 @@ WORKLOADS = {
     # name: (builder args, lc, LR options)
     "armchair7": dict(kind="armchair", n=7, sigma=0.01, lc=1,
                       opts=dict(nstates=30, nr_active_occ=1225, nr_active_virt=1225, diag_conv=1.0e-6,
+                                diag_maxiter=100)),
+    "armchair2": dict(kind="armchair", n=2, sigma=0.01, lc=1,
+                      opts=dict(nstates=4, nr_active_occ=60, nr_active_virt=60, diag_conv=1.0e-6,
                                 diag_maxiter=100)),
     "zigzag8": dict(kind="flake", n=8, sigma=0.01, lc=1,
                     opts=dict(nstates=30, nr_active_occ=300, nr_active_virt=300, diag_conv=1.0e-6,

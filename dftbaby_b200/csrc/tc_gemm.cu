@@ -38,11 +38,21 @@
 
 namespace tcg {
 
-constexpr int BM = 128, BN = 128, BK = 64, STAGES = 4;
+constexpr int BM = 128, BN = 128, BK = 64;
 constexpr int TILE_A_BYTES = BM * BK * 2;  // 16 KiB
-constexpr int TILE_B_BYTES = BN * BK * 2;  // 16 KiB
-constexpr int STAGE_BYTES = TILE_A_BYTES + TILE_B_BYTES;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /* alignment slack */ + 256 /* barriers */;
+// segment mode: one (A, B) tile pair per stage, 4 stages;
+// shared-split mode: A_hi, A_lo, B_hi, B_lo per stage (three MMAs reuse them), 3 stages
+template <bool SPLIT> struct Cfg {
+    // 128 x 128 output tiles in both modes (128 x 256 tiles with two stages measured slower in the
+    // solver: the mainloop is bound by copy latency, not by operand bytes)
+    static constexpr int BNX = 128;
+    static constexpr int TILE_BX = BNX * BK * 2;
+    static constexpr int STAGES = SPLIT ? 3 : 4;
+    static constexpr int STAGE_BYTES = SPLIT ? 2 * (TILE_A_BYTES + TILE_BX) : TILE_A_BYTES + TILE_BX;
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /* alignment slack */ + 256 /* barriers */;
+    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BNX >> 3) << 17) |
+                                      ((uint32_t)(BM >> 4) << 24);
+};
 constexpr unsigned long long kSpinLimit = 1ull << 24;  // bounded waits (well above any legitimate wait)
 
 struct Maps {
@@ -52,6 +62,7 @@ struct Maps {
 
 struct Params {
     int M, N, K, nseg;
+    int ksplit;  // K ranges per output tile (gridDim.z); > 1 accumulates C with atomics
     float alpha;
     const float *G;
     long long ldg;
@@ -118,12 +129,13 @@ __device__ __forceinline__ uint64_t smem_desc_k128(uint32_t saddr) {
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                             ((uint32_t)(BM >> 4) << 24);
 
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_c, uint64_t da, uint64_t db, uint32_t accumulate) {
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_c, uint64_t da, uint64_t db, uint32_t accumulate,
+                                          uint32_t idesc = kIdesc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_c),
-        "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate));
+        "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
@@ -143,7 +155,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+template <bool SPLIT>
 __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Maps maps, const Params p) {
+    constexpr int STAGES = Cfg<SPLIT>::STAGES, STAGE_BYTES = Cfg<SPLIT>::STAGE_BYTES;
+    constexpr int BNX = Cfg<SPLIT>::BNX, TILE_BX = Cfg<SPLIT>::TILE_BX;
+    constexpr uint32_t IDESC = Cfg<SPLIT>::IDESC;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
@@ -153,9 +169,14 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Ma
     int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    const int kblocks = (p.K + BK - 1) / BK;
-    const int total = kblocks * p.nseg;
+    // blockIdx.x walks the M tiles: the CTAs that share one B (N) tile run
+    // together, so B streams from DRAM once and the other M tiles hit L2
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BNX;
+    const int kblocks_all = (p.K + BK - 1) / BK;
+    const int kper = (kblocks_all + p.ksplit - 1) / p.ksplit;
+    const int kb0 = blockIdx.z * kper;
+    const int kblocks = max(0, min(kblocks_all, kb0 + kper) - kb0);
+    const int total = SPLIT ? kblocks : kblocks * p.nseg;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -169,9 +190,9 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Ma
     }
     __syncwarp();
     if (warp == 0) {
-        // allocate 128 TMEM columns (128 lanes x 128 FP32 accumulators)
+        // allocate BNX TMEM columns (128 lanes x BNX FP32 accumulators)
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(128));
+                     "r"(BNX));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     __syncthreads();
@@ -191,12 +212,20 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Ma
                 }
             }
             if (*(volatile int *)abort_flag) break;
-            const int seg = it / kblocks, kb = it % kblocks;
             uint8_t *sa = smem + s * STAGE_BYTES;
-            uint8_t *sb = sa + TILE_A_BYTES;
             mbar_expect_tx(&full[s], STAGE_BYTES);
-            tma_load_2d(sa, &maps.a[seg], &full[s], kb * BK, m0);
-            tma_load_2d(sb, &maps.b[seg], &full[s], kb * BK, n0);
+            if (SPLIT) {
+                // stage layout: A_hi | A_lo | B_hi | B_lo
+                const int kx = (kb0 + it) * BK;
+                tma_load_2d(sa, &maps.a[0], &full[s], kx, m0);
+                tma_load_2d(sa + TILE_A_BYTES, &maps.a[1], &full[s], kx, m0);
+                tma_load_2d(sa + 2 * TILE_A_BYTES, &maps.b[0], &full[s], kx, n0);
+                tma_load_2d(sa + 2 * TILE_A_BYTES + TILE_BX, &maps.b[1], &full[s], kx, n0);
+            } else {
+                const int seg = it / kblocks, kb = kb0 + it % kblocks;
+                tma_load_2d(sa, &maps.a[seg], &full[s], kb * BK, m0);
+                tma_load_2d(sa + TILE_A_BYTES, &maps.b[seg], &full[s], kb * BK, n0);
+            }
             ++issued;
         }
         // drain: wait (bounded) until every copy that was started has landed
@@ -214,11 +243,24 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Ma
             if (*(volatile int *)abort_flag) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
-            const uint32_t sb = sa + TILE_A_BYTES;
+            if (SPLIT) {
+                const uint32_t sal = sa + TILE_A_BYTES, sb = sa + 2 * TILE_A_BYTES, sbl = sb + TILE_BX;
 #pragma unroll
-            for (int k = 0; k < BK / 16; ++k) {
-                // advance 16 BF16 = 32 bytes along K inside the 128-byte swizzle atom
-                umma_bf16(tmem, smem_desc_k128(sa + k * 32), smem_desc_k128(sb + k * 32), (it > 0 || k > 0) ? 1u : 0u);
+                for (int k = 0; k < BK / 16; ++k) {
+                    const uint32_t o = k * 32;
+                    umma_bf16(tmem, smem_desc_k128(sa + o), smem_desc_k128(sb + o), (it > 0 || k > 0) ? 1u : 0u,
+                              IDESC);
+                    umma_bf16(tmem, smem_desc_k128(sa + o), smem_desc_k128(sbl + o), 1u, IDESC);
+                    umma_bf16(tmem, smem_desc_k128(sal + o), smem_desc_k128(sb + o), 1u, IDESC);
+                }
+            } else {
+                const uint32_t sb = sa + TILE_A_BYTES;
+#pragma unroll
+                for (int k = 0; k < BK / 16; ++k) {
+                    // advance 16 BF16 = 32 bytes along K inside the 128-byte swizzle atom
+                    umma_bf16(tmem, smem_desc_k128(sa + k * 32), smem_desc_k128(sb + k * 32),
+                              (it > 0 || k > 0) ? 1u : 0u);
+                }
             }
             umma_commit(&empty[s]);  // slot s may be refilled once these MMAs have read it
             ++consumed;
@@ -231,9 +273,9 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Ma
     const bool ok = mbar_wait(done, 0);
     if (!ok && threadIdx.x == 0) atomicExch(p.err, 3);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const bool live = ok && !*(volatile int *)abort_flag;
+    const bool live = ok && !*(volatile int *)abort_flag && total > 0;
     const int row = m0 + warp * 32 + lane;  // TMEM lane = tile row
-    for (int c0 = 0; c0 < BN; c0 += 16) {
+    for (int c0 = 0; c0 < BNX; c0 += 16) {
         float v[16];
         tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
         if (!live) continue;
@@ -242,6 +284,10 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Ma
             const int col = n0 + c0 + j;
             float x = p.alpha * v[j];
             if (row < p.M && col < p.N) {
+                if (p.ksplit > 1) {  // partial sum over this CTA's K range
+                    atomicAdd(&p.C[(long long)row * p.ldc + col], x);
+                    continue;
+                }
                 if (p.G) x *= p.G[(long long)row * p.ldg + col];
                 if (p.C) p.C[(long long)row * p.ldc + col] = x;
                 const __nv_bfloat16 hi = __float2bfloat16_rn(x);
@@ -260,7 +306,7 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Ma
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BNX));
     }
 }
 
@@ -315,11 +361,11 @@ int get_encode() {
     return 0;
 }
 
-int make_map(CUtensorMap *map, const void *base, int rows, int cols, long long ld) {
-    // 2D BF16 tensor: innermost dimension = columns (K), box 64 x 128, 128-byte swizzle, zero fill
+int make_map(CUtensorMap *map, const void *base, int rows, int cols, long long ld, int box_rows = BM) {
+    // 2D BF16 tensor: innermost dimension = columns (K), box 64 x box_rows, 128-byte swizzle, zero fill
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
-    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -338,11 +384,30 @@ extern "C" {
 
 const char *dftb_tc_last_error(void) { return tcg::g_err; }
 
+int dftb_bf16x3_gemm_ex(int M, int N, int K, int nseg, int shared_split, int ksplit, const void *const *A, int lda,
+                        const void *const *B, int ldb, float alpha, const float *G, int ldg, float *C, int ldc,
+                        void *Ohi, void *Olo, int ldo, void *Thi, void *Tlo, int ldt, int *err, void *stream);
+
 int dftb_bf16x3_gemm(int M, int N, int K, int nseg, const void *const *A, int lda, const void *const *B, int ldb,
                      float alpha, const float *G, int ldg, float *C, int ldc, void *Ohi, void *Olo, int ldo, void *Thi,
                      void *Tlo, int ldt, int *err, void *stream) {
+    return dftb_bf16x3_gemm_ex(M, N, K, nseg, 0, 1, A, lda, B, ldb, alpha, G, ldg, C, ldc, Ohi, Olo, ldo, Thi, Tlo,
+                               ldt, err, stream);
+}
+
+int dftb_bf16x3_gemm_ex(int M, int N, int K, int nseg, int shared_split, int ksplit, const void *const *A, int lda,
+                        const void *const *B, int ldb, float alpha, const float *G, int ldg, float *C, int ldc,
+                        void *Ohi, void *Olo, int ldo, void *Thi, void *Tlo, int ldt, int *err, void *stream) {
     using namespace tcg;
-    if (M <= 0 || N <= 0 || K <= 0 || nseg < 1 || nseg > 3) return DFTB_ERR_BAD_SIZE;
+    if (M <= 0 || N <= 0 || K <= 0 || nseg < 1 || nseg > 3 || ksplit < 1 || ksplit > 64) return DFTB_ERR_BAD_SIZE;
+    if (shared_split && nseg != 2) {
+        snprintf(g_err, sizeof(g_err), "bf16x3_gemm: shared-split mode takes the pairs (A_hi, A_lo), (B_hi, B_lo)");
+        return DFTB_ERR_BAD_SIZE;
+    }
+    if (ksplit > 1 && (!C || G || Ohi || Thi)) {
+        snprintf(g_err, sizeof(g_err), "bf16x3_gemm: split-K accumulates into C only (zeroed by the caller)");
+        return DFTB_ERR_BAD_SIZE;
+    }
     if (lda % 8 || ldb % 8 || lda < K || ldb < K) {
         snprintf(g_err, sizeof(g_err), "bf16x3_gemm: lda/ldb must be multiples of 8 and >= K");
         return DFTB_ERR_BAD_SIZE;
@@ -359,13 +424,16 @@ int dftb_bf16x3_gemm(int M, int N, int K, int nseg, const void *const *A, int ld
             snprintf(g_err, sizeof(g_err), "bf16x3_gemm: operands must be 16-byte aligned");
             return DFTB_ERR_BAD_SIZE;
         }
-        if (make_map(&maps.a[s], A[s], M, K, lda) || make_map(&maps.b[s], B[s], N, K, ldb)) return DFTB_ERR_CUDA;
+        if (make_map(&maps.a[s], A[s], M, K, lda) ||
+            make_map(&maps.b[s], B[s], N, K, ldb, shared_split ? Cfg<true>::BNX : Cfg<false>::BNX))
+            return DFTB_ERR_CUDA;
     }
     Params p;
     p.M = M;
     p.N = N;
     p.K = K;
     p.nseg = nseg;
+    p.ksplit = ksplit;
     p.alpha = alpha;
     p.G = G;
     p.ldg = ldg;
@@ -378,20 +446,29 @@ int dftb_bf16x3_gemm(int M, int N, int K, int nseg, const void *const *A, int ld
     p.Tlo = reinterpret_cast<__nv_bfloat16 *>(Tlo);
     p.ldt = ldt;
     p.err = err;
-    static bool attr_set[64] = {false};
+    static bool attr_set[2][64] = {{false}};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        if (cudaFuncSetAttribute(gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) !=
-            cudaSuccess) {
-            snprintf(g_err, sizeof(g_err), "bf16x3_gemm: cannot reserve %d bytes of shared memory", SMEM_BYTES);
+    const int mode = shared_split ? 1 : 0;
+    const int smem = shared_split ? Cfg<true>::SMEM_BYTES : Cfg<false>::SMEM_BYTES;
+    if (dev >= 0 && dev < 64 && !attr_set[mode][dev]) {
+        cudaError_t e = shared_split ? cudaFuncSetAttribute(gemm_kernel<true>,
+                                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+                                     : cudaFuncSetAttribute(gemm_kernel<false>,
+                                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) {
+            snprintf(g_err, sizeof(g_err), "bf16x3_gemm: cannot reserve %d bytes of shared memory", smem);
             return DFTB_ERR_CUDA;
         }
-        attr_set[dev] = true;
+        attr_set[mode][dev] = true;
     }
-    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+    const int bnx = shared_split ? Cfg<true>::BNX : Cfg<false>::BNX;
+    dim3 grid((M + BM - 1) / BM, (N + bnx - 1) / bnx, ksplit);
     if (grid.y > 65535u) return DFTB_ERR_BAD_SIZE;
-    gemm_kernel<<<grid, 128, SMEM_BYTES, reinterpret_cast<cudaStream_t>(stream)>>>(maps, p);
+    if (shared_split)
+        gemm_kernel<true><<<grid, 128, smem, reinterpret_cast<cudaStream_t>(stream)>>>(maps, p);
+    else
+        gemm_kernel<false><<<grid, 128, smem, reinterpret_cast<cudaStream_t>(stream)>>>(maps, p);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         snprintf(g_err, sizeof(g_err), "gemm_kernel: %s", cudaGetErrorString(e));

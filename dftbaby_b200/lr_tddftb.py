@@ -156,6 +156,7 @@ class ExchangeMixed(ExchangeAO):
             T.gemm(self.YV, self.Vp, K=nv, out_pair=self.W)
             for y in range(2):
                 T.gemm(self.XO, self.Wy[y], K=no, G=self.G2, out_pair=self.outN[y], out_pair_t=self.outT[y])
+            # (the Wy views carry both hi and lo parts, so all products use the shared-split kernel)
             T.gemm(self.YbarT, self.NN, K=2 * norb, out_pair=self.P1)
             T.gemm(self.YbarT, self.NT, K=2 * norb, out_pair=self.P2)
             T.gemm(self.P1, self.XbarT, K=2 * norb, alpha=0.25, out=self.K1t)

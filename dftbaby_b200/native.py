@@ -59,6 +59,8 @@ _SIGNATURES = {
     "dftb_dgemm": (_I, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _P]),
     "dftb_bf16x3_gemm": (_I, [_I, _I, _I, _I, ctypes.POINTER(_P), _I, ctypes.POINTER(_P), _I, ctypes.c_float, _P, _I,
                               _P, _I, _P, _P, _I, _P, _P, _I, _P, _P]),
+    "dftb_bf16x3_gemm_ex": (_I, [_I, _I, _I, _I, _I, _I, ctypes.POINTER(_P), _I, ctypes.POINTER(_P), _I,
+                                 ctypes.c_float, _P, _I, _P, _I, _P, _P, _I, _P, _P, _I, _P, _P]),
     "dftb_split_bf16": (_I, [_I, _I, _P, _I, _I, _P, _P, _I, _P]),
     "dftb_split_bf16_f64": (_I, [_I, _I, _P, _I, _I, _D, _P, _P, _I, _P]),
     "dftb_tc_last_error": (ctypes.c_char_p, []),

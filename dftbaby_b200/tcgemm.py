@@ -25,6 +25,9 @@ def _lib():
         L.dftb_bf16x3_gemm.restype = I
         L.dftb_bf16x3_gemm.argtypes = [I, I, I, I, ctypes.POINTER(P), I, ctypes.POINTER(P), I, F, P, I, P, I, P, P, I,
                                        P, P, I, P, P]
+        L.dftb_bf16x3_gemm_ex.restype = I
+        L.dftb_bf16x3_gemm_ex.argtypes = [I, I, I, I, I, I, ctypes.POINTER(P), I, ctypes.POINTER(P), I, F, P, I, P, I,
+                                          P, P, I, P, P, I, P, P]
         L.dftb_split_bf16.restype = I
         L.dftb_split_bf16.argtypes = [I, I, P, I, I, P, P, I, P]
         L.dftb_split_bf16_f64.restype = I
@@ -77,29 +80,50 @@ def _errword(device):
     return _err[key]
 
 
-def gemm(A, B, K=None, refine=True, alpha=1.0, G=None, out=None, out_pair=None, out_pair_t=None, segments=None):
+SMS = 148
+
+
+def gemm(A, B, K=None, refine=True, alpha=1.0, G=None, out=None, out_pair=None, out_pair_t=None, segments=None,
+         ksplit=None):
     """alpha * A B^T on the tensor cores.  A, B: Pair (K-major); K defaults to A.cols.
 
     G (FP32, M x N) multiplies the result elementwise; results go to ``out``
     (FP32 M x N), ``out_pair`` (Pair M x N) and/or ``out_pair_t`` (Pair N x M).
-    ``segments`` overrides the operand list with explicit (A_bf16, B_bf16) pairs.
+    With refine (default) the kernel loads A_hi, A_lo, B_hi, B_lo once per
+    K-block and accumulates hi.hi + hi.lo + lo.hi.  ``segments`` overrides the
+    operand list with explicit (A_bf16, B_bf16) pairs.  When the output alone
+    has too few 128x128 tiles to fill the GPU and only ``out`` is requested,
+    the K range is split over several CTAs that add into ``out``.
     """
     L = _lib()
     M, N = A.rows, B.rows
     K = K or A.cols
+    shared = segments is None and refine
     if segments is None:
         segments = [(A.hi, B.hi)] + ([(A.hi, B.lo), (A.lo, B.hi)] if refine else [])
-    nseg = len(segments)
-    Aptrs = (ctypes.c_void_p * 3)(*[s[0].data_ptr() for s in segments] + [0] * (3 - nseg))
-    Bptrs = (ctypes.c_void_p * 3)(*[s[1].data_ptr() for s in segments] + [0] * (3 - nseg))
+    if shared:
+        ptrA, ptrB = [A.hi.data_ptr(), A.lo.data_ptr()], [B.hi.data_ptr(), B.lo.data_ptr()]
+    else:
+        ptrA, ptrB = [s[0].data_ptr() for s in segments], [s[1].data_ptr() for s in segments]
+    nseg = len(ptrA)
+    Aptrs = (ctypes.c_void_p * 3)(*ptrA + [0] * (3 - nseg))
+    Bptrs = (ctypes.c_void_p * 3)(*ptrB + [0] * (3 - nseg))
     lda, ldb = segments[0][0].stride(0), segments[0][1].stride(0)
+    tiles = ((M + 127) // 128) * ((N + 127) // 128)
+    if ksplit is None:
+        ksplit = 1
+        if out is not None and G is None and out_pair is None and out_pair_t is None and tiles < SMS:
+            ksplit = max(1, min(16, (2 * SMS) // tiles, (K + 63) // 64 // 8))
+    if ksplit > 1:
+        out.zero_()
     err = _errword(A.hi.device)
     P = native.ptr
     timed = native.counters.timed is not None and "dftb_bf16x3_gemm" in native.counters.timed
     if timed:
         ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
         ev[0].record()
-    rc = L.dftb_bf16x3_gemm(M, N, K, nseg, Aptrs, lda, Bptrs, ldb, float(alpha), P(G), G.stride(0) if G is not None
+    rc = L.dftb_bf16x3_gemm_ex(M, N, K, nseg, int(shared), int(ksplit), Aptrs, lda, Bptrs, ldb, float(alpha), P(G),
+                               G.stride(0) if G is not None
                             else 0, P(out), out.stride(0) if out is not None else 0,
                             P(out_pair.hi) if out_pair else None, P(out_pair.lo) if out_pair else None,
                             out_pair.ld if out_pair else 0, P(out_pair_t.hi) if out_pair_t else None,
@@ -110,7 +134,7 @@ def gemm(A, B, K=None, refine=True, alpha=1.0, G=None, out=None, out_pair=None, 
     if timed:
         ev[1].record()
         native.counters.timed["dftb_bf16x3_gemm"].append(ev)
-        native.counters.flops.setdefault("dftb_bf16x3_gemm", []).append(2.0 * M * N * K * nseg)
+        native.counters.flops.setdefault("dftb_bf16x3_gemm", []).append(2.0 * M * N * K * len(segments))
     native.counters.launches += 1
     native.counters.calls["dftb_bf16x3_gemm"] = native.counters.calls.get("dftb_bf16x3_gemm", 0) + 1
 

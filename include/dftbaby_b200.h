@@ -200,6 +200,14 @@ int dftb_davidson_residual(int nov, int ncol, const double *AV, int ldav, const 
 int dftb_bf16x3_gemm(int M, int N, int K, int nseg, const void *const *A, int lda, const void *const *B, int ldb,
                      float alpha, const float *G, int ldg, float *C, int ldc, void *Ohi, void *Olo, int ldo,
                      void *Thi, void *Tlo, int ldt, int *err, void *stream);
+/* Same product with two execution options: shared_split = 1 takes nseg = 2
+ * pointers (A_hi, A_lo) and (B_hi, B_lo), loads the four tiles once per
+ * K-block and accumulates hi.hi + hi.lo + lo.hi; ksplit > 1 splits the K range
+ * over ksplit CTAs per output tile that add into C with atomics (C zeroed by the
+ * caller; G and the BF16 outputs are then not allowed). */
+int dftb_bf16x3_gemm_ex(int M, int N, int K, int nseg, int shared_split, int ksplit, const void *const *A, int lda,
+                        const void *const *B, int ldb, float alpha, const float *G, int ldg, float *C, int ldc,
+                        void *Ohi, void *Olo, int ldo, void *Thi, void *Tlo, int ldt, int *err, void *stream);
 /* X (rows x cols, FP32 or FP64, optionally transposed and scaled) -> BF16
  * hi/lo pair with leading dimension ld; columns beyond the matrix are zeroed. */
 int dftb_split_bf16(int rows, int cols, const float *X, int ldx, int transpose, void *hi, void *lo, int ld,

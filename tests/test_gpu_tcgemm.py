@@ -52,3 +52,23 @@ def test_gemm_epilogue_hadamard_and_pair_outputs():
     assert (rec - C.double()).abs().max().item() / scale < 1e-5
     rect = T.hi[:, :M].double() + T.lo[:, :M].double()
     assert (rect - C.double().T).abs().max().item() / scale < 1e-5
+
+
+@pytest.mark.parametrize("M,N,K,ks", [(300, 200, 1500, 4), (1225, 1225, 8292, None), (130, 1030, 900, 1)])
+def test_gemm_split_k_and_segment_mode_agree(M, N, K, ks):
+    native.load()
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device="cpu").manual_seed(7 + M)
+    A = torch.randn(M, K, generator=g, dtype=torch.float64).to(dev)
+    B = torch.randn(N, K, generator=g, dtype=torch.float64).to(dev)
+    ref = A @ B.T
+    pa, pb = tcgemm.split(A), tcgemm.split(B)
+    C_shared = torch.empty((M, N), dtype=torch.float32, device=dev)
+    tcgemm.gemm(pa, pb, K=K, out=C_shared, ksplit=ks)
+    C_seg = torch.empty((M, N), dtype=torch.float32, device=dev)
+    tcgemm.gemm(pa, pb, K=K, out=C_seg, segments=[(pa.hi, pb.hi), (pa.hi, pb.lo), (pa.lo, pb.hi)], ksplit=1)
+    torch.cuda.synchronize()
+    tcgemm.check_errors(dev)
+    scale = ref.abs().max().item()
+    assert (C_shared.double() - ref).abs().max().item() / scale < 5e-5
+    assert (C_seg.double() - ref).abs().max().item() / scale < 5e-5
