@@ -13,7 +13,7 @@ step and rank): SK matrices, gamma, SCC, transition charges, Davidson,
 transition dipoles and oscillator strengths.  Inputs are synthetic.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload armchair7|armchair2|zigzag8|polyene20]
+                    [--workload armchair7|ensemble512|armchair2|zigzag8|polyene20]
 
 With torchrun each rank solves its own geometries (independent replicas, weak
 scaling); the step time is the maximum over ranks.  ``--impl reference`` times
@@ -22,6 +22,8 @@ bounded, extrapolated sample and prints the same metric.
 """
 import argparse
 import json
+
+import numpy as np
 import os
 import statistics
 import subprocess
@@ -46,13 +48,32 @@ WORKLOADS = {
     "zigzag8": dict(kind="flake", n=8, sigma=0.01, lc=1,
                     opts=dict(nstates=30, nr_active_occ=300, nr_active_virt=300, diag_conv=1.0e-6,
                               diag_maxiter=100)),
+    "ensemble512": dict(kind="ensemble", n=512, sigma=0.03, lc=1,
+                        opts=dict(nstates=8, diag_conv=1.0e-6, diag_maxiter=100)),
     "polyene20": dict(kind="polyene", n=20, sigma=0.02, lc=0,
                       opts=dict(nstates=10, diag_conv=1.0e-6, diag_maxiter=100)),
 }
 
 
+def build_ensemble(n, sigma, seed):
+    """n seeded molecules: a 50/50 coin picks an all-trans polyene C_mH_{m+2} (m even, 10..60) or an
+    acene with 2..8 rings (C-C 1.40 A); every atom jittered by sigma."""
+    from dftbaby_b200 import geometry
+    rng = np.random.default_rng(seed)
+    mols = []
+    for i in range(n):
+        s = int(rng.integers(1 << 30))
+        if rng.random() < 0.5:
+            mols.append(geometry.polyene(int(rng.integers(5, 31)) * 2, sigma=sigma, seed=s))
+        else:
+            mols.append(geometry.acene(int(rng.integers(2, 9)), sigma=sigma, seed=s))
+    return mols
+
+
 def build_geometry(w, seed):
     from dftbaby_b200 import geometry
+    if w["kind"] == "ensemble":
+        return build_ensemble(w["n"], w["sigma"], seed)
     if w["kind"] == "flake":
         return geometry.hexagonal_flake(w["n"], sigma=w["sigma"], seed=seed)
     if w["kind"] == "armchair":
@@ -62,6 +83,14 @@ def build_geometry(w, seed):
 
 def workload_config(name, w, n_gpus, precision="fp64"):
     from dftbaby_b200 import geometry
+    if w["kind"] == "ensemble":
+        mols = build_geometry(w, 0)
+        norbs = [sum(1 if z == 1 else 4 for z, _ in al) for al in mols]
+        return {"workload": "%s: %d seeded polyenes C10-C60 / acenes 2-8 rings, lc-TD-DFTB, batched" % (name, w["n"]),
+                "molecules": w["n"], "orbitals_min_max": [min(norbs), max(norbs)], "long_range_correction": w["lc"],
+                "nstates_per_molecule": w["opts"]["nstates"], "davidson_residual": w["opts"]["diag_conv"],
+                "scf_conv": 1e-10, "precision": "fp64", "sigma_angstrom": w["sigma"],
+                "l2": "batched tensors of 4 groups x 128 molecules", "parallelism": "replicas x%d" % n_gpus}
     al = build_geometry(w, 0)
     nat = len(al)
     norb = sum(1 if z == 1 else 4 for z, _ in al)
@@ -199,6 +228,78 @@ def cpu_baseline_entry(args):
             "kind": "port", "sample": "one full oracle solve"}
 
 
+def run_ensemble(args, w, rank, world, barrier):
+    """Batched lockstep solve of the whole ensemble per step (dftbaby_b200.batched)."""
+    import torch
+    import torch.distributed as dist
+    from dftbaby_b200 import LR_TDDFTB, native
+    from dftbaby_b200.batched import BatchedLR_TDDFTB
+    opts = w["opts"]
+    for s in range(args.warmup):
+        BatchedLR_TDDFTB(build_geometry(w, 10_000 + s * world + rank)).getEnergies(**opts)
+    barrier()
+    native.counters.reset()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
+    sampler.start()
+    stream = torch.cuda.current_stream()
+    dev_ms, last = 0.0, None
+    for s in range(args.steps):
+        mols = build_geometry(w, 20_000 + s * world + rank)
+        bt = BatchedLR_TDDFTB(mols, long_range_correction=w["lc"])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        Om, f = bt.getEnergies(**opts)
+        e1.record(stream)
+        e1.synchronize()
+        dev_ms += e0.elapsed_time(e1)
+        last = (mols, Om, f, bt.stats)
+    barrier()
+    clocks = sampler.stop()
+    t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = t.item() / args.steps
+    nstates_total = w["n"] * opts["nstates"]
+    value = world * nstates_total / (ms / 1e3)
+    # plain one-molecule FP64 path on a seeded subset, extrapolated to the whole ensemble
+    mols, Om, f, stats = last
+    sub = list(range(0, w["n"], max(1, w["n"] // 16)))[:16]
+    t0 = time.perf_counter()
+    dmax, fmax = 0.0, 0.0
+    for i in sub:
+        td = LR_TDDFTB(mols[i], long_range_correction=w["lc"])
+        td.setGeometry(mols[i])
+        Os, fs = td.getEnergies(**opts)
+        dmax = max(dmax, float(np.abs(Os - Om[i]).max()) * 27211.396132)
+        fmax = max(fmax, cluster_df(Os, fs, f[i], 1.0e-3 / 27.211396132))
+    torch.cuda.synchronize()
+    per_mol = (time.perf_counter() - t0) / len(sub)
+    plain_ms = per_mol * w["n"] * 1e3
+    e2e_s = None
+    if not args.no_e2e:
+        t0 = time.perf_counter()
+        BatchedLR_TDDFTB(build_geometry(w, 30_000 + rank)).getEnergies(**opts)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometries)",
+            "config": workload_config(args.workload, w, world),
+            "e2e": {"value": (world * nstates_total / e2e_s) if e2e_s else None, "unit": UNIT,
+                    "h2d_bytes_per_step": int(sum(24 * len(al) for al in mols)),
+                    "d2h_bytes_per_step": int(16 * nstates_total)},
+            "gpu_launches": native.counters.launches, "clocks": clocks, "roofline": None,
+            "solver": {"scc_iterations_max_per_group": [max(x) for x in stats["scc_iterations"]],
+                       "davidson_iterations_max_per_group": [max(x) for x in stats["davidson_iterations"]]},
+            "plain_fp64": {"value": nstates_total / (plain_ms / 1e3), "ms_per_step": plain_ms,
+                           "how": "one-molecule FP64 path on %d seeded members, extrapolated" % len(sub),
+                           "max_dOmega_meV": dmax, "max_df": fmax},
+            "speedup_vs_plain_fp64": plain_ms / ms}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -246,6 +347,8 @@ def main():
         Om, f = td.getEnergies(**opts)
         return td, Om, f
 
+    if w["kind"] == "ensemble":
+        return run_ensemble(args, w, rank, world, barrier)
     for s in range(args.warmup):
         solve(10_000 + s * world + rank)
     barrier()

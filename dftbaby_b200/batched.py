@@ -1,0 +1,643 @@
+"""Many geometries at once: lockstep SCC and Davidson over a padded batch.
+
+``BatchedLR_TDDFTB(atomlists, **dftb2_opts).getEnergies(nstates=..., ...)``
+solves independent molecules of uneven size together (no counterpart in
+DFTBaby, whose objects hold one geometry).  Molecules are sorted by orbital
+count and cut into groups; inside a group every molecule is padded to the
+largest orbital / atom / active-space size:
+
+* padded orbitals have S = 1, H0 = +10 Ha on the diagonal and no couplings,
+  so they are empty, decoupled virtual orbitals above every real one and are
+  excluded from the active space;
+* padded excitations (i, a) carry omega = 1e3 Ha and zero transition
+  charges, so they never enter the lowest states.
+
+The per-molecule algorithms are DFTBaby's: SCC with linear mixing until the
+relative change drops below mixing_threshold, then DIIS_80, one extra
+undamped iteration after convergence (DFTB2.runSCC, DFTB2.py:940-1160); the
+Stratmann-Scuseria-Frisch Davidson with 2 nstates new vectors per iteration
+(Solver.nonHermitianDavidson, Solver.py:637-917) or its Hermitian twin
+without long-range correction.  The level shift of runSCC is part of the
+schedule: the converged SCC density depends on the path at the 1e-5 Ha
+level, so a molecule whose first (non-SCC) HOMO-LUMO gap lies below
+HOMO_LUMO_tol must see the same shifted iterations as in DFTBaby.  Every
+molecule stops at its own convergence (masks); the group iterates until all
+of its molecules have converged.  Correction vectors that fall inside the
+current span (and the slots of molecules that have converged) are replaced
+by random directions so that every basis stays orthonormal in lockstep; this
+only enlarges search spaces.
+Geometry-dependent matrices (S, H0, dipoles, gamma) come from the native
+kernels (one launch each per molecule); the lockstep loops (``solve_group``)
+run on batched device tensors.
+"""
+import numpy as np
+import torch
+
+from . import native
+from .exceptions import ExcitedStatesError, ExcitedStatesNotConverged, SCFNotConverged
+from .params import Parametrization
+
+PAD_H = 10.0
+PAD_OMEGA = 1.0e3
+
+_POOL = None
+_STREAMS = []
+
+
+def batched_eigh(A, workers=16):
+    """torch.linalg.eigh over a batch, spread over host threads with one CUDA stream each.
+
+    The dense symmetric eigensolver runs one matrix at a time and is bound by
+    launch and synchronisation latency at these sizes; independent streams let
+    the solves of different matrices overlap."""
+    global _POOL
+    B = A.shape[0]
+    if B < 2 * workers or A.device.type != "cuda":
+        return torch.linalg.eigh(A)
+    from concurrent.futures import ThreadPoolExecutor
+    if _POOL is None:
+        _POOL = ThreadPoolExecutor(max_workers=workers)
+    while len(_STREAMS) < workers:
+        _STREAMS.append(torch.cuda.Stream(device=A.device))
+    A = A.contiguous()
+    w = torch.empty(A.shape[:-1], dtype=A.dtype, device=A.device)
+    V = torch.empty_like(A)
+    main = torch.cuda.current_stream(A.device)
+    ev = torch.cuda.Event()
+    ev.record(main)
+    chunks = [(i, min(B, i + (B + workers - 1) // workers)) for i in range(0, B, (B + workers - 1) // workers)]
+
+    def work(j):
+        a, b = chunks[j]
+        st = _STREAMS[j]
+        with torch.cuda.stream(st):
+            st.wait_event(ev)
+            wj, Vj = torch.linalg.eigh(A[a:b])
+            w[a:b] = wj
+            V[a:b] = Vj
+            done = torch.cuda.Event()
+            done.record(st)
+        return done
+
+    events = list(_POOL.map(work, range(len(chunks))))
+    for e in events:
+        main.wait_event(e)
+    return w, V
+
+
+class _Mol:
+    pass
+
+
+class BatchedLR_TDDFTB:
+    def __init__(self, atomlists, long_range_correction=1, long_range_radius=3.03, distance_cutoff=30.0,
+                 device=None, group_size=128, **opts):
+        native.load()
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.lc = long_range_correction
+        self.r_lr = long_range_radius
+        self.cutoff = distance_cutoff
+        Zs = sorted({int(Z) for al in atomlists for Z, _ in al})
+        self.par = Parametrization(Zs)
+        self.atomlists = [[(int(Z), tuple(float(c) for c in p)) for Z, p in al] for al in atomlists]
+        self.group_size = group_size
+
+    # ------------------------------------------------------------ per-molecule setup (native kernels)
+    def _setup_molecule(self, al):
+        p, dev = self.par, self.device
+        m = _Mol()
+        ind, typ, ls, ms, orben, occ0, opa = [], [], [], [], [], [], []
+        for i, (Z, _) in enumerate(al):
+            opa.append(len(p.valorbs[Z]))
+            for k, (n, l, mm) in enumerate(p.valorbs[Z]):
+                ind.append(i)
+                typ.append(p.atom_type[Z])
+                ls.append(l)
+                ms.append(mm)
+                orben.append(p.orbital_energies[Z][(n, l)])
+                occ0.append(p.valorbs_occupation[Z][k])
+        nat, norb = len(al), len(ind)
+        i32 = lambda a: torch.tensor(a, dtype=torch.int32, device=dev)
+        f64 = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+        m.nat, m.norb, m.ind = nat, norb, i32(ind)
+        m.nelec = sum(p.ne_val[Z] for Z, _ in al)
+        pos = f64([q for _, q in al]).reshape(-1, 3).contiguous()
+        m.pos = pos
+        st, P = native.stream(), native.ptr
+        r = torch.empty((nat, nat), dtype=torch.float64, device=dev)
+        x, y, z = torch.empty_like(r), torch.empty_like(r), torch.empty_like(r)
+        native.call("dftb_directional_cosines", nat, P(pos), P(r), P(x), P(y), P(z), st)
+        mprox = (r < self.cutoff).to(torch.int32)
+        mprox.fill_diagonal_(1)
+        t = p.device_tables(dev)
+        typ_t, ls_t, ms_t, orben_t = i32(typ), i32(ls), i32(ms), f64(orben)
+        S = torch.empty((norb, norb), dtype=torch.float64, device=dev)
+        H0 = torch.empty_like(S)
+        native.call("dftb_h0_and_s", norb, nat, P(m.ind), P(typ_t), P(ls_t), P(ms_t), P(r), P(x), P(y), P(z),
+                    P(mprox), P(orben_t), p.deg, P(t["tab_filled_SH0"]), P(t["S_knots"]), P(t["S_coefs"]),
+                    P(t["H_knots"]), P(t["H_coefs"]), p.npair, p.nsk, p.npts, P(S), P(H0), st)
+        D = torch.empty((3, norb, norb), dtype=torch.float64, device=dev)
+        native.call("dftb_dipole_matrix", norb, nat, P(m.ind), P(typ_t), P(ls_t), P(ms_t), P(r), P(x), P(y), P(z),
+                    P(pos), P(mprox), P(S), p.deg, P(t["tab_filled_D"]), P(t["D_knots"]), P(t["D_coefs"]), p.npair,
+                    p.nskd, p.npts, P(D), st)
+        sigma = f64([p.sigmas[Z] for Z, _ in al])
+        g = torch.empty((nat, nat), dtype=torch.float64, device=dev)
+        glr = torch.empty_like(g)
+        native.call("dftb_gamma_matrices", nat, P(r), P(sigma), float(self.r_lr), P(g), P(glr), st)
+        m.S, m.H0, m.D, m.g, m.glr, m.p0 = S, H0, D, g, glr, f64(occ0)
+        m.opa = opa
+        return m
+
+    # ------------------------------------------------------------ public API
+    def getEnergies(self, nstates=8, diag_conv=1.0e-5, diag_maxiter=50, scf_conv=1.0e-10, maxiter=1000,
+                    mixing_threshold=1.0e-3, linear_mixing_coefficient=0.33, diis_m=5, level_shift=0.1,
+                    HOMO_LUMO_tol=0.05):
+        """Returns (Omega list, oscillator strength list) in the order of the atomlists.
+
+        The SCC keywords have DFTB2.runSCC's names and defaults."""
+        order = np.argsort([sum(4 if Z > 2 else 1 for Z, _ in al) for al in self.atomlists], kind="stable")
+        self.Omega = [None] * len(self.atomlists)
+        self.oscillator_strength = [None] * len(self.atomlists)
+        self.stats = {"groups": [], "scc_iterations": [], "davidson_iterations": []}
+        for g0 in range(0, len(order), self.group_size):
+            idx = [int(i) for i in order[g0:g0 + self.group_size]]
+            mols = [self._setup_molecule(self.atomlists[i]) for i in idx]
+            Om, f, it_scc, it_dav = solve_group(mols, self.lc, self.device, nstates, diag_conv, diag_maxiter,
+                                                scf_conv, maxiter, mixing_threshold, linear_mixing_coefficient,
+                                                diis_m, level_shift, HOMO_LUMO_tol)
+            for j, i in enumerate(idx):
+                self.Omega[i] = Om[j]
+                self.oscillator_strength[i] = f[j]
+            self.stats["groups"].append(len(idx))
+            self.stats["scc_iterations"].append(it_scc)
+            self.stats["davidson_iterations"].append(it_dav)
+        return self.Omega, self.oscillator_strength
+
+
+
+# ------------------------------------------------------------ one padded group
+def solve_group(mols, lc, dev, nstates, conv, dmaxiter, scf_conv=1.0e-10, maxiter=1000, mix_thr=1.0e-3,
+                alpha=0.33, diis_m=5, level_shift=0.1, homo_lumo_tol=0.05):
+    """Lockstep SCC + Davidson for one group of molecules.
+
+    ``mols`` hold per-molecule tensors on ``dev``: S, H0 (norb, norb), D (3, norb, norb), g, glr
+    (nat, nat), p0 (norb,) reference occupations, ind (norb,) orbital -> atom, and the ints nat,
+    norb, nelec.  Returns (Omega (B, nstates), f (B, nstates), SCC iterations, Davidson iterations)."""
+    B = len(mols)
+    N = max(m.norb for m in mols)
+    NA = max(m.nat for m in mols)
+    f64 = torch.float64
+    S = torch.zeros((B, N, N), dtype=f64, device=dev)
+    H0 = torch.zeros_like(S)
+    Glr = torch.zeros_like(S)     # AO-expanded gamma^lr
+    D = torch.zeros((B, 3, N, N), dtype=f64, device=dev)
+    P0 = torch.zeros((B, N), dtype=f64, device=dev)
+    gat = torch.zeros((B, NA, NA), dtype=f64, device=dev)
+    glrat = torch.zeros_like(gat)
+    orb_atom = torch.zeros((B, N), dtype=torch.long, device=dev)  # padded orbitals -> dummy atom NA
+    real = torch.zeros((B, N), dtype=torch.bool, device=dev)
+    for b, m in enumerate(mols):
+        n = m.norb
+        S[b, :n, :n] = m.S
+        H0[b, :n, :n] = m.H0
+        D[b, :, :n, :n] = m.D
+        P0[b, :n] = m.p0
+        gat[b, :m.nat, :m.nat] = m.g
+        glrat[b, :m.nat, :m.nat] = m.glr
+        ia = m.ind.long()
+        orb_atom[b, :n] = ia
+        orb_atom[b, n:] = NA
+        real[b, :n] = True
+        Glr[b, :n, :n] = m.glr[ia][:, ia]
+    pad = ~real
+    eye = torch.eye(N, dtype=f64, device=dev).expand(B, N, N)
+    S = torch.where(pad[:, :, None] | pad[:, None, :], eye, S)
+    H0 = H0 + torch.diag_embed(pad.to(f64) * PAD_H)
+    L = torch.linalg.cholesky(S)
+    Linv = torch.linalg.solve_triangular(L, torch.eye(N, dtype=f64, device=dev).expand(B, N, N), upper=False)
+    nel = torch.tensor([m.nelec for m in mols], dtype=f64, device=dev)
+    nocc = [int(m.nelec // 2) for m in mols]
+    if any(abs(m.nelec - 2 * (m.nelec // 2)) > 1e-12 for m in mols):
+        raise ValueError("the batched solver handles closed shells only")
+    # occupation (T = 0): the nocc lowest orbitals of each molecule (all real: padding sits at +10 Ha)
+    occmask = torch.zeros((B, N), dtype=f64, device=dev)
+    for b, n in enumerate(nocc):
+        occmask[b, :n] = 2.0
+    # atom-sum operator for Mulliken charges: (B, NA+1, N) one-hot of orb_atom
+    Aop = torch.zeros((B, NA + 1, N), dtype=f64, device=dev)
+    Aop.scatter_(1, orb_atom[:, None, :], 1.0)
+    Aop = Aop[:, :NA, :]
+    P0m = torch.diag_embed(P0)
+    # ---------------- lockstep SCC
+    dq = torch.zeros((B, NA), dtype=f64, device=dev)
+    P = P0m.clone()
+    P_last = P
+    converged = np.zeros(B, bool)
+    done = np.zeros(B, bool)
+    mixing = np.zeros(B, bool)
+    rel = np.ones(B)
+    diis = _BatchedDIIS(B, N * N, diis_m, dev)
+    orbs = orbe = None
+    scc_it = np.zeros(B, int)
+    shift_flag = np.zeros(B, bool)
+    gap = np.full(B, np.inf)
+    hom = torch.as_tensor([n - 1 for n in nocc], device=dev)
+    for it in range(maxiter):
+        live = torch.as_tensor(~done, device=dev)
+        estat = torch.bmm(gat, dq[:, :, None])[:, :, 0]                      # (B, NA)
+        eorb = torch.cat([estat, torch.zeros((B, 1), dtype=f64, device=dev)], 1).gather(1, orb_atom)
+        H = H0 + 0.5 * (eorb[:, :, None] + eorb[:, None, :]) * S
+        if lc:
+            dP = P - P0m
+            A1 = torch.bmm(S, dP)
+            t1 = torch.bmm(Glr * A1, S)
+            Hx = t1 + t1.transpose(1, 2) + Glr * torch.bmm(A1, S) + torch.bmm(torch.bmm(S, dP * Glr), S)
+            H = H + Hx * (-1.0 / 8.0) * real[:, :, None] * real[:, None, :]
+        # level shift (DFTB2.py:1047-1081): once the gap of the last iteration fell below
+        # HOMO_LUMO_tol before DIIS started, the virtual block is shifted by b in the basis of the
+        # last MOs; b halves below 1e5*scf_conv and vanishes below 1e3*scf_conv
+        if it > 0:
+            shift_flag |= (gap < homo_lumo_tol) & ~mixing & ~done
+        bshift = np.where(shift_flag, level_shift, 0.0)
+        bshift = np.where(shift_flag & (rel < 1.0e5 * scf_conv), 0.5 * bshift, bshift)
+        bshift = np.where(shift_flag & (rel < 1.0e3 * scf_conv), 0.0, bshift)
+        Xform = Linv.transpose(1, 2)
+        Hp = torch.bmm(torch.bmm(Linv, H), Xform)
+        if (bshift > 0.0).any():
+            sh = torch.as_tensor(bshift > 0.0, device=dev)
+            Hm = torch.bmm(torch.bmm(orbs.transpose(1, 2), H), orbs)
+            Hm = Hm + torch.diag_embed(torch.as_tensor(bshift, device=dev)[:, None] * (occmask == 0.0))
+            Hp = torch.where(sh[:, None, None], Hm, Hp)
+            Xform = torch.where(sh[:, None, None], orbs, Xform)
+        e_new, Cp = batched_eigh(Hp)
+        C_new = torch.bmm(Xform, Cp)
+        Pn = torch.bmm(C_new * occmask[:, None, :], C_new.transpose(1, 2))
+        # mixing, per molecule
+        Pmix = Pn.clone()
+        lin = torch.as_tensor((~converged) & (~mixing) & (~done), device=dev)
+        if bool(lin.any()):
+            nP = alpha * Pn + (1.0 - alpha) * P_last
+            scale = (Pn * S).sum((1, 2)) / (nP * S).sum((1, 2))
+            nP = nP * scale[:, None, None]
+            Pmix = torch.where(lin[:, None, None], nP, Pmix)
+        use_diis = (~converged) & mixing & (~done)
+        if use_diis.any():
+            Pd = diis.next_approximation(Pn.reshape(B, -1), use_diis).reshape(B, N, N)
+            Pmix = torch.where(torch.as_tensor(use_diis, device=dev)[:, None, None], Pd, Pmix)
+        # frozen molecules keep their state
+        P = torch.where(live[:, None, None], Pmix, P)
+        orbs = C_new if orbs is None else torch.where(live[:, None, None], C_new, orbs)
+        orbe = e_new if orbe is None else torch.where(live[:, None], e_new, orbe)
+        q = (torch.bmm(Aop, ((P - P0m) * S).sum(2)[:, :, None]))[:, :, 0]
+        dq = torch.where(live[:, None], q, dq)
+        # relative change per molecule
+        r_lin = torch.linalg.norm((P_last - P).reshape(B, -1), dim=1) / torch.linalg.norm(P.reshape(B, -1), dim=1)
+        r_diis = diis.relative_change()
+        gap_t = orbe.gather(1, hom[:, None] + 1)[:, 0] - orbe.gather(1, hom[:, None])[:, 0]
+        host = torch.stack([r_lin, r_diis, gap_t]).cpu().numpy()
+        gap = np.where(done, gap, host[2])
+        for b in range(B):
+            if done[b]:
+                continue
+            scc_it[b] = it + 1
+            if converged[b]:
+                done[b] = True
+                continue
+            rel[b] = host[1][b] if mixing[b] else host[0][b]
+            if rel[b] < scf_conv:
+                converged[b] = True
+            if rel[b] < mix_thr and not mixing[b]:
+                mixing[b] = True
+        P_last = P
+        if done.all():
+            break
+    else:
+        raise SCFNotConverged("batched SCC did not converge for %d molecules" % int((~done).sum()))
+    # ---------------- excited states (full active space of each molecule)
+    no_max = max(nocc)
+    nvir = [m.norb - n for m, n in zip(mols, nocc)]
+    nv_max = max(nvir)
+    nov = no_max * nv_max
+    Co = torch.zeros((B, N, no_max), dtype=f64, device=dev)
+    Cv = torch.zeros((B, N, nv_max), dtype=f64, device=dev)
+    omega = torch.full((B, no_max, nv_max), PAD_OMEGA, dtype=f64, device=dev)
+    for b, (n, nv) in enumerate(zip(nocc, nvir)):
+        # occupied: nocc lowest; active occupied in increasing energy, virtuals lowest first
+        Co[b, :, no_max - n:] = orbs[b, :, :n]
+        Cv[b, :, :nv] = orbs[b, :, n:n + nv]
+        omega[b, no_max - n:, :nv] = orbe[b, n:n + nv][None, :] - orbe[b, :n][:, None]
+    # transition charges q_ov (B, NA, nov) from C and S C, summed per atom
+    SCo, SCv = torch.bmm(S, Co), torch.bmm(S, Cv)
+    qov = 0.5 * (torch.einsum("bmi,bma->bmia", Co, SCv) + torch.einsum("bma,bmi->bmia", Cv, SCo))
+    qov = torch.bmm(Aop, qov.reshape(B, N, nov)).reshape(B, NA, nov)
+    om = omega.reshape(B, nov)
+    k = nstates
+    kmax = [n * nv for n, nv in zip(nocc, nvir)]
+    if lc:
+        prod = _BatchedProducts(gat, Glr, qov, om, Co, Cv, SCo, SCv, no_max, nv_max)
+        Om, C, XmY, XpY, dav_it = _batched_nonhermitian(prod, om, k, conv, dmaxiter, kmax)
+    else:
+        prod = _BatchedProducts(gat, None, qov, om, Co, Cv, SCo, SCv, no_max, nv_max)
+        Om, C, XmY, XpY, dav_it = _batched_hermitian(prod, om, k, conv, dmaxiter, kmax)
+    # oscillator strengths from C and the MO dipoles of the active block
+    t = torch.einsum("bmi,bcmn,bna->bcia", Co, D, Cv).reshape(B, 3, nov)
+    tdip = torch.einsum("bkn,bcn->bck", C, t)
+    fosc = 2.0 / 3.0 * Om * (tdip ** 2).sum(1)
+    return Om.cpu().numpy(), fosc.cpu().numpy(), scc_it.tolist(), dav_it
+
+
+class _BatchedDIIS:
+    """DIIS_80 (ConvAcceleration.py:27-143) for a batch: every molecule keeps its own history of
+    up to m trial vectors; the bookkeeping (pop when longer than m, start once the relative
+    change of a longer-than-3 history drops below 0.5) is the reference's, vectorised."""
+
+    def __init__(self, B, n, m, dev):
+        self.B, self.m, self.dev = B, m, dev
+        self.trial = torch.zeros((B, m, n), dtype=torch.float64, device=dev)
+        self.resid = torch.zeros((B, m, n), dtype=torch.float64, device=dev)
+        self.nt = np.zeros(B, int)   # trial vectors held
+        self.start = np.zeros(B, bool)
+
+    def next_approximation(self, Pflat, mask):
+        out = Pflat.clone()
+        idx = np.nonzero(mask)[0]
+        if len(idx) == 0:
+            return out
+        m = self.m
+        # append the new trial vector (rolling window of m)
+        for b in idx:
+            nt = self.nt[b]
+            if nt == m:
+                self.trial[b, :-1] = self.trial[b, 1:].clone()
+                self.resid[b, :-1] = self.resid[b, 1:].clone()
+                nt = m - 1
+            self.trial[b, nt] = Pflat[b]
+            if nt >= 1:
+                self.resid[b, nt - 1] = self.trial[b, nt] - self.trial[b, nt - 1]
+            self.nt[b] = nt + 1
+        run = [b for b in idx if self.start[b]]
+        if run:
+            rb = torch.as_tensor(run, device=self.dev)
+            nres = np.array([self.nt[b] - 1 for b in run])
+            n = int(nres.max())
+            R = self.resid[rb, :n]
+            gram = torch.bmm(R, R.transpose(1, 2))
+            A = torch.zeros((len(run), n + 1, n + 1), dtype=torch.float64, device=self.dev)
+            rhs = torch.zeros((len(run), n + 1), dtype=torch.float64, device=self.dev)
+            for j, nr in enumerate(nres):
+                A[j, :nr, :nr] = gram[j, :nr, :nr]
+                A[j, :nr, nr] = A[j, nr, :nr] = -1.0
+                rhs[j, nr] = -1.0
+                for q in range(nr + 1, n + 1):
+                    A[j, q, q] = 1.0
+            c = torch.linalg.solve(A, rhs)
+            for j, b in enumerate(run):
+                nr = int(nres[j])
+                p = torch.einsum("i,in->n", c[j, :nr], self.trial[b, :nr])
+                self.trial[b, nr] = p
+                self.resid[b, nr - 1] = p - self.trial[b, nr - 1]
+                out[b] = p
+        late = [b for b in idx if not self.start[b] and self.nt[b] > 3]
+        if late:
+            lb = torch.as_tensor(late, device=self.dev)
+            nt = torch.as_tensor([self.nt[b] for b in late], device=self.dev)
+            r = torch.linalg.norm(self.resid[lb, nt - 2], dim=1) / torch.linalg.norm(self.trial[lb, nt - 1], dim=1)
+            for b, v in zip(late, r.cpu().numpy()):
+                if v < 0.5:
+                    self.start[b] = True
+        return out
+
+    def relative_change(self):
+        ch = torch.ones(self.B, dtype=torch.float64, device=self.dev)
+        have = [b for b in range(self.B) if self.nt[b] >= 2]
+        if not have:
+            return ch
+        hb = torch.as_tensor(have, device=self.dev)
+        nt = torch.as_tensor([self.nt[b] for b in have], device=self.dev)
+        r1 = torch.linalg.norm(self.resid[hb, nt - 2], dim=1) / torch.linalg.norm(self.trial[hb, nt - 1], dim=1)
+        two = nt >= 3
+        r2 = torch.linalg.norm(self.resid[hb, (nt - 3).clamp_min(0)], dim=1) / torch.linalg.norm(
+            self.trial[hb, (nt - 2).clamp_min(0)], dim=1)
+        ch[hb] = torch.where(two, 0.5 * (r1 + r2), r1)
+        return ch
+
+
+class _BatchedProducts:
+    """(A+B).V and (A-B).V for a padded batch: Coulomb through q_ov, exchange in AO-factorised form."""
+
+    def __init__(self, gat, Glr, qov, om, Co, Cv, SCo, SCv, no, nv):
+        self.gat, self.Glr, self.qov, self.om = gat, Glr, qov, om
+        self.no, self.nv = no, nv
+        if Glr is not None:
+            self.Xo = torch.stack([Co, SCo], 1)        # (B, 2, N, no)
+            self.Yv = torch.stack([Cv, SCv], 1)        # (B, 2, N, nv)
+            self.Xo_bar = torch.stack([SCo, Co], 1)
+            self.Yv_bar = torch.stack([SCv, Cv], 1)
+
+    def __call__(self, V):
+        """V: (B, nov, m) -> (ApB V, AmB V)."""
+        B, nov, m = V.shape
+        T = torch.bmm(self.qov, V)                                    # (B, NA, m)
+        coul = self.om[:, :, None] * V + 4.0 * torch.bmm(self.qov.transpose(1, 2), torch.bmm(self.gat, T))
+        omv = self.om[:, :, None] * V
+        if self.Glr is None:
+            return coul, omv
+        no, nv = self.no, self.nv
+        Vb = V.permute(0, 2, 1).reshape(B, m, no, nv)
+        W = torch.matmul(Vb[:, :, None], self.Yv.transpose(2, 3)[:, None])        # (B, m, y, no, N)
+        M = torch.matmul(self.Xo[:, None, :, None], W[:, :, None])                # (B, m, x, y, N, N)
+        M = M * self.Glr[:, None, None, None]
+        P1 = torch.matmul(M, self.Yv_bar[:, None, None])                         # (B, m, x, y, N, nv)
+        k1 = torch.matmul(self.Xo_bar.transpose(2, 3)[:, None], P1.sum(3)).sum(2)  # (B, m, no, nv)
+        P2 = torch.matmul(M.transpose(-1, -2), self.Yv_bar[:, None, :, None])      # (B, m, x, y, N, nv)
+        k2 = torch.matmul(self.Xo_bar.transpose(2, 3)[:, None], P2.sum(2)).sum(2)
+        K1 = 0.25 * k1.reshape(B, m, nov).permute(0, 2, 1)
+        K2 = 0.25 * k2.reshape(B, m, nov).permute(0, 2, 1)
+        return coul - K1 - K2, omv + K2 - K1
+
+
+# diagonal given to unused (all-zero) columns of a projected matrix, in Hartree (Mp, Mm) and
+# Hartree^2 (R = Omega^2 problem): above every wanted excitation, but on the scale of the live
+# block, because the eigensolver's error grows with the norm of the whole matrix
+PAD_SUB = 4.0
+PAD_SUB_SQ = 16.0
+
+
+def _select_new(normsL, normsR, k, l_live, kmax, conv, two_sided):
+    """Which residual columns DFTBaby turns into new expansion vectors (Solver.py:531-548,
+    Solver.py:873-893): those whose norm exceeds eps = 0.01 conv, at most
+    dkmax = min(kmax - l, k) (Hermitian) or min(kmax - l, 2k) (L-residuals first, then R)."""
+    eps = 0.01 * conv
+    B = normsL.shape[0]
+    sel = np.zeros((B, 2 * k if two_sided else k), bool)
+    for b in range(B):
+        if two_sided:
+            dkmax = min(kmax[b] - l_live[b], 2 * k)
+            ncL, ncR = int(np.sum(normsL[b] > eps)), int(np.sum(normsR[b] > eps))
+            dkR = min(int(np.ceil(dkmax / 2.0)), ncL)
+            dkL = min(dkmax - dkR, ncR)
+            iL = np.nonzero(normsL[b] > eps)[0][:dkR]
+            iR = np.nonzero(normsR[b] > eps)[0][:dkL]
+            sel[b, iL] = True
+            sel[b, k + iR] = True
+        else:
+            dkmax = min(kmax[b] - l_live[b], k)
+            sel[b, [n for n in range(dkmax) if normsL[b, n] > eps]] = True
+    return sel
+
+
+def _orthonormal_extension(bs, Q, live):
+    """Columns orthonormal to bs that span the live columns of Q (block Gram-Schmidt twice + QR).
+
+    live (B, m) marks the columns DFTBaby would add; per molecule they are moved to the front
+    before the QR, so that the span of the first n_live output columns is exactly theirs, and
+    the remaining columns are returned as zeros.  A live column that lies (numerically) inside
+    span(bs) is replaced by a random direction, as an economic QR of a rank-deficient block
+    would.  Returns (Q, column-live mask)."""
+    B, nov, m = Q.shape
+    dev = Q.device
+    perm = torch.argsort((~live).to(torch.int8), dim=1, stable=True)
+    Q = torch.gather(Q, 2, perm[:, None, :].expand(B, nov, m))
+    n_live = live.sum(1)
+    keep = torch.arange(m, device=dev)[None, :] < n_live[:, None]
+    Q = Q * keep[:, None, :]
+    n0 = torch.linalg.norm(Q, dim=1)
+    for _ in range(2):
+        Q = Q - torch.bmm(bs, torch.bmm(bs.transpose(1, 2), Q))
+    n1 = torch.linalg.norm(Q, dim=1)
+    bad = keep & (n1 <= 1.0e-8 * n0.clamp_min(1e-300))
+    if bool(bad.any()):
+        g = torch.Generator(device=dev).manual_seed(12345)
+        R = torch.randn(Q.shape, dtype=Q.dtype, device=dev, generator=g)
+        for _ in range(2):
+            R = R - torch.bmm(bs, torch.bmm(bs.transpose(1, 2), R))
+        Q = torch.where(bad[:, None, :], R, Q)
+    Q, _ = torch.linalg.qr(Q)
+    Q = Q * keep[:, None, :]
+    Q = Q - torch.bmm(bs, torch.bmm(bs.transpose(1, 2), Q))
+    Q, _ = torch.linalg.qr(Q)
+    return Q * keep[:, None, :], keep
+
+
+def _pad_dead(M, live, pad=PAD_SUB):
+    """Projected matrix with pad on the diagonal of unused columns: the dead block decouples and
+    its eigenvalues sort above every wanted live one."""
+    return M + torch.diag_embed((~live).to(M.dtype) * pad)
+
+
+def _batched_hermitian(prod, om, k, conv, maxiter, kmax):
+    """Lockstep Hermitian Davidson (Solver.HermitianDavidson, lc = 0) over a batch; prod gives the
+    Coulomb product (A+B).V, from which R.V = omega^2 V + sqrt(omega) (A+B - omega)(sqrt(omega) V)."""
+    B, nov = om.shape
+    dev, f64 = om.device, torch.float64
+    sq = torch.sqrt(om)
+
+    def rv(V):
+        ap, _ = prod(sq[:, :, None] * V)
+        return om[:, :, None] ** 2 * V + sq[:, :, None] * (ap - om[:, :, None] * sq[:, :, None] * V)
+
+    idx = torch.argsort(om, dim=1, stable=True)[:, :k]
+    bs = torch.zeros((B, nov, k), dtype=f64, device=dev)
+    bs[torch.arange(B, device=dev)[:, None], idx, torch.arange(k, device=dev)[None, :]] = 1.0
+    live = torch.ones((B, k), dtype=torch.bool, device=dev)
+    RB = rv(bs)
+    active = np.ones(B, bool)
+    Om = torch.zeros((B, k), dtype=f64, device=dev)
+    T = torch.zeros((B, nov, k), dtype=f64, device=dev)
+    iters = np.zeros(B, int)
+    for it in range(maxiter):
+        Hb = torch.bmm(bs.transpose(1, 2), RB)
+        w2, Tb = batched_eigh(_pad_dead(0.5 * (Hb + Hb.transpose(1, 2)), live, PAD_SUB_SQ))
+        w = torch.sqrt(w2.clamp_min(0.0))
+        Tk = torch.bmm(bs, Tb[:, :, :k])
+        W = torch.bmm(RB, Tb[:, :, :k]) - Tk * w2[:, None, :k]
+        host = torch.cat([torch.linalg.norm(W, dim=1), live.sum(1, keepdim=True).to(f64)], 1).cpu().numpy()
+        norms, l_live = host[:, :k], host[:, k].astype(int)
+        act_t = torch.as_tensor(active, device=dev)
+        Om = torch.where(act_t[:, None], w[:, :k], Om)
+        T = torch.where(act_t[:, None, None], Tk, T)
+        newly = active & (norms < conv).all(1)
+        iters[active] = it + 1
+        active = active & ~newly
+        if not active.any():
+            break
+        sel = _select_new(norms, None, k, l_live, kmax, conv, False) & active[:, None]
+        wD = w[:, None, :k] - om[:, :, None]
+        wD = torch.where(wD.abs() < 1e-6, 1e-6 * om[:, :, None].expand_as(wD), wD)
+        Q, qlive = _orthonormal_extension(bs, W / wD, torch.as_tensor(sel, device=dev))
+        bs = torch.cat([bs, Q], 2)
+        live = torch.cat([live, qlive], 1)
+        RB = torch.cat([RB, rv(Q)], 2)
+    else:
+        raise ExcitedStatesNotConverged("batched Davidson: %d molecules did not converge" % int(active.sum()))
+    C = T.transpose(1, 2)
+    XpY = (sq[:, :, None] / torch.sqrt(Om)[:, None, :] * T).transpose(1, 2)
+    XmY = (torch.sqrt(Om)[:, None, :] / sq[:, :, None] * T).transpose(1, 2)
+    return Om, C, XmY, XpY, iters.tolist()
+
+
+def _batched_nonhermitian(prod, om, k, conv, maxiter, kmax):
+    """Lockstep Stratmann-Scuseria-Frisch Davidson over a batch (Solver.nonHermitianDavidson):
+    every molecule adds exactly the correction vectors DFTBaby would add, so its search space,
+    and with it the subspace-dependent C = bs Tb behind the oscillator strengths, is DFTBaby's."""
+    B, nov = om.shape
+    dev = om.device
+    f64 = torch.float64
+    # initial vectors: unit vectors on the k lowest omega_ia of each molecule
+    idx = torch.argsort(om, dim=1, stable=True)[:, :k]
+    bs = torch.zeros((B, nov, k), dtype=f64, device=dev)
+    bs[torch.arange(B, device=dev)[:, None], idx, torch.arange(k, device=dev)[None, :]] = 1.0
+    live = torch.ones((B, k), dtype=torch.bool, device=dev)
+    AP, AM = prod(bs)
+    active = np.ones(B, bool)
+    Om = torch.zeros((B, k), dtype=f64, device=dev)
+    C = torch.zeros((B, k, nov), dtype=f64, device=dev)
+    XmY = torch.zeros_like(C)
+    XpY = torch.zeros_like(C)
+    iters = np.zeros(B, int)
+    for it in range(maxiter):
+        Mp = _pad_dead(torch.bmm(bs.transpose(1, 2), AP), live)
+        Mm = _pad_dead(torch.bmm(bs.transpose(1, 2), AM), live)
+        lam, Vm = batched_eigh(0.5 * (Mm + Mm.transpose(1, 2)))
+        if bool((lam[torch.as_tensor(active, device=dev)] <= 0).any()):
+            raise ExcitedStatesError("(A-B) projected onto the expansion space is not positive definite")
+        lam = lam.clamp_min(1e-300)
+        Mmsq = torch.bmm(Vm * torch.sqrt(lam)[:, None, :], Vm.transpose(1, 2))
+        Mh = torch.bmm(torch.bmm(Mmsq, Mp), Mmsq)
+        w2, Tb = batched_eigh(Mh)
+        w = torch.sqrt(w2.clamp_min(0.0))
+        Rb = torch.bmm(Mmsq, Tb[:, :, :k]) / torch.sqrt(w[:, None, :k])
+        Lb = torch.bmm(Mp, Rb) / w[:, None, :k]
+        R, Lv = torch.bmm(bs, Rb), torch.bmm(bs, Lb)
+        WL = torch.bmm(AP, Rb) - Lv * w[:, None, :k]
+        WR = torch.bmm(AM, Lb) - R * w[:, None, :k]
+        nL, nR = torch.linalg.norm(WL, dim=1), torch.linalg.norm(WR, dim=1)
+        host = torch.cat([nL, nR, live.sum(1, keepdim=True).to(f64)], 1).cpu().numpy()
+        normsL, normsR, l_live = host[:, :k], host[:, k:2 * k], host[:, 2 * k].astype(int)
+        norms = normsL + normsR
+        act_t = torch.as_tensor(active, device=dev)
+        Om = torch.where(act_t[:, None], w[:, :k], Om)
+        Cn = torch.bmm(bs, Tb[:, :, :k]).transpose(1, 2)
+        C = torch.where(act_t[:, None, None], Cn, C)
+        XmY = torch.where(act_t[:, None, None], Lv.transpose(1, 2), XmY)
+        XpY = torch.where(act_t[:, None, None], R.transpose(1, 2), XpY)
+        newly = active & (norms < conv).all(1) & (it > 0)
+        iters[active] = it + 1
+        active = active & ~newly
+        if not active.any():
+            break
+        sel = _select_new(normsL, normsR, k, l_live, kmax, conv, True) & active[:, None]
+        # correction vectors: L residuals, then R residuals, (w - omega)^-1 preconditioner
+        wk = w[:, None, :k]
+        wD = wk - om[:, :, None]
+        small = wD.abs() < 1e-6
+        wD = torch.where(small, 1e-6 * om[:, :, None].expand_as(wD), wD)
+        Q, qlive = _orthonormal_extension(bs, torch.cat([WL / wD, WR / wD], dim=2), torch.as_tensor(sel, device=dev))
+        ap, am = prod(Q)
+        bs = torch.cat([bs, Q], 2)
+        live = torch.cat([live, qlive], 1)
+        AP = torch.cat([AP, ap], 2)
+        AM = torch.cat([AM, am], 2)
+    else:
+        raise ExcitedStatesNotConverged("batched Davidson: %d molecules did not converge" % int(active.sum()))
+    return Om, C, XmY, XpY, iters.tolist()
