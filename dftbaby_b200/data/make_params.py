@@ -13,7 +13,10 @@ needs for H/C molecules:
   orbital energies used as on-site H0 (``DFTB/SlaterKoster/free_pseudo_atoms``),
   as read by ``DFTB2.__init__`` (``DFTB/DFTB2.py:207-246``);
 * ionisation energies and electron affinities that define the Hubbard U
-  (``DFTB/Parameters.py:25-30``, ``DFTB/AtomicData.py:131-134``).
+  (``DFTB/Parameters.py:25-30``, ``DFTB/AtomicData.py:131-134``);
+* the repulsive potentials ``Vrep`` on their distance grids
+  (``DFTB/RepulsivePotential/reppot_tables/{h_h,h_c,c_c}.py``, loaded by
+  ``DFTB2.__init__``, ``DFTB/DFTB2.py:257-327``).
 
 Usage (needs the DFTBaby sources)::
 
@@ -53,6 +56,10 @@ def main(ref_root):
         for kind in ("S", "H", "Dipole"):
             for (l1, l2, i), arr in ns[kind].items():
                 out["sk/%s/%s/%d/%d/%d" % (tag, kind, l1, l2, i)] = np.asarray(arr, dtype=np.float64)
+        rep = _exec_module(os.path.join(dftb, "RepulsivePotential", "reppot_tables", tag + ".py"))
+        assert (min(rep["Z1"], rep["Z2"]), max(rep["Z1"], rep["Z2"])) == (z1, z2)
+        out["vrep/%s/d" % tag] = np.asarray(rep["d"], dtype=np.float64)
+        out["vrep/%s/Vrep" % tag] = np.asarray(rep["Vrep"], dtype=np.float64)
     atomic = open(os.path.join(dftb, "AtomicData.py")).read()
     ie = _dict_literal(atomic, "ionization_energies_eV")
     ea = _dict_literal(atomic, "electron_affinities_eV")

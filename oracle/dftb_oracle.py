@@ -81,6 +81,15 @@ def lib():
         L.oracle_trans_charges.argtypes = [c_int, c_int, c_int, c_int, D, D, D, I, D, D, D]
         L.oracle_monopoles.restype = None
         L.oracle_monopoles.argtypes = [c_int, c_int, D, D, D, I, D, D]
+        L.oracle_splder1.restype = c_double
+        L.oracle_splder1.argtypes = [D, c_int, D, c_int, c_double]
+        L.oracle_splev_ext.restype = c_double
+        L.oracle_splev_ext.argtypes = [D, c_int, D, c_int, c_double, c_int]
+        L.oracle_sk_rule_grad.restype = None
+        L.oracle_sk_rule_grad.argtypes = [c_int, c_int, c_int, c_int, c_double, D, D, D, D]
+        L.oracle_gradients_h0_and_s.restype = None
+        L.oracle_gradients_h0_and_s.argtypes = [c_int, c_int, I, I, I, I, D, I, c_int, I, D, D, D, D,
+                                                c_int, c_int, c_int, D, D]
         _lib = L
     return _lib
 
@@ -205,6 +214,24 @@ class Parametrization:
             else:
                 self.D_knots[ipair, i], self.D_coefs[ipair, i] = t, c
                 self.tab_filled_D[ipair, i] = 1
+        # repulsive potentials: interpolating cubic splines of the tabulated Vrep
+        # (RepulsivePotential.__init__, RepulsivePotential.py:21-78, smooth_decay=False)
+        self.vrep = {}
+        for a in range(ntype):
+            for b in range(a, ntype):
+                Zi, Zj = self.atomtypes[a], self.atomtypes[b]
+                tag = "%s_%s" % (ELEMENT_NAMES[Zi], ELEMENT_NAMES[Zj])
+                d, V = raw["vrep/%s/d" % tag], raw["vrep/%s/Vrep" % tag]
+                t, c, k = splrep(d, V, s=0)
+                self.vrep[(Zi, Zj)] = (t, c, k, float(d.min()), float(d.max()))
+
+    def getVrep(self, Z1, Z2, R, deriv=0):
+        """RepulsivePotential.getVrep (RepulsivePotential.py:87-100): spline value (or derivative)
+        below the last grid point, extrapolated below the first, zero from the last on."""
+        t, c, k, dmin, dmax = self.vrep[(min(Z1, Z2), max(Z1, Z2))]
+        if R >= dmax:
+            return 0.0
+        return lib().oracle_splev_ext(_d(_cd(t)), len(t), _d(_cd(c)), k, float(R), int(deriv))
 
 
 # ---------------------------------------------------------------- DIIS
@@ -310,6 +337,10 @@ class DFTB2:
         self.pos = pos
         R = pos[:, None, :] - pos[None, :, :]
         self.distances = np.sqrt(np.sum(R * R, axis=-1))
+        # directions[i, j] = unit vector from atom j to atom i (DFTB2._distance_matrix, DFTB2.py:575-600)
+        off = self.distances > 0.0
+        self.directions = np.zeros_like(R)
+        self.directions[off] = R[off] / self.distances[off][:, None]
         Mprox = (self.distances < self.distance_cutoff).astype(np.int32)
         np.fill_diagonal(Mprox, 1)
         self.Mproximity = Mprox
@@ -394,9 +425,17 @@ class DFTB2:
         if self.long_range_correction == 1:
             self.E_HF_x = self.lc_exchange_energy()
             self.E_elec += self.E_HF_x
-        self.E_nuc = 0.0  # repulsive potentials are not part of this path (dummy Vrep = 0)
+        self.E_nuc = self.getRepulsionEnergy()
         self.E_tot = self.E_elec + self.E_nuc
         return self.E_bs, self.E_coulomb, self.E_elec, self.E_nuc, self.E_tot
+
+    def getRepulsionEnergy(self):
+        """DFTB2.getRepulsionEnergy (DFTB2.py:2339-2359): sum of Vrep over atom pairs."""
+        E = 0.0
+        for i in range(1, len(self.atomlist)):
+            for j in range(i):
+                E += self.par.getVrep(self.atomlist[i][0], self.atomlist[j][0], self.distances[i, j])
+        return E
 
     def getEnergy(self, **scf_opts):
         """DFTB2.getEnergy (DFTB2.py:2278-2338)."""

@@ -12,6 +12,12 @@
  *                           DFTB/extensions/slako_transformations_dipole_lmax2.f90
  *   trans_charges           DFTB/extensions/tddftb.f90:12-112
  *   monopoles               DFTB/extensions/mulliken.f90:11-66
+ *   splev_deriv_uniform     DFTB/extensions/splines.f90:96-115 with splder.f (FITPACK)
+ *   gradients_H0andS        DFTB/extensions/slako.f90:402-569
+ *   SK gradient rules       DFTB/extensions/slako_transformations_grad_lmax2.f90
+ *   repulsive potential     scipy.interpolate.splev (FITPACK splev/splder, ext=0)
+ *                           as called by RepulsivePotential.getVrep
+ *                           (DFTB/RepulsivePotential/RepulsivePotential.py:87-100)
  *
  * Array layouts are C row-major.  Symmetric matrices (S, H0, P) are Norb x Norb.
  * The dipole matrix is returned as three planes D[c][mu][nu], c = x,y,z.
@@ -53,9 +59,29 @@ static void fpbspl(const double *t, int k, double x, int l, double *h)
  * beyond t(n-k) are clamped there.  A coefficient index below 1 (reachable
  * only for x < 3*dt, i.e. nuclei closer than ~0.12 bohr) reads outside the
  * array in the reference; it contributes zero here. */
+/* Test switch: when nonzero, oracle_splev_uniform evaluates the spline exactly
+ * (FITPACK interval search, argument clamped like splder) instead of the
+ * reference's shifted-interval shortcut, so that energies and their analytic
+ * gradients (which use splder) become consistent to rounding. */
+int oracle_exact_splines = 0;
+
 double oracle_splev_uniform(const double *t, int n, const double *c, int k, double x)
 {
     int k1 = k + 1, nk1 = n - k1;
+    if (oracle_exact_splines) {
+        double tb = t[k1 - 1], te = t[nk1];
+        double arg = x < tb ? tb : (x > te ? te : x);
+        int l = k1, l1 = l + 1;
+        while (!(arg < t[l1 - 1] || l == nk1)) {
+            l = l1;
+            l1 = l + 1;
+        }
+        double h[6];
+        fpbspl(t, k, arg, l, h);
+        double sp = 0.0;
+        for (int j = 1; j <= k1; ++j) sp += c[l - k1 + j - 1] * h[j - 1];
+        return sp;
+    }
     double tb = t[k1 - 1], te = t[nk1];
     double arg;
     int l;
@@ -82,6 +108,67 @@ double oracle_splev_uniform(const double *t, int n, const double *c, int k, doub
     return sp;
 }
 
+/* First derivative of a spline, FITPACK splder with nu = 1 as called by
+ * splev_deriv_uniform (splines.f90:96-115, splder.f).  The derivative is a
+ * spline of degree k-1 on the same knots with coefficients
+ * w(i) = k (c(i+1) - c(i)) / (t(i+k+1) - t(i+1)) (left at c(i) where that knot
+ * span is not positive); the argument is clamped to [t(k+1), t(n-k)] and the
+ * knot interval found by a linear search, unlike splev_uniform. */
+double oracle_splder1(const double *t, int n, const double *c, int k, double x)
+{
+    int k1 = k + 1, nk1 = n - k1;
+    double tb = t[k1 - 1], te = t[nk1];
+    double arg = x < tb ? tb : (x > te ? te : x);
+    int l = k1, l1 = l + 1;
+    while (!(arg < t[l1 - 1] || l == nk1)) {
+        l = l1;
+        l1 = l + 1;
+    }
+    double h[6];
+    fpbspl(t, k - 1, arg, l, h);
+    double sp = 0.0;
+    int ll = l - k1;
+    for (int j = 1; j <= k; ++j) {
+        ++ll;  /* 1-based index of the derivative coefficient */
+        double fac = t[ll + k] - t[ll];
+        double w = fac > 0.0 ? k * (c[ll] - c[ll - 1]) / fac : c[ll - 1];
+        sp += w * h[j - 1];
+    }
+    return sp;
+}
+
+/* FITPACK splev / splder (nu = 0 or 1) with extrapolation (scipy's ext=0): the
+ * knot interval is searched with t(l) <= x < t(l+1), k+1 <= l <= n-k-1, and x
+ * is not clamped.  Used for the repulsive potentials. */
+double oracle_splev_ext(const double *t, int n, const double *c, int k, double x, int nu)
+{
+    int k1 = k + 1, nk1 = n - k1;
+    int l = k1, l1 = l + 1;
+    while (!(x < t[l1 - 1] || l == nk1)) {
+        l = l1;
+        l1 = l + 1;
+    }
+    double h[6];
+    double sp = 0.0;
+    int ll = l - k1;
+    if (nu == 0) {
+        fpbspl(t, k, x, l, h);
+        for (int j = 1; j <= k1; ++j) {
+            ++ll;
+            sp += c[ll - 1] * h[j - 1];
+        }
+    } else {
+        fpbspl(t, k - 1, x, l, h);
+        for (int j = 1; j <= k; ++j) {
+            ++ll;
+            double fac = t[ll + k] - t[ll];
+            double w = fac > 0.0 ? k * (c[ll] - c[ll - 1]) / fac : c[ll - 1];
+            sp += w * h[j - 1];
+        }
+    }
+    return sp;
+}
+
 /* ---- Slater-Koster angular rules ------------------------------------- */
 
 /* real spherical harmonic index m -> Cartesian axis (m=-1: y, 0: z, 1: x) */
@@ -98,6 +185,33 @@ double oracle_sk_rule(int l1, int m1, int l2, int m2, const double *e, const dou
     if (l1 == 1 && l2 == 0) return e[axis_of_m(m1)] * V[4];
     int a = axis_of_m(m1), b = axis_of_m(m2);
     return (a == b ? V[5] : 0.0) + e[a] * e[b] * (V[6] - V[5]);
+}
+
+/* Gradient of oracle_sk_rule with respect to the vector r e from centre 1 to
+ * centre 2 (the position of centre 2), given the SK integrals V and their
+ * radial derivatives Vd at r.  Chain rule through the direction cosines,
+ * d e_a / d r_k = (delta_ak - e_a e_k) / r, and the radius, d r / d r_k = e_k.
+ * Equivalent to slako_transformations_grad_lmax2.f90 for l<=1. */
+void oracle_sk_rule_grad(int l1, int m1, int l2, int m2, double r, const double *e, const double *V,
+                         const double *Vd, double *g)
+{
+    for (int k = 0; k < 3; ++k) {
+        double gk;
+        if (l1 == 0 && l2 == 0) {
+            gk = Vd[0] * e[k];
+        } else if (l1 == 0 && l2 == 1) {
+            int b = axis_of_m(m2);
+            gk = V[2] * ((b == k ? 1.0 : 0.0) - e[b] * e[k]) / r + e[b] * Vd[2] * e[k];
+        } else if (l1 == 1 && l2 == 0) {
+            int a = axis_of_m(m1);
+            gk = V[4] * ((a == k ? 1.0 : 0.0) - e[a] * e[k]) / r + e[a] * Vd[4] * e[k];
+        } else {
+            int a = axis_of_m(m1), b = axis_of_m(m2);
+            double ang = (a == k ? e[b] : 0.0) + (b == k ? e[a] : 0.0) - 2.0 * e[a] * e[b] * e[k];
+            gk = (V[6] - V[5]) * ang / r + ((a == b ? Vd[5] : 0.0) + e[a] * e[b] * (Vd[6] - Vd[5])) * e[k];
+        }
+        g[k] = gk;
+    }
 }
 
 /* Dipole element <l1 m1| r_c |l2 m2> (c: 0=x,1=y,2=z) with dipole SK integrals
@@ -232,6 +346,101 @@ void oracle_h0_and_s(int norb, int nat, const int *ind, const int *typ, const in
             S[(size_t)mu * norb + nu] = S[(size_t)nu * norb + mu];
             H0[(size_t)mu * norb + nu] = H0[(size_t)nu * norb + mu];
         }
+}
+
+/* ---- gradients of H0 and S ------------------------------------------------ */
+
+/* Derivative of the S and H0 elements of the ordered pair (mu, nu) (the reference's
+ * orientation: direction from the atom of mu to the atom of nu) with respect to
+ * the position of the atom of nu.  slako.f90:466-560. */
+static void pair_gradient(int mu, int nu, int nat, const int *ind, const int *typ, const int *ls, const int *ms,
+                          const double *pos, int deg, const int *tab_filled, const double *S_knots,
+                          const double *S_coefs, const double *H_knots, const double *H_coefs, int nsk, int npts,
+                          double *sg, double *hg)
+{
+    (void)nat;
+    int i = ind[mu], typi = typ[mu], l1 = ls[mu], m1 = ms[mu];
+    int j = ind[nu], typj = typ[nu], l2 = ls[nu], m2 = ms[nu];
+    double rij, e[3], Si[16], Hi[16], Sd[16], Hd[16];
+    pair_geometry(pos, i, j, &rij, e);
+    int tmin = typi < typj ? typi : typj, tmax = typi < typj ? typj : typi;
+    int ipair = tmax * (tmax + 1) / 2 + tmin;
+    for (int tab = 0; tab < nsk; ++tab) {
+        Si[tab] = Hi[tab] = Sd[tab] = Hd[tab] = 0.0;
+        if (tab_filled[ipair * nsk + tab] == 1) {
+            size_t b = ((size_t)ipair * nsk + tab) * npts;
+            Si[tab] = oracle_splev_uniform(S_knots + b, npts, S_coefs + b, deg, rij);
+            Hi[tab] = oracle_splev_uniform(H_knots + b, npts, H_coefs + b, deg, rij);
+            Sd[tab] = oracle_splder1(S_knots + b, npts, S_coefs + b, deg, rij);
+            Hd[tab] = oracle_splder1(H_knots + b, npts, H_coefs + b, deg, rij);
+        }
+    }
+    if (typi <= typj) {
+        oracle_sk_rule_grad(l1, m1, l2, m2, rij, e, Si, Sd, sg);
+        oracle_sk_rule_grad(l1, m1, l2, m2, rij, e, Hi, Hd, hg);
+    } else {
+        /* centres swapped: the rule is a function of -e, i.e. of pos_i - pos_j */
+        double me[3] = {-e[0], -e[1], -e[2]};
+        oracle_sk_rule_grad(l2, m2, l1, m1, rij, me, Si, Sd, sg);
+        oracle_sk_rule_grad(l2, m2, l1, m1, rij, me, Hi, Hd, hg);
+        for (int c = 0; c < 3; ++c) {
+            sg[c] = -sg[c];
+            hg[c] = -hg[c];
+        }
+    }
+}
+
+/* Test switch: when nonzero, the element (mu, nu) with mu < nu is differentiated
+ * in the orientation (nu, mu) that H0andS uses for its value (it fills the
+ * mu >= nu triangle and mirrors it), making gradients and matrices consistent
+ * even where a pair's s-p and p-s tables disagree.  The reference
+ * differentiates every ordered pair in its own orientation (default, 0). */
+int oracle_consistent_gradients = 0;
+
+/* slako.f90:402-569.  gradS, gradH0 are [3*nat][norb][norb]; element
+ * [3j+c][mu][nu] (and its mirror [3j+c][nu][mu]) receives the derivative of
+ * S_mu,nu with respect to coordinate c of atom j = ind[nu], for every ordered
+ * pair mu != nu on different, proximate atoms.  Spline values come from
+ * splev_uniform, their radial derivatives from splder. */
+void oracle_gradients_h0_and_s(int norb, int nat, const int *ind, const int *typ, const int *ls, const int *ms,
+                               const double *pos, const int *mprox, int deg, const int *tab_filled,
+                               const double *S_knots, const double *S_coefs, const double *H_knots,
+                               const double *H_coefs, int npair, int nsk, int npts, double *gradS, double *gradH0)
+{
+    (void)npair;
+    size_t plane = (size_t)norb * norb;
+    memset(gradS, 0, sizeof(double) * 3 * nat * plane);
+    memset(gradH0, 0, sizeof(double) * 3 * nat * plane);
+    /* parallel over the atom j that owns the derivative: each thread writes only planes 3j..3j+2 */
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int j = 0; j < nat; ++j) {
+        for (int nu = 0; nu < norb; ++nu) {
+            if (ind[nu] != j) continue;
+            for (int mu = 0; mu < norb; ++mu) {
+                int i = ind[mu];
+                if (mprox[(size_t)i * nat + j] == 0 || mu == nu || i == j) continue;
+                double sg[3], hg[3];
+                if (oracle_consistent_gradients && mu < nu) {
+                    pair_gradient(nu, mu, nat, ind, typ, ls, ms, pos, deg, tab_filled, S_knots, S_coefs, H_knots,
+                                  H_coefs, nsk, npts, sg, hg);
+                    for (int c = 0; c < 3; ++c) {
+                        sg[c] = -sg[c];
+                        hg[c] = -hg[c];
+                    }
+                } else {
+                    pair_gradient(mu, nu, nat, ind, typ, ls, ms, pos, deg, tab_filled, S_knots, S_coefs, H_knots,
+                                  H_coefs, nsk, npts, sg, hg);
+                }
+                for (int c = 0; c < 3; ++c) {
+                    size_t pl = (size_t)(3 * j + c) * plane;
+                    gradS[pl + (size_t)mu * norb + nu] += sg[c];
+                    gradS[pl + (size_t)nu * norb + mu] += sg[c];
+                    gradH0[pl + (size_t)mu * norb + nu] += hg[c];
+                    gradH0[pl + (size_t)nu * norb + mu] += hg[c];
+                }
+            }
+        }
+    }
 }
 
 /* ---- dipole matrix ----------------------------------------------------- */

@@ -8,9 +8,14 @@ throw-away package under a temporary directory.  Modules run this way:
 * ``DFTB/Solver.py``            Casida, HermitianDavidson, nonHermitianDavidson, _ApBv, _AmBv
 * ``DFTB/GammaApproximation.py`` gaussian_decay, GammaGaussian, GammaGaussianLC, GammaMatrix
 * ``DFTB/ConvAcceleration.py``   DIIS_80
+* ``DFTB/ExcGradients.py``       Gradients.gradient (gradient_lc / gradient_nolc) with its
+                                 Python F and F^lr operators (SLAKO_IMPLEMENTATION = "PY");
+                                 gradS/gradH0 and the repulsive potentials are supplied by
+                                 the oracle, the gamma gradients come from DFTBaby's own
+                                 GammaMatrix.gamma_AOwise
 
-The Slater-Koster angular rules (``DFTB/extensions/slako_transformations_lmax2.f90``
-and ``..._dipole_lmax2.f90``) are Fortran ``SELECT CASE`` tables whose
+The Slater-Koster angular rules (``DFTB/extensions/slako_transformations_lmax2.f90``,
+``..._dipole_lmax2.f90`` and ``..._grad_lmax2.f90``) are Fortran ``SELECT CASE`` tables whose
 right-hand sides are also valid Python expressions; they are evaluated here for
 random directions and table values.
 
@@ -81,16 +86,26 @@ def load_reference_modules(ref_root):
     pkg = os.path.join(tmp, "DFTB")
     os.makedirs(os.path.join(pkg, "extensions"))
     open(os.path.join(pkg, "__init__.py"), "w").close()
-    open(os.path.join(pkg, "extensions", "__init__.py"), "w").write("tddftb = None\n")
+    open(os.path.join(pkg, "extensions", "__init__.py"), "w").write("tddftb = None\nslako = None\ngrad = None\n")
+    os.makedirs(os.path.join(pkg, "SlaterKoster"))
+    open(os.path.join(pkg, "SlaterKoster", "__init__.py"), "w").close()
+    open(os.path.join(pkg, "SlaterKoster", "SKIntegrals.py"), "w").write("combine_slako_tables_f90 = None\n")
+    open(os.path.join(pkg, "SKMatrixElements.py"), "w").write(
+        "SLAKO_IMPLEMENTATION = 'PY'\natomlist2orbitals = None\n")
+    open(os.path.join(pkg, "DiskMemory.py"), "w").write(
+        "class _M:\n    def memmap(self, f):\n        return f\nGlobalDiskMemory = _M()\n")
+    for stub in ("XYZ", "utils", "CPKS"):
+        open(os.path.join(pkg, stub + ".py"), "w").close()
     open(os.path.join(pkg, "Timer.py"), "w").write(
         "class _T:\n    def timer(self, f):\n        return f\nGlobalTimer = _T()\n")
     open(os.path.join(pkg, "AtomicData.py"), "w").write("atom_names = ['h','he','li','be','b','c']\n")
-    for name in ("Solver", "GammaApproximation", "ConvAcceleration"):
+    names = ("Solver", "GammaApproximation", "ConvAcceleration", "ExcGradients")
+    for name in names:
         src = open(os.path.join(ref_root, "DFTB", name + ".py")).read()
         open(os.path.join(pkg, name + ".py"), "w").write(py2to3(src))
     sys.path.insert(0, tmp)
     import importlib
-    mods = {n: importlib.import_module("DFTB." + n) for n in ("Solver", "GammaApproximation", "ConvAcceleration")}
+    mods = {n: importlib.import_module("DFTB." + n) for n in names}
     return tmp, mods
 
 
@@ -132,6 +147,91 @@ def make_sk_rules(ref_root, rng):
             dip_val[n, c] = eval(dip[tuple(key)], env)
     np.savez_compressed(os.path.join(HERE, "sk_rules.npz"), e=e, V=V, D=Dt, sh_keys=sh_keys, sh_val=sh_val,
                         dip_keys=dip_keys, dip_val=dip_val)
+
+
+def sk_grad_rule_cases(ref_root):
+    """{(l1,m1,l2,m2): {c: expr}} from slako_transformations_grad_lmax2.f90 (s and p only)."""
+    src = open(os.path.join(ref_root, "DFTB", "extensions", "slako_transformations_grad_lmax2.f90")).read()
+    src = re.sub(r"&\s*\n\s*&?", "", src)   # join Fortran continuation lines
+    pat = re.compile(r"CASE \((\d+)\)\s*\n\s*! \(([^)]*)\)\s*\n\s*grad\((\d)\) = ([^\n]*)")
+    cases = {}
+    for _, tup, c, expr in pat.findall(src):
+        key = tuple(int(v) for v in tup.split(","))
+        if key[0] <= 1 and key[2] <= 1:
+            cases.setdefault(key, {})[int(c) - 1] = expr
+    return cases
+
+
+def make_sk_grad_rules(ref_root, rng):
+    cases = sk_grad_rule_cases(ref_root)
+    ndir = 16
+    e = rng.normal(size=(ndir, 3))
+    e /= np.linalg.norm(e, axis=1)[:, None]
+    r = rng.uniform(1.0, 8.0, size=ndir)
+    V = rng.normal(size=(ndir, 7))
+    Vd = rng.normal(size=(ndir, 7))
+    keys = np.array(sorted(cases), dtype=np.int64)
+    val = np.zeros((ndir, len(keys), 3))
+    for n in range(ndir):
+        env = dict(x=e[n, 0], y=e[n, 1], z=e[n, 2], r=r[n], sqrt3=np.sqrt(3.0))
+        env["SorH"] = lambda k, n=n: V[n, k - 1]
+        env["SorHd"] = lambda k, n=n: Vd[n, k - 1]
+        for j, key in enumerate(keys):
+            for c in range(3):
+                val[n, j, c] = eval(cases[tuple(key)][c], env)
+    np.savez_compressed(os.path.join(HERE, "sk_grad_rules.npz"), e=e, r=r, V=V, Vd=Vd, keys=keys, val=val)
+
+
+def make_gradients(mods, rng):
+    """DFTBaby's ExcGradients.Gradients.gradient on a seeded C4H6, lc on and off, states 0, 1, 2."""
+    EG, GA = mods["ExcGradients"], mods["GammaApproximation"]
+    sys.path.insert(0, REPO)
+    from dftbaby_b200 import geometry
+    from oracle import dftb_oracle as O
+    from oracle import gradients_oracle as G
+
+    class _Vrep:
+        def __init__(self, par, Z1, Z2):
+            self.par, self.Z1, self.Z2 = par, Z1, Z2
+
+        def getVrep(self, R, deriv=0):
+            return self.par.getVrep(self.Z1, self.Z2, R, deriv)
+
+    al = geometry.polyene(4, sigma=0.05, seed=7)
+    out = {"Z": np.array([z for z, _ in al]), "pos": np.array([p for _, p in al])}
+    for lc in (1, 0):
+        td = O.LR_TDDFTB(al, long_range_correction=lc)
+        td.setGeometry(al)
+        td.getEnergies(nstates=4, diag_conv=1.0e-10, diag_maxiter=200)
+        d = td.dftb2
+        gS, gH = G.gradients_H0andS(d)
+        EG.gradients_H0andS = lambda *a, **k: (gS, gH)
+        fd = types.SimpleNamespace()
+        fd.atomlist = d.atomlist
+        fd.getGeometry = lambda: d.atomlist
+        fd.valorbs = d.valorbs
+        fd.distances, fd.directions = d.distances, d.directions
+        sig = GA.gaussian_decay(d.par.hubbard_U, d.valorbs, d.long_range_radius, lc, verbose=0)
+        fd.gm = GA.GammaMatrix(GA.GammaGaussian(sig))
+        fd.gm_lc = GA.GammaMatrix(GA.GammaGaussianLC(sig, d.long_range_radius))
+        fd.getKSEnergies, fd.getKSCoefficients = (lambda: d.orbe), (lambda: d.orbs)
+        fd.verbose, fd.SKT, fd.Mproximity, fd.S = 0, None, d.Mproximity, d.S
+        fd.density_matrix_ref = d.density_matrix_ref
+        fd.lc_implementation, fd.long_range_correction = None, lc
+        fd.VREP = {(a, b): _Vrep(d.par, a, b) for (a, b) in d.par.vrep}
+        ft = types.SimpleNamespace(dftb2=fd, ct_correction=0)
+        ft.getActiveOrbitals = lambda: (td.active_occupied_orbs, td.active_virtual_orbs)
+        ft.hasActiveSpace = lambda: False
+        ft.getXY = lambda: (td.XmY, td.XpY)
+        ft.getExcEnergies = lambda: td.Omega
+        ft.getTransitionCharges = lambda: (td.qtrans_oo, td.qtrans_vv, td.qtrans_ov)
+        grads = EG.Gradients(ft)
+        for I in (0, 1, 2):
+            gV, gE, gX = grads.gradient(I=I)
+            tag = "lc%d_I%d" % (lc, I)
+            out[tag + "_Vrep"], out[tag + "_E0"], out[tag + "_Exc"] = gV, gE, gX
+        out["lc%d_Omega" % lc] = td.Omega
+    np.savez_compressed(os.path.join(HERE, "gradients_c4h6.npz"), **out)
 
 
 def make_gamma(mods, rng):
@@ -221,6 +321,8 @@ def main(ref_root):
         make_gamma(mods, rng)
         make_diis(mods, rng)
         make_solvers(mods, rng)
+        make_sk_grad_rules(ref_root, rng)
+        make_gradients(mods, rng)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)
