@@ -5,7 +5,6 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "lib", "libdftbaby_b200.so")
-SRC = os.path.join(HERE, "csrc", "dftb_kernels.cu")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 
@@ -19,10 +18,12 @@ def _nvcc():
 
 def build_native(force=False, verbose=False):
     """Compile csrc/*.cu into lib/libdftbaby_b200.so when sources are newer."""
-    srcs = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc")) if f.endswith(".cu")]
+    csrc = os.path.join(HERE, "csrc")
+    srcs = [os.path.join(csrc, f) for f in os.listdir(csrc) if f.endswith(".cu")]
+    deps = [os.path.join(csrc, f) for f in os.listdir(csrc) if f.endswith(".cuh")]
     hdr = os.path.join(ROOT, "include", "dftbaby_b200.h")
     if not force and os.path.exists(LIB):
-        newest = max(os.path.getmtime(p) for p in srcs + [hdr])
+        newest = max(os.path.getmtime(p) for p in srcs + deps + [hdr])
         if os.path.getmtime(LIB) >= newest:
             return LIB
     os.makedirs(os.path.dirname(LIB), exist_ok=True)

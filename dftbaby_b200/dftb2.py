@@ -150,6 +150,7 @@ class DFTB2(object):
         self._opa = i32(self.orbsPerAtom)
         self.pos = f64([p for _, p in self.atomlist]).reshape(-1, 3).contiguous()
         self._sigma = f64([self.par.sigmas[Z] for Z, _ in self.atomlist])
+        self._atype = i32([self.par.atom_type[Z] for Z, _ in self.atomlist])
         self._U = f64([self.hubbard_U[Z] for Z, _ in self.atomlist])
 
     def getGeometry(self):
@@ -167,6 +168,7 @@ class DFTB2(object):
         x, y, z = torch.empty_like(r), torch.empty_like(r), torch.empty_like(r)
         native.call("dftb_directional_cosines", nat, P(self.pos), P(r), P(x), P(y), P(z), st)
         self.distances = r
+        self._dircos = (r, x, y, z)
         mprox = (r < self.distance_cutoff).to(torch.int32)
         mprox.fill_diagonal_(1)
         self.Mproximity = mprox
@@ -230,17 +232,27 @@ class DFTB2(object):
         return -E / 8.0
 
     def getEnergies(self):
-        """E_bs, E_coulomb, E_elec, E_nuc, E_tot (DFTB2.py:2235-2276); repulsive
-        potentials are not part of this path, E_nuc = 0."""
+        """E_bs, E_coulomb, E_elec, E_nuc, E_tot (DFTB2.py:2235-2276); E_nuc is the
+        repulsive energy (no dispersion, QM/MM or cavity terms on this path)."""
         self.E_bs = torch.sum(self.P * self.H0).item()
         self.E_coulomb = 0.5 * torch.dot(self.dq, self.gamma @ self.dq).item()
         self.E_elec = self.E_bs + self.E_coulomb
         if self.long_range_correction == 1:
             self.E_HF_x = self.lc_exchange_energy().item()
             self.E_elec += self.E_HF_x
-        self.E_nuc = 0.0
+        self.E_nuc = self.getRepulsiveEnergy()
         self.E_tot = self.E_elec + self.E_nuc
         return self.E_bs, self.E_coulomb, self.E_elec, self.E_nuc, self.E_tot
+
+    def getRepulsiveEnergy(self):
+        """Sum of the pair repulsive potentials (DFTB2.getRepulsiveEnergy, DFTB2.py:2339-2359)."""
+        nat = len(self.atomlist)
+        t = self.par.device_tables(self.device)
+        e = torch.empty(nat, dtype=torch.float64, device=self.device)
+        P = native.ptr
+        native.call("dftb_repulsive_energy", nat, P(self.pos), P(self._atype), P(t["vrep_knots"]),
+                    P(t["vrep_coefs"]), P(t["vrep_dmax"]), self.par.vrep_nknots, P(e), native.stream())
+        return float(e.sum().item())
 
     def getEnergy(self, **scf_opts):
         """DFTB2.getEnergy (DFTB2.py:2278-2338)."""

@@ -64,6 +64,13 @@ _SIGNATURES = {
     "dftb_split_bf16": (_I, [_I, _I, _P, _I, _I, _P, _P, _I, _P]),
     "dftb_split_bf16_f64": (_I, [_I, _I, _P, _I, _I, _D, _P, _P, _I, _P]),
     "dftb_tc_last_error": (ctypes.c_char_p, []),
+    "dftb_gradients_h0_and_s": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _I, _I,
+                                     _I, _P, _P, _P]),
+    "dftb_sk_gradient_contract": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _I, _I,
+                                       _I, _P, _P, _P, _P]),
+    "dftb_pair_gradients": (_I, [_I, _P, _P, _P, _D, _P, _P, _P, _P, _P, _I, _P, _P]),
+    "dftb_repulsive_energy": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),
+    "dftb_grad_last_error": (ctypes.c_char_p, []),
 }
 
 
@@ -101,7 +108,9 @@ def stream():
 
 def check(rc, what):
     if rc != DFTB_OK:
-        msg = _lib.dftb_last_error().decode() if _lib is not None else ""
+        msg = ""
+        if _lib is not None:
+            msg = _lib.dftb_last_error().decode() or _lib.dftb_grad_last_error().decode()
         raise NativeError("%s failed (%s): %s" % (what, _ERRORS.get(rc, rc), msg))
 
 
@@ -111,6 +120,8 @@ KERNELS_PER_CALL = {
     "dftb_ao_expand": 1, "dftb_scc_hamiltonian": 2, "dftb_monopoles": 1, "dftb_trans_charges": 6,
     "dftb_trans_charges_diag": 5, "dftb_trans_charges_noalloc": 6, "dftb_hermitian_rv": 3, "dftb_apbv": 3, "dftb_ambv": 1,
     "dftb_davidson_precondition": 1, "dftb_davidson_residual": 2, "dftb_dgemm": 1,
+    "dftb_gradients_h0_and_s": 3, "dftb_sk_gradient_contract": 1, "dftb_pair_gradients": 1,
+    "dftb_repulsive_energy": 1,
 }
 
 

@@ -93,6 +93,25 @@ class Parametrization:
             else:
                 self.D_knots[ipair, idx], self.D_coefs[ipair, idx] = t, c
                 self.tab_filled_D[ipair, idx] = 1
+        # repulsive potentials: interpolating cubic splines of the tabulated Vrep
+        # (RepulsivePotential.__init__, RepulsivePotential.py:21-78); all pairs share one knot count
+        vfits = {}
+        for a in range(ntype):
+            for b in range(a, ntype):
+                Zi, Zj = self.atomtypes[a], self.atomtypes[b]
+                tag = "%s_%s" % (ELEMENT_NAMES[Zi], ELEMENT_NAMES[Zj])
+                d, V = raw["vrep/%s/d" % tag], raw["vrep/%s/Vrep" % tag]
+                t, c, _ = splrep(d, V, s=0)
+                vfits[b * (b + 1) // 2 + a] = (t, c, float(d.max()))
+        nk = max(len(t) for t, _, _ in vfits.values())
+        if any(len(t) != nk for t, _, _ in vfits.values()):
+            raise ValueError("repulsive-potential grids of different lengths are not supported")
+        self.vrep_nknots = nk
+        self.vrep_knots = np.zeros((self.npair, nk))
+        self.vrep_coefs = np.zeros((self.npair, nk))
+        self.vrep_dmax = np.zeros(self.npair)
+        for ipair, (t, c, dmax) in vfits.items():
+            self.vrep_knots[ipair], self.vrep_coefs[ipair], self.vrep_dmax[ipair] = t, c, dmax
         self._device = {}
 
     def device_tables(self, device):
@@ -104,5 +123,6 @@ class Parametrization:
             self._device[key] = dict(
                 S_knots=f64(self.S_knots), S_coefs=f64(self.S_coefs), H_knots=f64(self.H_knots),
                 H_coefs=f64(self.H_coefs), D_knots=f64(self.D_knots), D_coefs=f64(self.D_coefs),
-                tab_filled_SH0=i32(self.tab_filled_SH0), tab_filled_D=i32(self.tab_filled_D))
+                tab_filled_SH0=i32(self.tab_filled_SH0), tab_filled_D=i32(self.tab_filled_D),
+                vrep_knots=f64(self.vrep_knots), vrep_coefs=f64(self.vrep_coefs), vrep_dmax=f64(self.vrep_dmax))
         return self._device[key]

@@ -222,6 +222,63 @@ const char *dftb_tc_last_error(void);
 int dftb_dgemm(int transa, int transb, int m, int n, int k, double alpha, const double *A, int lda,
                const double *B, int ldb, double beta, double *C, int ldc, void *stream);
 
+/* ---- analytic gradients (DFTB/ExcGradients.py) ------------------------------ */
+
+/* Dense gradients of S and H0.
+ * Replaces slako.gradients_h0ands (DFTB/extensions/slako.f90:402-569, called
+ * from ExcGradients._gradients_H0andS_f90, ExcGradients.py:151-177) with its
+ * spline values from splev_uniform and radial derivatives from FITPACK splder
+ * (splines.f90:96-115).  Arguments as dftb_h0_and_s (without orben);
+ * gradS, gradH0: (3 nat, norb, norb), element [3j+c][mu][nu] (and its mirror
+ * [3j+c][nu][mu]) = derivative of S_mu,nu with respect to coordinate c of the
+ * atom j of nu, in the orientation of the ordered pair (mu, nu); zero
+ * elsewhere.  norb <= 65535. */
+int dftb_gradients_h0_and_s(int norb, int nat, const int *ind, const int *typ, const int *ls, const int *ms,
+                            const double *r, const double *x, const double *y, const double *z, const int *mprox,
+                            int deg, const int *tab_filled, const double *S_knots, const double *S_coefs,
+                            const double *H_knots, const double *H_coefs, int npair, int nsk, int npts,
+                            double *gradS, double *gradH0, void *stream);
+
+/* Contraction of the same derivatives with adjoint matrices, without forming
+ * the dense tensors:
+ *   grad[3j+c] = sum_{nu on j} sum_{mu on other atoms} dS_mu,nu/dR_j,c XS[mu][nu]
+ *                                                    + dH0_mu,nu/dR_j,c XH[mu][nu].
+ * With XS = X + X^T this equals sum_{mu,nu} gradS[3j+c][mu][nu] X[mu][nu], the
+ * np.tensordot(gradS, X, axes=([1,2],[0,1])) of ExcGradients.py:501-506, 704-705.
+ * XS or XH may be NULL (term skipped).  grad: (3 nat), overwritten. */
+int dftb_sk_gradient_contract(int norb, int nat, const int *ind, const int *typ, const int *ls, const int *ms,
+                              const double *r, const double *x, const double *y, const double *z, const int *mprox,
+                              int deg, const int *tab_filled, const double *S_knots, const double *S_coefs,
+                              const double *H_knots, const double *H_coefs, int npair, int nsk, int npts,
+                              const double *XS, const double *XH, double *grad, void *stream);
+
+/* Atom-pair gradient terms:
+ *   grad[3i+c] = sum_{j != i} [ g1(R_ij) Yg[i][j] + g1lr(R_ij) Ylr[i][j] + Vrep'(R_ij) ] (R_i - R_j)_c / R_ij
+ * with g1, g1lr the radial derivatives of the Gaussian gamma and long-range
+ * gamma (GammaGaussian.g_deriv, GammaGaussianLC.g_deriv,
+ * GammaApproximation.py:141-148, 234-238; sigma per atom, r_lr the long-range
+ * radius) and Vrep' the derivative of the repulsive potential of the pair
+ * (gradient_Vrep, ExcGradients.py:181-211).  With Y = A + A^T for atom-block
+ * sums A this is the contraction of GammaMatrix.gamma_AOwise's g1_AO / g1_AT
+ * (GammaApproximation.py:406-447) with A.  Yg, Ylr: (nat, nat) or NULL;
+ * vrep_knots / vrep_coefs: (npair, nknots) cubic FITPACK splines, pair index
+ * tmax*(tmax+1)/2 + tmin of the atom types atype (nat), vrep_dmax (npair) the
+ * last grid point (Vrep = 0 from there on), or vrep_knots = NULL to skip the
+ * repulsive term.  grad: (3 nat), overwritten. */
+int dftb_pair_gradients(int nat, const double *pos, const int *atype, const double *sigma, double r_lr,
+                        const double *Yg, const double *Ylr, const double *vrep_knots, const double *vrep_coefs,
+                        const double *vrep_dmax, int nknots, double *grad, void *stream);
+
+/* Repulsive energy per atom, e_atom[i] = 1/2 sum_{j != i} Vrep(R_ij); the sum
+ * over atoms is DFTB2.getRepulsiveEnergy (DFTB2.py:2339-2359).  Tables as in
+ * dftb_pair_gradients. */
+int dftb_repulsive_energy(int nat, const double *pos, const int *atype, const double *vrep_knots,
+                          const double *vrep_coefs, const double *vrep_dmax, int nknots, double *e_atom,
+                          void *stream);
+
+/* Error string of the last failing gradient entry point on this host thread. */
+const char *dftb_grad_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
