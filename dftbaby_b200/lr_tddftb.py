@@ -28,7 +28,7 @@ import torch
 
 from . import native
 from .dftb2 import DFTB2
-from .exceptions import ExcitedStatesError
+from .exceptions import ExcitedStatesError, ExcitedStatesNotConverged
 from .solver import hermitian_davidson, nonhermitian_davidson
 
 
@@ -250,13 +250,17 @@ class LR_TDDFTB:
     def getEnergies(self, nr_active_occ=None, nr_active_virt=None, select_lm=None, oszis="Dipoles",
                     response_method="Casida", multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5,
                     diag_maxiter=50, diag_check=0, diag_L2threshold=0.0, diag_selected_irreps=None,
-                    ct_correction=0, stability=0, precision="fp64", refine_fp64=True, **scf_opts):
+                    ct_correction=0, stability=0, precision="fp64", refine_fp64=True, guess_model=None, **scf_opts):
         """LR_TDDFTB.getEnergies (LR_TDDFTB.py:37-114); returns (Omega, f) in Hartree.
 
         precision="mixed" (not in DFTBaby) evaluates the long-range exchange of
         the Davidson products with split-precision BF16 tensor-core GEMMs; with
         refine_fp64 the mixed result then seeds the FP64 solver, whose residual
         test (diag_conv) decides convergence as in the plain path.
+        guess_model (not in DFTBaby): a learned.GuessNet whose pair scores choose
+        the initial Davidson vectors and whose shifts correct the diagonal
+        preconditioner when no warm start is available; the solve runs to the
+        same residual threshold, and the plain start is used if it fails.
         """
         if select_lm is not None:
             raise ValueError("select_lm is not implemented")
@@ -277,7 +281,8 @@ class LR_TDDFTB:
             assert nstates > 0, "nstates==0, no excited states can be calculated!"
         self._solve_lr_equations(multiplicity=multiplicity, nstates=nstates, diag_ifact=diag_ifact,
                                  diag_conv=diag_conv, diag_maxiter=diag_maxiter, diag_check=diag_check,
-                                 diag_L2threshold=diag_L2threshold, precision=precision, refine_fp64=refine_fp64)
+                                 diag_L2threshold=diag_L2threshold, precision=precision, refine_fp64=refine_fp64,
+                                 guess_model=guess_model)
         ev[2].record()
         if oszis == "Dipoles":
             self._TransitionDipoles()
@@ -297,7 +302,8 @@ class LR_TDDFTB:
                 "properties": ev[2].elapsed_time(ev[3])}
 
     def _solve_lr_equations(self, multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5, diag_maxiter=50,
-                            diag_check=0, diag_L2threshold=0.0, precision="fp64", refine_fp64=True):
+                            diag_check=0, diag_L2threshold=0.0, precision="fp64", refine_fp64=True,
+                            guess_model=None):
         """LR_TDDFTB._solve_lr_equations (LR_TDDFTB.py:403-527)."""
         d = self.dftb2
         dev = d.device
@@ -313,6 +319,11 @@ class LR_TDDFTB:
         XmY0 = XpY0 = Om0 = None
         if torch.is_tensor(self.XpY) and self.XpY.shape == (nstates or -1, self.nocc, self.nvirt):
             XmY0, XpY0, Om0 = self.XmY, self.XpY, self._Omega_dev
+        learned = {}
+        if guess_model is not None and XpY0 is None and nstates is not None:
+            from . import learned as _learned
+            learned["guess_key"], learned["precond_diag"] = _learned.guess_inputs(guess_model, self)
+        self.stats["learned_start"] = bool(learned)
         if nstates is None:
             Om, C, XmY, XpY = self._casida(multiplicity)
         elif not lc:
@@ -328,9 +339,12 @@ class LR_TDDFTB:
                             native.ptr(ws), ws.numel(), native.stream())
                 return U
 
-            Om, C, XmY, XpY = hermitian_davidson(rv, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
-                                                 maxiter=diag_maxiter, XpYguess=XpY0, Oia=self.Oia,
-                                                 L2_thresh=diag_L2threshold, stats=self.stats)
+            def run(extra):
+                return hermitian_davidson(rv, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
+                                          maxiter=diag_maxiter, XpYguess=XpY0, Oia=self.Oia,
+                                          L2_thresh=diag_L2threshold, stats=self.stats, **extra)
+
+            Om, C, XmY, XpY = self._with_fallback(run, learned)
         else:
             Co, Cv = self._active_coefficients()
             prod = ExchangeAO(d.gamma, d.G_lr, self.qtrans_ov, self.omega.reshape(-1), Co, Cv, d.S,
@@ -342,18 +356,21 @@ class LR_TDDFTB:
                 mstats = {}
                 Om, C, XmY, XpY = nonhermitian_davidson(mixed, self.omega, nstates, ifact=diag_ifact,
                                                         conv=diag_conv, maxiter=diag_maxiter, XmYguess=XmY0,
-                                                        XpYguess=XpY0, w_guess=Om0, stats=mstats, symmetrize=True)
+                                                        XpYguess=XpY0, w_guess=Om0, stats=mstats, symmetrize=True,
+                                                        **learned)
                 tcgemm.check_errors(dev)
                 self.stats["mixed"] = {k: v for k, v in mstats.items() if k != "residual_norms"}
                 self.stats["mixed_products"] = mixed.products_applied
                 XmY0, XpY0, Om0, C0 = XmY, XpY, Om, C
                 del mixed
             if precision != "mixed" or refine_fp64:
-                Om, C, XmY, XpY = nonhermitian_davidson(prod, self.omega, nstates, ifact=diag_ifact,
-                                                        conv=diag_conv, maxiter=diag_maxiter, XmYguess=XmY0,
-                                                        XpYguess=XpY0, w_guess=Om0, stats=self.stats,
-                                                        accept_guess=(precision == "mixed"),
-                                                        Cguess=C0 if precision == "mixed" else None)
+                def run(extra):
+                    return nonhermitian_davidson(prod, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
+                                                 maxiter=diag_maxiter, XmYguess=XmY0, XpYguess=XpY0, w_guess=Om0,
+                                                 stats=self.stats, accept_guess=(precision == "mixed"),
+                                                 Cguess=C0 if precision == "mixed" else None, **extra)
+
+                Om, C, XmY, XpY = self._with_fallback(run, learned if XpY0 is None else {})
             self.stats["products"] = prod.products_applied
         self._Omega_dev = Om
         self.Omega = Om.cpu().numpy()
@@ -363,6 +380,16 @@ class LR_TDDFTB:
             err = np.sum(np.abs(self.Omega - Om_full[:nstates].cpu().numpy()))
             if err >= 1.0e-10:
                 raise ExcitedStatesError("eigenvalues differ, err = %s" % err)
+
+    def _with_fallback(self, run, learned):
+        """Run the Davidson solver with the learned start; on failure repeat it with DFTBaby's start."""
+        if not learned:
+            return run({})
+        try:
+            return run(learned)
+        except (ExcitedStatesNotConverged, ExcitedStatesError):
+            self.stats["learned_start"] = False
+            return run({})
 
     def _casida(self, multiplicity):
         """Full diagonalisation, Solver.Casida (Solver.py:98-181), on the device."""

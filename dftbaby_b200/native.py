@@ -71,6 +71,12 @@ _SIGNATURES = {
     "dftb_pair_gradients": (_I, [_I, _P, _P, _P, _D, _P, _P, _P, _P, _P, _I, _P, _P]),
     "dftb_repulsive_energy": (_I, [_I, _P, _P, _P, _P, _P, _I, _P, _P]),
     "dftb_grad_last_error": (ctypes.c_char_p, []),
+    "dftb_mlp_bias_relu": (_I, [_I, _I, _P, _I, _P, _P, _I, _P, _I, _P]),
+    "dftb_mlp_relu_backward": (_I, [_I, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P]),
+    "dftb_mlp_output": (_I, [_I, _I, _P, _I, _P, _P, _P, _P, ctypes.c_float, _P, _P, _I, _P, _I, _P, _P, _P]),
+    "dftb_mlp_adam": (_I, [_I, _I, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                           _I, ctypes.c_float, _P, _I, _P, _I, _P]),
+    "dftb_mlp_last_error": (ctypes.c_char_p, []),
 }
 
 
@@ -110,7 +116,8 @@ def check(rc, what):
     if rc != DFTB_OK:
         msg = ""
         if _lib is not None:
-            msg = _lib.dftb_last_error().decode() or _lib.dftb_grad_last_error().decode()
+            msg = (_lib.dftb_last_error().decode() or _lib.dftb_grad_last_error().decode()
+                   or _lib.dftb_mlp_last_error().decode())
         raise NativeError("%s failed (%s): %s" % (what, _ERRORS.get(rc, rc), msg))
 
 
@@ -121,7 +128,8 @@ KERNELS_PER_CALL = {
     "dftb_trans_charges_diag": 5, "dftb_trans_charges_noalloc": 6, "dftb_hermitian_rv": 3, "dftb_apbv": 3, "dftb_ambv": 1,
     "dftb_davidson_precondition": 1, "dftb_davidson_residual": 2, "dftb_dgemm": 1,
     "dftb_gradients_h0_and_s": 3, "dftb_sk_gradient_contract": 1, "dftb_pair_gradients": 1,
-    "dftb_repulsive_energy": 1,
+    "dftb_repulsive_energy": 1, "dftb_mlp_bias_relu": 1, "dftb_mlp_relu_backward": 1, "dftb_mlp_output": 1,
+    "dftb_mlp_adam": 1,
 }
 
 

@@ -129,11 +129,14 @@ def _precondition(W, src, state, w, omega_flat):
 
 
 def hermitian_davidson(rv, omega, nstates, ifact=1, conv=1.0e-14, maxiter=10, XpYguess=None, Oia=None,
-                       L2_thresh=0.0, stats=None):
+                       L2_thresh=0.0, stats=None, guess_key=None, precond_diag=None):
     """Lowest nstates of R T = Omega^2 T, R = (A-B)^1/2 (A+B) (A-B)^1/2.
 
     rv(V) returns R.V for a (nov, ncol) block.  Returns Omega (k), C, XmY, XpY
-    as (k, nocc, nvirt) device tensors.
+    as (k, nocc, nvirt) device tensors.  guess_key (nov) replaces omega in the
+    choice of the initial unit vectors (lowest key first) and precond_diag
+    (nov) replaces omega in the (w - omega) preconditioner; both default to
+    DFTBaby's omega.
     """
     nocc, nvirt = omega.shape
     om = omega.reshape(-1).contiguous()
@@ -141,8 +144,9 @@ def hermitian_davidson(rv, omega, nstates, ifact=1, conv=1.0e-14, maxiter=10, Xp
     lmax = min(ifact * nstates, kmax)
     k = nstates
     omega_sq = torch.sqrt(om)
+    pdiag = om if precond_diag is None else precond_diag.reshape(-1).contiguous()
     if XpYguess is None:
-        b0 = initial_expansion_vectors(om, lmax)
+        b0 = initial_expansion_vectors(om if guess_key is None else guess_key.reshape(-1), lmax)
     else:
         b0 = (XpYguess[:lmax].reshape(lmax, -1).T / omega_sq[:, None]).contiguous()
         b0 = b0 / torch.linalg.norm(b0, dim=0)
@@ -171,7 +175,7 @@ def hermitian_davidson(rv, omega, nstates, ifact=1, conv=1.0e-14, maxiter=10, Xp
         dkmax = min(kmax - l, k)
         eps = 0.01 * conv
         src = [n for n in range(dkmax) if norms[n] > eps]
-        Q = _precondition(W, src, src, w, om)
+        Q = _precondition(W, src, src, w, pdiag)
         Q = orthonormalize_new(bs, Q)
         B.append(Q, [rv(Q)])
         l = B.l
@@ -200,7 +204,7 @@ def _sqrtm_spd(M):
 
 def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxiter=10, XmYguess=None,
                           XpYguess=None, w_guess=None, stats=None, symmetrize=False, accept_guess=False,
-                          Cguess=None):
+                          Cguess=None, guess_key=None, precond_diag=None):
     """Lowest nstates of the non-Hermitian TD-DFTB problem (Stratmann-Scuseria-Frisch).
 
     products(V) returns ((A+B).V, (A-B).V) for a (nov, ncol) block.
@@ -214,15 +218,18 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
     Cguess then supplies the C vectors, which iteration 0 does not form).
     The guess block is orthonormalised before use -- DFTBaby orthonormalises
     the whole basis by QR at the end of iteration 0, which spans the same space.
+    guess_key and precond_diag replace omega in the choice of the initial unit
+    vectors and in the preconditioner, as in hermitian_davidson.
     """
     nocc, nvirt = omega.shape
     om = omega.reshape(-1).contiguous()
     kmax = nocc * nvirt
     k = nstates
     dev = om.device
+    pdiag = om if precond_diag is None else precond_diag.reshape(-1).contiguous()
     if XpYguess is None:
         lmax = min(ifact * nstates, kmax)
-        bs = initial_expansion_vectors(om, lmax)
+        bs = initial_expansion_vectors(om if guess_key is None else guess_key.reshape(-1), lmax)
     else:
         lmaxp = nstates
         lmaxm = min(nstates, kmax - nstates)
@@ -292,7 +299,7 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
                 src.append(k + n)
                 state.append(n)
         assert len(src) == dk
-        Q = _precondition(torch.cat([WL, WR], dim=1), src, state, w, om)
+        Q = _precondition(torch.cat([WL, WR], dim=1), src, state, w, pdiag)
         Q = orthonormalize_new(bs, Q)
         B.append(Q, list(products(Q)))
         l = B.l

@@ -279,6 +279,35 @@ int dftb_repulsive_energy(int nat, const double *pos, const int *atype, const do
 /* Error string of the last failing gradient entry point on this host thread. */
 const char *dftb_grad_last_error(void);
 
+/* ---- learned Davidson guess: MLP element-wise kernels ------------------------
+ * No counterpart in DFTBaby: the small network that scores excitation pairs
+ * for the initial Davidson vectors and corrects the diagonal preconditioner.
+ * Its matrix products run through dftb_bf16x3_gemm_ex (one BF16 segment, FP32
+ * accumulation); these kernels do the work in between.  Activations and
+ * weight copies are BF16 (passed as void *), everything else FP32; row-major. */
+
+/* H = relu(Z + b) for ns samples x nh units; H (ldh) and, unless HT is NULL,
+ * H^T (nh x ns, ldht). */
+int dftb_mlp_bias_relu(int ns, int nh, const float *Z, int ldz, const float *b, void *H, int ldh, void *HT, int ldht,
+                       void *stream);
+/* dZ = G o (H > 0): dZ (optional, ldz) and dZ^T (nh x ns, lddzt); db += column sums of dZ. */
+int dftb_mlp_relu_backward(int ns, int nh, const float *G, int ldg, const void *H, int ldh, void *dZ, int lddz,
+                           void *dZT, int lddzt, float *db, void *stream);
+/* Y = Z[:, :no] + b (ns x no, FP32).  With targets T (ns x no), sample weights m (ns)
+ * and output weights wout (no): loss += sum wout m (Y - T)^2 * inv_norm (FP64 scalar),
+ * dY = 2 wout m (Y - T) inv_norm into dYp (ns x lddy) and rows 0..no-1 of dYT
+ * (lddyt), db += column sums of dY.  T = NULL: inference only.  no <= 8. */
+int dftb_mlp_output(int ns, int no, const float *Z, int ldz, const float *b, const float *T, const float *m,
+                    const float *wout, float inv_norm, float *Y, void *dYp, int lddy, void *dYT, int lddyt, float *db,
+                    double *loss, void *stream);
+/* One Adam step (bias-corrected for step >= 1, decoupled weight decay) on FP32
+ * master weights W (rows x cols) with moments m1, m2; refreshes the BF16 copies
+ * Wb (row-major) and WbT (transposed) where given. */
+int dftb_mlp_adam(int rows, int cols, float *W, const float *G, float *m1, float *m2, float lr, float beta1,
+                  float beta2, float eps, int step, float weight_decay, void *Wb, int ldwb, void *WbT, int ldwbt,
+                  void *stream);
+const char *dftb_mlp_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
