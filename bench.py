@@ -52,6 +52,9 @@ WORKLOADS = {
                         opts=dict(nstates=8, diag_conv=1.0e-6, diag_maxiter=100)),
     "polyene20": dict(kind="polyene", n=20, sigma=0.02, lc=0,
                       opts=dict(nstates=10, diag_conv=1.0e-6, diag_maxiter=100)),
+    # learned Davidson start on held-out hexagonal flakes (n = 4..7: 120-336 atoms)
+    "guess": dict(kind="guess", flakes=(4, 5, 6, 7), polyenes=(40, 60), sigma=0.01, lc=1,
+                  opts=dict(nstates=10, diag_conv=1.0e-6, diag_maxiter=200)),
 }
 
 
@@ -83,6 +86,14 @@ def build_geometry(w, seed):
 
 def workload_config(name, w, n_gpus, precision="fp64"):
     from dftbaby_b200 import geometry
+    if w["kind"] == "guess":
+        return {"workload": "%s: learned Davidson start vs plain start, held-out seeded hexagonal flakes %s, "
+                            "lc-TD-DFTB" % (name, ", ".join(geometry.formula(geometry.hexagonal_flake(n))
+                                                            for n in w["flakes"])),
+                "nstates": w["opts"]["nstates"], "davidson_residual": w["opts"]["diag_conv"],
+                "sigma_angstrom": w["sigma"], "precision": "fp64",
+                "model": "GuessNet 64-256-256-2 trained on 20k eigenvectors of seeded polyenes C10-C60",
+                "parallelism": "replicas x%d" % n_gpus}
     if w["kind"] == "ensemble":
         mols = build_geometry(w, 0)
         norbs = [sum(1 if z == 1 else 4 for z, _ in al) for al in mols]
@@ -300,6 +311,64 @@ def run_ensemble(args, w, rank, world, barrier):
         print(json.dumps(line), flush=True)
 
 
+def run_guess(args, w, rank, world, barrier):
+    """Held-out flakes solved from the learned start and from DFTBaby's start (same FP64 solver,
+    same residual threshold); device time of the excited-state phase and Davidson iterations."""
+    import torch
+    from dftbaby_b200 import LR_TDDFTB, geometry, learned, native
+    net = learned.GuessNet.load(args.model or learned.DEFAULT_MODEL)
+    opts = w["opts"]
+
+    def solve(al, model):
+        td = LR_TDDFTB(al, long_range_correction=w["lc"])
+        td.setGeometry(al)
+        Om, _ = td.getEnergies(guess_model=model, **opts)
+        return td, Om
+
+    flakes = [geometry.hexagonal_flake(n, sigma=w["sigma"], seed=500 + n + 17 * rank) for n in w["flakes"]]
+    # in-distribution check: polyenes longer than most training molecules, seeds not used in training
+    extra = [geometry.polyene(n, sigma=0.03, seed=900 + n + 17 * rank) for n in w["polyenes"]]
+    barrier()
+    native.counters.reset()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
+    sampler.start()
+    rows, t_learned, t_plain = [], 0.0, 0.0
+    for al in flakes + extra:
+        row = {"formula": geometry.formula(al), "held_out": "flake" if al in flakes else "polyene"}
+        try:
+            # one untimed pass of each start first, so that neither pays the first-use allocations
+            solve(al, net)
+            solve(al, None)
+            tdl, Ol = solve(al, net)
+            tdp, Op = solve(al, None)
+        except Exception as exc:  # e.g. (A-B) not positive definite: the flake is singlet-unstable
+            row["skipped"] = str(exc)[:120]
+            rows.append(row)
+            continue
+        ml, mp = tdl.phase_ms()["excited_states"], tdp.phase_ms()["excited_states"]
+        if al in flakes:
+            t_learned += ml
+            t_plain += mp
+        row.update(iterations_learned=tdl.stats["iterations"], iterations_plain=tdp.stats["iterations"],
+                   learned_start_used=tdl.stats["learned_start"], excited_ms_learned=ml, excited_ms_plain=mp,
+                   max_dOmega_meV=float(np.abs(Ol - Op).max()) * 27211.396132)
+        rows.append(row)
+    barrier()
+    clocks = sampler.stop()
+    done = [r for r in rows if "skipped" not in r and r["held_out"] == "flake"]
+    nst = opts["nstates"] * len(done)
+    value = world * nst / (t_learned / 1e3) if t_learned else None
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": 1, "warmup": min(args.warmup, 1),
+            "ms_per_step": t_learned, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded geometries)", "config": workload_config(args.workload, w, world),
+            "timed": "excited-state phase (transition charges, Davidson, C) on the device, per flake",
+            "plain_start": {"value": world * nst / (t_plain / 1e3) if t_plain else None, "ms_per_step": t_plain},
+            "speedup_vs_plain_start": (t_plain / t_learned) if t_learned else None,
+            "flakes": rows, "gpu_launches": native.counters.launches, "clocks": clocks, "roofline": None}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -312,6 +381,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="mixed: tensor-core exchange + FP64 refinement (default); fp64: the plain path")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison solve")
+    ap.add_argument("--model", default=None, help="learned-guess weights (workload guess)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -347,6 +417,8 @@ def main():
         Om, f = td.getEnergies(**opts)
         return td, Om, f
 
+    if w["kind"] == "guess":
+        return run_guess(args, w, rank, world, barrier)
     if w["kind"] == "ensemble":
         return run_ensemble(args, w, rank, world, barrier)
     for s in range(args.warmup):
