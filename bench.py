@@ -52,6 +52,9 @@ WORKLOADS = {
                         opts=dict(nstates=8, diag_conv=1.0e-6, diag_maxiter=100)),
     "polyene20": dict(kind="polyene", n=20, sigma=0.02, lc=0,
                       opts=dict(nstates=10, diag_conv=1.0e-6, diag_maxiter=100)),
+    # 64 trajectories of C40H42 on S1: 5 states + S1 gradient every 0.5 fs step (velocity Verlet)
+    "trajectories": dict(kind="trajectories", n=40, ntraj=64, sigma=0.02, lc=1, threads=16,
+                         opts=dict(nstates=5, diag_conv=1.0e-6)),
     # learned Davidson start on held-out hexagonal flakes (n = 4..7: 120-336 atoms)
     "guess": dict(kind="guess", flakes=(4, 5, 6, 7), polyenes=(40, 60), sigma=0.01, lc=1,
                   opts=dict(nstates=10, diag_conv=1.0e-6, diag_maxiter=200)),
@@ -86,6 +89,14 @@ def build_geometry(w, seed):
 
 def workload_config(name, w, n_gpus, precision="fp64"):
     from dftbaby_b200 import geometry
+    if w["kind"] == "trajectories":
+        return {"workload": "%s: %d seeded C%dH%d trajectories on S1, lc-TD-DFTB, %d states + S1 gradient per "
+                            "0.5 fs velocity Verlet step" % (name, w["ntraj"], w["n"], w["n"] + 2,
+                                                              w["opts"]["nstates"]),
+                "nstates": w["opts"]["nstates"], "davidson_residual": w["opts"]["diag_conv"], "scf_conv": 1e-10,
+                "temperature_K": 300, "sigma_angstrom": w["sigma"], "precision": "fp64",
+                "concurrency": "%d host threads, one CUDA stream each" % w["threads"],
+                "parallelism": "replicas x%d" % n_gpus}
     if w["kind"] == "guess":
         return {"workload": "%s: learned Davidson start vs plain start, held-out seeded hexagonal flakes %s, "
                             "lc-TD-DFTB" % (name, ", ".join(geometry.formula(geometry.hexagonal_flake(n))
@@ -311,6 +322,46 @@ def run_ensemble(args, w, rank, world, barrier):
         print(json.dumps(line), flush=True)
 
 
+def run_trajectories(args, w, rank, world, barrier):
+    """All trajectories advance args.steps velocity Verlet steps per timed region; a step of one
+    trajectory is an SCC + Davidson solve of nstates states + the S1 gradient."""
+    import torch
+    import torch.distributed as dist
+    from dftbaby_b200 import dynamics, geometry, native
+    geoms = [geometry.polyene(w["n"], sigma=w["sigma"], seed=3000 + 97 * rank + i) for i in range(w["ntraj"])]
+    o = w["opts"]
+    trajs = dynamics.start(geoms, threads=w["threads"], nstates=o["nstates"], diag_conv=o["diag_conv"],
+                           seed=77 + 1000 * rank)
+    dynamics.run(trajs, args.warmup, threads=w["threads"])
+    barrier()
+    native.counters.reset()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
+    sampler.start()
+    t0 = time.perf_counter()
+    dynamics.run(trajs, args.steps, threads=w["threads"])
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    barrier()
+    clocks = sampler.stop()
+    t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dt = t.item()
+    nst = w["ntraj"] * args.steps * o["nstates"]
+    drift = [tr.energy_drift() for tr in trajs]
+    line = {"metric": METRIC, "value": world * nst / dt, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometries)",
+            "config": workload_config(args.workload, w, world),
+            "timed": "wall time of the timed steps of all trajectories (host threads + streams, synchronised)",
+            "trajectory_steps_per_s": world * w["ntraj"] * args.steps / dt,
+            "energy_drift_hartree": {"max": max(drift), "median": float(np.median(drift)),
+                                     "over_fs": 0.5 * (args.warmup + args.steps)},
+            "gpu_launches": native.counters.launches, "clocks": clocks, "roofline": None}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_guess(args, w, rank, world, barrier):
     """Held-out flakes solved from the learned start and from DFTBaby's start (same FP64 solver,
     same residual threshold); device time of the excited-state phase and Davidson iterations."""
@@ -419,6 +470,8 @@ def main():
 
     if w["kind"] == "guess":
         return run_guess(args, w, rank, world, barrier)
+    if w["kind"] == "trajectories":
+        return run_trajectories(args, w, rank, world, barrier)
     if w["kind"] == "ensemble":
         return run_ensemble(args, w, rank, world, barrier)
     for s in range(args.warmup):

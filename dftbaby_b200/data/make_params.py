@@ -65,6 +65,11 @@ def main(ref_root):
     ea = _dict_literal(atomic, "electron_affinities_eV")
     hartree_to_eV = float(re.search(r"^hartree_to_eV\s*=\s*([0-9.eE+-]+)", atomic, re.M).group(1))
     out["const/hartree_to_eV"] = np.array(hartree_to_eV)
+    # nuclear masses (electron masses), Boltzmann constant (Hartree/K) and the atomic time unit (fs)
+    # used by the trajectory driver (AtomicData.py:6-7, 50-51)
+    out["const/kBoltzmann"] = np.array(float(eval(re.search(r"^kBoltzmann\s*=\s*([^#\n]+)", atomic, re.M).group(1))))
+    out["const/autime2fs"] = np.array(float(re.search(r"^autime2fs\s*=\s*([0-9.eE+-]+)", atomic, re.M).group(1)))
+    masses = _dict_literal(atomic, "atom_masses")
     out["const/bohr_to_angs"] = np.array(
         float(re.search(r"^bohr_to_angs\s*=\s*([0-9.eE+-]+)", atomic, re.M).group(1)))
     for z, el in ELEMENTS.items():
@@ -83,6 +88,7 @@ def main(ref_root):
         # free-atom orbital energies keyed by (n-1, l)
         en = [(n - 1, l, e) for (n, l, e) in zip(free["nshell"], free["angular_momenta"], free["energies"])]
         out["atom/%d/free_energies" % z] = np.array(en, dtype=np.float64)
+        out["atom/%d/mass" % z] = np.array(float(masses[el]))
         out["atom/%d/IE_eV" % z] = np.array(ie[el])
         out["atom/%d/EA_eV" % z] = np.array(ea[el])
     dest = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hc_params.npz")
