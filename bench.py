@@ -53,7 +53,7 @@ WORKLOADS = {
     "polyene20": dict(kind="polyene", n=20, sigma=0.02, lc=0,
                       opts=dict(nstates=10, diag_conv=1.0e-6, diag_maxiter=100)),
     # 64 trajectories of C40H42 on S1: 5 states + S1 gradient every 0.5 fs step (velocity Verlet)
-    "trajectories": dict(kind="trajectories", n=40, ntraj=64, sigma=0.02, lc=1, threads=16,
+    "trajectories": dict(kind="trajectories", n=40, ntraj=64, sigma=0.02, lc=1, threads=4,
                          opts=dict(nstates=5, diag_conv=1.0e-6)),
     # learned Davidson start on held-out hexagonal flakes (n = 4..7: 120-336 atoms)
     "guess": dict(kind="guess", flakes=(4, 5, 6, 7), polyenes=(40, 60), sigma=0.01, lc=1,

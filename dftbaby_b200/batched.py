@@ -56,6 +56,8 @@ def batched_eigh(A, workers=16):
         return torch.linalg.eigh(A)
     from concurrent.futures import ThreadPoolExecutor
     if _POOL is None:
+        # torch loads its eigensolver wrapper lazily; that must not race between the pool's threads
+        torch.linalg.eigh(A[:1])
         _POOL = ThreadPoolExecutor(max_workers=workers)
     while len(_STREAMS) < workers:
         _STREAMS.append(torch.cuda.Stream(device=A.device))

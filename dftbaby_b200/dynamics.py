@@ -93,11 +93,24 @@ class Trajectory:
         return float(np.abs(e - e[0]).max())
 
 
+def _init_libraries(dev):
+    """First use of torch's dense linear algebra (cuSOLVER / cuBLAS handles, lazily loaded wrappers)
+    on the calling thread: that initialisation is not safe to race from several threads."""
+    A = torch.eye(4, dtype=torch.float64, device=dev) * 2.0
+    L = torch.linalg.cholesky(A)
+    torch.linalg.solve_triangular(L, A, upper=False)
+    torch.linalg.eigh(A)
+    torch.linalg.qr(A)
+    torch.linalg.solve(A, A)
+    torch.cuda.synchronize(dev)
+
+
 def run(trajectories, nsteps, threads=8):
     """Advance every trajectory by nsteps, spread over host threads with one CUDA stream each."""
     from concurrent.futures import ThreadPoolExecutor
     dev = torch.cuda.current_device()
     nthr = max(1, min(threads, len(trajectories)))
+    _init_libraries(dev)
     streams = [torch.cuda.Stream(device=dev) for _ in range(nthr)]
     parts = [trajectories[i::nthr] for i in range(nthr)]
 
@@ -119,6 +132,7 @@ def start(atomlists, threads=8, **opts):
     from concurrent.futures import ThreadPoolExecutor
     dev = torch.cuda.current_device()
     nthr = max(1, min(threads, len(atomlists)))
+    _init_libraries(dev)
     streams = [torch.cuda.Stream(device=dev) for _ in range(nthr)]
     out = [None] * len(atomlists)
     seed0 = opts.pop("seed", 0)

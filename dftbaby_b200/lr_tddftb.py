@@ -319,6 +319,16 @@ class LR_TDDFTB:
         XmY0 = XpY0 = Om0 = None
         if torch.is_tensor(self.XpY) and self.XpY.shape == (nstates or -1, self.nocc, self.nvirt):
             XmY0, XpY0, Om0 = self.XmY, self.XpY, self._Omega_dev
+            prev = getattr(self, "_mo_prev", None)
+            if prev is not None and prev[0].shape[1] == self.nocc and prev[1].shape[1] == self.nvirt:
+                # The previous amplitudes refer to the previous molecular orbitals, whose signs (and, for
+                # near-degenerate levels, mixing) the eigensolver chooses freely.  Project them onto the
+                # current orbitals through the overlap, X_new = Po^T X_old Pv, Po = C_old^T S C_new.
+                Co_new, Cv_new = self._active_coefficients()
+                Po = prev[0].T @ (d.S @ Co_new)
+                Pv = prev[1].T @ (d.S @ Cv_new)
+                XmY0 = Po.T[None] @ XmY0 @ Pv[None]
+                XpY0 = Po.T[None] @ XpY0 @ Pv[None]
         learned = {}
         if guess_model is not None and XpY0 is None and nstates is not None:
             from . import learned as _learned
@@ -375,6 +385,7 @@ class LR_TDDFTB:
         self._Omega_dev = Om
         self.Omega = Om.cpu().numpy()
         self.Cij, self.XmY, self.XpY = C, XmY, XpY
+        self._mo_prev = self._active_coefficients()
         if diag_check == 1 and nstates is not None:
             Om_full, _, XmY_full, XpY_full = self._casida(multiplicity)
             err = np.sum(np.abs(self.Omega - Om_full[:nstates].cpu().numpy()))

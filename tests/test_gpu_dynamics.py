@@ -60,3 +60,28 @@ def test_threaded_trajectories_match_sequential():
     for ta, tb in zip(a, b):
         assert np.abs(ta.x - tb.x).max() < 1e-10
         assert abs(ta.E_pot - tb.E_pot) < 1e-10
+
+
+def test_warm_start_after_a_small_step_needs_fewer_iterations():
+    """The previous step's X-Y / X+Y, projected onto the new orbitals, start the next solve."""
+    native.load()
+    from dftbaby_b200 import LR_TDDFTB
+    al = geometry.polyene(20, sigma=0.02, seed=8)
+    rng = np.random.default_rng(0)
+    moved = [(Z, tuple(np.array(p) + rng.normal(scale=0.002, size=3))) for Z, p in al]
+    opts = dict(nstates=5, diag_conv=1e-7, diag_maxiter=200)
+    td = LR_TDDFTB(al, long_range_correction=1)
+    td.setGeometry(al)
+    td.getEnergies(**opts)
+    cold_iters = td.stats["iterations"]
+    td.setGeometry(moved)
+    Ow, _ = td.getEnergies(**opts)
+    warm_iters = td.stats["iterations"]
+    fresh = LR_TDDFTB(moved, long_range_correction=1)
+    fresh.setGeometry(moved)
+    Oc, _ = fresh.getEnergies(**opts)
+    # the SCC restarted from the previous density converges to a point ~1e-6 Ha away (DIIS stops on its
+    # own relative change), so warm and cold solves agree to the 1 meV accuracy target, not to 1e-8 eV
+    assert np.abs(Ow - Oc).max() * 27.211396132 < 1e-3
+    print("Davidson iterations: cold %d, warm-started after a 0.002 bohr displacement %d" % (cold_iters, warm_iters))
+    assert warm_iters < cold_iters
