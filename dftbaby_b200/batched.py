@@ -44,14 +44,51 @@ _POOL = None
 _STREAMS = []
 
 
-def batched_eigh(A, workers=16):
-    """torch.linalg.eigh over a batch, spread over host threads with one CUDA stream each.
+_NATIVE_EIGH = {}   # n -> False once the batched cuSOLVER routine refused that size
 
-    The dense symmetric eigensolver runs one matrix at a time and is bound by
-    launch and synchronisation latency at these sizes; independent streams let
-    the solves of different matrices overlap."""
+
+def _native_batched_eigh(A):
+    """dftb_batched_eigh (one cuSOLVER call for the whole batch); None when unavailable."""
+    import ctypes
+    B, n, _ = A.shape
+    if _NATIVE_EIGH.get(n) is False:
+        return None
+    L = native.load()
+    if not _NATIVE_EIGH:
+        # load cuSOLVER through torch first, so that the batched routine resolves to the same copy
+        torch.linalg.eigh(torch.eye(2, dtype=A.dtype, device=A.device))
+        _NATIVE_EIGH[0] = True
+    size = ctypes.c_size_t(0)
+    if L.dftb_batched_eigh_workspace_size(n, B, ctypes.byref(size)) != 0:
+        _NATIVE_EIGH[n] = False
+        return None
+    V = A.contiguous().clone()
+    w = torch.empty((B, n), dtype=A.dtype, device=A.device)
+    ws = torch.empty(max(int(size.value), 16), dtype=torch.uint8, device=A.device)
+    info = torch.zeros(B, dtype=torch.int32, device=A.device)
+    rc = L.dftb_batched_eigh(n, B, native.ptr(V), native.ptr(w), native.ptr(ws), ws.numel(), native.ptr(info),
+                             native.stream())
+    if rc == native.DFTB_ERR_UNSUPPORTED:
+        _NATIVE_EIGH[n] = False
+        return None
+    native.check(rc, "dftb_batched_eigh")
+    native.counters.launches += 1
+    if bool((info != 0).any()):
+        raise ExcitedStatesError("batched eigensolver did not converge for %d matrices" % int((info != 0).sum()))
+    return w, V.transpose(1, 2)
+
+
+def batched_eigh(A, workers=16):
+    """Eigen-decomposition of a batch of symmetric matrices: one batched cuSOLVER call where the
+    library provides it, else torch.linalg.eigh spread over host threads with one CUDA stream each
+    (the dense solver runs one matrix at a time and is bound by launch and synchronisation latency at
+    these sizes; independent streams let the solves of different matrices overlap)."""
     global _POOL
     B = A.shape[0]
+    if A.device.type == "cuda" and B > 1:
+        out = _native_batched_eigh(A)
+        if out is not None:
+            return out
     if B < 2 * workers or A.device.type != "cuda":
         return torch.linalg.eigh(A)
     from concurrent.futures import ThreadPoolExecutor

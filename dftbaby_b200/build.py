@@ -27,7 +27,7 @@ def build_native(force=False, verbose=False):
         if os.path.getmtime(LIB) >= newest:
             return LIB
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-I" + os.path.join(ROOT, "include"), "-o", LIB] + sorted(srcs)
+    cmd = [_nvcc()] + NVCC_FLAGS + ["-I" + os.path.join(ROOT, "include"), "-o", LIB] + sorted(srcs) + ["-ldl"]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)

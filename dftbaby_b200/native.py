@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libdftbaby_b200.so")
 
 DFTB_OK = 0
 DFTB_ERR_WORKSPACE = -4
+DFTB_ERR_UNSUPPORTED = -5
 _ERRORS = {-1: "bad size", -2: "null pointer", -3: "CUDA error", -4: "workspace too small", -5: "unsupported"}
 
 
@@ -77,6 +78,9 @@ _SIGNATURES = {
     "dftb_mlp_adam": (_I, [_I, _I, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                            _I, ctypes.c_float, _P, _I, _P, _I, _P]),
     "dftb_mlp_last_error": (ctypes.c_char_p, []),
+    "dftb_batched_eigh_workspace_size": (_I, [_I, _I, ctypes.POINTER(_Z)]),
+    "dftb_batched_eigh": (_I, [_I, _I, _P, _P, _P, _Z, _P, _P]),
+    "dftb_eigh_last_error": (ctypes.c_char_p, []),
 }
 
 
@@ -117,7 +121,7 @@ def check(rc, what):
         msg = ""
         if _lib is not None:
             msg = (_lib.dftb_last_error().decode() or _lib.dftb_grad_last_error().decode()
-                   or _lib.dftb_mlp_last_error().decode())
+                   or _lib.dftb_mlp_last_error().decode() or _lib.dftb_eigh_last_error().decode())
         raise NativeError("%s failed (%s): %s" % (what, _ERRORS.get(rc, rc), msg))
 
 

@@ -308,6 +308,19 @@ int dftb_mlp_adam(int rows, int cols, float *W, const float *G, float *m1, float
                   void *stream);
 const char *dftb_mlp_last_error(void);
 
+/* ---- batched symmetric eigensolver --------------------------------------------
+ * No counterpart in DFTBaby, which calls LAPACK one matrix at a time
+ * (DFTB2.py:1086, Solver.py:486, 772).  Eigenvalues (ascending) and eigenvectors of
+ * batch symmetric n x n FP64 matrices stored contiguously in A (only the lower
+ * triangle of each row-major block is read, as torch.linalg.eigh reads it); A is overwritten by the eigenvectors in column-major order (eigenvector j
+ * is row j of each row-major n x n block), W receives batch x n eigenvalues, info
+ * batch status words.  Runs cuSOLVER's cusolverDnXsyevBatched, resolved at run
+ * time: DFTB_ERR_UNSUPPORTED when the loaded cuSOLVER lacks it or refuses the size.
+ * work: dftb_batched_eigh_workspace_size() bytes of device memory. */
+int dftb_batched_eigh_workspace_size(int n, int batch, size_t *bytes);
+int dftb_batched_eigh(int n, int batch, double *A, double *W, void *work, size_t work_bytes, int *info, void *stream);
+const char *dftb_eigh_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

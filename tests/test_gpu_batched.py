@@ -46,3 +46,24 @@ def test_batched_level_shift_and_threaded_eigensolver():
         Os, fs = _single(mols[j], 1, opts, HOMO_LUMO_tol=0.2)
         assert np.abs(Om_b[j] - Os).max() * HARTREE_TO_EV < 1e-7
         assert np.abs(f_b[j] - fs).max() < 1e-7
+
+
+@pytest.mark.parametrize("n", [12, 48, 150, 302, 440])
+def test_batched_eigh_matches_torch(n):
+    import torch
+    from dftbaby_b200 import batched
+    native.load()
+    g = torch.Generator(device="cpu").manual_seed(n)
+    A = torch.randn((40, n, n), dtype=torch.float64, generator=g).cuda()
+    A = A + A.transpose(1, 2)
+    out = batched._native_batched_eigh(A)
+    if out is None:
+        pytest.skip("this cuSOLVER has no batched syev for n = %d: %s" % (n, native.load().dftb_eigh_last_error()))
+    w, V = out
+    w_ref = torch.linalg.eigvalsh(A)
+    scale = w_ref.abs().max().item()
+    assert (w - w_ref).abs().max().item() < 1e-12 * scale
+    resid = torch.linalg.norm(A @ V - V * w[:, None, :], dim=(1, 2)).max().item()
+    assert resid < 1e-11 * scale * n
+    orth = (V.transpose(1, 2) @ V - torch.eye(n, dtype=A.dtype, device=A.device)).abs().max().item()
+    assert orth < 1e-11
