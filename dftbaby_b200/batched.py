@@ -680,3 +680,35 @@ def _batched_nonhermitian(prod, om, k, conv, maxiter, kmax):
     else:
         raise ExcitedStatesNotConverged("batched Davidson: %d molecules did not converge" % int(active.sum()))
     return Om, C, XmY, XpY, iters.tolist()
+
+
+def main(argv=None):
+    """Solve a seeded ensemble of polyenes and acenes: ``python -m dftbaby_b200.batched --molecules 128``."""
+    import argparse
+    import time
+    from . import geometry
+    ap = argparse.ArgumentParser(description="lockstep lc-TD-DFTB of a seeded ensemble")
+    ap.add_argument("--molecules", type=int, default=128)
+    ap.add_argument("--nstates", type=int, default=8)
+    ap.add_argument("--seed", type=int, default=20000)
+    args = ap.parse_args(argv)
+    rng = np.random.default_rng(args.seed)
+    mols = []
+    for _ in range(args.molecules):
+        s = int(rng.integers(1 << 30))
+        if rng.random() < 0.5:
+            mols.append(geometry.polyene(int(rng.integers(5, 31)) * 2, sigma=0.03, seed=s))
+        else:
+            mols.append(geometry.acene(int(rng.integers(2, 9)), sigma=0.03, seed=s))
+    bt = BatchedLR_TDDFTB(mols, long_range_correction=1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    bt.getEnergies(nstates=args.nstates, diag_conv=1e-6, diag_maxiter=100)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    print("%d molecules, %d states each: %.2f s, %.1f states/s" % (len(mols), args.nstates, dt,
+                                                                   len(mols) * args.nstates / dt))
+
+
+if __name__ == "__main__":
+    main()

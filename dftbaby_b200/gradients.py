@@ -312,3 +312,34 @@ def _trans_charges_full(d, Co, Cv):
                 native.ptr(d._opa), native.ptr(q[0]), native.ptr(q[1]), native.ptr(q[2]), native.ptr(ws), ws.numel(),
                 native.stream())
     return q[0], q[1], q[2]
+
+
+def main(argv=None):
+    """Gradient of one excited state of a seeded polyene: ``python -m dftbaby_b200.gradients --n 40``."""
+    import argparse
+    import time
+    from . import geometry
+    from .lr_tddftb import LR_TDDFTB
+    ap = argparse.ArgumentParser(description="analytic excited-state gradient of a seeded polyene")
+    ap.add_argument("--n", type=int, default=40, help="carbon atoms of the all-trans polyene (even)")
+    ap.add_argument("--state", type=int, default=1)
+    ap.add_argument("--nstates", type=int, default=5)
+    ap.add_argument("--lc", type=int, default=1)
+    ap.add_argument("--repeat", type=int, default=2)
+    args = ap.parse_args(argv)
+    al = geometry.polyene(args.n, sigma=0.02, seed=1)
+    td = LR_TDDFTB(al, long_range_correction=args.lc)
+    td.setGeometry(al)
+    td.getEnergies(nstates=args.nstates, diag_conv=1e-8, diag_maxiter=200)
+    grads = Gradients(td)
+    for _ in range(args.repeat):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g = np.sum(grads.gradient(args.state), axis=0)
+        torch.cuda.synchronize()
+        print("state %d gradient of %d atoms: |g|max %.6f Ha/bohr, %.1f ms" % (args.state, len(al), np.abs(g).max(),
+                                                                            (time.perf_counter() - t0) * 1e3))
+
+
+if __name__ == "__main__":
+    main()
