@@ -53,7 +53,7 @@ WORKLOADS = {
     "polyene20": dict(kind="polyene", n=20, sigma=0.02, lc=0,
                       opts=dict(nstates=10, diag_conv=1.0e-6, diag_maxiter=100)),
     # 64 trajectories of C40H42 on S1: 5 states + S1 gradient every 0.5 fs step (velocity Verlet)
-    "trajectories": dict(kind="trajectories", n=40, ntraj=64, sigma=0.02, lc=1, threads=4,
+    "trajectories": dict(kind="trajectories", n=40, ntraj=64, sigma=0.02, lc=1,
                          opts=dict(nstates=5, diag_conv=1.0e-6)),
     # learned Davidson start on held-out hexagonal flakes (n = 4..7: 120-336 atoms)
     "guess": dict(kind="guess", flakes=(4, 5, 6, 7), polyenes=(40, 60), sigma=0.01, lc=1,
@@ -95,7 +95,7 @@ def workload_config(name, w, n_gpus, precision="fp64"):
                                                               w["opts"]["nstates"]),
                 "nstates": w["opts"]["nstates"], "davidson_residual": w["opts"]["diag_conv"], "scf_conv": 1e-10,
                 "temperature_K": 300, "sigma_angstrom": w["sigma"], "precision": "fp64",
-                "concurrency": "%d host threads, one CUDA stream each" % w["threads"],
+                "concurrency": "all trajectories in lockstep (batched SCC, Davidson and gradients)",
                 "parallelism": "replicas x%d" % n_gpus}
     if w["kind"] == "guess":
         return {"workload": "%s: learned Davidson start vs plain start, held-out seeded hexagonal flakes %s, "
@@ -327,18 +327,20 @@ def run_trajectories(args, w, rank, world, barrier):
     trajectory is an SCC + Davidson solve of nstates states + the S1 gradient."""
     import torch
     import torch.distributed as dist
-    from dftbaby_b200 import dynamics, geometry, native
+    from dftbaby_b200 import geometry, native
+    from dftbaby_b200.batched_dynamics import BatchedTrajectories
     geoms = [geometry.polyene(w["n"], sigma=w["sigma"], seed=3000 + 97 * rank + i) for i in range(w["ntraj"])]
     o = w["opts"]
-    trajs = dynamics.start(geoms, threads=w["threads"], nstates=o["nstates"], diag_conv=o["diag_conv"],
-                           seed=77 + 1000 * rank)
-    dynamics.run(trajs, args.warmup, threads=w["threads"])
+    bt = BatchedTrajectories(geoms, state=1, nstates=o["nstates"], diag_conv=o["diag_conv"], seed=77 + 1000 * rank)
+    for _ in range(args.warmup):
+        bt.step()
     barrier()
     native.counters.reset()
     sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
     sampler.start()
     t0 = time.perf_counter()
-    dynamics.run(trajs, args.steps, threads=w["threads"])
+    for _ in range(args.steps):
+        bt.step()
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     barrier()
@@ -348,12 +350,14 @@ def run_trajectories(args, w, rank, world, barrier):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     dt = t.item()
     nst = w["ntraj"] * args.steps * o["nstates"]
-    drift = [tr.energy_drift() for tr in trajs]
+    drift = list(bt.energy_drift())
     line = {"metric": METRIC, "value": world * nst / dt, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometries)",
             "config": workload_config(args.workload, w, world),
-            "timed": "wall time of the timed steps of all trajectories (host threads + streams, synchronised)",
+            "timed": "wall time of the timed lockstep steps of all trajectories (synchronised)",
+            "solver": {"scc_iterations_max_per_step": bt.stats["scc_iterations"][-args.steps:],
+                       "davidson_iterations_max_per_step": bt.stats["davidson_iterations"][-args.steps:]},
             "trajectory_steps_per_s": world * w["ntraj"] * args.steps / dt,
             "energy_drift_hartree": {"max": max(drift), "median": float(np.median(drift)),
                                      "over_fs": 0.5 * (args.warmup + args.steps)},

@@ -185,6 +185,10 @@ class BatchedLR_TDDFTB:
         native.call("dftb_gamma_matrices", nat, P(r), P(sigma), float(self.r_lr), P(g), P(glr), st)
         m.S, m.H0, m.D, m.g, m.glr, m.p0 = S, H0, D, g, glr, f64(occ0)
         m.opa = opa
+        # device tables of the gradient kernels (gradients.contract)
+        m.typ, m.ls, m.ms, m.dircos, m.mprox = typ_t, ls_t, ms_t, (r, x, y, z), mprox
+        m.atype = i32([p.atom_type[Z] for Z, _ in al])
+        m.sigma = sigma
         return m
 
     # ------------------------------------------------------------ public API
@@ -215,87 +219,104 @@ class BatchedLR_TDDFTB:
 
 
 # ------------------------------------------------------------ one padded group
-def solve_group(mols, lc, dev, nstates, conv, dmaxiter, scf_conv=1.0e-10, maxiter=1000, mix_thr=1.0e-3,
-                alpha=0.33, diis_m=5, level_shift=0.1, homo_lumo_tol=0.05):
-    """Lockstep SCC + Davidson for one group of molecules.
+class _Group:
+    """Padded device tensors of one group of molecules (see the module docstring)."""
 
-    ``mols`` hold per-molecule tensors on ``dev``: S, H0 (norb, norb), D (3, norb, norb), g, glr
-    (nat, nat), p0 (norb,) reference occupations, ind (norb,) orbital -> atom, and the ints nat,
-    norb, nelec.  Returns (Omega (B, nstates), f (B, nstates), SCC iterations, Davidson iterations)."""
-    B = len(mols)
-    N = max(m.norb for m in mols)
-    NA = max(m.nat for m in mols)
+    def __init__(self, mols, dev):
+        self.mols, self.dev = mols, dev
+        B = self.B = len(mols)
+        N = self.N = max(m.norb for m in mols)
+        NA = self.NA = max(m.nat for m in mols)
+        f64 = torch.float64
+        S = torch.zeros((B, N, N), dtype=f64, device=dev)
+        H0 = torch.zeros_like(S)
+        Glr = torch.zeros_like(S)     # AO-expanded gamma^lr
+        D = torch.zeros((B, 3, N, N), dtype=f64, device=dev)
+        P0 = torch.zeros((B, N), dtype=f64, device=dev)
+        gat = torch.zeros((B, NA, NA), dtype=f64, device=dev)
+        glrat = torch.zeros_like(gat)
+        orb_atom = torch.zeros((B, N), dtype=torch.long, device=dev)  # padded orbitals -> dummy atom NA
+        real = torch.zeros((B, N), dtype=torch.bool, device=dev)
+        for b, m in enumerate(mols):
+            n = m.norb
+            S[b, :n, :n] = m.S
+            H0[b, :n, :n] = m.H0
+            D[b, :, :n, :n] = m.D
+            P0[b, :n] = m.p0
+            gat[b, :m.nat, :m.nat] = m.g
+            glrat[b, :m.nat, :m.nat] = m.glr
+            ia = m.ind.long()
+            orb_atom[b, :n] = ia
+            orb_atom[b, n:] = NA
+            real[b, :n] = True
+            Glr[b, :n, :n] = m.glr[ia][:, ia]
+        pad = ~real
+        eye = torch.eye(N, dtype=f64, device=dev).expand(B, N, N)
+        self.S = torch.where(pad[:, :, None] | pad[:, None, :], eye, S)
+        self.H0 = H0 + torch.diag_embed(pad.to(f64) * PAD_H)
+        L = torch.linalg.cholesky(self.S)
+        self.Linv = torch.linalg.solve_triangular(L, torch.eye(N, dtype=f64, device=dev).expand(B, N, N),
+                                                  upper=False)
+        self.D, self.Glr, self.gat, self.glrat, self.orb_atom, self.real = D, Glr, gat, glrat, orb_atom, real
+        if any(abs(m.nelec - 2 * (m.nelec // 2)) > 1e-12 for m in mols):
+            raise ValueError("the batched solver handles closed shells only")
+        self.nocc = [int(m.nelec // 2) for m in mols]
+        # occupation (T = 0): the nocc lowest orbitals of each molecule (all real: padding sits at +10 Ha)
+        self.occmask = torch.zeros((B, N), dtype=f64, device=dev)
+        for b, n in enumerate(self.nocc):
+            self.occmask[b, :n] = 2.0
+        # atom-sum operator for Mulliken charges: (B, NA, N) one-hot of orb_atom
+        Aop = torch.zeros((B, NA + 1, N), dtype=f64, device=dev)
+        Aop.scatter_(1, orb_atom[:, None, :], 1.0)
+        self.Aop = Aop[:, :NA, :]
+        self.P0m = torch.diag_embed(P0)
+
+
+def _lockstep_scc(G, lc, scf_conv=1.0e-10, maxiter=1000, mix_thr=1.0e-3, alpha=0.33, diis_m=5, level_shift=0.1,
+                  homo_lumo_tol=0.05, warm=None):
+    """DFTB2.runSCC (DFTB2.py:940-1160) for every molecule of the group at once.
+
+    warm: None for a start from the reference density, or the state returned by a previous call
+    (P, dq, orbs, orbe, rel, gap) for a restart from the previous density, as runSCC does with
+    start_from_previous=1: the DIIS history restarts, the last relative change and HOMO-LUMO gap
+    carry over into the level-shift switches.  Returns the new state and the iteration counts."""
+    B, N, dev = G.B, G.N, G.dev
     f64 = torch.float64
-    S = torch.zeros((B, N, N), dtype=f64, device=dev)
-    H0 = torch.zeros_like(S)
-    Glr = torch.zeros_like(S)     # AO-expanded gamma^lr
-    D = torch.zeros((B, 3, N, N), dtype=f64, device=dev)
-    P0 = torch.zeros((B, N), dtype=f64, device=dev)
-    gat = torch.zeros((B, NA, NA), dtype=f64, device=dev)
-    glrat = torch.zeros_like(gat)
-    orb_atom = torch.zeros((B, N), dtype=torch.long, device=dev)  # padded orbitals -> dummy atom NA
-    real = torch.zeros((B, N), dtype=torch.bool, device=dev)
-    for b, m in enumerate(mols):
-        n = m.norb
-        S[b, :n, :n] = m.S
-        H0[b, :n, :n] = m.H0
-        D[b, :, :n, :n] = m.D
-        P0[b, :n] = m.p0
-        gat[b, :m.nat, :m.nat] = m.g
-        glrat[b, :m.nat, :m.nat] = m.glr
-        ia = m.ind.long()
-        orb_atom[b, :n] = ia
-        orb_atom[b, n:] = NA
-        real[b, :n] = True
-        Glr[b, :n, :n] = m.glr[ia][:, ia]
-    pad = ~real
-    eye = torch.eye(N, dtype=f64, device=dev).expand(B, N, N)
-    S = torch.where(pad[:, :, None] | pad[:, None, :], eye, S)
-    H0 = H0 + torch.diag_embed(pad.to(f64) * PAD_H)
-    L = torch.linalg.cholesky(S)
-    Linv = torch.linalg.solve_triangular(L, torch.eye(N, dtype=f64, device=dev).expand(B, N, N), upper=False)
-    nel = torch.tensor([m.nelec for m in mols], dtype=f64, device=dev)
-    nocc = [int(m.nelec // 2) for m in mols]
-    if any(abs(m.nelec - 2 * (m.nelec // 2)) > 1e-12 for m in mols):
-        raise ValueError("the batched solver handles closed shells only")
-    # occupation (T = 0): the nocc lowest orbitals of each molecule (all real: padding sits at +10 Ha)
-    occmask = torch.zeros((B, N), dtype=f64, device=dev)
-    for b, n in enumerate(nocc):
-        occmask[b, :n] = 2.0
-    # atom-sum operator for Mulliken charges: (B, NA+1, N) one-hot of orb_atom
-    Aop = torch.zeros((B, NA + 1, N), dtype=f64, device=dev)
-    Aop.scatter_(1, orb_atom[:, None, :], 1.0)
-    Aop = Aop[:, :NA, :]
-    P0m = torch.diag_embed(P0)
-    # ---------------- lockstep SCC
-    dq = torch.zeros((B, NA), dtype=f64, device=dev)
-    P = P0m.clone()
+    S, H0, Glr, gat, Linv, occmask, P0m = G.S, G.H0, G.Glr, G.gat, G.Linv, G.occmask, G.P0m
+    if warm is None:
+        dq = torch.zeros((B, G.NA), dtype=f64, device=dev)
+        P = P0m.clone()
+        orbs = orbe = None
+        rel = np.ones(B)
+        gap = np.full(B, np.inf)
+        have_orbe = False
+    else:
+        P, dq, orbs, orbe, rel, gap = (warm[k] for k in ("P", "dq", "orbs", "orbe", "rel", "gap"))
+        rel, gap = rel.copy(), gap.copy()
+        have_orbe = True
     P_last = P
     converged = np.zeros(B, bool)
     done = np.zeros(B, bool)
     mixing = np.zeros(B, bool)
-    rel = np.ones(B)
     diis = _BatchedDIIS(B, N * N, diis_m, dev)
-    orbs = orbe = None
     scc_it = np.zeros(B, int)
     shift_flag = np.zeros(B, bool)
-    gap = np.full(B, np.inf)
-    hom = torch.as_tensor([n - 1 for n in nocc], device=dev)
+    hom = torch.as_tensor([n - 1 for n in G.nocc], device=dev)
     for it in range(maxiter):
         live = torch.as_tensor(~done, device=dev)
         estat = torch.bmm(gat, dq[:, :, None])[:, :, 0]                      # (B, NA)
-        eorb = torch.cat([estat, torch.zeros((B, 1), dtype=f64, device=dev)], 1).gather(1, orb_atom)
+        eorb = torch.cat([estat, torch.zeros((B, 1), dtype=f64, device=dev)], 1).gather(1, G.orb_atom)
         H = H0 + 0.5 * (eorb[:, :, None] + eorb[:, None, :]) * S
         if lc:
             dP = P - P0m
             A1 = torch.bmm(S, dP)
             t1 = torch.bmm(Glr * A1, S)
             Hx = t1 + t1.transpose(1, 2) + Glr * torch.bmm(A1, S) + torch.bmm(torch.bmm(S, dP * Glr), S)
-            H = H + Hx * (-1.0 / 8.0) * real[:, :, None] * real[:, None, :]
+            H = H + Hx * (-1.0 / 8.0) * G.real[:, :, None] * G.real[:, None, :]
         # level shift (DFTB2.py:1047-1081): once the gap of the last iteration fell below
         # HOMO_LUMO_tol before DIIS started, the virtual block is shifted by b in the basis of the
         # last MOs; b halves below 1e5*scf_conv and vanishes below 1e3*scf_conv
-        if it > 0:
+        if it > 0 or have_orbe:
             shift_flag |= (gap < homo_lumo_tol) & ~mixing & ~done
         bshift = np.where(shift_flag, level_shift, 0.0)
         bshift = np.where(shift_flag & (rel < 1.0e5 * scf_conv), 0.5 * bshift, bshift)
@@ -327,7 +348,7 @@ def solve_group(mols, lc, dev, nstates, conv, dmaxiter, scf_conv=1.0e-10, maxite
         P = torch.where(live[:, None, None], Pmix, P)
         orbs = C_new if orbs is None else torch.where(live[:, None, None], C_new, orbs)
         orbe = e_new if orbe is None else torch.where(live[:, None], e_new, orbe)
-        q = (torch.bmm(Aop, ((P - P0m) * S).sum(2)[:, :, None]))[:, :, 0]
+        q = (torch.bmm(G.Aop, ((P - P0m) * S).sum(2)[:, :, None]))[:, :, 0]
         dq = torch.where(live[:, None], q, dq)
         # relative change per molecule
         r_lin = torch.linalg.norm((P_last - P).reshape(B, -1), dim=1) / torch.linalg.norm(P.reshape(B, -1), dim=1)
@@ -352,37 +373,76 @@ def solve_group(mols, lc, dev, nstates, conv, dmaxiter, scf_conv=1.0e-10, maxite
             break
     else:
         raise SCFNotConverged("batched SCC did not converge for %d molecules" % int((~done).sum()))
-    # ---------------- excited states (full active space of each molecule)
+    return dict(P=P, dq=dq, orbs=orbs, orbe=orbe, rel=rel, gap=gap), scc_it
+
+
+def _excited(G, lc, scc, nstates, conv, dmaxiter, guess=None):
+    """Excited states of every molecule in the full active space: transition charges, the lockstep
+    Davidson and C.  guess = (XmY, XpY, Co, Cv) of a previous solve of the same group starts the
+    Davidson from those vectors, projected onto the current orbitals through the orbital overlap."""
+    B, N, NA, dev = G.B, G.N, G.NA, G.dev
+    f64 = torch.float64
+    orbs, orbe = scc["orbs"], scc["orbe"]
+    nocc = G.nocc
     no_max = max(nocc)
-    nvir = [m.norb - n for m, n in zip(mols, nocc)]
+    nvir = [m.norb - n for m, n in zip(G.mols, nocc)]
     nv_max = max(nvir)
     nov = no_max * nv_max
     Co = torch.zeros((B, N, no_max), dtype=f64, device=dev)
     Cv = torch.zeros((B, N, nv_max), dtype=f64, device=dev)
+    eo = torch.zeros((B, no_max), dtype=f64, device=dev)
+    ev = torch.zeros((B, nv_max), dtype=f64, device=dev)
     omega = torch.full((B, no_max, nv_max), PAD_OMEGA, dtype=f64, device=dev)
     for b, (n, nv) in enumerate(zip(nocc, nvir)):
         # occupied: nocc lowest; active occupied in increasing energy, virtuals lowest first
         Co[b, :, no_max - n:] = orbs[b, :, :n]
         Cv[b, :, :nv] = orbs[b, :, n:n + nv]
+        eo[b, no_max - n:] = orbe[b, :n]
+        ev[b, :nv] = orbe[b, n:n + nv]
         omega[b, no_max - n:, :nv] = orbe[b, n:n + nv][None, :] - orbe[b, :n][:, None]
     # transition charges q_ov (B, NA, nov) from C and S C, summed per atom
-    SCo, SCv = torch.bmm(S, Co), torch.bmm(S, Cv)
+    SCo, SCv = torch.bmm(G.S, Co), torch.bmm(G.S, Cv)
     qov = 0.5 * (torch.einsum("bmi,bma->bmia", Co, SCv) + torch.einsum("bma,bmi->bmia", Cv, SCo))
-    qov = torch.bmm(Aop, qov.reshape(B, N, nov)).reshape(B, NA, nov)
+    qov = torch.bmm(G.Aop, qov.reshape(B, N, nov)).reshape(B, NA, nov)
     om = omega.reshape(B, nov)
-    k = nstates
     kmax = [n * nv for n, nv in zip(nocc, nvir)]
+    start = None
+    if guess is not None:
+        XmY0, XpY0, Co0, Cv0 = guess
+        Po = torch.bmm(Co0.transpose(1, 2), SCo)                                  # (B, no, no)
+        Pv = torch.bmm(Cv0.transpose(1, 2), SCv)                                  # (B, nv, nv)
+        proj = lambda X: torch.matmul(torch.matmul(Po.transpose(1, 2)[:, None], X.reshape(B, -1, no_max, nv_max)),
+                                      Pv[:, None]).reshape(B, -1, nov)
+        start = (proj(XmY0), proj(XpY0))
+    prod = _BatchedProducts(G.gat, G.Glr if lc else None, qov, om, Co, Cv, SCo, SCv, no_max, nv_max)
     if lc:
-        prod = _BatchedProducts(gat, Glr, qov, om, Co, Cv, SCo, SCv, no_max, nv_max)
-        Om, C, XmY, XpY, dav_it = _batched_nonhermitian(prod, om, k, conv, dmaxiter, kmax)
+        Om, C, XmY, XpY, dav_it = _batched_nonhermitian(prod, om, nstates, conv, dmaxiter, kmax, start)
     else:
-        prod = _BatchedProducts(gat, None, qov, om, Co, Cv, SCo, SCv, no_max, nv_max)
-        Om, C, XmY, XpY, dav_it = _batched_hermitian(prod, om, k, conv, dmaxiter, kmax)
-    # oscillator strengths from C and the MO dipoles of the active block
-    t = torch.einsum("bmi,bcmn,bna->bcia", Co, D, Cv).reshape(B, 3, nov)
-    tdip = torch.einsum("bkn,bcn->bck", C, t)
-    fosc = 2.0 / 3.0 * Om * (tdip ** 2).sum(1)
-    return Om.cpu().numpy(), fosc.cpu().numpy(), scc_it.tolist(), dav_it
+        Om, C, XmY, XpY, dav_it = _batched_hermitian(prod, om, nstates, conv, dmaxiter, kmax, start)
+    return dict(Om=Om, C=C, XmY=XmY, XpY=XpY, Co=Co, Cv=Cv, SCo=SCo, SCv=SCv, eo=eo, ev=ev, qov=qov, om=om,
+                prod=prod, no=no_max, nv=nv_max, dav_it=dav_it)
+
+
+def _oscillator_strengths(G, exc):
+    B = G.B
+    nov = exc["om"].shape[1]
+    t = torch.einsum("bmi,bcmn,bna->bcia", exc["Co"], G.D, exc["Cv"]).reshape(B, 3, nov)
+    tdip = torch.einsum("bkn,bcn->bck", exc["C"], t)
+    return 2.0 / 3.0 * exc["Om"] * (tdip ** 2).sum(1)
+
+
+def solve_group(mols, lc, dev, nstates, conv, dmaxiter, scf_conv=1.0e-10, maxiter=1000, mix_thr=1.0e-3,
+                alpha=0.33, diis_m=5, level_shift=0.1, homo_lumo_tol=0.05):
+    """Lockstep SCC + Davidson for one group of molecules.
+
+    ``mols`` hold per-molecule tensors on ``dev``: S, H0 (norb, norb), D (3, norb, norb), g, glr
+    (nat, nat), p0 (norb,) reference occupations, ind (norb,) orbital -> atom, and the ints nat,
+    norb, nelec.  Returns (Omega (B, nstates), f (B, nstates), SCC iterations, Davidson iterations)."""
+    G = _Group(mols, dev)
+    scc, scc_it = _lockstep_scc(G, lc, scf_conv, maxiter, mix_thr, alpha, diis_m, level_shift, homo_lumo_tol)
+    exc = _excited(G, lc, scc, nstates, conv, dmaxiter)
+    fosc = _oscillator_strengths(G, exc)
+    return exc["Om"].cpu().numpy(), fosc.cpu().numpy(), scc_it.tolist(), exc["dav_it"]
 
 
 class _BatchedDIIS:
@@ -564,7 +624,16 @@ def _pad_dead(M, live, pad=PAD_SUB):
     return M + torch.diag_embed((~live).to(M.dtype) * pad)
 
 
-def _batched_hermitian(prod, om, k, conv, maxiter, kmax):
+def _guess_basis(guess, k, B, nov, dev):
+    """Orthonormal start block from previous X-Y / X+Y vectors (each (B, k, nov)): 2k live columns."""
+    XmY, XpY = guess
+    cols = torch.cat([XmY, XpY], dim=1).transpose(1, 2)                    # (B, nov, 2k)
+    cols = cols / torch.linalg.norm(cols, dim=1, keepdim=True).clamp_min(1e-300)
+    bs, _ = torch.linalg.qr(cols)
+    return bs.contiguous(), torch.ones((B, bs.shape[2]), dtype=torch.bool, device=dev)
+
+
+def _batched_hermitian(prod, om, k, conv, maxiter, kmax, guess=None):
     """Lockstep Hermitian Davidson (Solver.HermitianDavidson, lc = 0) over a batch; prod gives the
     Coulomb product (A+B).V, from which R.V = omega^2 V + sqrt(omega) (A+B - omega)(sqrt(omega) V)."""
     B, nov = om.shape
@@ -575,10 +644,17 @@ def _batched_hermitian(prod, om, k, conv, maxiter, kmax):
         ap, _ = prod(sq[:, :, None] * V)
         return om[:, :, None] ** 2 * V + sq[:, :, None] * (ap - om[:, :, None] * sq[:, :, None] * V)
 
-    idx = torch.argsort(om, dim=1, stable=True)[:, :k]
-    bs = torch.zeros((B, nov, k), dtype=f64, device=dev)
-    bs[torch.arange(B, device=dev)[:, None], idx, torch.arange(k, device=dev)[None, :]] = 1.0
-    live = torch.ones((B, k), dtype=torch.bool, device=dev)
+    if guess is not None:
+        # T is proportional to (X+Y)/sqrt(omega): the previous X+Y give the start block
+        cols = (guess[1] / sq[:, None, :]).transpose(1, 2)
+        cols = cols / torch.linalg.norm(cols, dim=1, keepdim=True).clamp_min(1e-300)
+        bs = torch.linalg.qr(cols)[0].contiguous()
+        live = torch.ones((B, k), dtype=torch.bool, device=dev)
+    else:
+        idx = torch.argsort(om, dim=1, stable=True)[:, :k]
+        bs = torch.zeros((B, nov, k), dtype=f64, device=dev)
+        bs[torch.arange(B, device=dev)[:, None], idx, torch.arange(k, device=dev)[None, :]] = 1.0
+        live = torch.ones((B, k), dtype=torch.bool, device=dev)
     RB = rv(bs)
     active = np.ones(B, bool)
     Om = torch.zeros((B, k), dtype=f64, device=dev)
@@ -615,18 +691,22 @@ def _batched_hermitian(prod, om, k, conv, maxiter, kmax):
     return Om, C, XmY, XpY, iters.tolist()
 
 
-def _batched_nonhermitian(prod, om, k, conv, maxiter, kmax):
+def _batched_nonhermitian(prod, om, k, conv, maxiter, kmax, guess=None):
     """Lockstep Stratmann-Scuseria-Frisch Davidson over a batch (Solver.nonHermitianDavidson):
     every molecule adds exactly the correction vectors DFTBaby would add, so its search space,
     and with it the subspace-dependent C = bs Tb behind the oscillator strengths, is DFTBaby's."""
     B, nov = om.shape
     dev = om.device
     f64 = torch.float64
-    # initial vectors: unit vectors on the k lowest omega_ia of each molecule
-    idx = torch.argsort(om, dim=1, stable=True)[:, :k]
-    bs = torch.zeros((B, nov, k), dtype=f64, device=dev)
-    bs[torch.arange(B, device=dev)[:, None], idx, torch.arange(k, device=dev)[None, :]] = 1.0
-    live = torch.ones((B, k), dtype=torch.bool, device=dev)
+    if guess is not None:
+        # warm start: the previous X-Y and X+Y span the start block
+        bs, live = _guess_basis(guess, k, B, nov, dev)
+    else:
+        # initial vectors: unit vectors on the k lowest omega_ia of each molecule
+        idx = torch.argsort(om, dim=1, stable=True)[:, :k]
+        bs = torch.zeros((B, nov, k), dtype=f64, device=dev)
+        bs[torch.arange(B, device=dev)[:, None], idx, torch.arange(k, device=dev)[None, :]] = 1.0
+        live = torch.ones((B, k), dtype=torch.bool, device=dev)
     AP, AM = prod(bs)
     active = np.ones(B, bool)
     Om = torch.zeros((B, k), dtype=f64, device=dev)

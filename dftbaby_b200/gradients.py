@@ -36,31 +36,79 @@ def _block_sum(Y, ind, nat):
     return Aop @ Y @ Aop.T
 
 
+def _mv(A, x):
+    return (A @ x.unsqueeze(-1)).squeeze(-1)
+
+
 def _F_adjoint(S, g, v, W):
     """(X, Y) with <W, F[v]>_n = <gradS_n, X> + <g1_AO_n, Y> for grad.f90's Fop (lines 10-73):
     F_ab = 1/4 [ dS_ab (gSv_a + gSv_b) + S_ab (dgSv_a + gdSv_a + dgSv_b + gdSv_b) ],
-    Sv = rowsum(S o (v + v^T)), gSv = g Sv, gdSv = g rowsum(dS o (v + v^T)), dgSv = dG Sv."""
-    vp = v + v.T
-    Sv = (S * vp).sum(1)
-    gSv = g @ Sv
-    SW = (S * (W + W.T)).sum(1)
-    gSW = g @ SW
-    X = W * (gSv[:, None] + gSv[None, :]) + gSW[:, None] * vp
-    Y = SW[:, None] * Sv[None, :]
+    Sv = rowsum(S o (v + v^T)), gSv = g Sv, gdSv = g rowsum(dS o (v + v^T)), dgSv = dG Sv.
+    Leading batch dimensions are allowed."""
+    vp = v + v.mT
+    Sv = (S * vp).sum(-1)
+    gSv = _mv(g, Sv)
+    SW = (S * (W + W.mT)).sum(-1)
+    gSW = _mv(g, SW)
+    X = W * (gSv.unsqueeze(-1) + gSv.unsqueeze(-2)) + gSW.unsqueeze(-1) * vp
+    Y = SW.unsqueeze(-1) * Sv.unsqueeze(-2)
     return 0.25 * X, 0.25 * Y
 
 
 def _Flr_adjoint(S, g, v, W):
     """(X, Y) with <W, Flr[v]>_n = <gradS_n, X> + <g1lr_AO_n, Y> for the twelve terms of grad.f90's
-    Flrop (lines 75-182), each moved onto dS or dG by trace identities."""
+    Flrop (lines 75-182), each moved onto dS or dG by trace identities.  Leading batch dimensions
+    are allowed."""
     Sv, vS = S @ v, v @ S
-    WS, WtS = W @ S, W.T @ S
+    WS, WtS = W @ S, W.mT @ S
     Wg = W * g
     X = (Wg @ Sv + (WS * g) @ v + W @ (Sv * g) + WS @ (g * v)
-         + vS @ Wg + (vS * g) @ W + (WtS * g) @ v.T + WtS @ (g * v.T))
-    SvT = S @ v.T
-    Y = W * (SvT @ S) + WS * SvT + WtS * Sv + (S @ W.T @ S) * v
+         + vS @ Wg + (vS * g) @ W + (WtS * g) @ v.mT + WtS @ (g * v.mT))
+    SvT = S @ v.mT
+    Y = W * (SvT @ S) + WS * SvT + WtS * Sv + (S @ W.mT @ S) * v
     return 0.25 * X, 0.25 * Y
+
+
+def contract(geo, par, r_lr, XS, XH, Yg, Ylr, vrep):
+    """3 Nat gradient of one molecule from adjoints: SK pair derivatives against XS, XH (Norb x Norb);
+    gamma and gamma^lr derivatives against the orbital adjoints Yg, Ylr (summed per atom block here);
+    plus the repulsive potential when vrep is set.
+
+    ``geo`` carries the molecule's device tables: ind, typ, ls, ms (orbital tables), dircos (r, x, y, z),
+    mprox, pos, atype, sigma."""
+    nat, norb = geo.pos.shape[0], geo.ind.shape[0]
+    dev = geo.pos.device
+    P, st = native.ptr, native.stream()
+    t = par.device_tables(dev)
+    r, x, y, z = geo.dircos
+    out = torch.zeros(3 * nat, dtype=torch.float64, device=dev)
+    if XS is not None or XH is not None:
+        XSs = (XS + XS.T).contiguous() if XS is not None else None
+        XHs = (XH + XH.T).contiguous() if XH is not None else None
+        g = torch.empty(3 * nat, dtype=torch.float64, device=dev)
+        native.call("dftb_sk_gradient_contract", norb, nat, P(geo.ind), P(geo.typ), P(geo.ls), P(geo.ms), P(r),
+                    P(x), P(y), P(z), P(geo.mprox), par.deg, P(t["tab_filled_SH0"]), P(t["S_knots"]),
+                    P(t["S_coefs"]), P(t["H_knots"]), P(t["H_coefs"]), par.npair, par.nsk, par.npts, P(XSs), P(XHs),
+                    P(g), st)
+        out += g
+    if Yg is not None or Ylr is not None or vrep:
+        Ygs = _block_sum(Yg + Yg.T, geo.ind, nat).contiguous() if Yg is not None else None
+        Ylrs = _block_sum(Ylr + Ylr.T, geo.ind, nat).contiguous() if Ylr is not None else None
+        g = torch.empty(3 * nat, dtype=torch.float64, device=dev)
+        native.call("dftb_pair_gradients", nat, P(geo.pos), P(geo.atype), P(geo.sigma), float(r_lr), P(Ygs),
+                    P(Ylrs), P(t["vrep_knots"]) if vrep else None, P(t["vrep_coefs"]), P(t["vrep_dmax"]),
+                    par.vrep_nknots, P(g), st)
+        out += g
+    return out
+
+
+class _Geometry:
+    """The device tables of a DFTB2 object that contract() reads."""
+
+    def __init__(self, d):
+        self.ind, self.typ, self.ls, self.ms = d._ind, d._typ, d._ls, d._ms
+        self.dircos, self.mprox, self.pos = d._dircos, d.Mproximity, d.pos
+        self.atype, self.sigma = d._atype, d._sigma
 
 
 class Gradients:
@@ -105,34 +153,8 @@ class Gradients:
                 XmY, XpY)
 
     def _contract(self, XS, XH, Yg, Ylr, vrep):
-        """3 Nat gradient from the adjoints: SK pair derivatives against XS, XH; gamma and gamma^lr
-        derivatives against Yg, Ylr; plus the repulsive potential when vrep is set."""
         d = self.dftb
-        nat = len(d.atomlist)
-        dev = d.device
-        P, st = native.ptr, native.stream()
-        t = d.par.device_tables(dev)
-        p = d.par
-        r, x, y, z = d._dircos
-        out = torch.zeros(3 * nat, dtype=torch.float64, device=dev)
-        if XS is not None or XH is not None:
-            XSs = (XS + XS.T).contiguous() if XS is not None else None
-            XHs = (XH + XH.T).contiguous() if XH is not None else None
-            g = torch.empty(3 * nat, dtype=torch.float64, device=dev)
-            native.call("dftb_sk_gradient_contract", d.dim, nat, P(d._ind), P(d._typ), P(d._ls), P(d._ms), P(r),
-                        P(x), P(y), P(z), P(d.Mproximity), p.deg, P(t["tab_filled_SH0"]), P(t["S_knots"]),
-                        P(t["S_coefs"]), P(t["H_knots"]), P(t["H_coefs"]), p.npair, p.nsk, p.npts, P(XSs), P(XHs),
-                        P(g), st)
-            out += g
-        if Yg is not None or Ylr is not None or vrep:
-            Ygs = _block_sum(Yg + Yg.T, d._ind, nat).contiguous() if Yg is not None else None
-            Ylrs = _block_sum(Ylr + Ylr.T, d._ind, nat).contiguous() if Ylr is not None else None
-            g = torch.empty(3 * nat, dtype=torch.float64, device=dev)
-            native.call("dftb_pair_gradients", nat, P(d.pos), P(d._atype), P(d._sigma), float(d.long_range_radius),
-                        P(Ygs), P(Ylrs), P(t["vrep_knots"]) if vrep else None, P(t["vrep_coefs"]),
-                        P(t["vrep_dmax"]), p.vrep_nknots, P(g), st)
-            out += g
-        return out
+        return contract(_Geometry(d), d.par, d.long_range_radius, XS, XH, Yg, Ylr, vrep)
 
     def _products(self, qov, omega, Co, Cv):
         """(A+B).V on (nov, m) columns for the Z-vector equation (Solver._ApBv, Solver.py:583-609)."""

@@ -88,3 +88,32 @@ def test_batched_diis_matches_oracle_diis():
             if mask[b]:
                 np.testing.assert_allclose(out[b], ref[b].next_approximation(P[b]), rtol=1e-12, atol=1e-12)
             np.testing.assert_allclose(rel[b], ref[b].relative_change(), rtol=1e-12)
+
+
+@pytest.mark.parametrize("lc", [1, 0])
+def test_batched_gradient_adjoints_match_oracle(lc):
+    """The lockstep gradient algebra (adjoints of F, F^lr, the Z-vector, W) of a padded group, contracted
+    with the oracle's dense derivative tensors, equals the oracle's gradients molecule by molecule."""
+    from dftbaby_b200.batched_dynamics import batched_adjoints
+    from oracle import gradients_oracle as G
+    mols_al = [geometry.polyene(4, sigma=0.03, seed=21), geometry.polyene(6, sigma=0.03, seed=22)]
+    mols = [_mol_inputs(al, lc) for al in mols_al]
+    grp = batched._Group(mols, torch.device("cpu"))
+    scc, _ = batched._lockstep_scc(grp, lc)
+    exc = batched._excited(grp, lc, scc, 3, 1e-10, 200)
+    XS, XH, Yg, Ylr = batched_adjoints(grp, lc, scc, exc, 1)
+    for b, al in enumerate(mols_al):
+        td = O.LR_TDDFTB(al, long_range_correction=lc)
+        td.setGeometry(al)
+        td.getEnergies(nstates=3, diag_conv=1e-10, diag_maxiter=200)
+        ref = np.sum(G.Gradients(td).gradient(1), axis=0)
+        d = td.dftb2
+        n = d.dim
+        gS, gH = G.gradients_H0andS(d)
+        _, _, _, g1 = G.gamma_AOwise(d, lr=False)
+        mine = (np.einsum("kab,ab->k", gS, XS[b, :n, :n].numpy()) + np.einsum("kab,ab->k", gH, XH[b, :n, :n].numpy())
+                + np.einsum("kab,ab->k", g1, Yg[b, :n, :n].numpy()) + G.gradient_Vrep(d))
+        if lc:
+            _, _, _, g1lr = G.gamma_AOwise(d, lr=True)
+            mine = mine + np.einsum("kab,ab->k", g1lr, Ylr[b, :n, :n].numpy())
+        np.testing.assert_allclose(mine, ref, rtol=0, atol=1e-8)

@@ -85,3 +85,23 @@ def test_warm_start_after_a_small_step_needs_fewer_iterations():
     assert np.abs(Ow - Oc).max() * 27.211396132 < 1e-3
     print("Davidson iterations: cold %d, warm-started after a 0.002 bohr displacement %d" % (cold_iters, warm_iters))
     assert warm_iters < cold_iters
+
+
+def test_batched_trajectories_match_single_trajectories():
+    """Lockstep trajectories of molecules of uneven size follow the one-molecule trajectories."""
+    native.load()
+    from dftbaby_b200.batched_dynamics import BatchedTrajectories
+    from dftbaby_b200.dynamics import Trajectory
+    geoms = [geometry.polyene(6, sigma=0.03, seed=s) for s in range(3)] + [geometry.polyene(8, sigma=0.03, seed=9)]
+    bt = BatchedTrajectories(geoms, state=1, nstates=3, seed=5, diag_conv=1e-9)
+    singles = [Trajectory(al, state=1, nstates=3, seed=5 + j, diag_conv=1e-9) for j, al in enumerate(geoms)]
+    for j, t in enumerate(singles):
+        assert abs(bt.E_pot[j] - t.E_pot) < 1e-9
+        assert np.abs(bt.a[j] - t.a).max() < 1e-9 * max(1.0, np.abs(t.a).max())
+    for _ in range(2):
+        bt.step()
+        for t in singles:
+            t.step()
+    for j, t in enumerate(singles):
+        assert np.abs(bt.x[j] - t.x).max() < 1e-9
+        assert abs(bt.E_pot[j] - t.E_pot) < 1e-8
