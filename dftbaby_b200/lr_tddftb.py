@@ -102,11 +102,18 @@ class ExchangeMixed(ExchangeAO):
         N_xy = Gamma o (X_o W_y), stored and transposed (fused epilogue)
         P1^T = Ybar^T N,  P2^T = Ybar^T N^T            (K = 2 Norb)
         K1^T = P1^T Xbar_o / 4,  K2^T = P2^T Xbar_o / 4
-    with Ybar = [S~_v; C_v] and Xbar = [S~_o; C_o].  The Coulomb term stays
-    FP64 (native q_ov products).
+    with Ybar = [S~_v; C_v] and Xbar = [S~_o; C_o].
+
+    The Coulomb term 4 q_ov^T gamma q_ov V stays FP64 (native q_ov products)
+    unless coulomb_on_tensor_cores is set: then it runs as two skinny
+    split-precision GEMMs, T = q_ov V (K = nocc nvirt, split-K) and
+    U = q_ov^T (gamma T) (K = Nat).  Its ~2^-16 relative error on a term of
+    electronvolt size leaves residuals near 1e-6, so a 1e-6 threshold needs
+    the FP64 Coulomb term (or the FP64 refinement stage).
     """
 
-    def __init__(self, gamma, G_lr, q_ov, omega_flat, Co, Cv, S, nat, nocc, nvirt, workspace, lc=1):
+    def __init__(self, gamma, G_lr, q_ov, omega_flat, Co, Cv, S, nat, nocc, nvirt, workspace, lc=1,
+                 coulomb_on_tensor_cores=False):
         from . import tcgemm as T
         super().__init__(gamma, G_lr, q_ov, omega_flat, Co, Cv, S, nat, nocc, nvirt, workspace, lc=lc,
                          max_bytes=1)
@@ -128,6 +135,13 @@ class ExchangeMixed(ExchangeAO):
         self.K1t = torch.empty((nvirt, nocc), dtype=torch.float32, device=dev)
         self.K2t = torch.empty((nvirt, nocc), dtype=torch.float32, device=dev)
         self.Vp = T.Pair(nocc, nvirt, dev)
+        self.coulomb_on_tensor_cores = coulomb_on_tensor_cores
+        if coulomb_on_tensor_cores:
+            # Coulomb operands: q_ov and its transpose as BF16 hi/lo pairs
+            q2 = q_ov.reshape(nat, -1)
+            self.QOV = T.split(q2)                     # (Nat, nov), K = nov
+            self.QOVT = T.split(q2, transpose=True)    # (nov, Nat), K = Nat
+            self._colpairs = {}
         # views for the per-y blocks (y = C, S~)
         self.Wy, self.outN, self.outT = [], [], []
         for y in range(2):
@@ -143,6 +157,31 @@ class ExchangeMixed(ExchangeAO):
             t.rows, t.cols, t.ld = norb, 2 * norb, self.NT.ld
             t.hi, t.lo = self.NT.hi[y * norb:], self.NT.lo[y * norb:]
             self.outT.append(t)
+
+    def _pairs(self, m):
+        """Column-block operands padded to at least 128 rows (one tensor-core tile)."""
+        rows = max(128, m)
+        if rows not in self._colpairs:
+            dev = self.Vp.hi.device
+            self._colpairs[rows] = (self.T.Pair(rows, self.omega.numel(), dev), self.T.Pair(rows, self.nat, dev))
+        return self._colpairs[rows]
+
+    def coulomb(self, V):
+        """u = omega v + 4 q_ov^T gamma q_ov v; both q_ov products on the tensor cores if enabled."""
+        if not self.coulomb_on_tensor_cores:
+            return super().coulomb(V)
+        T = self.T
+        V = V.contiguous()
+        nov, m = V.shape
+        Vt, Gt = self._pairs(m)
+        T.split(V, transpose=True, out=Vt)
+        Tm = torch.empty((self.nat, Vt.rows), dtype=torch.float32, device=V.device)
+        T.gemm(self.QOV, Vt, K=nov, out=Tm)
+        G = self.gamma @ Tm[:, :m].double()
+        T.split(G, transpose=True, out=Gt)
+        U = torch.empty((nov, Gt.rows), dtype=torch.float32, device=V.device)
+        T.gemm(self.QOVT, Gt, K=self.nat, out=U)
+        return self.omega[:, None] * V + 4.0 * U[:, :m].double()
 
     def exchange(self, V):
         T = self.T

@@ -41,6 +41,11 @@ def test_mixed_exchange_products_match_fp64():
     for a, b in ((K1m, K1r), (K2m, K2r)):
         rel = (a - b).abs().max().item() / b.abs().max().item()
         assert rel < 2e-4, rel
+    # the optional Coulomb product on the tensor cores against the native FP64 one
+    mix_c = ExchangeMixed(*args, lc=1, coulomb_on_tensor_cores=True)
+    Cm, Cr = mix_c.coulomb(V), ref.coulomb(V)
+    rel = ((Cm - Cr).abs().max() / (Cr - omega.reshape(-1, 1) * V).abs().max()).item()
+    assert rel < 2e-4, rel
 
 
 def test_mixed_solve_within_1meV_and_refined_solve_matches_fp64():
