@@ -313,7 +313,8 @@ def run_ensemble(args, w, rank, world, barrier):
                     "d2h_bytes_per_step": int(16 * nstates_total)},
             "gpu_launches": native.counters.launches, "clocks": clocks, "roofline": None,
             "solver": {"scc_iterations_max_per_group": [max(x) for x in stats["scc_iterations"]],
-                       "davidson_iterations_max_per_group": [max(x) for x in stats["davidson_iterations"]]},
+                       "davidson_iterations_max_per_group": [max(x) for x in stats["davidson_iterations"]],
+                       "phase_ms_per_group": stats.get("phase_ms")},
             "plain_fp64": {"value": nstates_total / (plain_ms / 1e3), "ms_per_step": plain_ms,
                            "how": "one-molecule FP64 path on %d seeded members, extrapolated" % len(sub),
                            "max_dOmega_meV": dmax, "max_df": fmax},

@@ -214,6 +214,7 @@ class BatchedLR_TDDFTB:
             self.stats["groups"].append(len(idx))
             self.stats["scc_iterations"].append(it_scc)
             self.stats["davidson_iterations"].append(it_dav)
+            self.stats.setdefault("phase_ms", []).append(getattr(solve_group, "last_phase_ms", None))
         return self.Omega, self.oscillator_strength
 
 
@@ -438,10 +439,22 @@ def solve_group(mols, lc, dev, nstates, conv, dmaxiter, scf_conv=1.0e-10, maxite
     ``mols`` hold per-molecule tensors on ``dev``: S, H0 (norb, norb), D (3, norb, norb), g, glr
     (nat, nat), p0 (norb,) reference occupations, ind (norb,) orbital -> atom, and the ints nat,
     norb, nelec.  Returns (Omega (B, nstates), f (B, nstates), SCC iterations, Davidson iterations)."""
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)] if dev.type == "cuda" else None
+    if ev:
+        ev[0].record()
     G = _Group(mols, dev)
+    if ev:
+        ev[1].record()
     scc, scc_it = _lockstep_scc(G, lc, scf_conv, maxiter, mix_thr, alpha, diis_m, level_shift, homo_lumo_tol)
+    if ev:
+        ev[2].record()
     exc = _excited(G, lc, scc, nstates, conv, dmaxiter)
     fosc = _oscillator_strengths(G, exc)
+    if ev:
+        ev[3].record()
+        ev[3].synchronize()
+        solve_group.last_phase_ms = {"padding": ev[0].elapsed_time(ev[1]), "scc": ev[1].elapsed_time(ev[2]),
+                                     "excited": ev[2].elapsed_time(ev[3])}
     return exc["Om"].cpu().numpy(), fosc.cpu().numpy(), scc_it.tolist(), exc["dav_it"]
 
 
@@ -611,11 +624,40 @@ def _orthonormal_extension(bs, Q, live):
         for _ in range(2):
             R = R - torch.bmm(bs, torch.bmm(bs.transpose(1, 2), R))
         Q = torch.where(bad[:, None, :], R, Q)
-    Q, _ = torch.linalg.qr(Q)
-    Q = Q * keep[:, None, :]
+    Q = _column_gram_schmidt(Q, keep)
     Q = Q - torch.bmm(bs, torch.bmm(bs.transpose(1, 2), Q))
-    Q, _ = torch.linalg.qr(Q)
-    return Q * keep[:, None, :], keep
+    Q = _column_gram_schmidt(Q, keep)
+    return Q, keep
+
+
+def _column_gram_schmidt(Q, keep):
+    """Orthonormalise the columns of every block of Q (B, n, m) among themselves, column by column
+    with re-orthogonalisation (CGS2); columns outside keep come back as zeros.  The same span as a
+    QR factorisation of the kept columns, but batched over the molecules (a batched QR runs one
+    factorisation per molecule).  A column that is (numerically) inside the span of the earlier ones
+    is replaced by the component of a seeded random vector orthogonal to them."""
+    B, n, m = Q.shape
+    out = torch.zeros_like(Q)
+    g = None
+    for j in range(m):
+        v = Q[:, :, j]
+        n0 = torch.linalg.norm(v, dim=1)
+        for _ in range(2):
+            if j > 0:
+                v = v - torch.bmm(out[:, :, :j], torch.bmm(out[:, :, :j].transpose(1, 2), v[:, :, None]))[:, :, 0]
+        nrm = torch.linalg.norm(v, dim=1)
+        bad = keep[:, j] & (nrm <= 1.0e-10 * n0.clamp_min(1e-300))
+        if bool(bad.any()):
+            if g is None:
+                g = torch.Generator(device=Q.device).manual_seed(4242)
+            r = torch.randn((B, n), dtype=Q.dtype, device=Q.device, generator=g)
+            for _ in range(2):
+                if j > 0:
+                    r = r - torch.bmm(out[:, :, :j], torch.bmm(out[:, :, :j].transpose(1, 2), r[:, :, None]))[:, :, 0]
+            v = torch.where(bad[:, None], r, v)
+            nrm = torch.linalg.norm(v, dim=1)
+        out[:, :, j] = torch.where(keep[:, j, None], v / nrm.clamp_min(1e-300)[:, None], torch.zeros_like(v))
+    return out
 
 
 def _pad_dead(M, live, pad=PAD_SUB):
@@ -629,8 +671,8 @@ def _guess_basis(guess, k, B, nov, dev):
     XmY, XpY = guess
     cols = torch.cat([XmY, XpY], dim=1).transpose(1, 2)                    # (B, nov, 2k)
     cols = cols / torch.linalg.norm(cols, dim=1, keepdim=True).clamp_min(1e-300)
-    bs, _ = torch.linalg.qr(cols)
-    return bs.contiguous(), torch.ones((B, bs.shape[2]), dtype=torch.bool, device=dev)
+    live = torch.ones((B, cols.shape[2]), dtype=torch.bool, device=dev)
+    return _column_gram_schmidt(cols, live).contiguous(), live
 
 
 def _batched_hermitian(prod, om, k, conv, maxiter, kmax, guess=None):
@@ -648,8 +690,8 @@ def _batched_hermitian(prod, om, k, conv, maxiter, kmax, guess=None):
         # T is proportional to (X+Y)/sqrt(omega): the previous X+Y give the start block
         cols = (guess[1] / sq[:, None, :]).transpose(1, 2)
         cols = cols / torch.linalg.norm(cols, dim=1, keepdim=True).clamp_min(1e-300)
-        bs = torch.linalg.qr(cols)[0].contiguous()
         live = torch.ones((B, k), dtype=torch.bool, device=dev)
+        bs = _column_gram_schmidt(cols, live).contiguous()
     else:
         idx = torch.argsort(om, dim=1, stable=True)[:, :k]
         bs = torch.zeros((B, nov, k), dtype=f64, device=dev)
