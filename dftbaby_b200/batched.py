@@ -461,7 +461,8 @@ def solve_group(mols, lc, dev, nstates, conv, dmaxiter, scf_conv=1.0e-10, maxite
 class _BatchedDIIS:
     """DIIS_80 (ConvAcceleration.py:27-143) for a batch: every molecule keeps its own history of
     up to m trial vectors; the bookkeeping (pop when longer than m, start once the relative
-    change of a longer-than-3 history drops below 0.5) is the reference's, vectorised."""
+    change of a longer-than-3 history drops below 0.5) is the reference's, vectorised over the
+    molecules."""
 
     def __init__(self, B, n, m, dev):
         self.B, self.m, self.dev = B, m, dev
@@ -475,57 +476,59 @@ class _BatchedDIIS:
         idx = np.nonzero(mask)[0]
         if len(idx) == 0:
             return out
-        m = self.m
+        m, dev = self.m, self.dev
         # append the new trial vector (rolling window of m)
-        for b in idx:
-            nt = self.nt[b]
-            if nt == m:
-                self.trial[b, :-1] = self.trial[b, 1:].clone()
-                self.resid[b, :-1] = self.resid[b, 1:].clone()
-                nt = m - 1
-            self.trial[b, nt] = Pflat[b]
-            if nt >= 1:
-                self.resid[b, nt - 1] = self.trial[b, nt] - self.trial[b, nt - 1]
-            self.nt[b] = nt + 1
-        run = [b for b in idx if self.start[b]]
-        if run:
-            rb = torch.as_tensor(run, device=self.dev)
-            nres = np.array([self.nt[b] - 1 for b in run])
+        full = idx[self.nt[idx] == m]
+        if len(full):
+            ft = torch.as_tensor(full, device=dev)
+            self.trial[ft] = torch.roll(self.trial[ft], -1, dims=1)
+            self.resid[ft] = torch.roll(self.resid[ft], -1, dims=1)
+            self.nt[full] = m - 1
+        it = torch.as_tensor(idx, device=dev)
+        nt = torch.as_tensor(self.nt[idx], device=dev)
+        self.trial[it, nt] = Pflat[it]
+        has = idx[self.nt[idx] >= 1]
+        if len(has):
+            ht = torch.as_tensor(has, device=dev)
+            nh = torch.as_tensor(self.nt[has], device=dev)
+            self.resid[ht, nh - 1] = self.trial[ht, nh] - self.trial[ht, nh - 1]
+        self.nt[idx] += 1
+        run = idx[self.start[idx]]
+        if len(run):
+            rb = torch.as_tensor(run, device=dev)
+            nres = self.nt[run] - 1
             n = int(nres.max())
             R = self.resid[rb, :n]
             gram = torch.bmm(R, R.transpose(1, 2))
-            A = torch.zeros((len(run), n + 1, n + 1), dtype=torch.float64, device=self.dev)
-            rhs = torch.zeros((len(run), n + 1), dtype=torch.float64, device=self.dev)
-            for j, nr in enumerate(nres):
-                A[j, :nr, :nr] = gram[j, :nr, :nr]
-                A[j, :nr, nr] = A[j, nr, :nr] = -1.0
-                rhs[j, nr] = -1.0
-                for q in range(nr + 1, n + 1):
-                    A[j, q, q] = 1.0
-            c = torch.linalg.solve(A, rhs)
-            for j, b in enumerate(run):
-                nr = int(nres[j])
-                p = torch.einsum("i,in->n", c[j, :nr], self.trial[b, :nr])
-                self.trial[b, nr] = p
-                self.resid[b, nr - 1] = p - self.trial[b, nr - 1]
-                out[b] = p
-        late = [b for b in idx if not self.start[b] and self.nt[b] > 3]
-        if late:
-            lb = torch.as_tensor(late, device=self.dev)
-            nt = torch.as_tensor([self.nt[b] for b in late], device=self.dev)
+            nr = torch.as_tensor(nres, device=dev)
+            ar = torch.arange(n + 1, device=dev)
+            inside = (ar[None, :] < nr[:, None]).to(torch.float64)              # (r, n+1)
+            onehot = (ar[None, :] == nr[:, None]).to(torch.float64)
+            A = torch.zeros((len(run), n + 1, n + 1), dtype=torch.float64, device=dev)
+            A[:, :n, :n] = gram
+            A = A * inside[:, :, None] * inside[:, None, :]
+            A = A - inside[:, :, None] * onehot[:, None, :] - onehot[:, :, None] * inside[:, None, :]
+            A = A + torch.diag_embed((ar[None, :] > nr[:, None]).to(torch.float64))
+            c = torch.linalg.solve(A, -onehot)
+            p = torch.einsum("ri,rin->rn", c[:, :n] * inside[:, :n], self.trial[rb, :n])
+            self.trial[rb, nr] = p
+            self.resid[rb, nr - 1] = p - self.trial[rb, nr - 1]
+            out[rb] = p
+        late = idx[~self.start[idx] & (self.nt[idx] > 3)]
+        if len(late):
+            lb = torch.as_tensor(late, device=dev)
+            nt = torch.as_tensor(self.nt[late], device=dev)
             r = torch.linalg.norm(self.resid[lb, nt - 2], dim=1) / torch.linalg.norm(self.trial[lb, nt - 1], dim=1)
-            for b, v in zip(late, r.cpu().numpy()):
-                if v < 0.5:
-                    self.start[b] = True
+            self.start[late[r.cpu().numpy() < 0.5]] = True
         return out
 
     def relative_change(self):
         ch = torch.ones(self.B, dtype=torch.float64, device=self.dev)
-        have = [b for b in range(self.B) if self.nt[b] >= 2]
-        if not have:
+        have = np.nonzero(self.nt >= 2)[0]
+        if len(have) == 0:
             return ch
         hb = torch.as_tensor(have, device=self.dev)
-        nt = torch.as_tensor([self.nt[b] for b in have], device=self.dev)
+        nt = torch.as_tensor(self.nt[have], device=self.dev)
         r1 = torch.linalg.norm(self.resid[hb, nt - 2], dim=1) / torch.linalg.norm(self.trial[hb, nt - 1], dim=1)
         two = nt >= 3
         r2 = torch.linalg.norm(self.resid[hb, (nt - 3).clamp_min(0)], dim=1) / torch.linalg.norm(
@@ -660,6 +663,14 @@ def _column_gram_schmidt(Q, keep):
     return out
 
 
+def _extend_projection(M, bs, Q, AB, AQ):
+    """Projected matrix of the basis [bs, Q] from the one of bs: the new blocks bs^T AQ, Q^T AB and
+    Q^T AQ (the same dot products a full bs^T A bs would form, without recomputing the old block)."""
+    top = torch.cat([M, torch.bmm(bs.transpose(1, 2), AQ)], 2)
+    bottom = torch.cat([torch.bmm(Q.transpose(1, 2), AB), torch.bmm(Q.transpose(1, 2), AQ)], 2)
+    return torch.cat([top, bottom], 1)
+
+
 def _pad_dead(M, live, pad=PAD_SUB):
     """Projected matrix with pad on the diagonal of unused columns: the dead block decouples and
     its eigenvalues sort above every wanted live one."""
@@ -698,12 +709,12 @@ def _batched_hermitian(prod, om, k, conv, maxiter, kmax, guess=None):
         bs[torch.arange(B, device=dev)[:, None], idx, torch.arange(k, device=dev)[None, :]] = 1.0
         live = torch.ones((B, k), dtype=torch.bool, device=dev)
     RB = rv(bs)
+    Hb = torch.bmm(bs.transpose(1, 2), RB)
     active = np.ones(B, bool)
     Om = torch.zeros((B, k), dtype=f64, device=dev)
     T = torch.zeros((B, nov, k), dtype=f64, device=dev)
     iters = np.zeros(B, int)
     for it in range(maxiter):
-        Hb = torch.bmm(bs.transpose(1, 2), RB)
         w2, Tb = batched_eigh(_pad_dead(0.5 * (Hb + Hb.transpose(1, 2)), live, PAD_SUB_SQ))
         w = torch.sqrt(w2.clamp_min(0.0))
         Tk = torch.bmm(bs, Tb[:, :, :k])
@@ -722,9 +733,11 @@ def _batched_hermitian(prod, om, k, conv, maxiter, kmax, guess=None):
         wD = w[:, None, :k] - om[:, :, None]
         wD = torch.where(wD.abs() < 1e-6, 1e-6 * om[:, :, None].expand_as(wD), wD)
         Q, qlive = _orthonormal_extension(bs, W / wD, torch.as_tensor(sel, device=dev))
+        RQ = rv(Q)
+        Hb = _extend_projection(Hb, bs, Q, RB, RQ)
         bs = torch.cat([bs, Q], 2)
         live = torch.cat([live, qlive], 1)
-        RB = torch.cat([RB, rv(Q)], 2)
+        RB = torch.cat([RB, RQ], 2)
     else:
         raise ExcitedStatesNotConverged("batched Davidson: %d molecules did not converge" % int(active.sum()))
     C = T.transpose(1, 2)
@@ -750,6 +763,8 @@ def _batched_nonhermitian(prod, om, k, conv, maxiter, kmax, guess=None):
         bs[torch.arange(B, device=dev)[:, None], idx, torch.arange(k, device=dev)[None, :]] = 1.0
         live = torch.ones((B, k), dtype=torch.bool, device=dev)
     AP, AM = prod(bs)
+    Mp0 = torch.bmm(bs.transpose(1, 2), AP)
+    Mm0 = torch.bmm(bs.transpose(1, 2), AM)
     active = np.ones(B, bool)
     Om = torch.zeros((B, k), dtype=f64, device=dev)
     C = torch.zeros((B, k, nov), dtype=f64, device=dev)
@@ -757,8 +772,8 @@ def _batched_nonhermitian(prod, om, k, conv, maxiter, kmax, guess=None):
     XpY = torch.zeros_like(C)
     iters = np.zeros(B, int)
     for it in range(maxiter):
-        Mp = _pad_dead(torch.bmm(bs.transpose(1, 2), AP), live)
-        Mm = _pad_dead(torch.bmm(bs.transpose(1, 2), AM), live)
+        Mp = _pad_dead(Mp0, live)
+        Mm = _pad_dead(Mm0, live)
         lam, Vm = batched_eigh(0.5 * (Mm + Mm.transpose(1, 2)))
         if bool((lam[torch.as_tensor(active, device=dev)] <= 0).any()):
             raise ExcitedStatesError("(A-B) projected onto the expansion space is not positive definite")
@@ -795,6 +810,8 @@ def _batched_nonhermitian(prod, om, k, conv, maxiter, kmax, guess=None):
         wD = torch.where(small, 1e-6 * om[:, :, None].expand_as(wD), wD)
         Q, qlive = _orthonormal_extension(bs, torch.cat([WL / wD, WR / wD], dim=2), torch.as_tensor(sel, device=dev))
         ap, am = prod(Q)
+        Mp0 = _extend_projection(Mp0, bs, Q, AP, ap)
+        Mm0 = _extend_projection(Mm0, bs, Q, AM, am)
         bs = torch.cat([bs, Q], 2)
         live = torch.cat([live, qlive], 1)
         AP = torch.cat([AP, ap], 2)

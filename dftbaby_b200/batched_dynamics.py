@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import native
-from .batched import BatchedLR_TDDFTB, _excited, _Group, _lockstep_scc, _orthonormal_extension
+from .batched import BatchedLR_TDDFTB, _excited, _extend_projection, _Group, _lockstep_scc, _orthonormal_extension
 from .dynamics import _constants
 from .exceptions import ExcitedStatesNotConverged
 from .gradients import _F_adjoint, _Flr_adjoint, contract
@@ -44,10 +44,11 @@ def _zvector(A, Adiag, R, conv=1.0e-14, maxiter=1000):
     live = (nrm[:, 0] > 0.0)
     bs = torch.where(live[:, None, :], b0 / nrm.clamp_min(1e-300), torch.zeros_like(b0))
     AB = A(bs)
+    M = torch.bmm(bs.transpose(1, 2), AB)
     active = np.ones(Bn, bool)
     X = torch.zeros((Bn, nov), dtype=R.dtype, device=dev)
     for it in range(maxiter):
-        Ab = torch.bmm(bs.transpose(1, 2), AB) + torch.diag_embed((~live).to(R.dtype))
+        Ab = M + torch.diag_embed((~live).to(R.dtype))
         Xb = torch.linalg.solve(Ab, torch.bmm(bs.transpose(1, 2), R[:, :, None]))
         Xn = torch.bmm(bs, Xb)[:, :, 0]
         W = torch.bmm(AB, Xb)[:, :, 0] - R
@@ -59,9 +60,11 @@ def _zvector(A, Adiag, R, conv=1.0e-14, maxiter=1000):
             return X, it + 1
         sel = torch.as_tensor(active & (norms > 0.01 * conv), device=dev)[:, None]
         Q, qlive = _orthonormal_extension(bs, (Ainv * W)[:, :, None], sel)
+        AQ = A(Q)
+        M = _extend_projection(M, bs, Q, AB, AQ)
         bs = torch.cat([bs, Q], 2)
         live = torch.cat([live, qlive], 1)
-        AB = torch.cat([AB, A(Q)], 2)
+        AB = torch.cat([AB, AQ], 2)
     raise ExcitedStatesNotConverged("batched Z-vector equations did not converge after %d iterations" % maxiter)
 
 
