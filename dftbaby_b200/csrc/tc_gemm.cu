@@ -42,6 +42,74 @@ constexpr int BM = 128, BN = 128, BK = 64;
 constexpr int TILE_A_BYTES = BM * BK * 2;  // 16 KiB
 // segment mode: one (A, B) tile pair per stage, 4 stages;
 // shared-split mode: A_hi, A_lo, B_hi, B_lo per stage (three MMAs reuse them), 3 stages
+// Row-chunk moves of the epilogue: 16 consecutive elements of one row, as 16- or 8-byte words
+// when the address is aligned and the chunk is whole, element by element otherwise.
+__device__ __forceinline__ void load_row16(const float *src, int n, float out[16]) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+    if (n == 16 && (a & 15) == 0) {
+        const float4 *s4 = reinterpret_cast<const float4 *>(src);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float4 t = s4[q];
+            out[4 * q] = t.x;
+            out[4 * q + 1] = t.y;
+            out[4 * q + 2] = t.z;
+            out[4 * q + 3] = t.w;
+        }
+    } else if (n == 16 && (a & 7) == 0) {
+        const float2 *s2 = reinterpret_cast<const float2 *>(src);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float2 t = s2[q];
+            out[2 * q] = t.x;
+            out[2 * q + 1] = t.y;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) out[j] = j < n ? src[j] : 0.0f;
+    }
+}
+
+__device__ __forceinline__ void store_row16(float *dst, int n, const float v[16]) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(dst);
+    if (n == 16 && (a & 15) == 0) {
+        float4 *d4 = reinterpret_cast<float4 *>(dst);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) d4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    } else if (n == 16 && (a & 7) == 0) {
+        float2 *d2 = reinterpret_cast<float2 *>(dst);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) d2[q] = make_float2(v[2 * q], v[2 * q + 1]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            if (j < n) dst[j] = v[j];
+    }
+}
+
+__device__ __forceinline__ void store_row16_bf16(__nv_bfloat16 *dst, int n, const __nv_bfloat16 v[16]) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(dst);
+    uint32_t w[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const __nv_bfloat162 pr = __halves2bfloat162(v[2 * q], v[2 * q + 1]);
+        w[q] = *reinterpret_cast<const uint32_t *>(&pr);
+    }
+    if (n == 16 && (a & 15) == 0) {
+        uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+        d4[0] = make_uint4(w[0], w[1], w[2], w[3]);
+        d4[1] = make_uint4(w[4], w[5], w[6], w[7]);
+    } else if (n == 16 && (a & 3) == 0) {
+        uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) d[q] = w[q];
+    } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            if (j < n) dst[j] = v[j];
+    }
+}
+
 template <bool SPLIT> struct Cfg {
     // 128 x 128 output tiles in both modes (128 x 256 tiles with two stages measured slower in the
     // solver: the mainloop is bound by copy latency, not by operand bytes)
@@ -279,26 +347,45 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Ma
         float v[16];
         tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
         if (!live) continue;
+        const int col0 = n0 + c0;
+        if (row >= p.M || col0 >= p.N) continue;
+        const int ncol = min(16, p.N - col0);
+        if (p.ksplit > 1) {  // partial sums over this CTA's K range
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const int col = n0 + c0 + j;
-            float x = p.alpha * v[j];
-            if (row < p.M && col < p.N) {
-                if (p.ksplit > 1) {  // partial sum over this CTA's K range
-                    atomicAdd(&p.C[(long long)row * p.ldc + col], x);
-                    continue;
-                }
-                if (p.G) x *= p.G[(long long)row * p.ldg + col];
-                if (p.C) p.C[(long long)row * p.ldc + col] = x;
-                const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-                const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-                if (p.Ohi) {
-                    p.Ohi[(long long)row * p.ldo + col] = hi;
-                    p.Olo[(long long)row * p.ldo + col] = lo;
-                }
-                if (p.Thi) {
-                    p.Thi[(long long)col * p.ldt + row] = hi;  // coalesced across the warp (consecutive rows)
-                    p.Tlo[(long long)col * p.ldt + row] = lo;
+            for (int j = 0; j < 16; ++j)
+                if (j < ncol) atomicAdd(&p.C[(long long)row * p.ldc + col0 + j], p.alpha * v[j]);
+            continue;
+        }
+        // Each thread owns 16 consecutive columns of one row: row-major reads and writes move them
+        // as whole 16/8/4-byte words where the address allows (the warp's 32 rows are 32 separate
+        // sectors either way); the transposed output stays element-wise, coalesced across the warp.
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] *= p.alpha;
+        if (p.G) {
+            float g[16];
+            load_row16(p.G + (long long)row * p.ldg + col0, ncol, g);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] *= g[j];
+        }
+        if (p.C) store_row16(p.C + (long long)row * p.ldc + col0, ncol, v);
+        if (p.Ohi || p.Thi) {
+            __nv_bfloat16 hi[16], lo[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                hi[j] = __float2bfloat16_rn(v[j]);
+                lo[j] = __float2bfloat16_rn(v[j] - __bfloat162float(hi[j]));
+            }
+            if (p.Ohi) {
+                store_row16_bf16(p.Ohi + (long long)row * p.ldo + col0, ncol, hi);
+                store_row16_bf16(p.Olo + (long long)row * p.ldo + col0, ncol, lo);
+            }
+            if (p.Thi) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    if (j < ncol) {
+                        p.Thi[(long long)(col0 + j) * p.ldt + row] = hi[j];
+                        p.Tlo[(long long)(col0 + j) * p.ldt + row] = lo[j];
+                    }
                 }
             }
         }
