@@ -34,15 +34,47 @@ def initial_expansion_vectors(omega_flat, lmax):
     return bs
 
 
+def orthonormal_columns(Q):
+    """Orthonormal basis of the column span of a tall block Q (nov, m), m small.
+
+    Cholesky QR applied twice: G = Q^T Q = L L^T, Q <- Q L^-T, which costs two
+    (nov x m x m) GEMMs per pass instead of a Householder factorisation of the
+    tall block.  The factor R of Q = Q' R is unique up to the signs of its
+    diagonal, so the result spans the same space as the Householder Q (columns
+    may differ in sign only).  When the Gram matrix is too ill-conditioned for
+    Cholesky (nearly dependent columns, condition number above ~1e7) or the
+    two passes leave |Q^T Q - 1| above 1e-12, the Householder QR of the input is
+    used instead, as DFTBaby's QR of the whole basis does.
+    """
+    m = Q.shape[1]
+    if m == 0:
+        return Q
+    Q0 = Q
+    eye = torch.eye(m, dtype=Q.dtype, device=Q.device)
+    ok = None
+    for _ in range(2):
+        G = Q.T @ Q
+        L, info = torch.linalg.cholesky_ex(0.5 * (G + G.T))
+        Linv = torch.linalg.solve_triangular(L, eye, upper=False)
+        Q = Q @ Linv.T
+        bad = (info != 0).reshape(())
+        ok = ~bad if ok is None else ok & ~bad
+    err = torch.max(torch.abs(Q.T @ Q - eye))
+    host = torch.stack([ok.to(torch.float64), err]).cpu().numpy()
+    if host[0] != 1.0 or not np.isfinite(host[1]) or host[1] > 1.0e-12:
+        Q, _ = torch.linalg.qr(Q0, mode="reduced")
+    return Q
+
+
 def orthonormalize_new(bs, Q):
-    """Orthonormalise the columns of Q against bs and among themselves (CGS2 + QR)."""
+    """Orthonormalise the columns of Q against bs (CGS2) and among themselves (Cholesky QR2)."""
     if bs is not None and bs.shape[1] > 0:
         for _ in range(2):
             Q = Q - bs @ (bs.T @ Q)
-    Q, _ = torch.linalg.qr(Q, mode="reduced")
+    Q = orthonormal_columns(Q)
     if bs is not None and bs.shape[1] > 0:
         Q = Q - bs @ (bs.T @ Q)
-        Q, _ = torch.linalg.qr(Q, mode="reduced")
+        Q = orthonormal_columns(Q)
     return Q
 
 
@@ -235,8 +267,7 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
         lmaxm = min(nstates, kmax - nstates)
         lmax = lmaxp + lmaxm
         cols = torch.cat([XmYguess.reshape(nstates, -1), XpYguess.reshape(nstates, -1)[:lmaxm]], dim=0).T
-        bs, _ = torch.linalg.qr(cols / torch.linalg.norm(cols, dim=0), mode="reduced")
-        bs = bs.contiguous()
+        bs = orthonormal_columns(cols / torch.linalg.norm(cols, dim=0)).contiguous()
     B = Basis(om.numel(), 2, dev, capacity=lmax + 8 * k)
     B.append(bs, list(products(bs)))
     l = lmax
