@@ -223,6 +223,30 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 32 consecutive accumulator columns of this warp's 32 TMEM lanes; load and wait in one statement so
+// no register is read before the load has landed
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Transposed-output staging in the (then idle) operand ring: [tile column][tile row] BF16, rows
+// padded to 136 elements (272 B) so that both the per-column writes of a warp (32 consecutive rows)
+// and the 16-byte row reads of the copy-out stay within the minimum number of bank wavefronts.
+constexpr int TPITCH = BM + 8;
+constexpr int TSTAGE_BYTES = 2 * 128 * TPITCH * 2;  // hi and lo, 128 tile columns
+
 template <bool SPLIT>
 __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Maps maps, const Params p) {
     constexpr int STAGES = Cfg<SPLIT>::STAGES, STAGE_BYTES = Cfg<SPLIT>::STAGE_BYTES;
@@ -266,6 +290,12 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Ma
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
+    if (p.G && p.ksplit == 1 && m0 + (int)threadIdx.x < p.M) {
+        // pull this tile's G rows into L2 while the mainloop runs (128-byte lines, inside the matrix)
+        const float *g = p.G + (long long)(m0 + threadIdx.x) * p.ldg + n0;
+        const int ncols = min(BNX, p.N - n0);
+        for (int c = 0; c < ncols; c += 32) asm volatile("prefetch.global.L2 [%0];" ::"l"(g + c));
+    }
 
     if (warp == 0 && lane == 0) {
         // ---------------- TMA producer
@@ -342,50 +372,90 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Ma
     if (!ok && threadIdx.x == 0) atomicExch(p.err, 3);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const bool live = ok && !*(volatile int *)abort_flag && total > 0;
-    const int row = m0 + warp * 32 + lane;  // TMEM lane = tile row
-    for (int c0 = 0; c0 < BNX; c0 += 16) {
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+    const int rloc = warp * 32 + lane;  // TMEM lane = tile row
+    const int row = m0 + rloc;
+    const bool stage_t = p.Thi != nullptr && p.ksplit == 1;
+    static_assert(TSTAGE_BYTES <= STAGES * STAGE_BYTES, "transpose staging must fit in the operand ring");
+    static_assert(BNX == 128, "transpose staging assumes 128 tile columns");
+    __nv_bfloat16 *ts_hi = reinterpret_cast<__nv_bfloat16 *>(smem);
+    __nv_bfloat16 *ts_lo = ts_hi + 128 * TPITCH;
+    for (int c0 = 0; c0 < BNX; c0 += 32) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
         if (!live) continue;
         const int col0 = n0 + c0;
         if (row >= p.M || col0 >= p.N) continue;
-        const int ncol = min(16, p.N - col0);
+        const int ncol = min(32, p.N - col0);
         if (p.ksplit > 1) {  // partial sums over this CTA's K range
 #pragma unroll
-            for (int j = 0; j < 16; ++j)
+            for (int j = 0; j < 32; ++j)
                 if (j < ncol) atomicAdd(&p.C[(long long)row * p.ldc + col0 + j], p.alpha * v[j]);
             continue;
         }
-        // Each thread owns 16 consecutive columns of one row: row-major reads and writes move them
-        // as whole 16/8/4-byte words where the address allows (the warp's 32 rows are 32 separate
-        // sectors either way); the transposed output stays element-wise, coalesced across the warp.
+        const int n1 = min(16, ncol), n2 = ncol - 16;  // the two 16-column halves (n2 <= 0: none)
+        // Each thread owns consecutive columns of one row: row-major reads and writes move them as
+        // whole 16/8/4-byte words where the address allows
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] *= p.alpha;
+        for (int j = 0; j < 32; ++j) v[j] *= p.alpha;
         if (p.G) {
-            float g[16];
-            load_row16(p.G + (long long)row * p.ldg + col0, ncol, g);
+            float g[32];
+            const float *gr = p.G + (long long)row * p.ldg + col0;
+            load_row16(gr, n1, g);
+            if (n2 > 0) load_row16(gr + 16, n2, g + 16);
 #pragma unroll
-            for (int j = 0; j < 16; ++j) v[j] *= g[j];
+            for (int j = 0; j < 32; ++j) v[j] *= g[j];
         }
-        if (p.C) store_row16(p.C + (long long)row * p.ldc + col0, ncol, v);
+        if (p.C) {
+            store_row16(p.C + (long long)row * p.ldc + col0, n1, v);
+            if (n2 > 0) store_row16(p.C + (long long)row * p.ldc + col0 + 16, n2, v + 16);
+        }
         if (p.Ohi || p.Thi) {
-            __nv_bfloat16 hi[16], lo[16];
+            __nv_bfloat16 hi[32], lo[32];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
+            for (int j = 0; j < 32; ++j) {
                 hi[j] = __float2bfloat16_rn(v[j]);
                 lo[j] = __float2bfloat16_rn(v[j] - __bfloat162float(hi[j]));
             }
             if (p.Ohi) {
-                store_row16_bf16(p.Ohi + (long long)row * p.ldo + col0, ncol, hi);
-                store_row16_bf16(p.Olo + (long long)row * p.ldo + col0, ncol, lo);
+                __nv_bfloat16 *oh = p.Ohi + (long long)row * p.ldo + col0, *ol = p.Olo + (long long)row * p.ldo + col0;
+                store_row16_bf16(oh, n1, hi);
+                store_row16_bf16(ol, n1, lo);
+                if (n2 > 0) {
+                    store_row16_bf16(oh + 16, n2, hi + 16);
+                    store_row16_bf16(ol + 16, n2, lo + 16);
+                }
             }
-            if (p.Thi) {
+            if (stage_t) {
+                // column c0+j of the tile: the warp's 32 lanes write 32 consecutive rows (64 B)
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    if (j < ncol) {
-                        p.Thi[(long long)(col0 + j) * p.ldt + row] = hi[j];
-                        p.Tlo[(long long)(col0 + j) * p.ldt + row] = lo[j];
-                    }
+                for (int j = 0; j < 32; ++j) {
+                    ts_hi[(c0 + j) * TPITCH + rloc] = hi[j];
+                    ts_lo[(c0 + j) * TPITCH + rloc] = lo[j];
+                }
+            }
+        }
+    }
+    // every thread reaches this barrier; the copy-out runs only when the whole CTA has a valid tile
+    const bool all_live = __syncthreads_and(live ? 1 : 0) != 0;
+    if (stage_t && all_live) {
+        // transposed copy-out: T(n0 + c, m0 + 8*part .. +7), 16 bytes per thread and array
+        const int nrow_valid = min(BM, p.M - m0), ncol_valid = min(BNX, p.N - n0);
+        for (int idx = threadIdx.x; idx < 128 * (BM / 8); idx += 128) {
+            const int c = idx / (BM / 8), part = idx % (BM / 8);
+            if (c >= ncol_valid) continue;
+            const int r0 = part * 8;
+            const int nv = min(8, nrow_valid - r0);
+            if (nv <= 0) continue;
+            const long long off = (long long)(n0 + c) * p.ldt + m0 + r0;
+            const __nv_bfloat16 *sh = ts_hi + c * TPITCH + r0, *sl = ts_lo + c * TPITCH + r0;
+            __nv_bfloat16 *dh = p.Thi + off, *dl = p.Tlo + off;
+            if (nv == 8 && ((reinterpret_cast<uintptr_t>(dh) | reinterpret_cast<uintptr_t>(dl)) & 15) == 0) {
+                *reinterpret_cast<uint4 *>(dh) = *reinterpret_cast<const uint4 *>(sh);
+                *reinterpret_cast<uint4 *>(dl) = *reinterpret_cast<const uint4 *>(sl);
+            } else {
+                for (int j = 0; j < nv; ++j) {
+                    dh[j] = sh[j];
+                    dl[j] = sl[j];
                 }
             }
         }
