@@ -110,6 +110,12 @@ __device__ __forceinline__ void store_row16_bf16(__nv_bfloat16 *dst, int n, cons
     }
 }
 
+// Transposed-output staging: per epilogue warp a [32 tile columns][32 tile rows] BF16 block for hi
+// and for lo, rows padded to 40 elements (80 B, a multiple of 16 B for the 16-byte reads).
+constexpr int EPI_THREADS = 128;
+constexpr int TPITCH = 40;
+constexpr int TSTAGE_BYTES = 4 * 2 * 32 * TPITCH * 2;
+
 template <bool SPLIT> struct Cfg {
     // 128 x 128 output tiles in both modes (128 x 256 tiles with two stages measured slower in the
     // solver: the mainloop is bound by copy latency, not by operand bytes)
@@ -117,7 +123,8 @@ template <bool SPLIT> struct Cfg {
     static constexpr int TILE_BX = BNX * BK * 2;
     static constexpr int STAGES = SPLIT ? 3 : 4;
     static constexpr int STAGE_BYTES = SPLIT ? 2 * (TILE_A_BYTES + TILE_BX) : TILE_A_BYTES + TILE_BX;
-    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /* alignment slack */ + 256 /* barriers */;
+    static constexpr int SMEM_BYTES =
+        STAGES * STAGE_BYTES + TSTAGE_BYTES + 1024 /* alignment slack */ + 256 /* barriers */;
     static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BNX >> 3) << 17) |
                                       ((uint32_t)(BM >> 4) << 24);
 };
@@ -241,229 +248,292 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Transposed-output staging in the (then idle) operand ring: [tile column][tile row] BF16, rows
-// padded to 136 elements (272 B) so that both the per-column writes of a warp (32 consecutive rows)
-// and the 16-byte row reads of the copy-out stay within the minimum number of bank wavefronts.
-constexpr int TPITCH = BM + 8;
-constexpr int TSTAGE_BYTES = 2 * 128 * TPITCH * 2;  // hi and lo, 128 tile columns
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 
+// Output tile t of a launch: tiles run M-fastest, then N, then the K range (split-K index), so the
+// CTAs working at one time share B tiles and the A operand stays in L2.
+struct TileCoords {
+    int m0, n0, kb0, kblocks;
+};
+
+__device__ __forceinline__ TileCoords tile_coords(int t, int mt, int nt, int bnx, int kblocks_all, int kper) {
+    TileCoords c;
+    const int mi = t % mt, rest = t / mt;
+    c.m0 = mi * BM;
+    c.n0 = (rest % nt) * bnx;
+    c.kb0 = (rest / nt) * kper;
+    c.kblocks = max(0, min(kblocks_all, c.kb0 + kper) - c.kb0);
+    return c;
+}
+
+// Persistent kernel: one CTA per SM walks the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
+//   warp 0 lane 0 : TMA producer over the operand ring (continues across tiles);
+//   warp 1 lane 0 : tcgen05.mma issuer into one of two 128-column TMEM accumulators
+//                   (tile j uses accumulator j % 2);
+//   warps 2..5    : epilogue of tile j while the MMAs of tile j + 1 run; warp w reads TMEM
+//                   lanes 32 (w % 4) .. 32 (w % 4) + 31.
+// Barriers: full/empty per ring slot, tfull (MMA -> epilogue, tcgen05.commit) and tempty
+// (epilogue -> MMA, 128 arrivals) per accumulator.  Every wait is bounded.
 template <bool SPLIT>
-__global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ Maps maps, const Params p) {
+__global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Maps maps, const Params p) {
     constexpr int STAGES = Cfg<SPLIT>::STAGES, STAGE_BYTES = Cfg<SPLIT>::STAGE_BYTES;
     constexpr int BNX = Cfg<SPLIT>::BNX, TILE_BX = Cfg<SPLIT>::TILE_BX;
     constexpr uint32_t IDESC = Cfg<SPLIT>::IDESC;
+    static_assert(BNX == 128, "epilogue assumes 128 tile columns");
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    __nv_bfloat16 *tstage = reinterpret_cast<__nv_bfloat16 *>(smem + STAGES * STAGE_BYTES);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES + TSTAGE_BYTES);
     uint64_t *empty = full + STAGES;
-    uint64_t *done = empty + STAGES;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    uint64_t *tfull = empty + STAGES;
+    uint64_t *tempty = tfull + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
     int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    // blockIdx.x walks the M tiles: the CTAs that share one B (N) tile run
-    // together, so B streams from DRAM once and the other M tiles hit L2
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BNX;
+    const int mt = (p.M + BM - 1) / BM, nt = (p.N + BNX - 1) / BNX;
+    const int ntiles = mt * nt * p.ksplit;
     const int kblocks_all = (p.K + BK - 1) / BK;
     const int kper = (kblocks_all + p.ksplit - 1) / p.ksplit;
-    const int kb0 = blockIdx.z * kper;
-    const int kblocks = max(0, min(kblocks_all, kb0 + kper) - kb0);
-    const int total = SPLIT ? kblocks : kblocks * p.nseg;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(done, 1);
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&tfull[a], 1);
+            mbar_init(&tempty[a], EPI_THREADS);
+        }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncwarp();
     if (warp == 0) {
-        // allocate BNX TMEM columns (128 lanes x BNX FP32 accumulators)
+        // two accumulators of BNX columns (128 lanes x 2 BNX FP32)
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(BNX));
+                     "r"(2 * BNX));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
-    if (p.G && p.ksplit == 1 && m0 + (int)threadIdx.x < p.M) {
-        // pull this tile's G rows into L2 while the mainloop runs (128-byte lines, inside the matrix)
-        const float *g = p.G + (long long)(m0 + threadIdx.x) * p.ldg + n0;
-        const int ncols = min(BNX, p.N - n0);
-        for (int c = 0; c < ncols; c += 32) asm volatile("prefetch.global.L2 [%0];" ::"l"(g + c));
-    }
 
-    if (warp == 0 && lane == 0) {
-        // ---------------- TMA producer
-        int issued = 0;
-        for (int it = 0; it < total; ++it) {
-            const int s = it % STAGES;
-            if (it >= STAGES) {
-                if (!mbar_wait(&empty[s], ((it / STAGES) - 1) & 1)) {
-                    atomicExch(p.err, 1);
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer
+            int it = 0;  // copies issued (ring position)
+            bool stop = false;
+            for (int t = blockIdx.x; t < ntiles && !stop; t += gridDim.x) {
+                const TileCoords tc = tile_coords(t, mt, nt, BNX, kblocks_all, kper);
+                const int total = SPLIT ? tc.kblocks : tc.kblocks * p.nseg;
+                for (int i = 0; i < total; ++i) {
+                    const int s = it % STAGES;
+                    if (it >= STAGES && !mbar_wait(&empty[s], ((it / STAGES) - 1) & 1)) {
+                        atomicExch(p.err, 1);
+                        *(volatile int *)abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    if (*(volatile int *)abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    uint8_t *sa = smem + s * STAGE_BYTES;
+                    mbar_expect_tx(&full[s], STAGE_BYTES);
+                    if (SPLIT) {
+                        // stage layout: A_hi | A_lo | B_hi | B_lo
+                        const int kx = (tc.kb0 + i) * BK;
+                        tma_load_2d(sa, &maps.a[0], &full[s], kx, tc.m0);
+                        tma_load_2d(sa + TILE_A_BYTES, &maps.a[1], &full[s], kx, tc.m0);
+                        tma_load_2d(sa + 2 * TILE_A_BYTES, &maps.b[0], &full[s], kx, tc.n0);
+                        tma_load_2d(sa + 2 * TILE_A_BYTES + TILE_BX, &maps.b[1], &full[s], kx, tc.n0);
+                    } else {
+                        const int seg = i / tc.kblocks, kb = tc.kb0 + i % tc.kblocks;
+                        tma_load_2d(sa, &maps.a[seg], &full[s], kb * BK, tc.m0);
+                        tma_load_2d(sa + TILE_A_BYTES, &maps.b[seg], &full[s], kb * BK, tc.n0);
+                    }
+                    ++it;
+                }
+            }
+            // drain: wait (bounded) until every copy that was started has landed
+            for (int j = max(0, it - STAGES); j < it; ++j) mbar_wait(&full[j % STAGES], (j / STAGES) & 1);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer
+            int it = 0, j = 0;
+            bool stop = false;
+            for (int t = blockIdx.x; t < ntiles && !stop; t += gridDim.x, ++j) {
+                const TileCoords tc = tile_coords(t, mt, nt, BNX, kblocks_all, kper);
+                const int total = SPLIT ? tc.kblocks : tc.kblocks * p.nseg;
+                const int acc = j & 1;
+                const uint32_t tacc = tmem + (uint32_t)(acc * BNX);
+                if (j >= 2 && !mbar_wait(&tempty[acc], ((j >> 1) - 1) & 1)) {
+                    atomicExch(p.err, 4);
                     *(volatile int *)abort_flag = 1;
                     break;
                 }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                for (int i = 0; i < total; ++i) {
+                    const int s = it % STAGES;
+                    if (!mbar_wait(&full[s], (it / STAGES) & 1)) {
+                        atomicExch(p.err, 2);
+                        *(volatile int *)abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    if (*(volatile int *)abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
+                    if (SPLIT) {
+                        const uint32_t sal = sa + TILE_A_BYTES, sb = sa + 2 * TILE_A_BYTES, sbl = sb + TILE_BX;
+#pragma unroll
+                        for (int k = 0; k < BK / 16; ++k) {
+                            const uint32_t o = k * 32;
+                            umma_bf16(tacc, smem_desc_k128(sa + o), smem_desc_k128(sb + o),
+                                      (i > 0 || k > 0) ? 1u : 0u, IDESC);
+                            umma_bf16(tacc, smem_desc_k128(sa + o), smem_desc_k128(sbl + o), 1u, IDESC);
+                            umma_bf16(tacc, smem_desc_k128(sal + o), smem_desc_k128(sb + o), 1u, IDESC);
+                        }
+                    } else {
+                        const uint32_t sb = sa + TILE_A_BYTES;
+#pragma unroll
+                        for (int k = 0; k < BK / 16; ++k) {
+                            // advance 16 BF16 = 32 bytes along K inside the 128-byte swizzle atom
+                            umma_bf16(tacc, smem_desc_k128(sa + k * 32), smem_desc_k128(sb + k * 32),
+                                      (i > 0 || k > 0) ? 1u : 0u);
+                        }
+                    }
+                    umma_commit(&empty[s]);  // slot s may be refilled once these MMAs have read it
+                    ++it;
+                }
+                umma_commit(&tfull[acc]);  // accumulator complete (or abandoned) -> epilogue
             }
-            if (*(volatile int *)abort_flag) break;
-            uint8_t *sa = smem + s * STAGE_BYTES;
-            mbar_expect_tx(&full[s], STAGE_BYTES);
-            if (SPLIT) {
-                // stage layout: A_hi | A_lo | B_hi | B_lo
-                const int kx = (kb0 + it) * BK;
-                tma_load_2d(sa, &maps.a[0], &full[s], kx, m0);
-                tma_load_2d(sa + TILE_A_BYTES, &maps.a[1], &full[s], kx, m0);
-                tma_load_2d(sa + 2 * TILE_A_BYTES, &maps.b[0], &full[s], kx, n0);
-                tma_load_2d(sa + 2 * TILE_A_BYTES + TILE_BX, &maps.b[1], &full[s], kx, n0);
-            } else {
-                const int seg = it / kblocks, kb = kb0 + it % kblocks;
-                tma_load_2d(sa, &maps.a[seg], &full[s], kb * BK, m0);
-                tma_load_2d(sa + TILE_A_BYTES, &maps.b[seg], &full[s], kb * BK, n0);
-            }
-            ++issued;
         }
-        // drain: wait (bounded) until every copy that was started has landed
-        for (int it = max(0, issued - STAGES); it < issued; ++it) mbar_wait(&full[it % STAGES], (it / STAGES) & 1);
-    } else if (warp == 1 && lane == 0) {
-        // ---------------- MMA issuer
-        int consumed = 0;
-        for (int it = 0; it < total; ++it) {
-            const int s = it % STAGES;
-            if (!mbar_wait(&full[s], (it / STAGES) & 1)) {
-                atomicExch(p.err, 2);
-                *(volatile int *)abort_flag = 1;
-                break;
+    } else {
+        // ---------------- epilogue (warps 2..5, 128 threads)
+        const int rq = warp & 3;  // TMEM lane quarter this warp may access
+        const int rloc = rq * 32 + lane;
+        const bool stage_t = p.Thi != nullptr && p.ksplit == 1;
+        __nv_bfloat16 *sh = tstage + (warp - 2) * (2 * 32 * TPITCH);
+        __nv_bfloat16 *sl = sh + 32 * TPITCH;
+        int j = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++j) {
+            const TileCoords tc = tile_coords(t, mt, nt, BNX, kblocks_all, kper);
+            const int total = SPLIT ? tc.kblocks : tc.kblocks * p.nseg;
+            const int acc = j & 1;
+            const int m0 = tc.m0, n0 = tc.n0;
+            const int row = m0 + rloc;
+            if (p.G && p.ksplit == 1 && row < p.M) {
+                // pull this tile's G row into L2 while its MMAs run (128-byte lines, inside the matrix)
+                const float *g = p.G + (long long)row * p.ldg + n0;
+                const int ncols = min(BNX, p.N - n0);
+                for (int c = 0; c < ncols; c += 32) asm volatile("prefetch.global.L2 [%0];" ::"l"(g + c));
             }
-            if (*(volatile int *)abort_flag) break;
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(&tfull[acc], (j >> 1) & 1) ? 1 : 0) != 0;
+            if (!ok && lane == 0) atomicExch(p.err, 3);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
-            if (SPLIT) {
-                const uint32_t sal = sa + TILE_A_BYTES, sb = sa + 2 * TILE_A_BYTES, sbl = sb + TILE_BX;
+            const bool live = ok && !*(volatile int *)abort_flag && total > 0;  // warp-uniform
+            for (int c0 = 0; c0 < BNX; c0 += 32) {
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)(rq * 32) << 16) + (uint32_t)(acc * BNX + c0), v);
+                const int col0 = n0 + c0;
+                if (live && row < p.M && col0 < p.N) {
+                    const int ncol = min(32, p.N - col0);
+                    if (p.ksplit > 1) {  // partial sums over this tile's K range
 #pragma unroll
-                for (int k = 0; k < BK / 16; ++k) {
-                    const uint32_t o = k * 32;
-                    umma_bf16(tmem, smem_desc_k128(sa + o), smem_desc_k128(sb + o), (it > 0 || k > 0) ? 1u : 0u,
-                              IDESC);
-                    umma_bf16(tmem, smem_desc_k128(sa + o), smem_desc_k128(sbl + o), 1u, IDESC);
-                    umma_bf16(tmem, smem_desc_k128(sal + o), smem_desc_k128(sb + o), 1u, IDESC);
+                        for (int q = 0; q < 32; ++q)
+                            if (q < ncol) atomicAdd(&p.C[(long long)row * p.ldc + col0 + q], p.alpha * v[q]);
+                    } else {
+                        const int n1 = min(16, ncol), n2 = ncol - 16;  // the two 16-column halves (n2 <= 0: none)
+#pragma unroll
+                        for (int q = 0; q < 32; ++q) v[q] *= p.alpha;
+                        if (p.G) {
+                            float g[32];
+                            const float *gr = p.G + (long long)row * p.ldg + col0;
+                            load_row16(gr, n1, g);
+                            if (n2 > 0) load_row16(gr + 16, n2, g + 16);
+#pragma unroll
+                            for (int q = 0; q < 32; ++q) v[q] *= g[q];
+                        }
+                        if (p.C) {
+                            store_row16(p.C + (long long)row * p.ldc + col0, n1, v);
+                            if (n2 > 0) store_row16(p.C + (long long)row * p.ldc + col0 + 16, n2, v + 16);
+                        }
+                        if (p.Ohi || stage_t) {
+                            __nv_bfloat16 hi[32], lo[32];
+#pragma unroll
+                            for (int q = 0; q < 32; ++q) {
+                                hi[q] = __float2bfloat16_rn(v[q]);
+                                lo[q] = __float2bfloat16_rn(v[q] - __bfloat162float(hi[q]));
+                            }
+                            if (p.Ohi) {
+                                __nv_bfloat16 *oh = p.Ohi + (long long)row * p.ldo + col0;
+                                __nv_bfloat16 *ol = p.Olo + (long long)row * p.ldo + col0;
+                                store_row16_bf16(oh, n1, hi);
+                                store_row16_bf16(ol, n1, lo);
+                                if (n2 > 0) {
+                                    store_row16_bf16(oh + 16, n2, hi + 16);
+                                    store_row16_bf16(ol + 16, n2, lo + 16);
+                                }
+                            }
+                            if (stage_t) {
+                                // column c0+q of the tile: the warp's 32 lanes write 32 consecutive rows
+#pragma unroll
+                                for (int q = 0; q < 32; ++q) {
+                                    sh[q * TPITCH + lane] = hi[q];
+                                    sl[q * TPITCH + lane] = lo[q];
+                                }
+                            }
+                        }
+                    }
                 }
-            } else {
-                const uint32_t sb = sa + TILE_A_BYTES;
+                if (stage_t) {
+                    __syncwarp();
+                    if (live && col0 < p.N) {
+                        // this warp's 32 x 32 block of T: T-rows col0 .. col0+31, T-columns m0+32rq .. +31
 #pragma unroll
-                for (int k = 0; k < BK / 16; ++k) {
-                    // advance 16 BF16 = 32 bytes along K inside the 128-byte swizzle atom
-                    umma_bf16(tmem, smem_desc_k128(sa + k * 32), smem_desc_k128(sb + k * 32),
-                              (it > 0 || k > 0) ? 1u : 0u);
-                }
-            }
-            umma_commit(&empty[s]);  // slot s may be refilled once these MMAs have read it
-            ++consumed;
-        }
-        umma_commit(done);  // all issued MMAs complete -> epilogue
-        (void)consumed;
-    }
-    // ---------------- epilogue (all 4 warps)
-    __syncwarp();
-    const bool ok = mbar_wait(done, 0);
-    if (!ok && threadIdx.x == 0) atomicExch(p.err, 3);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const bool live = ok && !*(volatile int *)abort_flag && total > 0;
-    const int rloc = warp * 32 + lane;  // TMEM lane = tile row
-    const int row = m0 + rloc;
-    const bool stage_t = p.Thi != nullptr && p.ksplit == 1;
-    static_assert(TSTAGE_BYTES <= STAGES * STAGE_BYTES, "transpose staging must fit in the operand ring");
-    static_assert(BNX == 128, "transpose staging assumes 128 tile columns");
-    __nv_bfloat16 *ts_hi = reinterpret_cast<__nv_bfloat16 *>(smem);
-    __nv_bfloat16 *ts_lo = ts_hi + 128 * TPITCH;
-    for (int c0 = 0; c0 < BNX; c0 += 32) {
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-        if (!live) continue;
-        const int col0 = n0 + c0;
-        if (row >= p.M || col0 >= p.N) continue;
-        const int ncol = min(32, p.N - col0);
-        if (p.ksplit > 1) {  // partial sums over this CTA's K range
-#pragma unroll
-            for (int j = 0; j < 32; ++j)
-                if (j < ncol) atomicAdd(&p.C[(long long)row * p.ldc + col0 + j], p.alpha * v[j]);
-            continue;
-        }
-        const int n1 = min(16, ncol), n2 = ncol - 16;  // the two 16-column halves (n2 <= 0: none)
-        // Each thread owns consecutive columns of one row: row-major reads and writes move them as
-        // whole 16/8/4-byte words where the address allows
-#pragma unroll
-        for (int j = 0; j < 32; ++j) v[j] *= p.alpha;
-        if (p.G) {
-            float g[32];
-            const float *gr = p.G + (long long)row * p.ldg + col0;
-            load_row16(gr, n1, g);
-            if (n2 > 0) load_row16(gr + 16, n2, g + 16);
-#pragma unroll
-            for (int j = 0; j < 32; ++j) v[j] *= g[j];
-        }
-        if (p.C) {
-            store_row16(p.C + (long long)row * p.ldc + col0, n1, v);
-            if (n2 > 0) store_row16(p.C + (long long)row * p.ldc + col0 + 16, n2, v + 16);
-        }
-        if (p.Ohi || p.Thi) {
-            __nv_bfloat16 hi[32], lo[32];
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                hi[j] = __float2bfloat16_rn(v[j]);
-                lo[j] = __float2bfloat16_rn(v[j] - __bfloat162float(hi[j]));
-            }
-            if (p.Ohi) {
-                __nv_bfloat16 *oh = p.Ohi + (long long)row * p.ldo + col0, *ol = p.Olo + (long long)row * p.ldo + col0;
-                store_row16_bf16(oh, n1, hi);
-                store_row16_bf16(ol, n1, lo);
-                if (n2 > 0) {
-                    store_row16_bf16(oh + 16, n2, hi + 16);
-                    store_row16_bf16(ol + 16, n2, lo + 16);
-                }
-            }
-            if (stage_t) {
-                // column c0+j of the tile: the warp's 32 lanes write 32 consecutive rows (64 B)
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    ts_hi[(c0 + j) * TPITCH + rloc] = hi[j];
-                    ts_lo[(c0 + j) * TPITCH + rloc] = lo[j];
+                        for (int q = 0; q < 4; ++q) {
+                            const int c = q * 8 + (lane >> 2), part = lane & 3;
+                            const int trow = col0 + c, tcol0 = m0 + rq * 32 + part * 8;
+                            const int nv = min(8, p.M - tcol0);
+                            if (trow < p.N && nv > 0) {
+                                const long long off = (long long)trow * p.ldt + tcol0;
+                                const __nv_bfloat16 *srh = sh + c * TPITCH + part * 8, *srl = sl + c * TPITCH + part * 8;
+                                __nv_bfloat16 *dh = p.Thi + off, *dl = p.Tlo + off;
+                                if (nv == 8 &&
+                                    ((reinterpret_cast<uintptr_t>(dh) | reinterpret_cast<uintptr_t>(dl)) & 15) == 0) {
+                                    *reinterpret_cast<uint4 *>(dh) = *reinterpret_cast<const uint4 *>(srh);
+                                    *reinterpret_cast<uint4 *>(dl) = *reinterpret_cast<const uint4 *>(srl);
+                                } else {
+                                    for (int e = 0; e < nv; ++e) {
+                                        dh[e] = srh[e];
+                                        dl[e] = srl[e];
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    __syncwarp();
                 }
             }
-        }
-    }
-    // every thread reaches this barrier; the copy-out runs only when the whole CTA has a valid tile
-    const bool all_live = __syncthreads_and(live ? 1 : 0) != 0;
-    if (stage_t && all_live) {
-        // transposed copy-out: T(n0 + c, m0 + 8*part .. +7), 16 bytes per thread and array
-        const int nrow_valid = min(BM, p.M - m0), ncol_valid = min(BNX, p.N - n0);
-        for (int idx = threadIdx.x; idx < 128 * (BM / 8); idx += 128) {
-            const int c = idx / (BM / 8), part = idx % (BM / 8);
-            if (c >= ncol_valid) continue;
-            const int r0 = part * 8;
-            const int nv = min(8, nrow_valid - r0);
-            if (nv <= 0) continue;
-            const long long off = (long long)(n0 + c) * p.ldt + m0 + r0;
-            const __nv_bfloat16 *sh = ts_hi + c * TPITCH + r0, *sl = ts_lo + c * TPITCH + r0;
-            __nv_bfloat16 *dh = p.Thi + off, *dl = p.Tlo + off;
-            if (nv == 8 && ((reinterpret_cast<uintptr_t>(dh) | reinterpret_cast<uintptr_t>(dl)) & 15) == 0) {
-                *reinterpret_cast<uint4 *>(dh) = *reinterpret_cast<const uint4 *>(sh);
-                *reinterpret_cast<uint4 *>(dl) = *reinterpret_cast<const uint4 *>(sl);
-            } else {
-                for (int j = 0; j < nv; ++j) {
-                    dh[j] = sh[j];
-                    dl[j] = sl[j];
-                }
-            }
+            // the accumulator has been read: hand it back to the MMA issuer
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(&tempty[acc]);
+            if (!ok) break;
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BNX));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BNX));
     }
 }
 
@@ -620,12 +690,21 @@ int dftb_bf16x3_gemm_ex(int M, int N, int K, int nseg, int shared_split, int ksp
         attr_set[mode][dev] = true;
     }
     const int bnx = shared_split ? Cfg<true>::BNX : Cfg<false>::BNX;
-    dim3 grid((M + BM - 1) / BM, (N + bnx - 1) / bnx, ksplit);
-    if (grid.y > 65535u) return DFTB_ERR_BAD_SIZE;
+    // persistent launch: one CTA per SM (the shared-memory footprint admits one), each walking tiles
+    const long long ntiles = (long long)((M + BM - 1) / BM) * ((N + bnx - 1) / bnx) * ksplit;
+    if (ntiles > (1LL << 30)) return DFTB_ERR_BAD_SIZE;
+    static int sm_count[64] = {0};
+    if (dev >= 0 && dev < 64 && sm_count[dev] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        sm_count[dev] = n;
+    }
+    const int sms = (dev >= 0 && dev < 64) ? sm_count[dev] : 148;
+    dim3 grid((unsigned)(ntiles < sms ? ntiles : sms));
     if (shared_split)
-        gemm_kernel<true><<<grid, 128, smem, reinterpret_cast<cudaStream_t>(stream)>>>(maps, p);
+        gemm_kernel<true><<<grid, 192, smem, reinterpret_cast<cudaStream_t>(stream)>>>(maps, p);
     else
-        gemm_kernel<false><<<grid, 128, smem, reinterpret_cast<cudaStream_t>(stream)>>>(maps, p);
+        gemm_kernel<false><<<grid, 192, smem, reinterpret_cast<cudaStream_t>(stream)>>>(maps, p);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         snprintf(g_err, sizeof(g_err), "gemm_kernel: %s", cudaGetErrorString(e));

@@ -72,3 +72,47 @@ def test_gemm_split_k_and_segment_mode_agree(M, N, K, ks):
     scale = ref.abs().max().item()
     assert (C_shared.double() - ref).abs().max().item() / scale < 5e-5
     assert (C_seg.double() - ref).abs().max().item() / scale < 5e-5
+
+
+@pytest.mark.parametrize("M,N,K", [(2000, 1500, 300), (4100, 2100, 70)])
+def test_gemm_many_tiles_per_cta(M, N, K):
+    """More output tiles than SMs: each persistent CTA walks several tiles, alternating its two
+    accumulators, with the G product and all three outputs on ragged edges."""
+    native.load()
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device="cpu").manual_seed(M + K)
+    A = torch.randn(M, K, generator=g, dtype=torch.float64).to(dev)
+    B = torch.randn(N, K, generator=g, dtype=torch.float64).to(dev)
+    G = torch.rand(M, N, generator=g, dtype=torch.float32).to(dev)
+    ref = (A @ B.T) * G.double()
+    pa, pb = tcgemm.split(A), tcgemm.split(B)
+    C = torch.empty((M, N), dtype=torch.float32, device=dev)
+    O = tcgemm.Pair(M, N, dev)
+    T = tcgemm.Pair(N, M, dev)
+    tcgemm.gemm(pa, pb, K=K, G=G, out=C, out_pair=O, out_pair_t=T)
+    C_seg = torch.empty((M, N), dtype=torch.float32, device=dev)
+    tcgemm.gemm(pa, pb, K=K, G=G, out=C_seg, segments=[(pa.hi, pb.hi), (pa.hi, pb.lo), (pa.lo, pb.hi)])
+    torch.cuda.synchronize()
+    tcgemm.check_errors(dev)
+    scale = ref.abs().max().item()
+    assert (C.double() - ref).abs().max().item() / scale < 5e-5
+    assert (C_seg.double() - ref).abs().max().item() / scale < 5e-5
+    assert (O.hi[:, :N].double() + O.lo[:, :N].double() - C.double()).abs().max().item() / scale < 1e-5
+    assert (T.hi[:, :M].double() + T.lo[:, :M].double() - C.double().T).abs().max().item() / scale < 1e-5
+
+
+def test_gemm_split_k_with_an_empty_range():
+    """K = 150 in 4 ranges of one 64-wide block: the last range is empty and adds nothing."""
+    native.load()
+    dev = torch.device("cuda", 0)
+    M, N, K = 300, 200, 150
+    g = torch.Generator(device="cpu").manual_seed(3)
+    A = torch.randn(M, K, generator=g, dtype=torch.float64).to(dev)
+    B = torch.randn(N, K, generator=g, dtype=torch.float64).to(dev)
+    ref = A @ B.T
+    pa, pb = tcgemm.split(A), tcgemm.split(B)
+    C = torch.empty((M, N), dtype=torch.float32, device=dev)
+    tcgemm.gemm(pa, pb, K=K, out=C, ksplit=4)
+    torch.cuda.synchronize()
+    tcgemm.check_errors(dev)
+    assert (C.double() - ref).abs().max().item() / ref.abs().max().item() < 5e-5
