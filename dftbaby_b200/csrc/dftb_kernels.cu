@@ -5,7 +5,9 @@
 // All matrices are row-major FP64 in device memory.  Nothing here allocates:
 // scratch space comes from caller-provided workspaces.
 
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <string.h>
@@ -527,9 +529,93 @@ __global__ void omega_scale_kernel(long long nov, int nvec, const double *omega,
 }
 
 // Coulomb part shared by the Hermitian and (A+B) products:
+// cuBLAS for the two plain FP64 GEMMs of the Coulomb product.  The library is resolved at run
+// time (dlopen / dlsym, reusing the copy the process has already loaded), so the shared library
+// loads without it and the product falls back to dgemm_kernel.
+using blas_create_t = cublasStatus_t (*)(cublasHandle_t *);
+using blas_stream_t = cublasStatus_t (*)(cublasHandle_t, cudaStream_t);
+using blas_dgemm_t = cublasStatus_t (*)(cublasHandle_t, cublasOperation_t, cublasOperation_t, int, int, int,
+                                        const double *, const double *, int, const double *, int, const double *,
+                                        double *, int);
+struct Blas {
+    blas_create_t create = nullptr;
+    blas_stream_t set_stream = nullptr;
+    blas_dgemm_t dgemm = nullptr;
+    bool ok = false;
+};
+
+Blas &blas() {
+    static Blas b;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *h = dlopen("libcublas.so.12", RTLD_NOW | RTLD_NOLOAD);
+        if (!h) h = dlopen("libcublas.so.12", RTLD_NOW | RTLD_GLOBAL);
+        if (!h) h = dlopen("libcublas.so", RTLD_NOW | RTLD_GLOBAL);
+        if (!h) return;
+        b.create = reinterpret_cast<blas_create_t>(dlsym(h, "cublasCreate_v2"));
+        b.set_stream = reinterpret_cast<blas_stream_t>(dlsym(h, "cublasSetStream_v2"));
+        b.dgemm = reinterpret_cast<blas_dgemm_t>(dlsym(h, "cublasDgemm_v2"));
+        b.ok = b.create && b.set_stream && b.dgemm;
+    });
+    return b;
+}
+
+// one handle per host thread and device, bound to the caller's stream; nullptr if unavailable
+cublasHandle_t blas_handle(cudaStream_t st) {
+    Blas &b = blas();
+    if (!b.ok) return nullptr;
+    thread_local cublasHandle_t handles[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (!handles[dev] && b.create(&handles[dev]) != CUBLAS_STATUS_SUCCESS) {
+        handles[dev] = nullptr;
+        return nullptr;
+    }
+    if (b.set_stream(handles[dev], st) != CUBLAS_STATUS_SUCCESS) return nullptr;
+    return handles[dev];
+}
+
+// us(ia, n) = omega_ia v(ia, n) + fac us(ia, n)   (in place; the non-Hermitian Coulomb epilogue)
+__global__ void rv_inplace_kernel(long long total, int nvec, const double *omega, const double *vs, double *us,
+                                  double fac) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    us[i] = omega[i / nvec] * vs[i] + fac * us[i];
+}
+
 //   T = q_ov . (s o V)   (split-K, atomic), G = gamma . T,  us = epilogue(q_ov^T G)
+// The non-Hermitian form (s = 1) runs its two large GEMMs in cuBLAS when it is available:
+// row-major X (r x c) is the column-major X^T, so T^T = V^T q_ov^T and us^T = G^T q_ov.
 int coulomb_product(int nat, int nov, int nvec, const double *gamma, const double *q_ov, const double *omega,
                     const double *vs, double *us, double *T, double *G, int hermitian, cudaStream_t st) {
+    cublasHandle_t bh = hermitian ? nullptr : blas_handle(st);
+    if (bh) {
+        const double one = 1.0, zero = 0.0;
+        if (blas().dgemm(bh, CUBLAS_OP_N, CUBLAS_OP_N, nvec, nat, nov, &one, vs, nvec, q_ov, nov, &zero, T, nvec) !=
+            CUBLAS_STATUS_SUCCESS)
+            return fail(DFTB_ERR_CUDA, "coulomb: cublasDgemm (q_ov V) failed");
+        GemmP g = gemm_defaults();
+        g.M = nat;
+        g.N = nvec;
+        g.K = nat;
+        g.A = gamma;
+        g.sam = nat;
+        g.sak = 1;
+        g.B = T;
+        g.sbk = nvec;
+        g.sbn = 1;
+        g.C = G;
+        g.scm = nvec;
+        g.scn = 1;
+        int rc = launch_gemm(g, EPI_STORE, 1, st);
+        if (rc) return rc;
+        if (blas().dgemm(bh, CUBLAS_OP_N, CUBLAS_OP_T, nvec, nov, nat, &one, G, nvec, q_ov, nov, &zero, us, nvec) !=
+            CUBLAS_STATUS_SUCCESS)
+            return fail(DFTB_ERR_CUDA, "coulomb: cublasDgemm (q_ov^T G) failed");
+        const long long total = (long long)nov * nvec;
+        rv_inplace_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(total, nvec, omega, vs, us, 4.0);
+        return check_launch("rv_inplace_kernel");
+    }
     cudaError_t e = cudaMemsetAsync(T, 0, sizeof(double) * (size_t)nat * nvec, st);
     if (e != cudaSuccess) return fail(DFTB_ERR_CUDA, "memset T");
     GemmP p = gemm_defaults();

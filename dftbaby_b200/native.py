@@ -129,7 +129,7 @@ def check(rc, what):
 KERNELS_PER_CALL = {
     "dftb_directional_cosines": 1, "dftb_h0_and_s": 1, "dftb_dipole_matrix": 1, "dftb_gamma_matrices": 1,
     "dftb_ao_expand": 1, "dftb_scc_hamiltonian": 2, "dftb_monopoles": 1, "dftb_trans_charges": 6,
-    "dftb_trans_charges_diag": 5, "dftb_trans_charges_noalloc": 6, "dftb_hermitian_rv": 3, "dftb_apbv": 3, "dftb_ambv": 1,
+    "dftb_trans_charges_diag": 5, "dftb_trans_charges_noalloc": 6, "dftb_hermitian_rv": 3, "dftb_apbv": 2, "dftb_ambv": 1,
     "dftb_davidson_precondition": 1, "dftb_davidson_residual": 2, "dftb_dgemm": 1,
     "dftb_gradients_h0_and_s": 3, "dftb_sk_gradient_contract": 1, "dftb_pair_gradients": 1,
     "dftb_repulsive_energy": 1, "dftb_mlp_bias_relu": 1, "dftb_mlp_relu_backward": 1, "dftb_mlp_output": 1,
