@@ -516,6 +516,32 @@ __global__ void residual_kernel(int nov, int ncol, const double *AV, int ldav, c
     }
 }
 
+// Row-blocked form for ncol <= 256: a block of 256 threads covers R = 256 / ncol rows x all columns
+// per step (consecutive threads read consecutive elements of a row), so each thread keeps one
+// column and its squared norm in a register; the R partial sums of a column meet in shared memory.
+__global__ void residual_rows_kernel(int nov, int ncol, const double *AV, int ldav, const double *X, int ldx,
+                                     const double *lam, double *W, int ldw, double *nrm2) {
+    __shared__ double red[256];
+    const int R = blockDim.x / ncol;
+    const int tc = threadIdx.x % ncol, tr = threadIdx.x / ncol;
+    double acc = 0.0;
+    if (tr < R) {
+        const double l = lam[tc];
+        for (long long ia = (long long)blockIdx.x * R + tr; ia < nov; ia += (long long)gridDim.x * R) {
+            const double r = AV[ia * ldav + tc] - l * X[ia * ldx + tc];
+            W[ia * ldw + tc] = r;
+            acc += r * r;
+        }
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x < ncol) {
+        double sum = 0.0;
+        for (int j = 0; j < R; ++j) sum += red[threadIdx.x + j * ncol];
+        atomicAdd(&nrm2[threadIdx.x], sum);
+    }
+}
+
 __global__ void sqrt_kernel(int n, double *x) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x[i] = sqrt(x[i]);
@@ -1016,10 +1042,19 @@ int dftb_davidson_residual(int nov, int ncol, const double *AV, int ldav, const 
     cudaStream_t st = S(stream);
     if (cudaMemsetAsync(norms, 0, sizeof(double) * ncol, st) != cudaSuccess)
         return fail(DFTB_ERR_CUDA, "residual: memset");
-    unsigned gx = cdiv(nov, 256);
-    if (gx > 592) gx = 592;
-    residual_kernel<<<dim3(gx, ncol), 256, 0, st>>>(nov, ncol, AV, ldav, X, ldx, lam, W, ldw, norms);
-    int rc = check_launch("residual_kernel");
+    int rc;
+    if (ncol <= 256) {
+        const int R = 256 / ncol;
+        unsigned gx = cdiv(nov, R);
+        if (gx > 148 * 8) gx = 148 * 8;
+        residual_rows_kernel<<<gx, 256, 0, st>>>(nov, ncol, AV, ldav, X, ldx, lam, W, ldw, norms);
+        rc = check_launch("residual_rows_kernel");
+    } else {
+        unsigned gx = cdiv(nov, 256);
+        if (gx > 592) gx = 592;
+        residual_kernel<<<dim3(gx, ncol), 256, 0, st>>>(nov, ncol, AV, ldav, X, ldx, lam, W, ldw, norms);
+        rc = check_launch("residual_kernel");
+    }
     if (rc) return rc;
     sqrt_kernel<<<cdiv(ncol, 128), 128, 0, st>>>(ncol, norms);
     return check_launch("sqrt_kernel");
