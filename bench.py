@@ -425,6 +425,26 @@ def run_guess(args, w, rank, world, barrier):
         print(json.dumps(line), flush=True)
 
 
+def write_kernel_table(path, run, workload):
+    """Per-kernel device time of one untimed solve, from CUDA activity records (CUPTI via
+    torch.profiler): launches, total ms and share of all kernel time, largest first."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        run()
+        torch.cuda.synchronize()
+    rows = [(k.key, k.count, k.device_time_total / 1e3) for k in prof.key_averages()
+            if k.device_type.name == "CUDA" and k.device_time_total > 0]
+    rows.sort(key=lambda r: -r[2])
+    total = sum(r[2] for r in rows)
+    with open(path, "w") as fh:
+        fh.write("# kernel table, one %s solve: %d launches, %.1f ms of kernel time\n\n" % (
+            workload, sum(r[1] for r in rows), total))
+        fh.write("| launches | ms | share | kernel |\n|---|---|---|---|\n")
+        for name, n, ms in rows:
+            fh.write("| %d | %.2f | %.1f %% | `%s` |\n" % (n, ms, 100.0 * ms / total, name[:110].replace("|", "/")))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -438,6 +458,9 @@ def main():
                     help="mixed: tensor-core exchange + FP64 refinement (default); fp64: the plain path")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison solve")
     ap.add_argument("--model", default=None, help="learned-guess weights (workload guess)")
+    ap.add_argument("--kernel-table", default=None, metavar="PATH",
+                    help="after the timed region, profile one extra solve (CUDA activity records) and write its "
+                         "per-kernel launches, device time and share to PATH (markdown)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -560,6 +583,9 @@ def main():
     if world > 1:
         dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
     e2e_value = None if args.no_e2e else world * opts["nstates"] * args.steps / e2e_s.item()
+
+    if args.kernel_table and rank == 0:
+        write_kernel_table(args.kernel_table, lambda: solve(40_000 + rank), args.workload)
 
     # ---- roofline of the dominant native kernel group
     peak, peak_kind = measured_peaks()

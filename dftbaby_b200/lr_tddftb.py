@@ -200,8 +200,9 @@ class ExchangeMixed(ExchangeAO):
             T.gemm(self.YbarT, self.NT, K=2 * norb, out_pair=self.P2)
             T.gemm(self.P1, self.XbarT, K=2 * norb, alpha=0.25, out=self.K1t)
             T.gemm(self.P2, self.XbarT, K=2 * norb, alpha=0.25, out=self.K2t)
-            K1[:, c] = self.K1t.T.reshape(-1).double()
-            K2[:, c] = self.K2t.T.reshape(-1).double()
+            # transpose, widen to FP64 and scatter into column c in one copy
+            K1[:, c].view(no, nv).copy_(self.K1t.T)
+            K2[:, c].view(no, nv).copy_(self.K2t.T)
         return K1, K2
 
 
