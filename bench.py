@@ -61,6 +61,15 @@ WORKLOADS = {
 }
 
 
+# DRAM bytes (read + write) per tensor-core GEMM launch, from ncu captures of the four exchange
+# shapes of one product column (W, 2x N, 2x P, 2x K): sum over the 7 launches / 7.
+GEMM_TRAFFIC_PER_LAUNCH = {
+    "armchair7": (3.768e8, "ncu dram__bytes_read.sum + dram__bytes_write.sum of the shapes 8292x1225x1225, "
+                           "8292x4146x1225 (G, pair + transposed pair), 1225x8292x8292 and 1225x1225x8292 "
+                           "(gemm_bench), averaged over the 7 launches of one product column"),
+}
+
+
 def build_ensemble(n, sigma, seed):
     """n seeded molecules: a 50/50 coin picks an all-trans polyene C_mH_{m+2} (m even, 10..60) or an
     acene with 2..8 rings (C-C 1.40 A); every atom jittered by sigma."""
@@ -603,9 +612,11 @@ def main():
         fl = sum(entry_flops.get(dom, []))
         ms = totals[dom]
         nl = len(entry_ms[dom])
+        traffic = GEMM_TRAFFIC_PER_LAUNCH.get(args.workload)
         roof = {"kernel": "tcg::gemm_kernel (tcgen05 BF16, split-precision segments)", "bound": "tensor",
                 "achieved": fl / (ms / 1e3) / 1e12, "peak": tpeak, "unit": "TFLOP/s",
-                "frac": fl / (ms / 1e3) / 1e12 / tpeak, "traffic": None, "launches": nl,
+                "frac": fl / (ms / 1e3) / 1e12 / tpeak, "traffic": traffic[0] if traffic else None,
+                "traffic_source": traffic[1] if traffic else None, "launches": nl,
                 "algorithmic_flops_per_launch": fl / nl, "ms_per_launch": ms / nl,
                 "peak_source": "measured (bf16 sustained)" if pk else "fallback"}
     elif dom == "dftb_apbv":
