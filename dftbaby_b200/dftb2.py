@@ -196,10 +196,8 @@ class DFTB2(object):
         sig = 1.329 / np.sqrt(8.0 * np.log(2.0)) / self._U
         sAB = sig[:, None] ** 2 + sig[None, :] ** 2
         self.gaussOmega = 1.0 / torch.pow(2.0 * np.pi * sAB, 1.5) * torch.exp(-0.5 / sAB * r * r)
-        # S^(-1/2)-type transform for the generalised eigenproblem: S = L L^T
-        L = torch.linalg.cholesky(self.S)
-        eye = torch.eye(norb, dtype=torch.float64, device=dev)
-        self._Linv = torch.linalg.solve_triangular(L, eye, upper=False)
+        # Cholesky factor for the generalised eigenproblem H C = S C e: S = L L^T
+        self._L = torch.linalg.cholesky(self.S)
 
     @property
     def D(self):
@@ -325,9 +323,12 @@ class DFTB2(object):
                 self.orbe, Cp = torch.linalg.eigh(Hm)
                 self.orbs = B @ Cp
             else:
-                Hp = self._Linv @ Hk @ self._Linv.T
+                # L^-1 Hk L^-T and L^-T C' by triangular solves (n^3 FLOPs each instead of the
+                # 2 n^3 of a product with an explicit inverse); eigh reads the lower triangle
+                Y = torch.linalg.solve_triangular(self._L, Hk, upper=False)
+                Hp = torch.linalg.solve_triangular(self._L, Y.mT, upper=False).mT
                 self.orbe, Cp = torch.linalg.eigh(Hp)
-                self.orbs = self._Linv.T @ Cp
+                self.orbs = torch.linalg.solve_triangular(self._L.mT, Cp, upper=True)
             have_orbe = True
             self.f = self._occupation(self.orbe)
             occ = self.f > 0.0

@@ -9,7 +9,9 @@ and error checks.  Two deliberate, result-preserving differences:
 * products of the matrix with expansion vectors are kept: each new vector is
   multiplied once, residuals use (A.b) Tb instead of re-multiplying
   A (b Tb) (the products are linear), and the projected matrices b^T A b
-  are extended by the new rows and columns instead of being recomputed;
+  are extended by the new rows and columns instead of being recomputed (with
+  FP64 products the new rows are the transposed new columns, the operators
+  being symmetric);
 * new vectors are orthonormalised against the current (orthonormal) basis by
   block Gram-Schmidt with re-orthogonalisation instead of re-factorising the
   whole basis by QR; both produce the same subspace.
@@ -83,10 +85,14 @@ class Basis:
 
     Columns are appended in place (capacity grows geometrically) and the
     projected matrices b^T (A b) are extended by the new rows and columns only.
+    With mirror=True (products in FP64, symmetric operators) the new rows are
+    the transposed new columns; products in reduced precision keep both blocks,
+    whose average then cancels the antisymmetric part of their error.
     """
 
-    def __init__(self, nov, nprod, device, capacity=64):
+    def __init__(self, nov, nprod, device, capacity=64, mirror=False):
         self.nov, self.nprod, self.device = nov, nprod, device
+        self.mirror = mirror
         self.l = 0
         self.cap = 0
         self.V = None
@@ -120,7 +126,11 @@ class Basis:
             M = torch.empty((l1, l1), dtype=torch.float64, device=self.device)
             M[:l0, :l0] = self.M[i]
             M[:, l0:l1] = V.T @ Pn
-            M[l0:l1, :l0] = Q.T @ self.P[i][:, :l0]
+            if self.mirror:
+                # A+B, A-B and R are symmetric: the new rows are the transposed new columns
+                M[l0:l1, :l0] = M[:l0, l0:l1].T
+            else:
+                M[l0:l1, :l0] = Q.T @ self.P[i][:, :l0]
             self.M[i] = M
         self.l = l1
 
@@ -182,7 +192,7 @@ def hermitian_davidson(rv, omega, nstates, ifact=1, conv=1.0e-14, maxiter=10, Xp
     else:
         b0 = (XpYguess[:lmax].reshape(lmax, -1).T / omega_sq[:, None]).contiguous()
         b0 = b0 / torch.linalg.norm(b0, dim=0)
-    B = Basis(om.numel(), 1, om.device, capacity=lmax + 4 * k)
+    B = Basis(om.numel(), 1, om.device, capacity=lmax + 4 * k, mirror=True)
     B.append(b0, [rv(b0)])
     l = lmax
     for it in range(maxiter):
@@ -268,7 +278,7 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
         lmax = lmaxp + lmaxm
         cols = torch.cat([XmYguess.reshape(nstates, -1), XpYguess.reshape(nstates, -1)[:lmaxm]], dim=0).T
         bs = orthonormal_columns(cols / torch.linalg.norm(cols, dim=0)).contiguous()
-    B = Basis(om.numel(), 2, dev, capacity=lmax + 8 * k)
+    B = Basis(om.numel(), 2, dev, capacity=lmax + 8 * k, mirror=not symmetrize)
     B.append(bs, list(products(bs)))
     l = lmax
     for it in range(maxiter):
