@@ -161,7 +161,11 @@ int dftb_hermitian_rv(int nat, int nocc, int nvirt, int nvec, const double *gamm
  *   g, g_lr: (nat, nat); q_oo, q_ov, q_vv as for dftb_trans_charges;
  *   omega: (nocc, nvirt); vs, us: (nocc, nvirt, nvec);
  *   work: dftb_apbv_workspace_size() bytes with lc = 1, and
- *   dftb_hermitian_rv_workspace_size() bytes with lc = 0. */
+ *   dftb_hermitian_rv_workspace_size() bytes with lc = 0.
+ * The two q_ov contractions of the Coulomb term run in cuBLAS (cublasDgemm,
+ * one handle per calling thread and device, bound to `stream`) when
+ * libcublas.so.12 can be loaded at run time, otherwise in the library's own
+ * FP64 GEMM; vs and us must not overlap. */
 size_t dftb_apbv_workspace_size(int nat, int nocc, int nvirt, int nvec);
 int dftb_apbv(int nat, int nocc, int nvirt, int nvec, int lc, const double *g, const double *g_lr,
               const double *q_oo, const double *q_ov, const double *q_vv, const double *omega, const double *vs,
