@@ -87,6 +87,8 @@ def lib():
         L.oracle_splev_ext.argtypes = [D, c_int, D, c_int, c_double, c_int]
         L.oracle_sk_rule_grad.restype = None
         L.oracle_sk_rule_grad.argtypes = [c_int, c_int, c_int, c_int, c_double, D, D, D, D]
+        L.oracle_overlap12.restype = None
+        L.oracle_overlap12.argtypes = [c_int, c_int, I, I, I, I, D, D, c_int, I, D, D, c_int, c_int, c_int, D]
         L.oracle_gradients_h0_and_s.restype = None
         L.oracle_gradients_h0_and_s.argtypes = [c_int, c_int, I, I, I, I, D, I, c_int, I, D, D, D, D,
                                                 c_int, c_int, c_int, D, D]

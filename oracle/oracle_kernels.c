@@ -348,6 +348,60 @@ void oracle_h0_and_s(int norb, int nat, const int *ind, const int *typ, const in
         }
 }
 
+/* ---- overlap between two geometries ------------------------------------- */
+
+/* slako.f90:576-687 (overlap12, called by ScalarCoupling._overlap_AB_f90, ScalarCoupling.py:105-137).
+ * S(mu, nu) = <phi_mu(geometry 1) | phi_nu(geometry 2)> for every orbital pair: no proximity
+ * cutoff and no on-site shortcut (an atom and its displaced copy are evaluated with the SK tables,
+ * whose splev_uniform clamps r below the first knot).  The direction runs from the atom of mu in
+ * geometry 1 to the atom of nu in geometry 2 (the reference reads r(j,i) of
+ * directional_cosines(pos1, pos2), slako.f90:31-70), and each element is evaluated in its own
+ * orientation.  pos1, pos2: (nat, 3); S: (norb, norb) row-major. */
+void oracle_overlap12(int norb, int nat, const int *ind, const int *typ, const int *ls, const int *ms,
+                      const double *pos1, const double *pos2, int deg, const int *tab_filled,
+                      const double *S_knots, const double *S_coefs, int npair, int nsk, int npts, double *S)
+{
+    (void)npair;
+    (void)nat;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int nu = 0; nu < norb; ++nu) {
+        double Si[16];
+        int j = ind[nu], typj = typ[nu], l2 = ls[nu], m2 = ms[nu];
+        for (int mu = 0; mu < norb; ++mu) {
+            int i = ind[mu], typi = typ[mu], l1 = ls[mu], m1 = ms[mu];
+            double xc = pos2[3 * j] - pos1[3 * i], yc = pos2[3 * j + 1] - pos1[3 * i + 1],
+                   zc = pos2[3 * j + 2] - pos1[3 * i + 2];
+            double rij = sqrt(xc * xc + yc * yc + zc * zc), e[3];
+            if (rij > 0.0) {
+                e[0] = xc / rij;
+                e[1] = yc / rij;
+                e[2] = zc / rij;
+            } else {
+                e[0] = 0.0;
+                e[1] = 0.0;
+                e[2] = 1.0;
+            }
+            int tmin = typi < typj ? typi : typj, tmax = typi < typj ? typj : typi;
+            int ipair = tmax * (tmax + 1) / 2 + tmin;
+            for (int tab = 0; tab < nsk; ++tab) {
+                if (tab_filled[ipair * nsk + tab] == 1) {
+                    size_t b = ((size_t)ipair * nsk + tab) * npts;
+                    Si[tab] = oracle_splev_uniform(S_knots + b, npts, S_coefs + b, deg, rij);
+                } else {
+                    Si[tab] = 0.0;
+                }
+            }
+            size_t o = (size_t)mu * norb + nu;
+            if (typi <= typj) {
+                S[o] = oracle_sk_rule(l1, m1, l2, m2, e, Si);
+            } else {
+                double me[3] = {-e[0], -e[1], -e[2]};
+                S[o] = oracle_sk_rule(l2, m2, l1, m1, me, Si);
+            }
+        }
+    }
+}
+
 /* ---- gradients of H0 and S ------------------------------------------------ */
 
 /* Derivative of the S and H0 elements of the ordered pair (mu, nu) (the reference's
