@@ -505,5 +505,54 @@ class LR_TDDFTB:
     def getExcEnergies(self):
         return self.Omega
 
+    # ------------------------------------------------------------ analysis and output
+    def determineActiveSpace(self, threshold=1.0e-5):
+        """LR_TDDFTB.determineActiveSpace (LR_TDDFTB.py:196-243): the number of occupied orbitals below
+        and including the HOMO and of virtual orbitals above it whose excitations carry all but
+        ``threshold`` of every computed state's probability sum_ia C_ia^2.  Returns
+        (nr_active_occ, nr_active_virt)."""
+        C = self.Cij.detach().cpu().numpy()
+        occ_mins, virt_maxs = [], []
+        for n in range(C.shape[0]):
+            Cn = C[n]
+            Cn2 = np.ravel(Cn * Cn)
+            order = np.argsort(-Cn2)
+            Sn = np.cumsum(Cn2[order])
+            active = order[np.where(Sn <= 1.0 - threshold)]
+            if len(active) == 0 and Sn[0] > 1.0 - threshold:
+                active = order[0]  # a single dominant excitation
+            occ, virt = np.unravel_index(active, Cn.shape)
+            occ_mins.append(self.active_occupied_orbs[np.min(occ)])
+            virt_maxs.append(self.active_virtual_orbs[np.max(virt)])
+        HOMO = self.occupied_orbs.max()
+        return int(HOMO - min(occ_mins) + 1), int(max(virt_maxs) - HOMO)
+
+    def TransitionChargesState(self, I):
+        """LR_TDDFTB.TransitionChargesState (LR_TDDFTB.py:900-908): q_A = sum_ia C_I,ia q_A^ia (numpy, Nat)."""
+        return torch.einsum("ia,Aia->A", self.Cij[I], self.qtrans_ov).cpu().numpy()
+
+    def saveAbsorptionSpectrum(self, spectrum_file="absorption_spectrum.dat"):
+        """LR_TDDFTB.saveAbsorptionSpectrum (LR_TDDFTB.py:807-831): excitation energies (Hartree) and
+        oscillator strengths.  States are not classified by symmetry here, so there is one file."""
+        import os
+        with open(os.path.expanduser(os.path.expandvars(spectrum_file)), "w") as fh:
+            fh.write("# Absorption spectrum\n")
+            fh.write("# exc. energy / hartree  osc.strength\n")
+            for om, f in zip(np.asarray(self.Omega), np.asarray(self.oscillator_strength)):
+                fh.write("%s   %s\n" % (("%.7f" % om).rjust(20), ("%.7f" % f).rjust(20)))
+
+    def saveTransitionCharges(self, save_transition_charges=None):
+        """LR_TDDFTB.saveTransitionCharges (LR_TDDFTB.py:1008-1025): Mulliken transition charges between the
+        ground and the excited states, one row per atom, one column per state, in units of -e."""
+        if save_transition_charges is None:
+            return
+        import os
+        tq = torch.einsum("Aia,kia->Ak", self.qtrans_ov, self.Cij).cpu().numpy()
+        with open(os.path.expandvars(os.path.expanduser(save_transition_charges)), "w") as fh:
+            fh.write("# Mulliken transition charges (in unit of -e) between ground and excited states\n")
+            fh.write("# ROWS: atoms\n")
+            fh.write("# COLUMNS: excited states\n")
+            np.savetxt(fh, -tq)
+
     def getXY(self):
         return self.XmY, self.XpY
