@@ -4,8 +4,9 @@ Each step re-solves the SCC ground state, the lowest excited states (Davidson, w
 from the previous step's X-Y / X+Y and density matrix, as DFTBaby's objects do across calls,
 Solver.py:707-748, DFTB2.py:990-1019) and the analytic gradient of the followed state
 (ExcGradients.py), then moves the nuclei with velocity Verlet as DFTBaby's SurfaceHopping.verlet
-does at constant energy (Dynamics/SurfaceHopping.py:468-545).  Surface hops, scalar couplings
-and decoherence corrections are not part of this path: a trajectory stays on its state.
+does at constant energy (Dynamics/SurfaceHopping.py:468-545).  A trajectory here stays on its
+state; surface hops, scalar couplings and decoherence corrections are added by
+``surface_hopping.SurfaceHoppingTrajectory``.
 
 Initial momenta are drawn from a seeded Maxwell-Boltzmann distribution, freed of centre-of-mass
 motion and scaled so that E_kin = 1/2 nvib kB T, the normalisation of

@@ -16,7 +16,8 @@ Per step, in the reference's order (SurfaceHopping.verlet, SurfaceHopping.py:468
 The small matrices (Nst x Nst) live on the host as in the reference; the hopping draws come from a
 seeded numpy generator instead of Python's global ``random``.  The thermostat ("T"), metadynamics
 ("M"), the brightest/fragment initial states, restarts and the output files are not part of this
-path.
+path, nor is the handler's fallback to the ground state after a failed solve
+(Dynamics/dftbaby_handler.py:106-143): a failed SCC or Davidson solve raises.
 """
 import numpy as np
 import torch
