@@ -57,7 +57,12 @@ int dftb_directional_cosines(int nat, const double *pos, double *r, double *x, d
  *   tab_filled       : (npair, nsk) int; knots/coefs: (npair, nsk, npts);
  *   S, H0            : (norb, norb) outputs, every element written.
  * Only s and p orbitals (l <= 1) are implemented: elements that involve an
- * orbital with l > 1 are written as NaN. */
+ * orbital with l > 1 are written as NaN.
+ * Two geometries (slako.overlap12, slako.f90:576-687): call it on the union
+ * of the atoms ordered [geometry 2, geometry 1] (atom indices of geometry 1
+ * shifted by nat, r/x/y/z from dftb_directional_cosines of the union, mprox
+ * all ones); rows norb.. and columns ..norb of S are overlap12's
+ * <phi_mu(geometry 1)|phi_nu(geometry 2)>, evaluated in the same orientation. */
 int dftb_h0_and_s(int norb, int nat, const int *ind, const int *typ, const int *ls, const int *ms,
                   const double *r, const double *x, const double *y, const double *z, const int *mprox,
                   const double *orben, int deg, const int *tab_filled, const double *S_knots,
