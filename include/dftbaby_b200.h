@@ -11,7 +11,10 @@
  *   - the return value is a status code (DFTB_OK or a negative DFTB_ERR_*);
  *     no entry point allocates device memory -- where scratch space is needed
  *     the caller passes a workspace whose size the *_workspace_size query
- *     returns.
+ *     returns.  The one exception is library state: dftb_apbv (cuBLAS) and
+ *     dftb_batched_eigh (cuSOLVER) create one handle per calling thread and
+ *     device on first use, and those handles hold the libraries' own device
+ *     memory until the process exits.
  *
  * Each function cites the DFTBaby interface it replaces (file:line inside the
  * DFTBaby project).
