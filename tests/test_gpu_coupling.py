@@ -77,3 +77,25 @@ def test_surface_hopping_steps():
     assert np.allclose(tr.last_coupl, -tr.last_coupl.T)
     e = np.array([r[3] for r in tr.log])
     assert np.abs(e - e[0]).max() < 5e-3
+
+
+def test_pes_interface():
+    native.load()
+    from dftbaby_b200.gradients import Gradients
+    from dftbaby_b200.lr_tddftb import LR_TDDFTB
+    from dftbaby_b200.pes import PotentialEnergySurfaces
+    al = geometry.polyene(6, sigma=0.03, seed=2)
+    pes = PotentialEnergySurfaces(al, Nst=3, long_range_correction=1, diag_conv=1e-8)
+    x0 = np.array([p for _, p in al]).reshape(-1)
+    E, g = pes.getEnergiesAndGradient(x0, 1)
+    td = LR_TDDFTB(al, long_range_correction=1)
+    td.setGeometry(al)
+    Om, _ = td.getEnergies(nstates=2, diag_conv=1e-8)
+    assert np.allclose(E, [td.dftb2.E_tot, td.dftb2.E_tot + Om[0], td.dftb2.E_tot + Om[1]], atol=1e-8)
+    assert np.allclose(g, np.sum(Gradients(td).gradient(I=1), axis=0), atol=1e-8)
+    coupl, olap = pes.getScalarCouplings()
+    x1 = x0 + 0.005 * np.random.default_rng(0).standard_normal(x0.shape)
+    pes.getEnergiesAndGradient(x1, 1)
+    coupl, olap = pes.getScalarCouplings()
+    assert np.all(np.diag(olap) > 0.9) and np.allclose(coupl, -coupl.T)
+    assert np.allclose(pes.getEnergy_S0(x1)[0], pes.getEnergies(x1)[0], atol=1e-8)

@@ -1,0 +1,80 @@
+"""The PES interface's host logic (PES.py:17-131, 169-179, 265-272) with stand-in solver objects."""
+import numpy as np
+import torch
+
+from dftbaby_b200.pes import PotentialEnergySurfaces, _vector2atomlist
+
+
+class _FakeDFTB2:
+    def __init__(self):
+        self.E_tot = -12.5
+        self.dq = torch.ones(3)
+        self.geometries = []
+
+    def density_matrix_ref(self):
+        return torch.eye(4)
+
+
+class _FakeTD:
+    def __init__(self):
+        self.dftb2 = _FakeDFTB2()
+        self.calls = []
+        self.XmY = self.XpY = torch.zeros(1)
+
+    def setGeometry(self, atomlist, **opts):
+        self.dftb2.geometries.append((atomlist, opts))
+
+    def getEnergies(self, **opts):
+        self.calls.append(opts)
+        return None
+
+    def getExcEnergies(self):
+        return np.array([0.1, 0.15, 0.2])
+
+
+class _FakeGrads:
+    def gradient(self, I=0):
+        n = 6
+        return np.full(n, 1.0 * I), np.full(n, 0.5), np.arange(n, dtype=float)
+
+
+def _pes(Nst=3):
+    p = PotentialEnergySurfaces.__new__(PotentialEnergySurfaces)
+    p.atomlist = [(6, (0.0, 0.0, 0.0)), (1, (0.0, 0.0, 2.0))]
+    p.tddftb, p.grads = _FakeTD(), _FakeGrads()
+    p.Nst = Nst
+    p.options = {"nstates": Nst - 1, "diag_conv": 1e-6}
+    p.scf_options = {}
+    return p
+
+
+def test_split_options():
+    init, scf, opts = PotentialEnergySurfaces.split_options(
+        dict(long_range_correction=1, scf_conv=1e-9, nr_active_occ=10, charge=0.0, verbose=0))
+    assert init == {"long_range_correction": 1, "verbose": 0}
+    assert scf == {"scf_conv": 1e-9}
+    assert opts == {"scf_conv": 1e-9, "nr_active_occ": 10}
+
+
+def test_energies_and_gradient_assembly():
+    p = _pes(Nst=3)
+    x = np.array([0.0, 0.0, 0.1, 0.0, 0.0, 2.1])
+    E = p.getEnergies(x)
+    assert np.allclose(E, [-12.5, -12.4, -12.35])
+    atomlist, opts = p.tddftb.dftb2.geometries[-1]
+    assert atomlist == _vector2atomlist(x, p.atomlist) and opts == {"keep_charge": True}
+    assert p.tddftb.calls[-1] == {"nstates": 2, "diag_conv": 1e-6}
+    E, g = p.getEnergiesAndGradient(x, 2)
+    assert np.allclose(g, 2.0 + 0.5 + np.arange(6))
+
+
+def test_resets_and_alignment():
+    p = _pes()
+    p.resetXY()
+    assert p.tddftb.XmY is None and p.tddftb.XpY is None
+    p.resetSCF()
+    assert torch.equal(p.tddftb.dftb2.dq, torch.zeros(3)) and torch.equal(p.tddftb.dftb2.P, torch.eye(4))
+    c = np.array([1.0, 2.0])
+    assert np.array_equal(p.alignCoefficients(c), c)
+    p.P = np.diag([1.0, -1.0, 1.0])
+    assert np.array_equal(p.alignCoefficients(c), [-1.0, 2.0])
