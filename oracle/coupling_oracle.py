@@ -8,9 +8,9 @@
   Humeniuk's thesis for the excited-excited block, sqrt(2)-weighted ground-excited blocks.
 
 Parity of ``overlap12`` rests on the SK machinery pinned for H0/S (the same spline and rule
-functions); the reference's Fortran is not compiled here (no Fortran compiler in the image) and its
-Python is Python 2, so the CI overlap has no golden vectors of its own: parity unpinned beyond
-this restatement.
+functions; the reference's Fortran is not compiled here, the image has no Fortran compiler).
+``ci_overlap`` is pinned to DFTBaby's own ScalarCoupling.ci_overlap, run through the py2->py3 shim
+of tests/golden/make_golden.py on a supplied AO overlap (tests/golden/couplings.npz).
 """
 import numpy as np
 

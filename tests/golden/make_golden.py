@@ -24,9 +24,15 @@ energy differences) come from a small seeded polyene; they are stored in the
 fixtures next to the reference outputs, so the tests feed identical inputs to
 the code under test.
 
+Coupling and surface-hopping fixtures (``couplings.npz``) run single method texts of
+``DFTB/ScalarCoupling.py`` (ci_overlap, with the AO overlap supplied), ``DFTB/PES.py``
+(getScalarCouplings, with the CI overlaps supplied) and ``DFTB/Dynamics/SurfaceHopping.py``
+(local diabatization, hopping with scripted random draws, rescaling, decoherence, centre of mass and
+rotation) on stand-in objects, through the same shim.
+
 Usage::
 
-    python tests/golden/make_golden.py /path/to/DFTBaby
+    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings]
 """
 import io
 import os
@@ -312,21 +318,192 @@ def make_solvers(mods, rng):
     np.savez_compressed(os.path.join(HERE, "solvers_c10h12.npz"), **out)
 
 
-def main(ref_root):
+def method_source(path, name):
+    """The text of method ``name`` of a DFTBaby source file, dedented and passed through the shim.
+    Tabs are expanded to 8 columns (Python 2's rule for mixed indentation) and ``<>`` becomes ``!=``."""
+    import textwrap
+    lines = open(path).read().expandtabs(8).splitlines(keepends=True)
+    start = next(i for i, ln in enumerate(lines) if re.match(r"\s*def %s\(" % name, ln))
+    indent = len(lines[start]) - len(lines[start].lstrip())
+    end = start + 1
+    while end < len(lines):
+        ln = lines[end]
+        if ln.strip() and not ln.lstrip().startswith("#") and len(ln) - len(ln.lstrip()) <= indent:
+            break
+        end += 1
+    return py2to3(textwrap.dedent("".join(lines[start:end])).replace("<>", "!="))
+
+
+def _reference_methods(path, names, namespace):
+    ns = dict(namespace)
+    for n in names:
+        exec(compile(method_source(path, n), "%s:%s" % (os.path.basename(path), n), "exec"), ns)
+    return ns
+
+
+def make_couplings(ref_root, rng):
+    """ScalarCoupling.ci_overlap (AO overlap supplied), PES.getScalarCouplings (phase alignment) and the
+    electronic and nuclear steps of SurfaceHopping.MolecularDynamics, run from DFTBaby's own method
+    texts on synthetic inputs."""
+    import numpy.linalg as la
+    import scipy.linalg as sla
+    out = {}
+    # ---- CI overlaps: 16 orbitals, 6 doubly occupied, active occ 2..5, virt 6..10
+    norb, nelec, occ, virt, nst = 16, 12, np.arange(2, 6), np.arange(6, 11), 5
+    Q1, _ = np.linalg.qr(rng.standard_normal((norb, norb)))
+    Q2, _ = np.linalg.qr(Q1 + 0.1 * rng.standard_normal((norb, norb)))
+    Sao = np.eye(norb) + 0.05 * rng.standard_normal((norb, norb))
+    C1 = 0.5 * rng.standard_normal((nst, len(occ), len(virt)))
+    C2 = 0.5 * rng.standard_normal((nst, len(occ), len(virt)))
+    C1[:, 1, 2] = 4e-3
+    C2[:, 0, 4] = -2e-3
+    ns = _reference_methods(os.path.join(ref_root, "DFTB", "ScalarCoupling.py"), ["ci_overlap"],
+                            {"np": np, "la": la, "overlap_AB": lambda *a: Sao})
+
+    class _D:
+        verbose, qmmm, valorbs, SKT, Nelec_val = 0, None, None, None, nelec
+
+    class _TD:
+        dftb2 = _D()
+
+        def getActiveOrbitals(self):
+            return occ, virt
+
+    sc = types.SimpleNamespace(tddftb=_TD())
+    for k, thr in enumerate((1e-3, 1e-2)):
+        out["sci_%d" % k] = ns["ci_overlap"](sc, None, Q1, C1, None, Q2, C2, nst + 1, threshold=thr)
+    out.update(sao=Sao, orbs1=Q1, orbs2=Q2, C1=C1, C2=C2, nelec=nelec, occ=occ, virt=virt,
+               thresholds=np.array([1e-3, 1e-2]))
+    # ---- phase alignment over two calls (PES.py:180-252)
+    Sci_steps = []
+    for step in range(2):
+        A = 0.05 * rng.standard_normal((4, 4))
+        S = np.eye(4) + A - A.T + 0.01 * rng.standard_normal((4, 4))
+        S = S @ np.diag([1.0, -1.0, 1.0, -1.0] if step == 0 else [1.0, 1.0, -1.0, -1.0])
+        if step == 1:
+            S[0, 1:] *= -1.0
+            S[1:, 0] *= -1.0
+        Sci_steps.append(S)
+    Cj = [rng.standard_normal((3, 2, 3)) for _ in range(2)]
+    it = iter(Sci_steps)
+
+    class _SC:
+        def __init__(self, td):
+            pass
+
+        def ci_overlap(self, *args, **kw):
+            return next(it)
+
+    ns = _reference_methods(os.path.join(ref_root, "DFTB", "PES.py"), ["getScalarCouplings"],
+                            {"np": np, "ScalarCoupling": _SC, "utils": None})
+    pes = types.SimpleNamespace(atomlist=None, Nst=4, last_calculation=None,
+                                tddftb=types.SimpleNamespace(dftb2=types.SimpleNamespace(orbs=None, verbose=0)))
+    for step in range(2):
+        pes.tddftb.Cij = Cj[step]
+        coupl, olap = ns["getScalarCouplings"](pes, threshold=0.01)
+        out["pes_sci_%d" % step] = Sci_steps[step]
+        out["pes_C_%d" % step] = Cj[step]
+        out["pes_coupl_%d" % step], out["pes_olap_%d" % step] = coupl, olap
+        out["pes_P_%d" % step] = pes.P
+        out["pes_C_aligned_%d" % step] = pes.last_calculation[2]
+    # ---- surface hopping steps (SurfaceHopping.py:149-201, 262-399)
+    sh_path = os.path.join(ref_root, "DFTB", "Dynamics", "SurfaceHopping.py")
+    draws = iter([0.05, 0.1, 0.6])
+    ns = _reference_methods(sh_path, ["getLocalDiabatization", "getNewState", "getUniformlyRescaledVelocities",
+                                      "getDecoherenceE", "getCenterOfMass", "shiftToCenterOfMass", "momentum",
+                                      "eliminateTranslation", "myCrossProduct", "angularMomentum",
+                                      "momentOfInertia", "getAngularVelocity", "eliminateRotation",
+                                      "eliminateTransRot", "getKineticEnergy"],
+                            {"np": np, "la": la, "sla": sla,
+                             "random": types.SimpleNamespace(random=lambda: next(draws))})
+
+    class _MD:
+        pass
+
+    for name in [k for k in ns if callable(ns[k]) and not k.startswith("_") and k[0].islower()]:
+        if name in ("random",):
+            continue
+        setattr(_MD, name, ns[name])
+    md = _MD()
+    nat = 5
+    md.masses = np.array([12.0, 12.0, 1.0, 1.0, 16.0]) * 1822.888
+    md.totalmass = md.masses.sum()
+    md.coordinates = rng.standard_normal((nat, 3)) * 2.0
+    md.velocities = rng.standard_normal((nat, 3)) * 1e-3
+    md.nat = nat
+    md.printcoeff = 0
+    md.switch_to_groundstate = 1
+    md.decoherence_constant = 0.1
+    md.tstep = 20.0
+    md.time = 0.0
+    md.au_to_fs = 0.0241888
+    md.nstates = 4
+    A = 0.08 * rng.standard_normal((4, 4))
+    md.olap = sla.expm(A - A.T)
+    md.energy_last = np.array([-10.0, -9.85, -9.80, -9.70])
+    md.energy = np.array([-10.001, -9.845, -9.815, -9.69])
+    md.c = np.array([0.1, 0.9, 0.3 + 0.2j, 0.2j], dtype=complex)
+    md.c /= np.linalg.norm(md.c)
+    out.update(sh_olap=md.olap, sh_E0=md.energy_last, sh_E1=md.energy, sh_c0=md.c.copy(), sh_dt=md.tstep)
+    md.getLocalDiabatization()
+    out["sh_c1"] = md.c.copy()
+    # hops: flux out of state 1 into 2 and 3, three scripted draws
+    c_old = np.sqrt(np.array([0.0, 0.9, 0.06, 0.04])).astype(complex)
+    c_new = np.sqrt(np.array([0.0, 0.8, 0.12, 0.08])).astype(complex)
+    states = []
+    for _ in range(3):
+        md.state, md.c_old, md.c = 1, c_old.copy(), c_new.copy()
+        md.getNewState()
+        states.append(md.state)
+    out.update(hop_c_old=c_old, hop_c=c_new, hop_draws=np.array([0.05, 0.1, 0.6]), hop_states=np.array(states))
+    # rescaling and decoherence
+    md.kinetic_energy = md.getKineticEnergy(md.velocities, md.masses)
+    v0 = md.velocities.copy()
+    md.state, md.oldstate = 2, 1
+    md.getUniformlyRescaledVelocities()
+    out.update(res_v0=v0, res_ekin=md.kinetic_energy, res_state=md.state, res_v=md.velocities.copy())
+    md.velocities = v0.copy()
+    md.energy = np.array([-10.0, -9.9, -9.9 + 3 * md.kinetic_energy, -9.7])
+    md.state, md.oldstate = 2, 1
+    md.getUniformlyRescaledVelocities()
+    out.update(rej_E=md.energy.copy(), rej_state=md.state, rej_v=md.velocities.copy())
+    md.energy = np.array([-10.001, -9.845, -9.815, -9.69])
+    md.c = out["sh_c0"].copy()
+    md.state = 1
+    md.getDecoherenceE()
+    out["dec_c"] = md.c.copy()
+    # centre of mass, translation and rotation
+    x0, v0 = md.coordinates.copy(), md.velocities.copy()
+    md.coordinates = md.shiftToCenterOfMass(md.coordinates)
+    md.velocities = v0.copy()
+    md.eliminateTransRot()
+    out.update(com_x0=x0, com_x=md.coordinates.copy(), com_v0=v0, com_v=md.velocities.copy(), com_m=md.masses)
+    np.savez_compressed(os.path.join(HERE, "couplings.npz"), **out)
+
+
+PARTS = ("sk_rules", "gamma", "diis", "solvers", "sk_grad_rules", "gradients")
+
+
+def main(ref_root, only=None):
     sys.path.insert(0, REPO)
     rng = np.random.default_rng(20261203)
     tmp, mods = load_reference_modules(ref_root)
     try:
-        make_sk_rules(ref_root, rng)
-        make_gamma(mods, rng)
-        make_diis(mods, rng)
-        make_solvers(mods, rng)
-        make_sk_grad_rules(ref_root, rng)
-        make_gradients(mods, rng)
+        if only in (None, "core"):
+            make_sk_rules(ref_root, rng)
+            make_gamma(mods, rng)
+            make_diis(mods, rng)
+            make_solvers(mods, rng)
+            make_sk_grad_rules(ref_root, rng)
+            make_gradients(mods, rng)
+        if only in (None, "couplings"):
+            make_couplings(ref_root, np.random.default_rng(20261204))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--only=")]
+    only = next((a.split("=", 1)[1] for a in sys.argv[1:] if a.startswith("--only=")), None)
+    main(args[0] if args else "/root/reference", only)
