@@ -32,7 +32,7 @@ rotation) on stand-in objects, through the same shim.
 
 Usage::
 
-    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings]
+    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python]
 """
 import io
 import os
@@ -318,12 +318,14 @@ def make_solvers(mods, rng):
     np.savez_compressed(os.path.join(HERE, "solvers_c10h12.npz"), **out)
 
 
-def method_source(path, name):
+def method_source(path, name, after=None):
     """The text of method ``name`` of a DFTBaby source file, dedented and passed through the shim.
-    Tabs are expanded to 8 columns (Python 2's rule for mixed indentation) and ``<>`` becomes ``!=``."""
+    Tabs are expanded to 8 columns (Python 2's rule for mixed indentation) and ``<>`` becomes ``!=``.
+    With ``after`` (a regular expression) the search starts at the first line matching it."""
     import textwrap
     lines = open(path).read().expandtabs(8).splitlines(keepends=True)
-    start = next(i for i, ln in enumerate(lines) if re.match(r"\s*def %s\(" % name, ln))
+    first = 0 if after is None else next(i for i, ln in enumerate(lines) if re.match(after, ln))
+    start = next(i for i in range(first, len(lines)) if re.match(r"\s*def %s\(" % name, lines[i]))
     indent = len(lines[start]) - len(lines[start].lstrip())
     end = start + 1
     while end < len(lines):
@@ -481,6 +483,97 @@ def make_couplings(ref_root, rng):
     np.savez_compressed(os.path.join(HERE, "couplings.npz"), **out)
 
 
+def make_mulliken_trans_charges(ref_root, rng):
+    """Mulliken.monopoles (Mulliken.py:10-48, the Python twin of mulliken.f90) and the Python loop of
+    LR_TDDFTB._MullikenTransitionCharges (LR_TDDFTB.py:267-296, the twin of tddftb.trans_charges,
+    which the reference keeps in a string next to the Fortran call), on a C4H6 orbital layout."""
+    import textwrap
+    Zs = [6, 6, 6, 6, 1, 1, 1, 1, 1, 1]
+    valorbs = {1: [(1, 0, 0)], 6: [(2, 0, 0), (2, 1, -1), (2, 1, 0), (2, 1, 1)]}
+    atomlist = [(Z, (0.0, 0.0, float(k))) for k, Z in enumerate(Zs)]
+    norb = sum(len(valorbs[Z]) for Z in Zs)
+    X = rng.standard_normal((norb, norb))
+    S = np.eye(norb) + 0.1 * (X + X.T)
+    X = rng.standard_normal((norb, norb))
+    P = 0.5 * (X + X.T)
+    P0 = np.diag(rng.random(norb))
+    ns = {"np": np}
+    exec(compile(method_source(os.path.join(ref_root, "DFTB", "Mulliken.py"), "monopoles"), "Mulliken.py", "exec"),
+         ns)
+    q, dq = ns["monopoles"](atomlist, P, P0, S, valorbs)
+    # the Python block of _MullikenTransitionCharges, between "# PYTHON CODE" and the closing quotes
+    lines = open(os.path.join(ref_root, "DFTB", "LR_TDDFTB.py")).read().expandtabs(8).splitlines(keepends=True)
+    start = next(i for i, ln in enumerate(lines) if ln.strip() == "# PYTHON CODE")
+    end = next(i for i in range(start + 1, len(lines)) if lines[i].strip() == '"""')
+    block = py2to3(textwrap.dedent("".join(lines[start:end])))
+    orbs = np.linalg.qr(rng.standard_normal((norb, norb)))[0]
+    occ, virt = np.array([3, 5, 6, 7, 8]), np.array([11, 12, 14, 20])
+    fake = types.SimpleNamespace(active_occupied_orbs=occ, active_virtual_orbs=virt)
+    ns = {"zeros": np.zeros, "dot": np.dot, "self": fake, "atomlist": atomlist, "valorbs": valorbs,
+          "orbs": orbs, "S": S}
+    exec(compile(block, "LR_TDDFTB.py:_MullikenTransitionCharges", "exec"), ns)
+    np.savez_compressed(os.path.join(HERE, "mulliken_trans_charges.npz"), Z=np.array(Zs), S=S, P=P, P0=P0,
+                        q=q, dq=dq, orbs=orbs, occ=occ, virt=virt, q_oo=fake.qtrans_oo, q_ov=fake.qtrans_ov,
+                        q_vv=fake.qtrans_vv)
+
+
+def make_sk_python(ref_root, rng):
+    """S and H0 from DFTBaby's Python Slater-Koster path: SKMatrixElements._H0andS (SKMatrixElements.py:64-131)
+    over SlakoTransformations (SKIntegrals.py:832-996), whose splines are splrep(s=None) fits of the
+    shipped tables (spline_slako_integrals, SKIntegrals.py:793-827) evaluated exactly, with the Python
+    angular rules of slako_transformations.py.  Two compact geometries (all pairs inside the 10-bohr
+    tables), every pair interacting."""
+    from scipy import interpolate
+
+    sys.path.insert(0, REPO)
+    from oracle import dftb_oracle as O
+    sk = os.path.join(ref_root, "DFTB", "SlaterKoster")
+
+    def load(path, shim):
+        src = open(path).read()
+        if shim:
+            src = py2to3(src.expandtabs(8))
+        mod = types.ModuleType(os.path.basename(path)[:-3])
+        exec(compile(src, path, "exec"), mod.__dict__)
+        return mod
+
+    T = load(os.path.join(sk, "slako_transformations.py"), True)
+    tables = {key: load(os.path.join(sk, "slako_tables", name + ".py"), False)
+              for key, name in (((1, 1), "h_h"), ((1, 6), "h_c"), ((6, 6), "c_c"))}
+    ns = {"np": np, "interpolate": interpolate, "T": T, "sqrt": np.sqrt, "reshape": np.reshape,
+          "where": np.where, "zeros": np.zeros}
+    ski = os.path.join(sk, "SKIntegrals.py")
+    exec(compile(method_source(ski, "spline_slako_integrals"), "SKIntegrals.py", "exec"), ns)
+    for n in ("__init__", "_directional_cosines", "getOverlap", "getHamiltonian0", "haveDipoles"):
+        exec(compile(method_source(ski, n, after=r"class SlakoTransformations"), "SKIntegrals.py", "exec"), ns)
+    ST = type("SlakoTransformations", (), {n: ns[n] for n in
+                                          ("__init__", "_directional_cosines", "getOverlap", "getHamiltonian0",
+                                           "haveDipoles")})
+    SKT = {key: ST(mod) for key, mod in tables.items()}
+    skm = os.path.join(ref_root, "DFTB", "SKMatrixElements.py")
+    ns2 = {"np": np}
+    for n in ("count_orbitals", "_H0andS"):
+        exec(compile(method_source(skm, n), "SKMatrixElements.py", "exec"), ns2)
+    par = O.Parametrization([1, 6])
+    out = {}
+    geoms = []
+    from dftbaby_b200 import geometry
+    geoms.append(geometry.polyene(2, sigma=0.05, seed=3))  # C2H4
+    while True:  # a random C3H3 cluster, all pairs 1.8-9 bohr apart
+        pos = rng.uniform(-3.0, 3.0, size=(6, 3))
+        d = np.linalg.norm(pos[:, None] - pos[None], axis=-1)[np.triu_indices(6, 1)]
+        if d.min() > 1.8 and d.max() < 9.0:
+            break
+    geoms.append([(Z, tuple(p)) for Z, p in zip([6, 1, 6, 1, 6, 1], pos)])
+    for k, al in enumerate(geoms):
+        nat = len(al)
+        S, H0 = ns2["_H0andS"](al, al, par.valorbs, SKT, par.orbital_energies, np.ones((nat, nat), dtype=int))
+        out["Z_%d" % k] = np.array([Z for Z, _ in al])
+        out["pos_%d" % k] = np.array([p for _, p in al])
+        out["S_%d" % k], out["H0_%d" % k] = S, H0
+    np.savez_compressed(os.path.join(HERE, "sk_python.npz"), **out)
+
+
 PARTS = ("sk_rules", "gamma", "diis", "solvers", "sk_grad_rules", "gradients")
 
 
@@ -498,6 +591,10 @@ def main(ref_root, only=None):
             make_gradients(mods, rng)
         if only in (None, "couplings"):
             make_couplings(ref_root, np.random.default_rng(20261204))
+        if only in (None, "mulliken"):
+            make_mulliken_trans_charges(ref_root, np.random.default_rng(20261205))
+        if only in (None, "sk_python"):
+            make_sk_python(ref_root, np.random.default_rng(20261206))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)
