@@ -333,7 +333,10 @@ def method_source(path, name, after=None):
         if ln.strip() and not ln.lstrip().startswith("#") and len(ln) - len(ln.lstrip()) <= indent:
             break
         end += 1
-    return py2to3(textwrap.dedent("".join(lines[start:end])).replace("<>", "!="))
+    # comment lines indented less than the def (trailing section headers) are not part of the method
+    body = [ln for ln in lines[start:end]
+            if not (ln.lstrip().startswith("#") and len(ln) - len(ln.lstrip()) < indent)]
+    return py2to3(textwrap.dedent("".join(body)).replace("<>", "!="))
 
 
 def _reference_methods(path, names, namespace):
@@ -518,8 +521,8 @@ def make_mulliken_trans_charges(ref_root, rng):
 
 
 def make_sk_python(ref_root, rng):
-    """S and H0 from DFTBaby's Python Slater-Koster path: SKMatrixElements._H0andS (SKMatrixElements.py:64-131)
-    over SlakoTransformations (SKIntegrals.py:832-996), whose splines are splrep(s=None) fits of the
+    """S, H0 and D from DFTBaby's Python Slater-Koster path: SKMatrixElements._H0andS and _DipoleMatrix
+    (SKMatrixElements.py:64-131, 263-318) over SlakoTransformations (SKIntegrals.py:832-1070), whose splines are splrep(s=None) fits of the
     shipped tables (spline_slako_integrals, SKIntegrals.py:793-827) evaluated exactly, with the Python
     angular rules of slako_transformations.py.  Two compact geometries (all pairs inside the 10-bohr
     tables), every pair interacting."""
@@ -538,21 +541,21 @@ def make_sk_python(ref_root, rng):
         return mod
 
     T = load(os.path.join(sk, "slako_transformations.py"), True)
+    Tdip = load(os.path.join(sk, "slako_transformations_dipole.py"), True)
     tables = {key: load(os.path.join(sk, "slako_tables", name + ".py"), False)
               for key, name in (((1, 1), "h_h"), ((1, 6), "h_c"), ((6, 6), "c_c"))}
-    ns = {"np": np, "interpolate": interpolate, "T": T, "sqrt": np.sqrt, "reshape": np.reshape,
-          "where": np.where, "zeros": np.zeros}
+    ns = {"np": np, "interpolate": interpolate, "T": T, "Tdip": Tdip, "sqrt": np.sqrt, "reshape": np.reshape,
+          "where": np.where, "zeros": np.zeros, "AtomicData": None, "NoSKDipolesException": RuntimeError}
     ski = os.path.join(sk, "SKIntegrals.py")
     exec(compile(method_source(ski, "spline_slako_integrals"), "SKIntegrals.py", "exec"), ns)
-    for n in ("__init__", "_directional_cosines", "getOverlap", "getHamiltonian0", "haveDipoles"):
+    names = ("__init__", "_directional_cosines", "getOverlap", "getHamiltonian0", "haveDipoles", "getDipole")
+    for n in names:
         exec(compile(method_source(ski, n, after=r"class SlakoTransformations"), "SKIntegrals.py", "exec"), ns)
-    ST = type("SlakoTransformations", (), {n: ns[n] for n in
-                                          ("__init__", "_directional_cosines", "getOverlap", "getHamiltonian0",
-                                           "haveDipoles")})
+    ST = type("SlakoTransformations", (), {n: ns[n] for n in names})
     SKT = {key: ST(mod) for key, mod in tables.items()}
     skm = os.path.join(ref_root, "DFTB", "SKMatrixElements.py")
     ns2 = {"np": np}
-    for n in ("count_orbitals", "_H0andS"):
+    for n in ("count_orbitals", "_H0andS", "_DipoleMatrix"):
         exec(compile(method_source(skm, n), "SKMatrixElements.py", "exec"), ns2)
     par = O.Parametrization([1, 6])
     out = {}
@@ -571,6 +574,7 @@ def make_sk_python(ref_root, rng):
         out["Z_%d" % k] = np.array([Z for Z, _ in al])
         out["pos_%d" % k] = np.array([p for _, p in al])
         out["S_%d" % k], out["H0_%d" % k] = S, H0
+        out["D_%d" % k] = ns2["_DipoleMatrix"](al, al, par.valorbs, SKT, np.ones((nat, nat), dtype=int))
     np.savez_compressed(os.path.join(HERE, "sk_python.npz"), **out)
 
 

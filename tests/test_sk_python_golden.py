@@ -61,3 +61,54 @@ def test_h0_and_s_against_reference_python_path(k):
         & (ind[:, None] != ind[None, :])
     assert np.abs((H_f - H_py)[~sp_cc]).max() < 1e-14
     assert 1e-6 < np.abs((H_f - H_py)[sp_cc]).max() < 1e-3
+
+
+def _oracle_dipoles(al, reverse):
+    d = O.DFTB2(al, long_range_correction=0)
+    d.setGeometry(al)
+    ind, typ, ls, ms, _ = d._orbital_tables()
+    n, nat, p = d.dim, len(al), d.par
+    order = np.arange(n)[::-1].copy() if reverse else np.arange(n)
+    c = lambda a: np.ascontiguousarray(a[order])
+    S, _ = _oracle_h0_and_s(al, reverse)
+    Sr = np.ascontiguousarray(S[np.ix_(order, order)])
+    pos = np.ascontiguousarray(np.array([q for _, q in al], dtype=np.float64))
+    D = np.zeros((3, n, n))
+    L = O.lib()
+    flag = ctypes.c_int.in_dll(L, "oracle_exact_splines")
+    flag.value = 1
+    try:
+        L.oracle_dipole_matrix(n, nat, O._i(c(ind)), O._i(c(typ)), O._i(c(ls)), O._i(c(ms)), O._d(pos),
+                               O._i(np.ones((nat, nat), dtype=np.int32)), O._d(Sr), p.deg, O._i(p.tab_filled_D),
+                               O._d(p.D_knots), O._d(p.D_coefs), p.npair, p.nskd, p.npts, O._d(D))
+    finally:
+        flag.value = 0
+    inv = np.argsort(order)
+    return np.moveaxis(D[:, inv][:, :, inv], 0, -1), d, ind, pos
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_dipole_matrix_against_reference_python_path(k):
+    """D = SK dipole + R * S.  Off the atom-diagonal blocks the oracle (twin orientation) equals the Python
+    path to rounding.  On them the Python path adds R * <mu|nu> evaluated from the SK tables at r = 0
+    (getOverlap of an atom with itself), where the Fortran uses the on-site S (1 on the diagonal, 0
+    between different orbitals of one atom); that difference is reproduced exactly."""
+    from oracle import coupling_oracle as CO
+    al = [(int(z), tuple(q)) for z, q in zip(G["Z_%d" % k], G["pos_%d" % k])]
+    D, d, ind, pos = _oracle_dipoles(al, reverse=True)
+    D_py = G["D_%d" % k]
+    same = ind[:, None] == ind[None, :]
+    assert np.abs((D - D_py)[~same]).max() < 1e-14
+    L = O.lib()
+    flag = ctypes.c_int.in_dll(L, "oracle_exact_splines")
+    flag.value = 1
+    try:
+        S_r0 = CO.overlap12(d, pos, pos)  # every pair from the tables, the same-atom pairs at r = 0
+    finally:
+        flag.value = 0
+    S_onsite = np.eye(len(ind))
+    corr = pos[ind][:, None, :] * (S_r0 - S_onsite)[:, :, None]
+    assert np.abs((D + corr - D_py)[same]).max() < 1e-14
+    # the Fortran orientation differs only through the dipole tables' s-p / p-s disagreement
+    D_f, _, _, _ = _oracle_dipoles(al, reverse=False)
+    assert np.abs((D_f - D_py)[~same]).max() < 1e-7
