@@ -32,7 +32,7 @@ rotation) on stand-in objects, through the same shim.
 
 Usage::
 
-    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python]
+    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc]
 """
 import io
 import os
@@ -578,6 +578,77 @@ def make_sk_python(ref_root, rng):
     np.savez_compressed(os.path.join(HERE, "sk_python.npz"), **out)
 
 
+def _twisted_ethylene():
+    """C2H4 twisted by 90 degrees about the C=C bond (bohr): HOMO and LUMO nearly degenerate."""
+    cc, ch, a = 2.53, 2.05, np.deg2rad(121.0)
+    hx, hr = ch * np.cos(np.pi - a), ch * np.sin(np.pi - a)
+    return [(6, (0.0, 0.0, 0.0)), (6, (cc, 0.0, 0.0)),
+            (1, (-hx, hr, 0.0)), (1, (-hx, -hr, 0.0)),
+            (1, (cc + hx, 0.0, hr)), (1, (cc + hx, 0.0, -hr))]
+
+
+def make_scc(ref_root, mods):
+    """DFTB2.runSCC (DFTB2.py:940-1160) with its helpers (_coulomb_hamiltonian/_construct_h1, lc_exact_exchange,
+    density_matrix_ref, _constructDensityMatrix/_density_matrix with fermi_occupation, _MullikenAnalysis,
+    getHOMO_LUMO_gap/getFrontierOrbitals) run from DFTBaby's text on the oracle's S, H0, gamma and G_lr, with
+    the default DIIS_80 mixer of the shimmed ConvAcceleration.  Mulliken charges come from the oracle's
+    restatement of mulliken.f90 (pinned against Mulliken.monopoles); the energies are not needed by the
+    iteration and are skipped.  Three cases: C10H12 with the long-range correction, C6H8 without, and a
+    90-degree twisted ethylene whose near-degenerate frontier orbitals switch the level shift on."""
+    import scipy.linalg as sla
+
+    sys.path.insert(0, REPO)
+    from dftbaby_b200 import geometry
+    from oracle import dftb_oracle as O
+
+    class SCFNotConverged(Exception):
+        pass
+
+    class SCFChargeInconsistency(Exception):
+        pass
+
+    dftb2 = os.path.join(ref_root, "DFTB", "DFTB2.py")
+    mull = types.SimpleNamespace(mulliken=types.SimpleNamespace(
+        monopoles=lambda P, P0, S, opa: O.monopoles(P, P0, S, np.asarray(opa, dtype=np.int32))))
+    ns = {"np": np, "la": np.linalg, "array": np.array, "zeros": np.zeros, "sqrt": np.sqrt, "log": np.log,
+          "exp": np.exp, "dot": np.dot, "argsort": np.argsort, "where": np.where, "sum": np.sum,
+          "eigh": sla.eigh, "norm": sla.norm, "inv": sla.inv, "sqrtm": sla.sqrtm, "copy": np.copy,
+          "DIIS_80": mods["ConvAcceleration"].DIIS_80, "mulliken": mull, "SCFNotConverged": SCFNotConverged,
+          "SCFChargeInconsistency": SCFChargeInconsistency, "kBoltzmann": 3.166811382e-6}
+    for n in ("fermi_occupation", "fermi_occupation_T0"):
+        exec(compile(method_source(dftb2, n), "DFTB2.py", "exec"), ns)
+    names = ("runSCC", "_coulomb_hamiltonian", "_construct_h1", "lc_exact_exchange", "density_matrix_ref",
+             "_constructDensityMatrix", "_density_matrix", "_MullikenAnalysis", "getHOMO_LUMO_gap",
+             "getFrontierOrbitals")
+    for n in names:
+        exec(compile(method_source(dftb2, n, after=r"class DFTB2"), "DFTB2.py", "exec"), ns)
+    Ref = type("DFTB2", (), dict({n: ns[n] for n in names}, getEnergies=lambda self: None))
+    out = {}
+    cases = (("c10h12_lc", geometry.polyene(10, sigma=0.02, seed=11), 1),
+             ("c6h8", geometry.polyene(6, sigma=0.02, seed=12), 0),
+             ("twisted_c2h4_lc", _twisted_ethylene(), 1))
+    for name, al, lc in cases:
+        od = O.DFTB2(al, long_range_correction=lc)
+        od.setGeometry(al)
+        od.getEnergy()  # builds the oracle's matrices (and runs its own SCC, not used here)
+        r = Ref()
+        r.atomlist, r.valorbs, r.valorbs_occupation = od.atomlist, od.par.valorbs, od.par.valorbs_occupation
+        r.dim, r.S, r.H0, r.gamma = od.dim, od.S, od.H0, od.gamma
+        r.G_lr = od.G_lr if lc else None
+        r.long_range_correction, r.lc_implementation = lc, "new"
+        r.Nelec_val, r.nr_unpaired_electrons, r.charge = od.Nelec_val, 0, 0.0
+        r.orbsPerAtom, r.charge_guess, r.verbose = od.orbsPerAtom, None, 0
+        r.mulliken_dipoles, r.point_charges, r.onsite_correction, r.save_converged_charges = 0, [], 0, None
+        r.runSCC()
+        out["%s_Z" % name] = np.array([Z for Z, _ in al])
+        out["%s_pos" % name] = np.array([p for _, p in al])
+        out["%s_lc" % name] = lc
+        out["%s_iterations" % name] = r.i + 1
+        for key in ("P", "dq", "orbe", "f", "HLgap", "relative_change", "S", "H0"):
+            out["%s_%s" % (name, key)] = getattr(r, key)
+    np.savez_compressed(os.path.join(HERE, "scc.npz"), **out)
+
+
 PARTS = ("sk_rules", "gamma", "diis", "solvers", "sk_grad_rules", "gradients")
 
 
@@ -599,6 +670,8 @@ def main(ref_root, only=None):
             make_mulliken_trans_charges(ref_root, np.random.default_rng(20261205))
         if only in (None, "sk_python"):
             make_sk_python(ref_root, np.random.default_rng(20261206))
+        if only in (None, "scc"):
+            make_scc(ref_root, mods)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)
