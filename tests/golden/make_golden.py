@@ -32,7 +32,7 @@ rotation) on stand-in objects, through the same shim.
 
 Usage::
 
-    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc]
+    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue]
 """
 import io
 import os
@@ -53,6 +53,8 @@ def py2to3(src):
     """Mechanical conversion of print statements and renamed dict/range methods."""
     src = src.replace(".iteritems()", ".items()").replace("xrange(", "range(")
     src = re.sub(r"\.has_key\(", ".__contains__(", src)
+    # one-line "print>>fh, a, b" statements -> print(a, b, file=fh)
+    src = re.sub(r"^(\s*)print\s*>>\s*([^,\n]+),\s*(.*)$", r"\1print(\3, file=\2)", src, flags=re.M)
     toks = list(tokenize.generate_tokens(io.StringIO(src).readline))
     edits = []
     for k, t in enumerate(toks):
@@ -64,6 +66,8 @@ def py2to3(src):
         if j >= 0 and toks[j].type not in (tokenize.NEWLINE, tokenize.INDENT, tokenize.DEDENT) \
                 and toks[j].string != ":":
             continue
+        if toks[k + 1].string == "(" and toks[k + 1].start[1] == t.end[1]:
+            continue  # already a call (converted above)
         m = k + 1
         while toks[m].type not in (tokenize.NEWLINE, tokenize.ENDMARKER):
             m += 1
@@ -649,6 +653,66 @@ def make_scc(ref_root, mods):
     np.savez_compressed(os.path.join(HERE, "scc.npz"), **out)
 
 
+def make_lr_glue(ref_root, rng):
+    """LR_TDDFTB.setActiveOrbitals, _TransitionDipoles, _TransitionDipolesMulliken, getOscillatorStrengths,
+    determineActiveSpace, TransitionChargesState, saveAbsorptionSpectrum and saveTransitionCharges
+    (LR_TDDFTB.py:167-243, 567-592, 698-705, 807-831, 900-908, 1008-1025) run from DFTBaby's text on a
+    stand-in solved object: 14 orbitals (6 doubly occupied), active window 3 x 4, 3 states."""
+    lr = os.path.join(ref_root, "DFTB", "LR_TDDFTB.py")
+    names = ("setActiveOrbitals", "_TransitionDipoles", "_TransitionDipolesMulliken", "getOscillatorStrengths",
+             "determineActiveSpace", "TransitionChargesState", "saveAbsorptionSpectrum", "saveTransitionCharges")
+    ns = {"np": np, "where": np.where, "argsort": np.argsort, "dot": np.dot, "meshgrid": np.meshgrid,
+          "path": os.path}
+    for n in names:
+        exec(compile(method_source(lr, n, after=r"class LR_TDDFTB"), "LR_TDDFTB.py", "exec"), ns)
+    Ref = type("LR_TDDFTB", (), {n: ns[n] for n in names})
+    norb, nat = 14, 5
+    orbe = np.sort(rng.standard_normal(norb))
+    orbe[[2, 3]] = orbe[[3, 2]]  # occupations follow the energies, not the index order
+    f = np.zeros(norb)
+    f[np.argsort(orbe)[:6]] = 2.0
+    orbs = np.linalg.qr(rng.standard_normal((norb, norb)))[0]
+    X = rng.standard_normal((norb, norb, 3))
+    D = X + X.transpose(1, 0, 2)
+    pos = rng.standard_normal((nat, 3))
+    atomlist = [(6, tuple(p)) for p in pos]
+    dftb2 = types.SimpleNamespace(getOccupation=lambda: f, getKSEnergies=lambda: orbe,
+                                  getDipoleMatrix=lambda: D, getKSCoefficients=lambda: orbs,
+                                  getGeometry=lambda: atomlist, verbose=0)
+    r = Ref()
+    r.dftb2 = dftb2
+    r.setActiveOrbitals(nr_active_occ=3, nr_active_virt=4)
+    C = rng.standard_normal((3, 3, 4))
+    C /= np.sqrt((C * C).sum(axis=(1, 2)))[:, None, None]
+    C[0] *= 0.0
+    C[0, 2, 0], C[0, 1, 1] = np.sqrt(0.995), np.sqrt(0.005)
+    r.Cij, r.Omega, r.multiplicity, r.Irreps = C, np.array([0.11, 0.17, 0.23]), "S", ["", "", ""]
+    r.qtrans_ov = rng.standard_normal((nat, 3, 4))
+    out = dict(orbe=orbe, f=f, orbs=orbs, D=D, pos=pos, C=C, Omega=r.Omega, qtrans_ov=r.qtrans_ov,
+               occupied_orbs=r.occupied_orbs, virtual_orbs=r.virtual_orbs,
+               active_occupied_orbs=r.active_occupied_orbs, active_virtual_orbs=r.active_virtual_orbs)
+    r._TransitionDipolesMulliken()
+    out["tdip_mulliken"] = np.array([r.tdipX, r.tdipY, r.tdipZ])
+    r._TransitionDipoles()
+    out["tdip"] = np.array([r.tdipX, r.tdipY, r.tdipZ])
+    out["osc"] = r.getOscillatorStrengths()
+    out["active_space_1e-5"] = np.array(r.determineActiveSpace())
+    out["active_space_1e-2"] = np.array(r.determineActiveSpace(threshold=1e-2))
+    out["tq_state_1"] = r.TransitionChargesState(1)
+    tmp = tempfile.mkdtemp(prefix="dftbaby_lr_")
+    real_string = sys.modules.get("string")
+    sys.modules["string"] = types.SimpleNamespace(rjust=lambda text, width: text.rjust(width))
+    try:
+        r.saveAbsorptionSpectrum(os.path.join(tmp, "spec.dat"))
+        r.saveTransitionCharges(os.path.join(tmp, "tq.dat"))
+    finally:
+        sys.modules["string"] = real_string
+    out["spectrum_text"] = np.array(open(os.path.join(tmp, "spec.dat")).read())
+    out["transition_charges_text"] = np.array(open(os.path.join(tmp, "tq.dat")).read())
+    shutil.rmtree(tmp, ignore_errors=True)
+    np.savez_compressed(os.path.join(HERE, "lr_glue.npz"), **out)
+
+
 PARTS = ("sk_rules", "gamma", "diis", "solvers", "sk_grad_rules", "gradients")
 
 
@@ -672,6 +736,8 @@ def main(ref_root, only=None):
             make_sk_python(ref_root, np.random.default_rng(20261206))
         if only in (None, "scc"):
             make_scc(ref_root, mods)
+        if only in (None, "lr_glue"):
+            make_lr_glue(ref_root, np.random.default_rng(20261207))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)

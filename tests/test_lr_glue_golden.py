@@ -1,0 +1,57 @@
+"""LR_TDDFTB's active-space selection, transition dipoles (matrix-element and Mulliken forms),
+oscillator strengths, active-space suggestion, per-state transition charges and output files, run on
+CPU tensors against DFTBaby's own methods (tests/golden/lr_glue.npz, made by
+tests/golden/make_golden.py on the same stand-in solved object)."""
+import os
+import types
+
+import numpy as np
+import torch
+
+from dftbaby_b200.lr_tddftb import LR_TDDFTB
+
+G = np.load(os.path.join(os.path.dirname(__file__), "golden", "lr_glue.npz"))
+
+
+def _solved():
+    t = lambda a: torch.tensor(np.asarray(a))
+    d = types.SimpleNamespace(device=torch.device("cpu"), orbs=t(G["orbs"]), D3=t(np.moveaxis(G["D"], -1, 0)),
+                              pos=t(G["pos"]), getOccupation=lambda: t(G["f"]), getKSEnergies=lambda: t(G["orbe"]))
+    td = LR_TDDFTB.__new__(LR_TDDFTB)
+    td.dftb2 = d
+    td.setActiveOrbitals(nr_active_occ=3, nr_active_virt=4)
+    td.Cij, td.Omega, td.multiplicity = t(G["C"]), G["Omega"].copy(), "S"
+    td.qtrans_ov = t(G["qtrans_ov"])
+    return td
+
+
+def test_active_orbitals_against_reference():
+    td = _solved()
+    for key in ("occupied_orbs", "virtual_orbs", "active_occupied_orbs", "active_virtual_orbs"):
+        assert np.array_equal(getattr(td, key), G[key])
+    assert tuple(td.determineActiveSpace()) == tuple(G["active_space_1e-5"])
+    assert tuple(td.determineActiveSpace(threshold=1e-2)) == tuple(G["active_space_1e-2"])
+
+
+def test_transition_dipoles_and_oscillator_strengths_against_reference():
+    td = _solved()
+    td._TransitionDipolesMulliken()
+    assert np.abs(np.array([td.tdipX.numpy(), td.tdipY.numpy(), td.tdipZ.numpy()]) - G["tdip_mulliken"]).max() < 1e-13
+    td._TransitionDipoles()
+    assert np.abs(np.array([td.tdipX.numpy(), td.tdipY.numpy(), td.tdipZ.numpy()]) - G["tdip"]).max() < 1e-13
+    assert np.abs(td.getOscillatorStrengths() - G["osc"]).max() < 1e-13
+    assert np.abs(td.TransitionChargesState(1) - G["tq_state_1"]).max() < 1e-14
+
+
+def test_output_files_against_reference(tmp_path):
+    td = _solved()
+    td._TransitionDipoles()
+    td.getOscillatorStrengths()
+    td.saveAbsorptionSpectrum(str(tmp_path / "spec.dat"))
+    assert (tmp_path / "spec.dat").read_text() == str(G["spectrum_text"])
+    td.saveTransitionCharges(str(tmp_path / "tq.dat"))
+    got = np.loadtxt(str(tmp_path / "tq.dat"))
+    ref_text = str(G["transition_charges_text"])
+    assert (tmp_path / "tq.dat").read_text().splitlines()[:3] == ref_text.splitlines()[:3]
+    ref = np.array([[float(x) for x in ln.split()] for ln in ref_text.splitlines()[3:]])
+    assert np.abs(got - ref).max() < 1e-14
