@@ -32,7 +32,7 @@ rotation) on stand-in objects, through the same shim.
 
 Usage::
 
-    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue]
+    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda]
 """
 import io
 import os
@@ -713,6 +713,39 @@ def make_lr_glue(ref_root, rng):
     np.savez_compressed(os.path.join(HERE, "lr_glue.npz"), **out)
 
 
+def make_lambda(ref_root, rng):
+    """DFTB2._construct_gaussian_overlap (DFTB2.py:1287-1317) on a C6H8 geometry with the Hubbard parameters
+    of the shipped tables, and LR_TDDFTB._Lambda2_calcOia / _Lambda2_diagnostics (LR_TDDFTB.py:538-565) on
+    synthetic diagonal transition charges with that overlap, run from DFTBaby's text."""
+    sys.path.insert(0, REPO)
+    from dftbaby_b200 import geometry
+    from oracle import dftb_oracle as O
+    ns = {"np": np, "zeros": np.zeros, "sqrt": np.sqrt, "log": np.log, "exp": np.exp, "dot": np.dot,
+          "array": np.array, "pi": np.pi, "sum": np.sum}
+    exec(compile(method_source(os.path.join(ref_root, "DFTB", "DFTB2.py"), "_construct_gaussian_overlap",
+                               after=r"class DFTB2"), "DFTB2.py", "exec"), ns)
+    for n in ("_Lambda2_calcOia", "_Lambda2_diagnostics"):
+        exec(compile(method_source(os.path.join(ref_root, "DFTB", "LR_TDDFTB.py"), n, after=r"class LR_TDDFTB"),
+                     "LR_TDDFTB.py", "exec"), ns)
+    al = geometry.polyene(6, sigma=0.03, seed=21)
+    par = O.Parametrization([1, 6])
+    d = types.SimpleNamespace(atomlist=al, hubbard_U=par.hubbard_U)
+    gaussOmega = ns["_construct_gaussian_overlap"](d)
+    nat, no, nv, ns_ = len(al), 4, 5, 3
+    q_oo = rng.standard_normal((nat, no, no))
+    q_vv = rng.standard_normal((nat, nv, nv))
+    C = rng.standard_normal((ns_, no, nv))
+    td = types.SimpleNamespace(dftb2=types.SimpleNamespace(getGaussianOverlap=lambda: gaussOmega,
+                                                           getGeometry=lambda: al),
+                               active_occupied_orbs=np.arange(no), active_virtual_orbs=np.arange(no, no + nv),
+                               qtrans_oo=q_oo, qtrans_vv=q_vv, Cij=C)
+    ns["_Lambda2_calcOia"](td)
+    Lambda2 = ns["_Lambda2_diagnostics"](td)
+    np.savez_compressed(os.path.join(HERE, "lambda.npz"), Z=np.array([Z for Z, _ in al]),
+                        pos=np.array([p for _, p in al]), gaussOmega=gaussOmega, q_oo=q_oo, q_vv=q_vv, C=C,
+                        Oia=td.Oia, Lambda2=Lambda2)
+
+
 PARTS = ("sk_rules", "gamma", "diis", "solvers", "sk_grad_rules", "gradients")
 
 
@@ -738,6 +771,8 @@ def main(ref_root, only=None):
             make_scc(ref_root, mods)
         if only in (None, "lr_glue"):
             make_lr_glue(ref_root, np.random.default_rng(20261207))
+        if only in (None, "lambda"):
+            make_lambda(ref_root, np.random.default_rng(20261208))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)
