@@ -32,7 +32,7 @@ rotation) on stand-in objects, through the same shim.
 
 Usage::
 
-    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda]
+    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda|repulsive]
 """
 import io
 import os
@@ -746,6 +746,35 @@ def make_lambda(ref_root, rng):
                         Oia=td.Oia, Lambda2=Lambda2)
 
 
+def make_repulsive(ref_root, rng):
+    """RepulsivePotential.__init__ / getVrep (RepulsivePotential.py:17-100, as DFTB2.py:327 builds them: no
+    smooth tail) on the shipped H-H, H-C and C-C tables, run from DFTBaby's text: values and first
+    derivatives below the grid, inside it and beyond its last point."""
+    from collections import defaultdict
+    from scipy import interpolate
+    rp = os.path.join(ref_root, "DFTB", "RepulsivePotential", "RepulsivePotential.py")
+    ns = {"np": np, "interpolate": interpolate, "defaultdict": defaultdict, "argmax": np.argmax,
+          "exp": np.exp, "pow": pow}
+    for n in ("__init__", "getVrep"):
+        exec(compile(method_source(rp, n, after=r"class RepulsivePotential"), "RepulsivePotential.py", "exec"), ns)
+    RP = type("RepulsivePotential", (), {"__init__": ns["__init__"], "getVrep": ns["getVrep"]})
+    out = {}
+    for name in ("h_h", "h_c", "c_c"):
+        path = os.path.join(ref_root, "DFTB", "RepulsivePotential", "reppot_tables", name + ".py")
+        mod = types.ModuleType(name)
+        exec(compile(open(path).read(), path, "exec"), mod.__dict__)
+        pot = RP(mod)
+        R = np.sort(np.concatenate([rng.uniform(0.6 * pot.dmin, pot.dmin, 3), rng.uniform(pot.dmin, pot.dmax, 25),
+                                    [pot.dmax, pot.dmax * 1.2]]))
+        import contextlib
+        with contextlib.redirect_stdout(io.StringIO()):  # the reference warns below the grid
+            out[name + "_R"] = R
+            out[name + "_V"] = np.array([float(pot.getVrep(r)) for r in R])
+            out[name + "_dV"] = np.array([float(pot.getVrep(r, deriv=1)) for r in R])
+        out[name + "_Z"] = np.array([mod.Z1, mod.Z2])
+    np.savez_compressed(os.path.join(HERE, "repulsive.npz"), **out)
+
+
 PARTS = ("sk_rules", "gamma", "diis", "solvers", "sk_grad_rules", "gradients")
 
 
@@ -773,6 +802,8 @@ def main(ref_root, only=None):
             make_lr_glue(ref_root, np.random.default_rng(20261207))
         if only in (None, "lambda"):
             make_lambda(ref_root, np.random.default_rng(20261208))
+        if only in (None, "repulsive"):
+            make_repulsive(ref_root, np.random.default_rng(20261209))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)
