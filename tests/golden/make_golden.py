@@ -32,7 +32,7 @@ rotation) on stand-in objects, through the same shim.
 
 Usage::
 
-    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda|repulsive]
+    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda|repulsive|lr_e2e]
 """
 import io
 import os
@@ -591,18 +591,14 @@ def _twisted_ethylene():
             (1, (cc + hx, 0.0, hr)), (1, (cc + hx, 0.0, -hr))]
 
 
-def make_scc(ref_root, mods):
-    """DFTB2.runSCC (DFTB2.py:940-1160) with its helpers (_coulomb_hamiltonian/_construct_h1, lc_exact_exchange,
-    density_matrix_ref, _constructDensityMatrix/_density_matrix with fermi_occupation, _MullikenAnalysis,
-    getHOMO_LUMO_gap/getFrontierOrbitals) run from DFTBaby's text on the oracle's S, H0, gamma and G_lr, with
-    the default DIIS_80 mixer of the shimmed ConvAcceleration.  Mulliken charges come from the oracle's
-    restatement of mulliken.f90 (pinned against Mulliken.monopoles); the energies are not needed by the
-    iteration and are skipped.  Three cases: C10H12 with the long-range correction, C6H8 without, and a
-    90-degree twisted ethylene whose near-degenerate frontier orbitals switch the level shift on."""
+def _reference_dftb2(ref_root, mods):
+    """A DFTB2 stand-in class carrying DFTBaby's own runSCC and its helpers (DFTB2.py:702-717, 804-879,
+    940-1160, 1239-1266, 2516-2610, and the frontier-orbital accessors), run from their text.  Mulliken
+    charges come from the oracle's restatement of mulliken.f90 (pinned against Mulliken.monopoles); the
+    energies, which the iteration does not use, are skipped."""
     import scipy.linalg as sla
 
     sys.path.insert(0, REPO)
-    from dftbaby_b200 import geometry
     from oracle import dftb_oracle as O
 
     class SCFNotConverged(Exception):
@@ -626,7 +622,29 @@ def make_scc(ref_root, mods):
              "getFrontierOrbitals")
     for n in names:
         exec(compile(method_source(dftb2, n, after=r"class DFTB2"), "DFTB2.py", "exec"), ns)
-    Ref = type("DFTB2", (), dict({n: ns[n] for n in names}, getEnergies=lambda self: None))
+    return type("DFTB2", (), dict({n: ns[n] for n in names}, getEnergies=lambda self: None))
+
+
+def _load_into(ref, od, lc):
+    """Copy the oracle's matrices for one geometry into a reference DFTB2 stand-in."""
+    ref.atomlist, ref.valorbs, ref.valorbs_occupation = od.atomlist, od.par.valorbs, od.par.valorbs_occupation
+    ref.dim, ref.S, ref.H0, ref.gamma = od.dim, od.S, od.H0, od.gamma
+    ref.G_lr = od.G_lr if lc else None
+    ref.gamma_lr = od.gamma_lr if lc else None
+    ref.long_range_correction, ref.lc_implementation = lc, "new"
+    ref.Nelec_val, ref.nr_unpaired_electrons, ref.charge = od.Nelec_val, 0, 0.0
+    ref.orbsPerAtom, ref.charge_guess, ref.verbose = od.orbsPerAtom, None, 0
+    ref.mulliken_dipoles, ref.point_charges, ref.onsite_correction, ref.save_converged_charges = 0, [], 0, None
+
+
+def make_scc(ref_root, mods):
+    """DFTB2.runSCC (DFTB2.py:940-1160) with its helpers run from DFTBaby's text (``_reference_dftb2``) on
+    the oracle's S, H0, gamma and G_lr, with the default DIIS_80 mixer of the shimmed ConvAcceleration.
+    Three cases: C10H12 with the long-range correction, C6H8 without, and a 90-degree twisted ethylene
+    whose near-degenerate frontier orbitals switch the level shift on."""
+    from dftbaby_b200 import geometry
+    from oracle import dftb_oracle as O
+    Ref = _reference_dftb2(ref_root, mods)
     out = {}
     cases = (("c10h12_lc", geometry.polyene(10, sigma=0.02, seed=11), 1),
              ("c6h8", geometry.polyene(6, sigma=0.02, seed=12), 0),
@@ -636,13 +654,7 @@ def make_scc(ref_root, mods):
         od.setGeometry(al)
         od.getEnergy()  # builds the oracle's matrices (and runs its own SCC, not used here)
         r = Ref()
-        r.atomlist, r.valorbs, r.valorbs_occupation = od.atomlist, od.par.valorbs, od.par.valorbs_occupation
-        r.dim, r.S, r.H0, r.gamma = od.dim, od.S, od.H0, od.gamma
-        r.G_lr = od.G_lr if lc else None
-        r.long_range_correction, r.lc_implementation = lc, "new"
-        r.Nelec_val, r.nr_unpaired_electrons, r.charge = od.Nelec_val, 0, 0.0
-        r.orbsPerAtom, r.charge_guess, r.verbose = od.orbsPerAtom, None, 0
-        r.mulliken_dipoles, r.point_charges, r.onsite_correction, r.save_converged_charges = 0, [], 0, None
+        _load_into(r, od, lc)
         r.runSCC()
         out["%s_Z" % name] = np.array([Z for Z, _ in al])
         out["%s_pos" % name] = np.array([p for _, p in al])
@@ -775,6 +787,69 @@ def make_repulsive(ref_root, rng):
     np.savez_compressed(os.path.join(HERE, "repulsive.npz"), **out)
 
 
+def make_lr_e2e(ref_root, mods):
+    """LR_TDDFTB.getEnergies end to end from DFTBaby's text (LR_TDDFTB.py:167-188, 254-320, 378-527, 538-705,
+    741-758 and determineActiveSpace) over the reference SCC stand-in (``_reference_dftb2``) and the shimmed
+    Solver module, on the oracle's S, H0, D, gamma, gamma_lr and Gaussian overlap.  The Fortran
+    tddftb.trans_charges is served by the oracle's restatement (pinned against the reference's Python twin);
+    getTransitionDipolesExc (excited-excited dipoles, not used for Omega and f) is skipped.  Cases: C6H8
+    without long-range correction (Hermitian Davidson), C6H8 with it (non-Hermitian Davidson) and C4H6 with
+    it solved by full Casida."""
+    import importlib
+
+    from dftbaby_b200 import geometry
+    from oracle import dftb_oracle as O
+    ext = importlib.import_module("DFTB.extensions")
+    ext.tddftb = types.SimpleNamespace(tddftb=types.SimpleNamespace(
+        trans_charges=lambda oo, ov, S, opa: O.trans_charges(np.ascontiguousarray(oo), np.ascontiguousarray(ov),
+                                                             np.ascontiguousarray(S), np.asarray(opa, np.int32))))
+    Ref = _reference_dftb2(ref_root, mods)
+    lr = os.path.join(ref_root, "DFTB", "LR_TDDFTB.py")
+    names = ("setActiveOrbitals", "setMultiplicity", "_solve_lr_equations", "_MullikenTransitionCharges",
+             "_Lambda2_calcOia", "_Lambda2_diagnostics", "_getOrbitalEnDifferences", "_getOrbitalOccDifferences",
+             "_TransitionDipoles", "getOscillatorStrengths", "_SymmetryOfExcitations", "determineActiveSpace",
+             "getEnergies")
+    ns = {"np": np, "la": np.linalg, "array": np.array, "where": np.where, "argsort": np.argsort,
+          "zeros": np.zeros, "dot": np.dot, "tensordot": np.tensordot, "transpose": np.transpose,
+          "diag": np.diag, "reshape": np.reshape, "sqrt": np.sqrt, "arange": np.arange, "outer": np.outer,
+          "sum": np.sum, "meshgrid": np.meshgrid, "eigh": np.linalg.eigh, "path": os.path,
+          "Solver": mods["Solver"], "StabilityAnalysis": None, "LongRangeCTCorrection": None,
+          "SymmetryAssignmentEx": None}
+    for n in names:
+        exec(compile(method_source(lr, n, after=r"class LR_TDDFTB"), "LR_TDDFTB.py", "exec"), ns)
+    LR = type("LR_TDDFTB", (), dict({n: ns[n] for n in names}, getTransitionDipolesExc=lambda self, Nst: None))
+    out = {}
+    cases = (("c6h8", geometry.polyene(6, sigma=0.02, seed=31), 0, 4),
+             ("c6h8_lc", geometry.polyene(6, sigma=0.02, seed=32), 1, 4),
+             ("c4h6_lc_casida", geometry.polyene(4, sigma=0.02, seed=33), 1, None))
+    for name, al, lc, nstates in cases:
+        od = O.DFTB2(al, long_range_correction=lc)
+        od.setGeometry(al)
+        od.getEnergy()
+        d = Ref()
+        _load_into(d, od, lc)
+        d.D, d.gaussOmega, d.parameter_set, d.use_symmetry = od.D, od.gaussOmega, "homegrown", 0
+        d.getEnergy = types.MethodType(lambda self, **opts: (self.runSCC(**opts), 0.0)[1], d)
+        for acc, attr in (("getKSEnergies", "orbe"), ("getOccupation", "f"), ("getKSCoefficients", "orbs"),
+                          ("getGeometry", "atomlist"), ("getValorbs", "valorbs"), ("getOverlapMatrix", "S"),
+                          ("getGamma", "gamma"), ("getGamma_lr", "gamma_lr"), ("getDipoleMatrix", "D"),
+                          ("getGaussianOverlap", "gaussOmega")):
+            setattr(d, acc, (lambda a: (lambda: getattr(d, a)))(attr))
+        td = LR()
+        td.dftb2, td.XmY, td.XpY, td.Omega = d, None, None, None
+        opts = dict(nstates=nstates, diag_conv=1.0e-10, diag_maxiter=100)
+        Om, f = td.getEnergies(**opts)
+        out["%s_Z" % name] = np.array([Z for Z, _ in al])
+        out["%s_pos" % name] = np.array([p for _, p in al])
+        out["%s_lc" % name] = lc
+        out["%s_nstates" % name] = -1 if nstates is None else nstates
+        out["%s_Omega" % name], out["%s_f" % name] = np.asarray(Om), np.asarray(f)
+        out["%s_Lambda2" % name] = np.asarray(td.Lambda2)
+        n = len(Om) if nstates is None else nstates
+        out["%s_tdip" % name] = np.array([td.tdipX[:n], td.tdipY[:n], td.tdipZ[:n]])
+    np.savez_compressed(os.path.join(HERE, "lr_e2e.npz"), **out)
+
+
 PARTS = ("sk_rules", "gamma", "diis", "solvers", "sk_grad_rules", "gradients")
 
 
@@ -804,6 +879,8 @@ def main(ref_root, only=None):
             make_lambda(ref_root, np.random.default_rng(20261208))
         if only in (None, "repulsive"):
             make_repulsive(ref_root, np.random.default_rng(20261209))
+        if only in (None, "lr_e2e"):
+            make_lr_e2e(ref_root, mods)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)
