@@ -525,8 +525,9 @@ def make_mulliken_trans_charges(ref_root, rng):
 
 
 def make_sk_python(ref_root, rng):
-    """S, H0 and D from DFTBaby's Python Slater-Koster path: SKMatrixElements._H0andS and _DipoleMatrix
-    (SKMatrixElements.py:64-131, 263-318) over SlakoTransformations (SKIntegrals.py:832-1070), whose splines are splrep(s=None) fits of the
+    """S, H0, D and the gradients of S and H0 from DFTBaby's Python Slater-Koster path:
+    SKMatrixElements._H0andS and _DipoleMatrix (SKMatrixElements.py:64-131, 263-318) and
+    ExcGradients._gradients_H0andS (ExcGradients.py:52-141) over SlakoTransformations (SKIntegrals.py:832-1070), whose splines are splrep(s=None) fits of the
     shipped tables (spline_slako_integrals, SKIntegrals.py:793-827) evaluated exactly, with the Python
     angular rules of slako_transformations.py.  Two compact geometries (all pairs inside the 10-bohr
     tables), every pair interacting."""
@@ -561,6 +562,9 @@ def make_sk_python(ref_root, rng):
     ns2 = {"np": np}
     for n in ("count_orbitals", "_H0andS", "_DipoleMatrix"):
         exec(compile(method_source(skm, n), "SKMatrixElements.py", "exec"), ns2)
+    ns3 = {"np": np}
+    exec(compile(method_source(os.path.join(ref_root, "DFTB", "ExcGradients.py"), "_gradients_H0andS"),
+                 "ExcGradients.py", "exec"), ns3)
     par = O.Parametrization([1, 6])
     out = {}
     geoms = []
@@ -579,6 +583,8 @@ def make_sk_python(ref_root, rng):
         out["pos_%d" % k] = np.array([p for _, p in al])
         out["S_%d" % k], out["H0_%d" % k] = S, H0
         out["D_%d" % k] = ns2["_DipoleMatrix"](al, al, par.valorbs, SKT, np.ones((nat, nat), dtype=int))
+        out["gradS_%d" % k], out["gradH0_%d" % k] = ns3["_gradients_H0andS"](al, par.valorbs, SKT,
+                                                                              np.ones((nat, nat), dtype=int))
     np.savez_compressed(os.path.join(HERE, "sk_python.npz"), **out)
 
 

@@ -112,3 +112,32 @@ def test_dipole_matrix_against_reference_python_path(k):
     # the Fortran orientation differs only through the dipole tables' s-p / p-s disagreement
     D_f, _, _, _ = _oracle_dipoles(al, reverse=False)
     assert np.abs((D_f - D_py)[~same]).max() < 1e-7
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_sk_gradients_against_reference_python_path(k):
+    """gradS, gradH0 (3 Nat, Norb, Norb) of the oracle's restatement of slako.gradients_h0ands against
+    DFTBaby's ExcGradients._gradients_H0andS (exact splines, every pair interacting).  gradS agrees to
+    rounding.  For gradH0 the Python path differentiates each element with respect to its first atom in
+    the element's own orientation, the Fortran one in the transposed orientation: the two agree except on
+    the C-C s-p elements, where DFTBaby's s-p and p-s H tables disagree."""
+    from oracle import gradients_oracle as GO
+    al = [(int(z), tuple(q)) for z, q in zip(G["Z_%d" % k], G["pos_%d" % k])]
+    d = O.DFTB2(al, long_range_correction=0)
+    d.setGeometry(al)
+    d._geometry()
+    d.Mproximity[:] = 1
+    L = O.lib()
+    flag = ctypes.c_int.in_dll(L, "oracle_exact_splines")
+    flag.value = 1
+    try:
+        gS, gH = GO.gradients_H0andS(d)
+    finally:
+        flag.value = 0
+    assert np.abs(gS - G["gradS_%d" % k]).max() < 1e-14
+    ind, typ, ls, ms, _ = d._orbital_tables()
+    sp_cc = (typ[:, None] == typ[None, :]) & (typ[:, None] == d.par.atom_type[6]) & (ls[:, None] != ls[None, :]) \
+        & (ind[:, None] != ind[None, :])
+    diff = np.abs(gH - G["gradH0_%d" % k])
+    assert diff[:, ~sp_cc].max() < 1e-14
+    assert 1e-6 < diff[:, sp_cc].max() < 1e-3
