@@ -10,7 +10,7 @@ numbers:
   vectors are divided by (w - omega - d) instead of DFTBaby's (w - omega)
   (Solver.py:530-537, 863-866).
 
-The plain solver stays the judge: a learned start only changes where the search begins and how
+The plain solver still decides the result: a learned start only changes where the search begins and how
 residuals are scaled; the solve still runs to the same residual threshold, and
 ``LR_TDDFTB.getEnergies(..., guess_model=...)`` falls back to the plain start if the learned run
 fails to converge.

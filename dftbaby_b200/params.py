@@ -36,7 +36,7 @@ class Parametrization:
         raw = raw_params()
         unknown = sorted(set(atomtypes) - set(ELEMENT_NAMES))
         if unknown:
-            raise ValueError("no parameters for atomic numbers %s (this build carries H and C)" % unknown)
+            raise ValueError("no parameters for atomic numbers %s (the packaged tables cover H and C)" % unknown)
         h2ev = float(raw["const/hartree_to_eV"])
         self.atomtypes = sorted(set(int(z) for z in atomtypes))
         self.valorbs, self.valorbs_occupation, self.ne_val = {}, {}, {}
