@@ -7,7 +7,7 @@ on the CPU: numpy for the Python parts of the reference (``DFTB2.py``,
 kernels (``slako.f90``, ``splines.f90``, ``tddftb.f90``, ``mulliken.f90``).
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` may use it, and only as the checker or the timed CPU baseline.
+``bench.py`` may use it, and only to verify results or as the timed CPU baseline.
 The product package ``dftbaby_b200`` never imports it.
 
 Parity pinning: the reference cannot be executed here (Python 2 code and f2py
