@@ -493,6 +493,45 @@ class LR_TDDFTB:
         fvec = d.pos.T @ tdm
         self.tdipX, self.tdipY, self.tdipZ = fvec[0], fvec[1], fvec[2]
 
+    def getTransitionDipolesExc(self, Nst):
+        """LR_TDDFTB.getTransitionDipolesExc (LR_TDDFTB.py:593-697): dipole matrix elements <Psi_A|r|Psi_B>
+        in e*bohr (electrons counted positive, as in the reference) between the ground state (A = 0) and
+        the lowest Nst - 1 excited states, as a numpy array (Nst, Nst, 3).
+
+        The ground-state dipole d0 is 2 sum_k <k|r|k> over all occupied orbitals minus the valence nuclear
+        charges times their positions.  Ground-excited elements are the transition dipoles
+        sum_ia C_A,ia <i|r|a>.  Excited-excited elements follow from the CIS-like coefficients:
+        d0 P0 - sum_ij Pij <i|r|j> + sum_ab Pab <a|r|b> with P0 = C_A.C_B,
+        Pij = sum_a C_A,ia C_B,ja, Pab = sum_i C_A,ia C_B,ib."""
+        d = self.dftb2
+        dev = d.device
+        idx = lambda a: torch.as_tensor(np.asarray(a), dtype=torch.long, device=dev)
+
+        def mo_dipoles(rows, cols):  # (len(rows), len(cols), 3) = C_rows^T D C_cols
+            return torch.einsum("mr,cmn,ns->rsc", d.orbs[:, idx(rows)], d.D3, d.orbs[:, idx(cols)])
+
+        occ, virt = np.asarray(self.active_occupied_orbs), np.asarray(self.active_virtual_orbs)
+        occ_all = np.asarray(self.occupied_orbs)
+        if int(round(float(d.Nelec_val))) % 2 != 0:
+            raise ValueError("transition dipoles between excited states need a closed-shell ground state")
+        t_oo, t_ov, t_vv = mo_dipoles(occ, occ), mo_dipoles(occ, virt), mo_dipoles(virt, virt)
+        t_all = mo_dipoles(occ_all, occ_all)
+        d0 = 2.0 * torch.einsum("kkc->c", t_all)  # inactive and active occupied orbitals together
+        Z = torch.as_tensor([float(d.ne_val[Zat]) for Zat, _ in d.atomlist], dtype=torch.float64, device=dev)
+        pos = torch.as_tensor(np.array([p for _, p in d.atomlist], dtype=np.float64), device=dev)
+        d0 = d0 - (Z[:, None] * pos).sum(0)
+        C = self.Cij[:Nst - 1].to(torch.float64)
+        tdip = torch.zeros((Nst, Nst, 3), dtype=torch.float64, device=dev)
+        tdip[0, 0] = d0
+        t0 = torch.einsum("Aia,iac->Ac", C, t_ov)
+        tdip[0, 1:] = t0
+        tdip[1:, 0] = t0
+        P0 = torch.einsum("Aia,Bia->AB", C, C)
+        oo = torch.einsum("Aia,Bja,ijc->ABc", C, C, t_oo)
+        vv = torch.einsum("Aia,Bib,abc->ABc", C, C, t_vv)
+        tdip[1:, 1:] = d0[None, None, :] * P0[:, :, None] - oo + vv
+        return tdip.cpu().numpy()
+
     def getOscillatorStrengths(self):
         """f = 2/3 Omega |t|^2 for singlets, 0 for triplets (LR_TDDFTB.py:698-705)."""
         if self.multiplicity == "S":

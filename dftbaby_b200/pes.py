@@ -111,6 +111,19 @@ class PotentialEnergySurfaces:
         self.last_calculation = (atomlist2, orbs2.clone(), torch.as_tensor(C2a, device=orbs2.device))
         return coupl, olap
 
+    def getTransitionDipoles(self):
+        """PES.getTransitionDipoles (:273-300): dipole matrix elements between all Nst states (Nst, Nst, 3),
+        each element's sign aligned with the previous call's (eigenvectors carry arbitrary phases).
+        Call once after each energy evaluation."""
+        tdip = self.tddftb.getTransitionDipolesExc(self.Nst)
+        old = getattr(self, "tdip_old", None)
+        if old is None:
+            old = tdip
+        flip = np.sum(old * tdip, axis=-1) < 0.0
+        tdip[flip] *= -1.0
+        self.tdip_old = tdip
+        return tdip
+
     def alignCoefficients(self, c):
         """PES.alignCoefficients (:265-272): apply the last phase alignment to excited-state coefficients."""
         if hasattr(self, "P"):

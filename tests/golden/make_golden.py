@@ -672,15 +672,18 @@ def make_scc(ref_root, mods):
 
 
 def make_lr_glue(ref_root, rng):
-    """LR_TDDFTB.setActiveOrbitals, _TransitionDipoles, _TransitionDipolesMulliken, getOscillatorStrengths,
-    determineActiveSpace, TransitionChargesState, saveAbsorptionSpectrum and saveTransitionCharges
-    (LR_TDDFTB.py:167-243, 567-592, 698-705, 807-831, 900-908, 1008-1025) run from DFTBaby's text on a
+    """LR_TDDFTB.setActiveOrbitals, _TransitionDipoles, _TransitionDipolesMulliken, getTransitionDipolesExc,
+    getOscillatorStrengths, determineActiveSpace, TransitionChargesState, saveAbsorptionSpectrum and
+    saveTransitionCharges (LR_TDDFTB.py:167-243, 567-705, 807-831, 900-908, 1008-1025) run from DFTBaby's text on a
     stand-in solved object: 14 orbitals (6 doubly occupied), active window 3 x 4, 3 states."""
     lr = os.path.join(ref_root, "DFTB", "LR_TDDFTB.py")
     names = ("setActiveOrbitals", "_TransitionDipoles", "_TransitionDipolesMulliken", "getOscillatorStrengths",
-             "determineActiveSpace", "TransitionChargesState", "saveAbsorptionSpectrum", "saveTransitionCharges")
+             "determineActiveSpace", "TransitionChargesState", "saveAbsorptionSpectrum", "saveTransitionCharges",
+             "getTransitionDipolesExc")
+    atomic = types.SimpleNamespace(valence_electrons={"h": 1, "c": 4}, atom_names=["h", "he", "li", "be", "b", "c"],
+                                   ebohr_to_debye=2.541746)
     ns = {"np": np, "where": np.where, "argsort": np.argsort, "dot": np.dot, "meshgrid": np.meshgrid,
-          "path": os.path}
+          "path": os.path, "AtomicData": atomic, "la": np.linalg}
     for n in names:
         exec(compile(method_source(lr, n, after=r"class LR_TDDFTB"), "LR_TDDFTB.py", "exec"), ns)
     Ref = type("LR_TDDFTB", (), {n: ns[n] for n in names})
@@ -696,7 +699,7 @@ def make_lr_glue(ref_root, rng):
     atomlist = [(6, tuple(p)) for p in pos]
     dftb2 = types.SimpleNamespace(getOccupation=lambda: f, getKSEnergies=lambda: orbe,
                                   getDipoleMatrix=lambda: D, getKSCoefficients=lambda: orbs,
-                                  getGeometry=lambda: atomlist, verbose=0)
+                                  getGeometry=lambda: atomlist, verbose=0, Nelec_val=12.0)
     r = Ref()
     r.dftb2 = dftb2
     r.setActiveOrbitals(nr_active_occ=3, nr_active_virt=4)
@@ -717,6 +720,7 @@ def make_lr_glue(ref_root, rng):
     out["active_space_1e-5"] = np.array(r.determineActiveSpace())
     out["active_space_1e-2"] = np.array(r.determineActiveSpace(threshold=1e-2))
     out["tq_state_1"] = r.TransitionChargesState(1)
+    out["tdip_exc"] = r.getTransitionDipolesExc(4)
     tmp = tempfile.mkdtemp(prefix="dftbaby_lr_")
     real_string = sys.modules.get("string")
     sys.modules["string"] = types.SimpleNamespace(rjust=lambda text, width: text.rjust(width))

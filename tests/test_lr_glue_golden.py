@@ -15,8 +15,10 @@ G = np.load(os.path.join(os.path.dirname(__file__), "golden", "lr_glue.npz"))
 
 def _solved():
     t = lambda a: torch.tensor(np.asarray(a))
+    atomlist = [(6, tuple(p)) for p in G["pos"]]
     d = types.SimpleNamespace(device=torch.device("cpu"), orbs=t(G["orbs"]), D3=t(np.moveaxis(G["D"], -1, 0)),
-                              pos=t(G["pos"]), getOccupation=lambda: t(G["f"]), getKSEnergies=lambda: t(G["orbe"]))
+                              pos=t(G["pos"]), getOccupation=lambda: t(G["f"]), getKSEnergies=lambda: t(G["orbe"]),
+                              atomlist=atomlist, ne_val={6: 4.0}, Nelec_val=12.0)
     td = LR_TDDFTB.__new__(LR_TDDFTB)
     td.dftb2 = d
     td.setActiveOrbitals(nr_active_occ=3, nr_active_virt=4)
@@ -55,3 +57,12 @@ def test_output_files_against_reference(tmp_path):
     assert (tmp_path / "tq.dat").read_text().splitlines()[:3] == ref_text.splitlines()[:3]
     ref = np.array([[float(x) for x in ln.split()] for ln in ref_text.splitlines()[3:]])
     assert np.abs(got - ref).max() < 1e-14
+
+
+def test_dipoles_between_excited_states_against_reference():
+    """getTransitionDipolesExc (LR_TDDFTB.py:593-697): ground-state dipole (electronic and valence nuclear
+    parts), ground-excited and excited-excited dipole matrix elements."""
+    td = _solved()
+    tdip = td.getTransitionDipolesExc(4)
+    assert tdip.shape == (4, 4, 3)
+    assert np.abs(tdip - G["tdip_exc"]).max() < 1e-12

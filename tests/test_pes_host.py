@@ -78,3 +78,16 @@ def test_resets_and_alignment():
     assert np.array_equal(p.alignCoefficients(c), c)
     p.P = np.diag([1.0, -1.0, 1.0])
     assert np.array_equal(p.alignCoefficients(c), [-1.0, 2.0])
+
+
+def test_transition_dipole_signs_follow_the_previous_call():
+    p = _pes(Nst=3)
+    rng = np.random.default_rng(0)
+    t1 = rng.standard_normal((3, 3, 3))
+    t2 = t1 * np.array([1.0, -1.0, 1.0])[:, None, None] * np.array([1.0, 1.0, -1.0])[None, :, None]
+    seq = iter([t1.copy(), t2.copy()])
+    p.tddftb.getTransitionDipolesExc = lambda Nst: next(seq)
+    first = p.getTransitionDipoles()
+    assert np.array_equal(first, t1)
+    second = p.getTransitionDipoles()  # sign flips of whole elements are undone
+    assert np.allclose(second, t1)
