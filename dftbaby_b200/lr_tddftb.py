@@ -229,6 +229,35 @@ class LR_TDDFTB:
         self.nocc = len(self.active_occupied_orbs)
         self.nvirt = len(self.active_virtual_orbs)
 
+    def setActiveLMOrbitals(self, nr_active_occ=1000, nr_active_virt=1000, select_lm=((1, 0),)):
+        """LR_TDDFTB.setActiveLMOrbitals (LR_TDDFTB.py:125-166): only molecular orbitals with weight on atomic
+        orbitals whose (l, m) is in select_lm (sum of squared coefficients above 1e-15) form the occupied,
+        virtual and active sets, e.g. select_lm=[(1, 0)] keeps the p_z orbitals of a planar pi system;
+        within them the window is chosen as in setActiveOrbitals.  select_lm may be given as the
+        reference's command-line string, e.g. "[(1,0)]"."""
+        import ast
+        if isinstance(select_lm, str):
+            select_lm = ast.literal_eval(select_lm)
+        selected = {tuple(lm) for lm in select_lm}
+        d = self.dftb2
+        lm_idx = []
+        iao = 0
+        for Z, _ in d.atomlist:
+            for (n, l, m) in d.valorbs[Z]:
+                if (l, m) in selected:
+                    lm_idx.append(iao)
+                iao += 1
+        orbs = d.orbs.detach().cpu().numpy()
+        is_lm = np.sum(np.abs(orbs[np.array(lm_idx, dtype=int), :]) ** 2, axis=0) > 1.0e-15
+        f = d.getOccupation().cpu().numpy()
+        orbe = d.getKSEnergies().cpu().numpy()
+        self.occupied_orbs = np.where((f > 0.1) & is_lm)[0]
+        self.virtual_orbs = np.where((f <= 0.1) & is_lm)[0]
+        self.active_occupied_orbs = self.occupied_orbs[np.argsort(orbe[self.occupied_orbs])[::-1][:nr_active_occ][::-1]]
+        self.active_virtual_orbs = self.virtual_orbs[np.argsort(orbe[self.virtual_orbs])[:nr_active_virt]]
+        self.nocc = len(self.active_occupied_orbs)
+        self.nvirt = len(self.active_virtual_orbs)
+
     def getActiveOrbitals(self):
         return self.active_occupied_orbs, self.active_virtual_orbs
 
@@ -302,8 +331,6 @@ class LR_TDDFTB:
         preconditioner when no warm start is available; the solve runs to the
         same residual threshold, and the plain start is used if it fails.
         """
-        if select_lm is not None:
-            raise ValueError("select_lm is not implemented")
         if response_method != "Casida":
             raise ValueError("only response_method='Casida' is implemented")
         if ct_correction or stability:
@@ -314,7 +341,10 @@ class LR_TDDFTB:
         self.en0 = d.getEnergy(**scf_opts)
         ev[1].record()
         self._phase_events = ev
-        self.setActiveOrbitals(nr_active_occ, nr_active_virt)
+        if select_lm is not None:
+            self.setActiveLMOrbitals(nr_active_occ, nr_active_virt, select_lm=select_lm)
+        else:
+            self.setActiveOrbitals(nr_active_occ, nr_active_virt)
         self.setMultiplicity(multiplicity)
         self.nstates = nstates
         if nstates is not None:

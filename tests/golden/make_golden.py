@@ -672,7 +672,7 @@ def make_scc(ref_root, mods):
 
 
 def make_lr_glue(ref_root, rng):
-    """LR_TDDFTB.setActiveOrbitals, _TransitionDipoles, _TransitionDipolesMulliken, getTransitionDipolesExc,
+    """LR_TDDFTB.setActiveOrbitals, setActiveLMOrbitals, _TransitionDipoles, _TransitionDipolesMulliken, getTransitionDipolesExc,
     getOscillatorStrengths, determineActiveSpace, TransitionChargesState, saveAbsorptionSpectrum and
     saveTransitionCharges (LR_TDDFTB.py:167-243, 567-705, 807-831, 900-908, 1008-1025) run from DFTBaby's text on a
     stand-in solved object: 14 orbitals (6 doubly occupied), active window 3 x 4, 3 states."""
@@ -720,6 +720,35 @@ def make_lr_glue(ref_root, rng):
     out["active_space_1e-5"] = np.array(r.determineActiveSpace())
     out["active_space_1e-2"] = np.array(r.determineActiveSpace(threshold=1e-2))
     out["tq_state_1"] = r.TransitionChargesState(1)
+    # setActiveLMOrbitals on a planar-like C3H2 layout: the MO coefficients split into blocks over the p_z, the
+    # s and the in-plane p atomic orbitals, so a selection of (l, m) keeps exactly the MOs of its blocks
+    exec(compile(method_source(lr, "setActiveLMOrbitals", after=r"class LR_TDDFTB"), "LR_TDDFTB.py", "exec"), ns)
+    sys.path.insert(0, REPO)
+    from oracle import dftb_oracle as O
+    valorbs = O.Parametrization([1, 6]).valorbs
+    lm_atoms = [(6, (0.0, 0.0, 0.0)), (6, (2.6, 0.0, 0.0)), (6, (1.3, 2.2, 0.0)), (1, (-1.9, -0.5, 0.0)),
+                (1, (4.5, -0.5, 0.0))]
+    lms = [(l, m) for Z, _ in lm_atoms for (_, l, m) in valorbs[Z]]
+    assert len(lms) == norb
+    orbs_lm = np.zeros((norb, norb))
+    cols = rng.permutation(norb)
+    c0 = 0
+    for block in ([(1, 0)], [(0, 0)], [(1, -1), (1, 1)]):
+        rows = [k for k, lm in enumerate(lms) if lm in block]
+        orbs_lm[np.ix_(rows, cols[c0:c0 + len(rows)])] = np.linalg.qr(rng.standard_normal((len(rows), len(rows))))[0]
+        c0 += len(rows)
+    assert c0 == norb
+    lm_d = types.SimpleNamespace(getGeometry=lambda: lm_atoms, getValorbs=lambda: valorbs,
+                                 getKSCoefficients=lambda: orbs_lm, getOccupation=lambda: f, getKSEnergies=lambda: orbe)
+    import contextlib
+    out.update(lm_orbs=orbs_lm, lm_Z=np.array([Z for Z, _ in lm_atoms]), lm_pos=np.array([p for _, p in lm_atoms]))
+    for tag, sel in (("pz", [(1, 0)]), ("s_pz", [(0, 0), (1, 0)])):
+        lm_r = types.SimpleNamespace(dftb2=lm_d)
+        with contextlib.redirect_stdout(io.StringIO()):
+            ns["setActiveLMOrbitals"](lm_r, nr_active_occ=2, nr_active_virt=3, select_lm=sel)
+        out.update({"lm_%s_occupied" % tag: lm_r.occupied_orbs, "lm_%s_virtual" % tag: lm_r.virtual_orbs,
+                    "lm_%s_active_occ" % tag: lm_r.active_occupied_orbs,
+                    "lm_%s_active_virt" % tag: lm_r.active_virtual_orbs})
     out["tdip_exc"] = r.getTransitionDipolesExc(4)
     tmp = tempfile.mkdtemp(prefix="dftbaby_lr_")
     real_string = sys.modules.get("string")

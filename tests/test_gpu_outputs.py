@@ -30,3 +30,32 @@ def test_outputs_after_solve(tmp_path):
     assert np.allclose(-tq[:, 2], td.TransitionChargesState(2))
     # transition charges of a singlet excitation sum to zero
     assert np.abs(tq.sum(axis=0)).max() < 1e-8
+
+
+def test_select_lm_active_space():
+    """select_lm (LR_TDDFTB.py:125-166): every (l, m) present reproduces the energy-window solve, and p_z
+    alone on a planar polyene keeps exactly its pi orbitals (the Slater-Koster blocks between p_z and
+    in-plane orbitals vanish in the molecular plane)."""
+    native.load()
+    from dftbaby_b200.lr_tddftb import LR_TDDFTB
+    al = geometry.polyene(8)
+    assert all(p[2] == 0.0 for _, p in al)
+    td = LR_TDDFTB(al, long_range_correction=1)
+    td.setGeometry(al)
+    Om, f = td.getEnergies(nstates=4, diag_conv=1e-8)
+    td_all = LR_TDDFTB(al, long_range_correction=1)
+    td_all.setGeometry(al)
+    Om_all, f_all = td_all.getEnergies(nstates=4, diag_conv=1e-8, select_lm=[(0, 0), (1, -1), (1, 0), (1, 1)])
+    assert np.array_equal(td_all.active_occupied_orbs, td.active_occupied_orbs)
+    assert np.array_equal(td_all.active_virtual_orbs, td.active_virtual_orbs)
+    assert np.abs(Om_all - Om).max() < 1e-9 and np.abs(f_all - f).max() < 1e-8
+    td_pi = LR_TDDFTB(al, long_range_correction=1)
+    td_pi.setGeometry(al)
+    Om_pi, f_pi = td_pi.getEnergies(nstates=4, diag_conv=1e-8, select_lm="[(1,0)]")
+    assert (td_pi.nocc, td_pi.nvirt) == (4, 4)
+    orbs = td_pi.dftb2.orbs.cpu().numpy()
+    pz = np.array([(l, m) == (1, 0) for Z, _ in al for (_, l, m) in td_pi.dftb2.valorbs[Z]])
+    w = np.sum(orbs[pz] ** 2, axis=0)
+    sel = np.r_[td_pi.active_occupied_orbs, td_pi.active_virtual_orbs]
+    assert np.all(w[sel] > 1e-3) and np.all(np.delete(w, sel) < 1e-15)
+    assert np.all(np.isfinite(Om_pi)) and np.all(Om_pi > 0) and np.all(np.isfinite(f_pi))

@@ -1,4 +1,4 @@
-"""LR_TDDFTB's active-space selection, transition dipoles (matrix-element and Mulliken forms),
+"""LR_TDDFTB's active-space selection (by energy window and by (l, m) of the atomic orbitals), transition dipoles (matrix-element and Mulliken forms),
 oscillator strengths, active-space suggestion, per-state transition charges and output files, run on
 CPU tensors against DFTBaby's own methods (tests/golden/lr_glue.npz, made by
 tests/golden/make_golden.py on the same stand-in solved object)."""
@@ -33,6 +33,22 @@ def test_active_orbitals_against_reference():
         assert np.array_equal(getattr(td, key), G[key])
     assert tuple(td.determineActiveSpace()) == tuple(G["active_space_1e-5"])
     assert tuple(td.determineActiveSpace(threshold=1e-2)) == tuple(G["active_space_1e-2"])
+
+
+def test_lm_active_orbitals_against_reference():
+    from oracle import dftb_oracle as O
+    t = lambda a: torch.tensor(np.asarray(a))
+    d = types.SimpleNamespace(atomlist=[(int(Z), tuple(p)) for Z, p in zip(G["lm_Z"], G["lm_pos"])],
+                              valorbs=O.Parametrization([1, 6]).valorbs, orbs=t(G["lm_orbs"]),
+                              getOccupation=lambda: t(G["f"]), getKSEnergies=lambda: t(G["orbe"]))
+    for tag, sel in (("pz", [(1, 0)]), ("s_pz", "[(0,0), (1,0)]")):
+        td = LR_TDDFTB.__new__(LR_TDDFTB)
+        td.dftb2 = d
+        td.setActiveLMOrbitals(nr_active_occ=2, nr_active_virt=3, select_lm=sel)
+        for key, ref in (("occupied_orbs", "occupied"), ("virtual_orbs", "virtual"),
+                         ("active_occupied_orbs", "active_occ"), ("active_virtual_orbs", "active_virt")):
+            assert np.array_equal(getattr(td, key), G["lm_%s_%s" % (tag, ref)])
+        assert (td.nocc, td.nvirt) == (len(G["lm_%s_active_occ" % tag]), len(G["lm_%s_active_virt" % tag]))
 
 
 def test_transition_dipoles_and_oscillator_strengths_against_reference():
