@@ -122,18 +122,32 @@ class Gradients:
         self.I = None
 
     # ------------------------------------------------------------ helpers
-    def _full_space(self):
-        """Orbitals, orbital energies, X-Y / X+Y and transition charges over all occupied and
-        virtual orbitals; an active space is zero-padded as ExcGradients.py:236-260 does."""
+    def _orbital_space(self):
+        """(occupied, virtual) orbital indices the gradient runs over and whether they are the solver's
+        own active space (ExcGradients.py:220-260): the active space when it spans every orbital the solver
+        chose from (LR_TDDFTB.hasActiveSpace() false, LR_TDDFTB.py:244-253; after a select_lm solve these
+        are the selected orbitals), otherwise all orbitals by occupation, which is what the reference
+        resets to with setActiveOrbitals(None, None).  Before any excited-state solve it is all orbitals
+        by occupation."""
         td, d = self.tddftb, self.dftb
-        occ = np.asarray(td.occupied_orbs)
-        virt = np.asarray(td.virtual_orbs)
+        if getattr(td, "active_occupied_orbs", None) is not None:
+            ao, av = np.asarray(td.active_occupied_orbs), np.asarray(td.active_virtual_orbs)
+            if len(ao) == len(td.occupied_orbs) and len(av) == len(td.virtual_orbs):
+                return ao, av, True
+        f = d.getOccupation()
+        f = f.cpu().numpy() if torch.is_tensor(f) else np.asarray(f)
+        return np.where(f > 0.1)[0], np.where(f <= 0.1)[0], False
+
+    def _full_space(self):
+        """Orbitals, orbital energies, X-Y / X+Y and transition charges over the orbital space of
+        _orbital_space; a smaller active space is zero-padded as ExcGradients.py:236-260 does."""
+        td, d = self.tddftb, self.dftb
+        occ, virt, own = self._orbital_space()
         dev = d.device
         XmY, XpY = td.XmY, td.XpY
-        full = len(td.active_occupied_orbs) == len(occ) and len(td.active_virtual_orbs) == len(virt)
-        if full:
+        if own:
             qoo, qvv, qov = td.getTransitionCharges()
-            occ_a, virt_a = np.asarray(td.active_occupied_orbs), np.asarray(td.active_virtual_orbs)
+            occ_a, virt_a = occ, virt
         else:
             Co = d.orbs[:, torch.as_tensor(occ, device=dev)].contiguous()
             Cv = d.orbs[:, torch.as_tensor(virt, device=dev)].contiguous()
@@ -195,10 +209,16 @@ class Gradients:
         state, I = n the n-th excited state (ExcGradients.py:234-284)."""
         d, td = self.dftb, self.tddftb
         lc = d.long_range_correction == 1
-        if getattr(td, "multiplicity", "S") != "S":
-            raise ValueError("gradients are implemented for singlet states")
         dev = d.device
-        orbe_occ, orbe_virt, Co, Cv, qoo, qvv, qov, XmY_all, XpY_all = self._full_space()
+        if I == 0:
+            # the ground state needs the occupied orbitals only: no X+-Y, so it also runs after a failed
+            # or skipped excited-state solve
+            oi = torch.as_tensor(self._orbital_space()[0], device=dev)
+            orbe_occ, Co = d.orbe[oi], d.orbs[:, oi].contiguous()
+        else:
+            if getattr(td, "multiplicity", "S") != "S":
+                raise ValueError("gradients are implemented for singlet states")
+            orbe_occ, orbe_virt, Co, Cv, qoo, qvv, qov, XmY_all, XpY_all = self._full_space()
         S = d.S
         nat = len(d.atomlist)
         ind = d._ind.long()

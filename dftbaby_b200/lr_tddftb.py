@@ -600,6 +600,56 @@ class LR_TDDFTB:
         """LR_TDDFTB.TransitionChargesState (LR_TDDFTB.py:900-908): q_A = sum_ia C_I,ia q_A^ia (numpy, Nat)."""
         return torch.einsum("ia,Aia->A", self.Cij[I], self.qtrans_ov).cpu().numpy()
 
+    def _particle_hole(self, Cs):
+        """Particle and hole charges of the excitation amplitudes Cs (nocc, nvirt), real or complex:
+        p_A = sum_o Cs[o,:]^H q_vv^A Cs[o,:] and h_A = -sum_v Cs[:,v]^H q_oo^A Cs[:,v] (real parts).  With the
+        Mulliken charges q^A_pq = 1/2 sum_{mu in A} (C_mu,p (SC)_mu,q + C_mu,q (SC)_mu,p) each is a sum over
+        the atomic orbitals of A of Re(conj(U) * (S U)), U = C_v Cs^T for particles and C_o Cs for holes, so
+        the (Nat, nvirt, nvirt) and (Nat, nocc, nocc) charge tensors are never formed."""
+        d = self.dftb2
+        Co, Cv = self._active_coefficients()
+        Cs = torch.as_tensor(Cs, device=Co.device)
+        S = d.S
+        if Cs.is_complex():
+            Co, Cv, S = Co.to(Cs.dtype), Cv.to(Cs.dtype), S.to(Cs.dtype)
+        U = Cv @ Cs.T
+        W = Co @ Cs
+        pu = (U.conj() * (S @ U)).real.sum(dim=1)
+        hw = (W.conj() * (S @ W)).real.sum(dim=1)
+        nat = len(d.atomlist)
+        ind = d._ind.long()
+        particle = torch.zeros(nat, dtype=torch.float64, device=Co.device).index_add_(0, ind, pu)
+        hole = -torch.zeros(nat, dtype=torch.float64, device=Co.device).index_add_(0, ind, hw)
+        return particle.cpu().numpy(), hole.cpu().numpy()
+
+    def ParticleHoleCharges(self, I):
+        """LR_TDDFTB.ParticleHoleCharges (LR_TDDFTB.py:910-947): the density difference between excited state
+        I (0-based) and the ground state as particle and hole charges on the atoms (numpy, Nat each)."""
+        return self._particle_hole(self.Cij[I])
+
+    def ParticleHoleChargesSuperposition(self, coeffs):
+        """LR_TDDFTB.ParticleHoleChargesSuperposition (LR_TDDFTB.py:948-1006): particle and hole charges of the
+        superposition sum_I coeffs[I] |I> of the excited states (coeffs may be complex)."""
+        n = len(self.Omega)
+        c = torch.as_tensor(np.asarray(coeffs)[:n], dtype=torch.complex128, device=self.Cij.device)
+        Csuper = torch.einsum("I,Iia->ia", c, self.Cij[:n].to(torch.complex128))
+        return self._particle_hole(Csuper)
+
+    def analyseParticleHole(self, particle_hole_states=(), particle_hole_dir=None):
+        """LR_TDDFTB.analyseParticleHole (LR_TDDFTB.py:997-1007): for each excited state I (1-based) in
+        particle_hole_states, columns (particle, hole) per atom go to particle_hole_dir/particle_hole_charges_I.chrg.
+        particle_hole_states may be given as the reference's option string, e.g. "[1, 3]"."""
+        import ast
+        import os
+        if isinstance(particle_hole_states, str):
+            particle_hole_states = ast.literal_eval(particle_hole_states)
+        for I in particle_hole_states:
+            particle, hole = self.ParticleHoleCharges(I - 1)
+            if particle_hole_dir is not None:
+                ph_file = os.path.join(os.path.expanduser(os.path.expandvars(particle_hole_dir)),
+                                       "particle_hole_charges_%d.chrg" % I)
+                np.savetxt(ph_file, np.vstack((particle, hole)).T)
+
     def saveAbsorptionSpectrum(self, spectrum_file="absorption_spectrum.dat"):
         """LR_TDDFTB.saveAbsorptionSpectrum (LR_TDDFTB.py:807-831): excitation energies (Hartree) and
         oscillator strengths.  States are not classified by symmetry here, so there is one file."""

@@ -3,9 +3,7 @@ solver: what external drivers (geometry optimisers, surface hopping) call.
 
 Options go in as keyword arguments (DFTB2, runSCC and getEnergies options alike) instead of being
 parsed from the command line; coordinates are flat numpy vectors in bohr, x[3i:3i+3] for atom i.
-Not built: the solvent cavity and QM/MM terms (off by default in the reference), and the
-ground-state-only gradient after a skipped excited-state solve (``getEnergyAndGradient_S0``): the
-gradient code reads the excited-state solver's active space.
+Not built: the solvent cavity and QM/MM terms (off by default in the reference).
 """
 import inspect
 
@@ -74,6 +72,18 @@ class PotentialEnergySurfaces:
         self.tddftb.getEnergies(**self.options)
         gradVrep, gradE0, gradExc = self.grads.gradient(I=gradient_state)
         return self._energies(), gradVrep + gradE0 + gradExc
+
+    def getEnergyAndGradient_S0(self, x, has_scf=False):
+        """PES.getEnergyAndGradient_S0 (:133-170): (E0, ground-state gradient) without an excited-state solve.
+        has_scf=True, right after a failed excited-state calculation, reuses its converged SCC instead of
+        running one at x."""
+        if has_scf:
+            E0 = float(self.tddftb.dftb2.E_tot)
+        else:
+            self._set(x)
+            E0 = float(self.tddftb.dftb2.getEnergy(**self.scf_options))
+        gradVrep, gradE0, gradExc = self.grads.gradient(I=0, save_intermediates_CPKS=1)
+        return E0, gradVrep + gradE0 + gradExc
 
     def resetXY(self):
         """PES.resetXY (:169-173): start the next excited-state solve without a guess."""

@@ -32,7 +32,7 @@ rotation) on stand-in objects, through the same shim.
 
 Usage::
 
-    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda|repulsive|lr_e2e]
+    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda|repulsive|lr_e2e|particle_hole|handler]
 """
 import io
 import os
@@ -53,7 +53,10 @@ def py2to3(src):
     """Mechanical conversion of print statements and renamed dict/range methods."""
     src = src.replace(".iteritems()", ".items()").replace("xrange(", "range(")
     src = re.sub(r"\.has_key\(", ".__contains__(", src)
-    # one-line "print>>fh, a, b" statements -> print(a, b, file=fh)
+    src = src.replace(".translate(None, digits)", ".translate(str.maketrans('', '', digits))")
+    # one-line "print>>fh, a, b" statements -> print(a, b, file=fh); a trailing comma keeps the line open
+    # (end=" " writes the space Python 2's softspace would write before the next item on that line)
+    src = re.sub(r"^(\s*)print\s*>>\s*([^,\n]+),\s*(.*?),\s*$", r'\1print(\3, end=" ", file=\2)', src, flags=re.M)
     src = re.sub(r"^(\s*)print\s*>>\s*([^,\n]+),\s*(.*)$", r"\1print(\3, file=\2)", src, flags=re.M)
     toks = list(tokenize.generate_tokens(io.StringIO(src).readline))
     edits = []
@@ -797,6 +800,162 @@ def make_lambda(ref_root, rng):
                         Oia=td.Oia, Lambda2=Lambda2)
 
 
+def _reference_atomic_data(ref_root):
+    """DFTB/AtomicData.py executed through the shim (names, masses, conversion factors)."""
+    ns = {}
+    exec(compile(py2to3(open(os.path.join(ref_root, "DFTB", "AtomicData.py")).read()), "AtomicData.py", "exec"), ns)
+    return types.SimpleNamespace(**{k: v for k, v in ns.items() if not k.startswith("__")})
+
+
+def make_particle_hole(ref_root, rng):
+    """LR_TDDFTB.ParticleHoleCharges, ParticleHoleChargesSuperposition and analyseParticleHole
+    (LR_TDDFTB.py:910-1007) run from DFTBaby's text on the C4H6 layout of make_mulliken_trans_charges,
+    with the Mulliken transition charges q_oo, q_vv made by DFTBaby's own Python loop
+    (LR_TDDFTB.py:267-296) from the stored S and orbitals."""
+    import string
+    import textwrap
+    Zs = [6, 6, 6, 6, 1, 1, 1, 1, 1, 1]
+    valorbs = {1: [(1, 0, 0)], 6: [(2, 0, 0), (2, 1, -1), (2, 1, 0), (2, 1, 1)]}
+    pos = rng.standard_normal((len(Zs), 3)) * 2.0
+    atomlist = [(Z, tuple(p)) for Z, p in zip(Zs, pos)]
+    norb = sum(len(valorbs[Z]) for Z in Zs)
+    X = rng.standard_normal((norb, norb))
+    S = np.eye(norb) + 0.05 * (X + X.T)
+    orbs = np.linalg.qr(rng.standard_normal((norb, norb)))[0]
+    occ, virt = np.array([2, 4, 5, 7, 8]), np.array([11, 12, 15, 19])
+    lines = open(os.path.join(ref_root, "DFTB", "LR_TDDFTB.py")).read().expandtabs(8).splitlines(keepends=True)
+    start = next(i for i, ln in enumerate(lines) if ln.strip() == "# PYTHON CODE")
+    end = next(i for i in range(start + 1, len(lines)) if lines[i].strip() == '"""')
+    block = py2to3(textwrap.dedent("".join(lines[start:end])))
+    nst = 3
+    C = rng.standard_normal((nst, len(occ), len(virt)))
+    C /= np.sqrt((C * C).sum(axis=(1, 2)))[:, None, None]
+    coeffs = rng.standard_normal(nst) + 1j * rng.standard_normal(nst)
+    r = types.SimpleNamespace(active_occupied_orbs=occ, active_virtual_orbs=virt, Cij=C, Omega=np.array([0.1, 0.2, 0.3]),
+                              dftb2=types.SimpleNamespace(getGeometry=lambda: atomlist, verbose=0))
+    ns = {"zeros": np.zeros, "dot": np.dot, "self": r, "atomlist": atomlist, "valorbs": valorbs, "orbs": orbs,
+          "S": S}
+    exec(compile(block, "LR_TDDFTB.py:_MullikenTransitionCharges", "exec"), ns)
+    ns = {"np": np, "la": np.linalg, "string": string, "path": os.path, "atom_names": ["h", "he", "li", "be", "b", "c"]}
+    for n in ("ParticleHoleCharges", "ParticleHoleChargesSuperposition", "analyseParticleHole"):
+        exec(compile(method_source(os.path.join(ref_root, "DFTB", "LR_TDDFTB.py"), n, after=r"class LR_TDDFTB"),
+                     "LR_TDDFTB.py", "exec"), ns)
+    r.ParticleHoleCharges = lambda I: ns["ParticleHoleCharges"](r, I)
+    ph = [ns["ParticleHoleCharges"](r, I) for I in range(nst)]
+    sup_p, sup_h = ns["ParticleHoleChargesSuperposition"](r, coeffs)
+    tmp = tempfile.mkdtemp(prefix="dftbaby_ph_")
+    ns["analyseParticleHole"](r, particle_hole_states=[1, 3], particle_hole_dir=tmp)
+    chrg = [open(os.path.join(tmp, "particle_hole_charges_%d.chrg" % I)).read() for I in (1, 3)]
+    shutil.rmtree(tmp, ignore_errors=True)
+    np.savez_compressed(os.path.join(HERE, "particle_hole.npz"), Z=np.array(Zs), pos=pos, S=S, orbs=orbs, occ=occ,
+                        virt=virt, C=C, coeffs=coeffs, ph_p=np.array([p for p, _ in ph]),
+                        ph_h=np.array([h for _, h in ph]), sup_p=sup_p, sup_h=sup_h, chrg_1=np.array(chrg[0]),
+                        chrg_3=np.array(chrg[1]))
+
+
+def handler_data(rng, nst=4, Zs=(6, 6, 1, 1, 1)):
+    """The arrays the scripted PES of tests/golden/fake_pes.py returns."""
+    nat = len(Zs)
+    A = rng.standard_normal((nst, nst))
+    P = np.diag(rng.choice([-1.0, 1.0], nst))
+    ph_p = rng.random((nst - 1, nat))
+    return dict(Z=np.array(Zs), pos=rng.standard_normal((nat, 3)),
+                E=np.sort(rng.standard_normal((3, nst)), axis=1) - 40.0,
+                grad=rng.standard_normal((3, nst, 3 * nat)), E0=rng.standard_normal(2) - 40.0,
+                grad0=rng.standard_normal((2, 3 * nat)), coupl=A - A.T, olap=np.eye(nst) + 0.05 * A,
+                tdip=rng.standard_normal((nst, nst, 3)), P=P, ph_p=ph_p, ph_h=-ph_p[:, ::-1],
+                lambda2=rng.random(nst - 1), tq=rng.standard_normal((nst - 1, nat)))
+
+
+def make_handler(ref_root, rng):
+    """dftbaby_handler.getBrightestState, getAll_S0, getAll, writeTimeSeries, getAvgParticleHoleCharges and
+    getParticleHoleChargesSuperposition (Dynamics/dftbaby_handler.py:30-319) run from DFTBaby's text on the
+    scripted PES of tests/golden/fake_pes.py: returned arrays, PES call sequences, printed text, time-series
+    files, and which failures propagate."""
+    import contextlib
+    sys.path.insert(0, HERE)
+    from fake_pes import FakePES
+    src = os.path.join(ref_root, "DFTB", "Dynamics", "dftbaby_handler.py")
+    names = ("getBrightestState", "getAll_S0", "getAll", "writeTimeSeries", "getAvgParticleHoleCharges",
+             "getParticleHoleChargesSuperposition")
+    errors = {n: type(n, (Exception,), {}) for n in ("SCFNotConverged", "SCFChargeInconsistency",
+                                                      "ExcitedStatesNotConverged", "ExcitedStatesError")}
+    atomic = _reference_atomic_data(ref_root)
+    xyz = types.SimpleNamespace(atomlist2vector=lambda al: np.hstack([np.asarray(p, dtype=float) for _, p in al]))
+    ns = dict(np=np, os=os, XYZ=xyz, AtomicData=atomic, **errors)
+    for n in names:
+        exec(compile(method_source(src, n, after=r"class dftbaby_handler"), "dftbaby_handler.py", "exec"), ns)
+    Ref = type("dftbaby_handler", (), {n: ns[n] for n in names})
+    data = handler_data(rng)
+    nst, nat = data["E"].shape[1], len(data["Z"])
+    atomlist = [(int(Z), tuple(p)) for Z, p in zip(data["Z"], data["pos"])]
+    masses = np.array(atomic.atomlist2masses(atomlist))
+    coords = [data["pos"] + 0.01 * k for k in range(4)]
+
+    def handler(pes):
+        h = Ref()
+        h.dt_nuc, h.nstates, h.sc_threshold, h.Nat, h.masses, h.pes, h.last_step = 20.0, nst, 0.002, nat, masses, pes, None
+        return h
+
+    out = dict(masses=masses, dt_nuc=20.0, sc_threshold=0.002, **{"data_" + k: v for k, v in data.items()})
+    # A: a good step, an excited-state failure (ground-state fallback), an excited-state failure whose
+    # ground-state fallback fails too (last step reused), a good step
+    pes = FakePES(data, errors, fail_exc={1: "ExcitedStatesNotConverged", 2: "ExcitedStatesError"},
+                  fail_s0={1: "SCFNotConverged"})
+    h = handler(pes)
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        out["brightest"] = h.getBrightestState(coords[0])
+        for k, st in enumerate((2, 2, 2, 1)):
+            res = h.getAll(coords[k], st)
+            for name, a in zip(("energies", "accel", "coupl", "tdip", "olap"), res):
+                out["A%d_%s" % (k, name)] = np.asarray(a)
+        fish = types.SimpleNamespace(c=np.array([0.1 + 0.2j, 0.5 - 0.1j, 0.3j, 0.7]), time=413.4, fs_to_au=41.341,
+                                     au_to_ang=0.529177, state=2)
+        series = ["particle-hole charges", "particle-hole charges current", "Lambda2 current", "Lambda2",
+                  "transition charges current"]
+        tmp = tempfile.mkdtemp(prefix="dftbaby_ts_")
+        cwd = os.getcwd()
+        os.chdir(tmp)
+        try:
+            h.writeTimeSeries(fish, series)
+            fish.state, fish.time = 0, 434.1
+            h.writeTimeSeries(fish, series)
+            for fn in sorted(os.listdir(tmp)):
+                out["file_" + fn] = np.array(open(fn).read())
+        finally:
+            os.chdir(cwd)
+            shutil.rmtree(tmp, ignore_errors=True)
+        out["avg_p"], out["avg_h"] = h.getAvgParticleHoleCharges(fish.c)
+        out["fish_c"] = fish.c
+    out["A_stdout"] = np.array(buf.getvalue())
+    out["A_log"] = np.array(pes.log)
+    # B: a failed first step on an excited state propagates; C: on the ground state it falls back;
+    # D: getAll_S0 without a previous step propagates the SCF failure; E: a charge inconsistency is not caught
+    scen = {"B": (dict(fail_exc={0: "ExcitedStatesError"}), [(0, 2)]),
+            "C": (dict(fail_exc={0: "SCFNotConverged"}), [(0, 0)]),
+            "D": (dict(fail_s0={0: "SCFNotConverged"}), None),
+            "E": (dict(fail_exc={1: "SCFChargeInconsistency"}), [(0, 1), (1, 1)])}
+    for tag, (script, steps) in scen.items():
+        pes = FakePES(data, errors, **script)
+        h = handler(pes)
+        raised = ""
+        with contextlib.redirect_stdout(io.StringIO()):
+            try:
+                if steps is None:
+                    h.getAll_S0(coords[0])
+                else:
+                    for k, st in steps:
+                        res = h.getAll(coords[k], st)
+                        for name, a in zip(("energies", "accel", "coupl", "tdip", "olap"), res):
+                            out["%s%d_%s" % (tag, k, name)] = np.asarray(a)
+            except Exception as e:  # the class name is what the test compares
+                raised = type(e).__name__
+        out[tag + "_raised"] = np.array(raised)
+        out[tag + "_log"] = np.array(pes.log)
+    np.savez_compressed(os.path.join(HERE, "handler.npz"), **out)
+
+
 def make_repulsive(ref_root, rng):
     """RepulsivePotential.__init__ / getVrep (RepulsivePotential.py:17-100, as DFTB2.py:327 builds them: no
     smooth tail) on the shipped H-H, H-C and C-C tables, run from DFTBaby's text: values and first
@@ -920,6 +1079,10 @@ def main(ref_root, only=None):
             make_repulsive(ref_root, np.random.default_rng(20261209))
         if only in (None, "lr_e2e"):
             make_lr_e2e(ref_root, mods)
+        if only in (None, "particle_hole"):
+            make_particle_hole(ref_root, np.random.default_rng(20261210))
+        if only in (None, "handler"):
+            make_handler(ref_root, np.random.default_rng(20261211))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)

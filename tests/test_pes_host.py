@@ -1,4 +1,4 @@
-"""The PES interface's host logic (PES.py:17-131, 169-179, 265-272) with stand-in solver objects."""
+"""The PES interface's host logic (PES.py:17-179, 265-272) with stand-in solver objects."""
 import numpy as np
 import torch
 
@@ -13,6 +13,10 @@ class _FakeDFTB2:
 
     def density_matrix_ref(self):
         return torch.eye(4)
+
+    def getEnergy(self, **opts):
+        self.scf_calls = getattr(self, "scf_calls", 0) + 1
+        return -13.0
 
 
 class _FakeTD:
@@ -33,7 +37,8 @@ class _FakeTD:
 
 
 class _FakeGrads:
-    def gradient(self, I=0):
+    def gradient(self, I=0, save_intermediates_CPKS=0):
+        self.last_I = I
         n = 6
         return np.full(n, 1.0 * I), np.full(n, 0.5), np.arange(n, dtype=float)
 
@@ -91,3 +96,15 @@ def test_transition_dipole_signs_follow_the_previous_call():
     assert np.array_equal(first, t1)
     second = p.getTransitionDipoles()  # sign flips of whole elements are undone
     assert np.allclose(second, t1)
+
+
+def test_ground_state_energy_and_gradient():
+    p = _pes()
+    x = np.array([0.0, 0.0, 0.1, 0.0, 0.0, 2.1])
+    E0, g = p.getEnergyAndGradient_S0(x, has_scf=True)  # reuses the last SCC: no geometry update, no SCC
+    assert E0 == -12.5 and not p.tddftb.dftb2.geometries and p.grads.last_I == 0
+    assert np.allclose(g, 0.5 + np.arange(6))
+    E0, g = p.getEnergyAndGradient_S0(x)
+    assert E0 == -13.0 and p.tddftb.dftb2.scf_calls == 1
+    assert p.tddftb.dftb2.geometries[-1] == (_vector2atomlist(x, p.atomlist), {"keep_charge": True})
+    assert not p.tddftb.calls  # no excited-state solve
