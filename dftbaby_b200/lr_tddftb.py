@@ -331,8 +331,11 @@ class LR_TDDFTB:
         preconditioner when no warm start is available; the solve runs to the
         same residual threshold, and the plain start is used if it fails.
         """
+        if response_method == "Tamm-Dancoff":
+            # DFTBaby's own Solver.TDA raises before doing anything ("Revise the TDA code", Solver.py:194)
+            raise ValueError("response_method='Tamm-Dancoff' is disabled in DFTBaby itself (Solver.TDA)")
         if response_method != "Casida":
-            raise ValueError("only response_method='Casida' is implemented")
+            raise ValueError('response_method should be "Casida" or "Tamm-Dancoff"')
         if ct_correction or stability:
             raise ValueError("ct_correction and stability analysis are not implemented")
         d = self.dftb2

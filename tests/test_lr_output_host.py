@@ -1,6 +1,7 @@
 """Active-space suggestion and the output files of LR_TDDFTB (LR_TDDFTB.py:196-243, 807-831, 900-908,
 1008-1025) on a hand-made solved object (host logic only)."""
 import numpy as np
+import pytest
 import torch
 
 from dftbaby_b200.lr_tddftb import LR_TDDFTB
@@ -62,3 +63,15 @@ def test_absorption_spectrum_file(tmp_path):
     assert lines[:2] == ["# Absorption spectrum", "# exc. energy / hartree  osc.strength"]
     assert lines[2] == "           0.1234567              0.5000000"
     assert np.allclose(np.loadtxt(str(path)), np.c_[td.Omega, td.oscillator_strength], atol=1e-7)
+
+
+def test_options_outside_the_path_raise_before_any_work():
+    """response_method="Tamm-Dancoff" is disabled in DFTBaby itself (Solver.TDA raises first thing,
+    Solver.py:184-194); the CT correction and the stability analysis are not provided.  Each raises
+    before the SCC runs."""
+    td = LR_TDDFTB.__new__(LR_TDDFTB)
+    td.dftb2 = None  # any use of the ground state would fail differently
+    for opts in (dict(response_method="Tamm-Dancoff"), dict(response_method="RPA"), dict(ct_correction=1),
+                 dict(stability=1)):
+        with pytest.raises(ValueError):
+            td.getEnergies(nstates=2, **opts)
