@@ -65,6 +65,9 @@ def main(ref_root):
     ea = _dict_literal(atomic, "electron_affinities_eV")
     hartree_to_eV = float(re.search(r"^hartree_to_eV\s*=\s*([0-9.eE+-]+)", atomic, re.M).group(1))
     out["const/hartree_to_eV"] = np.array(hartree_to_eV)
+    # wavelength in nm = hartree_to_nm / energy in Hartree (AtomicData.py:3)
+    out["const/hartree_to_nm"] = np.array(
+        float(re.search(r"^hartree_to_nm\s*=\s*([0-9.eE+-]+)", atomic, re.M).group(1)))
     # nuclear masses (electron masses), Boltzmann constant (Hartree/K) and the atomic time unit (fs)
     # used by the trajectory driver (AtomicData.py:6-7, 50-51)
     out["const/kBoltzmann"] = np.array(float(eval(re.search(r"^kBoltzmann\s*=\s*([^#\n]+)", atomic, re.M).group(1))))

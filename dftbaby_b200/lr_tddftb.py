@@ -29,6 +29,7 @@ import torch
 from . import native
 from .dftb2 import DFTB2
 from .exceptions import ExcitedStatesError, ExcitedStatesNotConverged
+from .params import raw_params
 from .solver import hermitian_davidson, nonhermitian_davidson
 
 
@@ -363,7 +364,11 @@ class LR_TDDFTB:
             self._TransitionDipolesMulliken()
         self.getOscillatorStrengths()
         self.Lambda2 = torch.sum(self.Cij ** 2 * self.Oia[None], dim=(1, 2))
+        # states are not classified by symmetry: empty labels, as DFTBaby without use_symmetry
+        self.Irreps = [""] * len(self.Omega)
         ev[3].record()
+        if getattr(d, "verbose", 0) > 0:
+            self._writeExcitations()
         return self.Omega, self.oscillator_strength
 
     def phase_ms(self):
@@ -652,6 +657,95 @@ class LR_TDDFTB:
                 ph_file = os.path.join(os.path.expanduser(os.path.expandvars(particle_hole_dir)),
                                        "particle_hole_charges_%d.chrg" % I)
                 np.savetxt(ph_file, np.vstack((particle, hole)).T)
+
+    # ------------------------------------------------------------ excitation table
+    def _dominant(self, I, dominant_probability):
+        """(local occupied index, local virtual index, coefficient) of the leading excitations of state I."""
+        C = self.Cij[I].cpu().numpy() if torch.is_tensor(self.Cij) else np.asarray(self.Cij[I])
+        order = np.argsort(-abs(C) ** 2, axis=None)
+        out, prob_sum = [], 0.0
+        for i, a in zip(order // C.shape[1], order % C.shape[1]):
+            if prob_sum >= dominant_probability:
+                break
+            dp = abs(C[i, a]) ** 2
+            if dp > 1.0e-10:
+                out.append((int(i), int(a), C[i, a]))
+            prob_sum += dp
+        return out
+
+    def _dominant_excitations(self, I, dominant_probability=0.99):
+        """LR_TDDFTB._dominant_excitations (LR_TDDFTB.py:706-741): the single excitations of state I (0-based),
+        largest |C_ia|^2 first, taken until their weights reach dominant_probability (weights below 1e-10
+        are skipped).  Returns (occupied orbitals, virtual orbitals, coefficients) as lists."""
+        dom = self._dominant(I, dominant_probability)
+        occ, virt = np.asarray(self.active_occupied_orbs), np.asarray(self.active_virtual_orbs)
+        return [occ[i] for i, _, _ in dom], [virt[a] for _, a, _ in dom], [c for _, _, c in dom]
+
+    def _writeExcitations(self, print_max_states=1000000, nr_dominant_ex=2, print_MO_tdip=False):
+        """LR_TDDFTB._writeExcitations (LR_TDDFTB.py:759-806): prints DFTBaby's excitation table, one line per
+        state: energy in Hartree, eV and nm, oscillator strength, the nr_dominant_ex leading excitations
+        (orbitals counted from 1; with print_MO_tdip their orbital transition dipoles), the Kohn-Sham energy
+        difference of the leading one, the transition dipole and Lambda."""
+        raw = raw_params()
+        h2ev, h2nm = float(raw["const/hartree_to_eV"]), float(raw["const/hartree_to_nm"])
+        num = lambda a: a.cpu().numpy() if torch.is_tensor(a) else np.asarray(a)
+        orbe = num(self.dftb2.getKSEnergies())
+        tdx, tdy, tdz, lam = num(self.tdipX), num(self.tdipY), num(self.tdipZ), num(self.Lambda2)
+        osc, Om = num(self.oscillator_strength), np.asarray(self.Omega)
+        irreps = getattr(self, "Irreps", None) or [""] * len(Om)
+        occ, virt = np.asarray(self.active_occupied_orbs), np.asarray(self.active_virtual_orbs)
+        en0 = float(self.en0)
+        txt = " ground state energy: %s %s\n\n" % (("%.7f hartree" % en0).rjust(15),
+                                                    ("%.7f eV" % (en0 * h2ev)).rjust(15))
+        txt += "           Excited States\n"
+        txt += "           ==============\n"
+        symstr = "   "  # the point-group column stays blank: states are not classified by symmetry here
+        txt += ("     Spn %s     exc. en. /hartree      exc. en. / eV   exc. en. / nm    osc. strength             "
+                "dominant contrib.               en_KS / eV      transition dipole [TDx TDy TDz]   /\\ diagn.\n"
+                % symstr)
+        for I in range(0, min(print_max_states, len(Om))):
+            dom = self._dominant(I, 0.99)
+            domex_str, domKS_str = 7 * " ", 6 * " "
+            for count, (i, a, c) in enumerate(dom):
+                iocc, avirt = occ[i], virt[a]
+                if count == 0:
+                    domKS_str = "%2.4f" % ((orbe[avirt] - orbe[iocc]) * h2ev)
+                MOtdip = ""
+                if print_MO_tdip:
+                    t = self._mo_dipole(iocc, avirt)
+                    MOtdip = ",[%+2.7f %+2.7f %+2.7f]" % (t[0], t[1], t[2])
+                domex_str += "%d->%d(%+.3e%s)" % (iocc + 1, avirt + 1, c, MOtdip)
+                if count < min(nr_dominant_ex, len(dom)) - 1:
+                    domex_str += ","
+                if count == nr_dominant_ex - 1:
+                    break
+            txt += "%s %s %s: %s %s %s  %s %s %s %s %s\n" % (
+                str(I + 1).rjust(5), self.multiplicity, irreps[I].rjust(3), ("%.7f hartree" % Om[I]).rjust(20),
+                ("%.7f eV" % (Om[I] * h2ev)).rjust(17), ("%.7f nm" % (h2nm / Om[I])).rjust(17),
+                ("%.7f" % osc[I]).rjust(12), domex_str.rjust(45), domKS_str.rjust(8),
+                ("[%+2.7f %+2.7f %+2.7f]" % (tdx[I], tdy[I], tdz[I])).rjust(40), ("%.4f" % lam[I]).rjust(7))
+        print(txt)
+
+    def _mo_dipole(self, p, q):
+        """<p|r|q> (x, y, z) between molecular orbitals p and q."""
+        d = self.dftb2
+        cp, cq = d.orbs[:, int(p)], d.orbs[:, int(q)]
+        return torch.einsum("m,cmn,n->c", cp, d.D3, cq).cpu().numpy()
+
+    def hasActiveSpace(self):
+        """LR_TDDFTB.hasActiveSpace (LR_TDDFTB.py:244-253): True when the active window leaves out some of the
+        occupied or virtual orbitals the solver chose from."""
+        return not (len(self.occupied_orbs) == len(self.active_occupied_orbs)
+                    and len(self.virtual_orbs) == len(self.active_virtual_orbs))
+
+    def energy_func(self, x, atomlist, I, **options):
+        """LR_TDDFTB.energy_func (LR_TDDFTB.py:115-124): the excitation energy of state I (0-based) at the flat
+        coordinates x (bohr), for numerical differentiation; getEnergies and SCC options as keywords
+        (the reference reads them from its command line)."""
+        x = np.asarray(x, dtype=np.float64).reshape(-1)
+        self.setGeometry([(Z, tuple(x[3 * i:3 * i + 3])) for i, (Z, _) in enumerate(atomlist)])
+        self.getEnergies(**options)
+        return self.Omega[I]
 
     def saveAbsorptionSpectrum(self, spectrum_file="absorption_spectrum.dat"):
         """LR_TDDFTB.saveAbsorptionSpectrum (LR_TDDFTB.py:807-831): excitation energies (Hartree) and

@@ -676,8 +676,9 @@ def make_scc(ref_root, mods):
 
 def make_lr_glue(ref_root, rng):
     """LR_TDDFTB.setActiveOrbitals, setActiveLMOrbitals, _TransitionDipoles, _TransitionDipolesMulliken, getTransitionDipolesExc,
-    getOscillatorStrengths, determineActiveSpace, TransitionChargesState, saveAbsorptionSpectrum and
-    saveTransitionCharges (LR_TDDFTB.py:167-243, 567-705, 807-831, 900-908, 1008-1025) run from DFTBaby's text on a
+    getOscillatorStrengths, determineActiveSpace, TransitionChargesState, saveAbsorptionSpectrum,
+    saveTransitionCharges, _dominant_excitations and _writeExcitations (LR_TDDFTB.py:125-243, 567-831, 900-908,
+    1008-1025) run from DFTBaby's text on a
     stand-in solved object: 14 orbitals (6 doubly occupied), active window 3 x 4, 3 states."""
     lr = os.path.join(ref_root, "DFTB", "LR_TDDFTB.py")
     names = ("setActiveOrbitals", "_TransitionDipoles", "_TransitionDipolesMulliken", "getOscillatorStrengths",
@@ -764,6 +765,40 @@ def make_lr_glue(ref_root, rng):
     out["spectrum_text"] = np.array(open(os.path.join(tmp, "spec.dat")).read())
     out["transition_charges_text"] = np.array(open(os.path.join(tmp, "tq.dat")).read())
     shutil.rmtree(tmp, ignore_errors=True)
+    # the excitation table getEnergies prints at verbose > 0 (_dominant_excitations, _writeExcitations,
+    # LR_TDDFTB.py:706-806), with utils.argsort_2d (utils.py:96-117; its integer division made explicit)
+    for n in ("_dominant_excitations", "_writeExcitations"):
+        exec(compile(method_source(lr, n, after=r"class LR_TDDFTB"), "LR_TDDFTB.py", "exec"), ns)
+    ns_u = {"argsort": np.argsort}
+    argsort_src = method_source(os.path.join(ref_root, "DFTB", "utils.py"), "argsort_2d")
+    assert "sort_indx / ncols" in argsort_src
+    exec(compile(argsort_src.replace("sort_indx / ncols", "sort_indx // ncols"), "utils.py", "exec"), ns_u)
+    ad = _reference_atomic_data(ref_root)
+    ns.update(utils=types.SimpleNamespace(argsort_2d=ns_u["argsort_2d"]), hartree_to_eV=ad.hartree_to_eV,
+              hartree_to_nm=ad.hartree_to_nm)
+    r._dominant_excitations = lambda I, dominant_probability=0.99: ns["_dominant_excitations"](r, I,
+                                                                                               dominant_probability)
+    dftb2.use_symmetry = 0
+    r.Lambda2 = rng.random(3)
+    r.en0 = -12.3456789
+    r._TransitionDipoles()
+    r.getOscillatorStrengths()
+    out.update(Lambda2=r.Lambda2, en0=r.en0)
+    for k, p in enumerate((0.99, 0.5)):
+        for I in range(3):
+            o, v, c = r._dominant_excitations(I, dominant_probability=p)
+            out["domex_%d_%d" % (k, I)] = np.array([o, v, c], dtype=float)
+    import contextlib
+    sys.modules["string"] = types.SimpleNamespace(rjust=lambda text, width: text.rjust(width))
+    try:
+        for k, kw in enumerate((dict(), dict(nr_dominant_ex=3, print_MO_tdip=True),
+                                dict(print_max_states=2, nr_dominant_ex=1))):
+            buf = io.StringIO()
+            with contextlib.redirect_stdout(buf):
+                ns["_writeExcitations"](r, **kw)
+            out["excitations_text_%d" % k] = np.array(buf.getvalue())
+    finally:
+        sys.modules["string"] = real_string
     np.savez_compressed(os.path.join(HERE, "lr_glue.npz"), **out)
 
 

@@ -82,3 +82,27 @@ def test_dipoles_between_excited_states_against_reference():
     tdip = td.getTransitionDipolesExc(4)
     assert tdip.shape == (4, 4, 3)
     assert np.abs(tdip - G["tdip_exc"]).max() < 1e-12
+
+
+def test_excitation_table_against_reference(capsys):
+    td = _solved()
+    td.Lambda2, td.en0 = torch.tensor(G["Lambda2"]), float(G["en0"])
+    td._TransitionDipoles()
+    td.getOscillatorStrengths()
+    for k, p in enumerate((0.99, 0.5)):
+        for I in range(3):
+            o, v, c = td._dominant_excitations(I, dominant_probability=p)
+            ref = G["domex_%d_%d" % (k, I)]
+            assert np.array_equal(np.array(o), ref[0]) and np.array_equal(np.array(v), ref[1])
+            assert np.abs(np.array(c) - ref[2]).max() < 1e-15
+    for k, kw in enumerate((dict(), dict(nr_dominant_ex=3, print_MO_tdip=True),
+                            dict(print_max_states=2, nr_dominant_ex=1))):
+        td._writeExcitations(**kw)
+        assert capsys.readouterr().out == str(G["excitations_text_%d" % k])
+
+
+def test_has_active_space():
+    td = _solved()
+    assert td.hasActiveSpace()
+    td.setActiveOrbitals()
+    assert not td.hasActiveSpace()
