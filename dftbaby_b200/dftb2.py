@@ -12,12 +12,14 @@ stream.
 Every array attribute (``S``, ``H0``, ``P``, ``orbs``, ``orbe``, ``dq``,
 ``gamma``, ...) is a float64 CUDA tensor; accessors return these tensors.
 """
+import os
+
 import numpy as np
 import torch
 
 from . import native
 from .exceptions import SCFChargeInconsistency, SCFNotConverged
-from .params import Parametrization
+from .params import ELEMENT_NAMES, Parametrization
 
 
 class DIIS_80:
@@ -86,7 +88,8 @@ class DFTB2(object):
     def __init__(self, atomlist, parameter_set="homegrown", missing_reppots="dummy", verbose=0,
                  distance_cutoff=30.0, long_range_correction=1, long_range_radius=3.03, long_range_T=1.0,
                  long_range_switching="erf", lc_implementation=None, hubbard_scaling=1.0, hubbard_override=None,
-                 fluctuation_functions="Gaussian", nr_unpaired_electrons=0, use_symmetry=0, device=None, **opts):
+                 fluctuation_functions="Gaussian", nr_unpaired_electrons=0, use_symmetry=0, device=None,
+                 initial_charge_guess=None, save_converged_charges=None, **opts):
         if parameter_set != "homegrown":
             raise ValueError("only the 'homegrown' parameter set is carried")
         if fluctuation_functions != "Gaussian":
@@ -111,6 +114,12 @@ class DFTB2(object):
         self.hubbard_U = self.par.hubbard_U
         self.ne_val = self.par.ne_val
         self.workspace = native.Workspace(self.device)
+        # partial charges read from / written to text files, one atom per line (DFTB2.py:405-409, 1158-1160)
+        charge_guess = None
+        if initial_charge_guess is not None:
+            charge_guess = np.loadtxt(os.path.expandvars(os.path.expanduser(initial_charge_guess)))
+        self.setChargeGuess(charge_guess)
+        self.save_converged_charges = save_converged_charges
 
     # ------------------------------------------------------------ geometry
     def setGeometry(self, atomlist, charge=0.0, keep_charge=False, update_symmetry=True):
@@ -282,7 +291,13 @@ class DFTB2(object):
             raise ValueError("density_mixer must be a DIIS_80 instance or None")
         nat, norb, dev = len(self.atomlist), self.dim, self.device
         st, P = native.stream(), native.ptr
-        if not hasattr(self, "dq") or start_from_previous == 0 or self.dq.numel() != nat:
+        if getattr(self, "charge_guess", None) is not None:
+            # every SCC starts from the guess while one is set (DFTB2.py:976-989)
+            guess = torch.as_tensor(np.asarray(self.charge_guess, dtype=np.float64).reshape(-1), device=dev)
+            if guess.numel() != nat:
+                raise ValueError("the charge guess has %d partial charges for %d atoms" % (guess.numel(), nat))
+            self.dq = self._balance_partial_charges(guess)
+        elif not hasattr(self, "dq") or start_from_previous == 0 or self.dq.numel() != nat:
             self.dq = torch.zeros(nat, dtype=torch.float64, device=dev)
         if density_mixer is not None:
             density_mixer.reset()
@@ -367,6 +382,65 @@ class DFTB2(object):
         else:
             raise SCFNotConverged("SCF calculation did not converge after %s iterations!!!" % (self.i + 1))
         self.scc_iterations = self.i + 1
+        if getattr(self, "save_converged_charges", None) is not None:
+            np.savetxt(os.path.expandvars(os.path.expanduser(self.save_converged_charges)), self.dq.cpu().numpy())
+
+    def setCharge(self, charge):
+        """DFTB2.setCharge (DFTB2.py:429-435): net charge (units of e) and the valence electron count."""
+        self.charge = charge
+        self.Nelec_val = sum(self.q0) - self.charge
+        if self.Nelec_val < 0.5:
+            print("\nWARNING: There are no valence electrons in this molecule, \n         charge = %+d,  nr. valence "
+                  "electrons = %s !\n" % (self.charge, self.Nelec_val))
+
+    def _balance_partial_charges(self, dq):
+        """DFTB2._balance_partial_charges (DFTB2.py:839-848): dq shifted evenly so that the partial charges add
+        up to the net charge (sum dq = -charge: dq counts electrons)."""
+        return dq - (dq.sum() + self.charge) / dq.numel()
+
+    def setChargeGuess(self, charge_guess):
+        """DFTB2.setChargeGuess (DFTB2.py:524-525): partial charges (one per atom) every later SCC starts from;
+        None returns to the previous step's charges."""
+        self.charge_guess = charge_guess
+
+    # ------------------------------------------------------------ ground-state properties
+    def getDipoleMoment(self):
+        """DFTB2.getDipoleMoment (DFTB2.py:2470-2486): sum_{mu,nu} P_mu,nu D^i_mu,nu, i = x, y, z (numpy (3,),
+        electrons counted positive, as in the reference)."""
+        return torch.einsum("mn,cmn->c", self.P, self.D3).cpu().numpy()
+
+    def getMullikenDipoleMoment(self):
+        """DFTB2.getMullikenDipoleMoment (DFTB2.py:2456-2469): sum_i (R_i - R_cc) q_i with the Mulliken
+        populations q_i and R_cc the centre of the nuclear charges Z_i (DFTB2.py:849-860)."""
+        Z = np.array([Zi for Zi, _ in self.atomlist], dtype=np.float64)
+        R = np.array([p for _, p in self.atomlist], dtype=np.float64)
+        Rcc = (Z[:, None] * R).sum(axis=0) / Z.sum()
+        q = self.q.cpu().numpy() if torch.is_tensor(self.q) else np.asarray(self.q)
+        return ((R - Rcc) * q[:, None]).sum(axis=0)
+
+    def write_Mulliken_charges(self):
+        """DFTB2.write_Mulliken_charges (DFTB2.py:1712-1721): prints Mulliken populations and excess charges."""
+        q = self.q.cpu().numpy() if torch.is_tensor(self.q) else np.asarray(self.q)
+        dq = self.dq.cpu().numpy() if torch.is_tensor(self.dq) else np.asarray(self.dq)
+        txt = "  Mulliken Charges (Excess Charges)\n"
+        txt += "  =================================\n"
+        for i, (Zi, _) in enumerate(self.atomlist):
+            txt += "%s: %.3f\t(%.3f)\n" % (("%s-%s" % (ELEMENT_NAMES[Zi], i)).center(12), q[i], dq[i])
+        print(txt)
+        print("sum q0 = %s" % sum(self.q0))
+        print("sum q  = %s" % np.sum(q))
+        print("sum dq = %s" % np.sum(dq))
+
+    def _energy_func(self, x, atomlist, which_en):
+        """DFTB2._energy_func (DFTB2.py:2388-2404): one energy term ("Ebs", "Ecoulomb", "Eelec", "Enuc" or
+        "Etot") at the flat coordinates x (bohr), for numerical differentiation."""
+        x = np.asarray(x, dtype=np.float64).reshape(-1)
+        self.setGeometry([(Z, tuple(x[3 * i:3 * i + 3])) for i, (Z, _) in enumerate(atomlist)])
+        self.getEnergy()
+        names = ("Ebs", "Ecoulomb", "Eelec", "Enuc", "Etot")
+        if which_en not in names:
+            raise ValueError("which_en must be one of %s" % (names,))
+        return self.getEnergies()[names.index(which_en)]
 
     # ------------------------------------------------------------ accessors
     def getOverlapMatrix(self):

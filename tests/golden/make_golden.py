@@ -32,7 +32,7 @@ rotation) on stand-in objects, through the same shim.
 
 Usage::
 
-    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda|repulsive|lr_e2e|particle_hole|handler]
+    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda|repulsive|lr_e2e|particle_hole|handler|dftb2_props]
 """
 import io
 import os
@@ -991,6 +991,62 @@ def make_handler(ref_root, rng):
     np.savez_compressed(os.path.join(HERE, "handler.npz"), **out)
 
 
+def make_dftb2_props(ref_root, rng):
+    """DFTB2.getDipoleMoment, getMullikenDipoleMoment (with _center_of_nuclear_charge), write_Mulliken_charges,
+    _balance_partial_charges and setCharge (DFTB2.py:429-435, 839-860, 1712-1721, 2456-2486) run from DFTBaby's
+    text on a stand-in C2H4 ground state: random symmetric density and dipole matrices, Mulliken populations."""
+    import contextlib
+    names = ("getDipoleMoment", "getMullikenDipoleMoment", "_center_of_nuclear_charge", "write_Mulliken_charges",
+             "_balance_partial_charges", "setCharge")
+    ns = {"np": np, "zeros": np.zeros, "array": np.array, "sum": np.sum,
+          "atom_names": ["h", "he", "li", "be", "b", "c"]}
+    for n in names:
+        exec(compile(method_source(os.path.join(ref_root, "DFTB", "DFTB2.py"), n, after=r"class DFTB2"), "DFTB2.py",
+                     "exec"), ns)
+    Ref = type("DFTB2", (), {n: ns[n] for n in names})
+    Zs = [6, 6, 1, 1, 1, 1]
+    pos = rng.standard_normal((len(Zs), 3)) * 1.5
+    norb = 12
+    X = rng.standard_normal((norb, norb))
+    P = X + X.T
+    X = rng.standard_normal((norb, norb, 3))
+    D = X + X.transpose(1, 0, 2)
+    q0 = np.array([4.0, 4.0, 1.0, 1.0, 1.0, 1.0])
+    dq = 0.1 * rng.standard_normal(len(Zs))
+    r = Ref()
+    r.atomlist = [(Z, tuple(p)) for Z, p in zip(Zs, pos)]
+    r.P, r.q0, r.dq, r.q = P, q0, dq, q0 - dq
+    r.getDipoleMatrix = lambda: D
+    out = dict(Z=np.array(Zs), pos=pos, P=P, D=D, q0=q0, dq=dq)
+    with contextlib.redirect_stdout(io.StringIO()):
+        out["dipole"] = r.getDipoleMoment()  # the reference also prints P here
+    r._center_of_nuclear_charge()
+    out["Rcc"], out["mulliken_dipole"] = r.Rcc, r.getMullikenDipoleMoment()
+    real_string = sys.modules.get("string")
+    sys.modules["string"] = types.SimpleNamespace(center=lambda text, width: text.center(width))
+    buf = io.StringIO()
+    try:
+        with contextlib.redirect_stdout(buf):
+            r.write_Mulliken_charges()
+    finally:
+        sys.modules["string"] = real_string
+    out["mulliken_text"] = np.array(buf.getvalue())
+    for k, charge in enumerate((0.0, 1.0, -2.0)):
+        r.charge = charge
+        r.dq = dq.copy()
+        r._balance_partial_charges()
+        out["balanced_%d" % k] = r.dq
+        buf = io.StringIO()
+        with contextlib.redirect_stdout(buf):
+            r.setCharge(charge)
+        out["nelec_%d" % k], out["setcharge_text_%d" % k] = r.Nelec_val, np.array(buf.getvalue())
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        r.setCharge(12.0)  # no valence electrons left: the reference warns
+    out["nelec_empty"], out["setcharge_text_empty"] = r.Nelec_val, np.array(buf.getvalue())
+    np.savez_compressed(os.path.join(HERE, "dftb2_props.npz"), **out)
+
+
 def make_repulsive(ref_root, rng):
     """RepulsivePotential.__init__ / getVrep (RepulsivePotential.py:17-100, as DFTB2.py:327 builds them: no
     smooth tail) on the shipped H-H, H-C and C-C tables, run from DFTBaby's text: values and first
@@ -1118,6 +1174,8 @@ def main(ref_root, only=None):
             make_particle_hole(ref_root, np.random.default_rng(20261210))
         if only in (None, "handler"):
             make_handler(ref_root, np.random.default_rng(20261211))
+        if only in (None, "dftb2_props"):
+            make_dftb2_props(ref_root, np.random.default_rng(20261212))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)

@@ -1,0 +1,49 @@
+"""Ground-state properties and charge handling of DFTB2 against DFTBaby's own methods
+(tests/golden/dftb2_props.npz, made by tests/golden/make_golden.py): the dipole moment from the density
+matrix, the Mulliken dipole about the centre of nuclear charge, the printed Mulliken charges, the balancing
+of a charge guess and setCharge."""
+import os
+
+import numpy as np
+import torch
+
+from dftbaby_b200.dftb2 import DFTB2
+
+G = np.load(os.path.join(os.path.dirname(__file__), "golden", "dftb2_props.npz"))
+
+
+def _ground_state():
+    d = DFTB2.__new__(DFTB2)
+    d.atomlist = [(int(Z), tuple(p)) for Z, p in zip(G["Z"], G["pos"])]
+    d.P = torch.tensor(G["P"])
+    d.D3 = torch.tensor(np.ascontiguousarray(np.moveaxis(G["D"], -1, 0)))
+    d.q0 = list(G["q0"])
+    d.dq = torch.tensor(G["dq"])
+    d.q = torch.tensor(G["q0"] - G["dq"])
+    d.charge = 0.0
+    return d
+
+
+def test_dipole_moments_against_reference():
+    d = _ground_state()
+    assert np.abs(d.getDipoleMoment() - G["dipole"]).max() < 1e-13
+    assert np.abs(d.getMullikenDipoleMoment() - G["mulliken_dipole"]).max() < 1e-14
+
+
+def test_mulliken_printout_against_reference(capsys):
+    _ground_state().write_Mulliken_charges()
+    assert capsys.readouterr().out == str(G["mulliken_text"])
+
+
+def test_charge_guess_balancing_and_set_charge_against_reference(capsys):
+    d = _ground_state()
+    for k, charge in enumerate((0.0, 1.0, -2.0)):
+        d.charge = charge
+        assert np.abs(d._balance_partial_charges(torch.tensor(G["dq"])).numpy() - G["balanced_%d" % k]).max() < 1e-15
+        d.setCharge(charge)
+        assert d.Nelec_val == float(G["nelec_%d" % k])
+        assert capsys.readouterr().out == str(G["setcharge_text_%d" % k])
+    d.setCharge(12.0)
+    assert d.Nelec_val == float(G["nelec_empty"])
+    assert capsys.readouterr().out == str(G["setcharge_text_empty"])
+

@@ -59,3 +59,20 @@ def test_select_lm_active_space():
     sel = np.r_[td_pi.active_occupied_orbs, td_pi.active_virtual_orbs]
     assert np.all(w[sel] > 1e-3) and np.all(np.delete(w, sel) < 1e-15)
     assert np.all(np.isfinite(Om_pi)) and np.all(Om_pi > 0) and np.all(np.isfinite(f_pi))
+
+
+def test_saved_charges_seed_the_next_scc(tmp_path):
+    """save_converged_charges / initial_charge_guess (DFTB2.py:405-409, 976-989, 1158-1160): the charges one
+    SCC writes, read back as the guess of a new object, reproduce its energy in no more iterations."""
+    native.load()
+    from dftbaby_b200.dftb2 import DFTB2
+    al = geometry.polyene(8, sigma=0.02, seed=7)
+    fn = str(tmp_path / "dq.dat")
+    d = DFTB2(al, long_range_correction=1, save_converged_charges=fn)
+    d.setGeometry(al)
+    E = d.getEnergy()
+    assert np.array_equal(np.loadtxt(fn), d.dq.cpu().numpy())
+    d2 = DFTB2(al, long_range_correction=1, initial_charge_guess=fn)
+    d2.setGeometry(al)
+    E2 = d2.getEnergy()
+    assert abs(E2 - E) < 1e-8 and d2.scc_iterations <= d.scc_iterations
