@@ -1,5 +1,4 @@
 """The tcgen05 split-precision BF16 GEMM against FP64 products."""
-import numpy as np
 import pytest
 import torch
 

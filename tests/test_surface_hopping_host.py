@@ -2,7 +2,6 @@
 on synthetic data: local diabatization, fewest switches, hop rescaling, decoherence, phase alignment,
 centre-of-mass and rotation removal."""
 import numpy as np
-import pytest
 
 from dftbaby_b200 import surface_hopping as SH
 
