@@ -13,6 +13,7 @@ Every array attribute (``S``, ``H0``, ``P``, ``orbs``, ``orbe``, ``dq``,
 ``gamma``, ...) is a float64 CUDA tensor; accessors return these tensors.
 """
 import os
+import re
 
 import numpy as np
 import torch
@@ -285,10 +286,15 @@ class DFTB2(object):
         """Self-consistent charges (DFTB2.runSCC, DFTB2.py:940-1160), T = 0."""
         if fock_interpolator is not None:
             raise ValueError("Fock interpolation is not implemented")
-        if isinstance(density_mixer, str) and density_mixer == "default":
-            density_mixer = DIIS_80(5)
-        elif isinstance(density_mixer, str):
-            raise ValueError("density_mixer must be a DIIS_80 instance or None")
+        if isinstance(density_mixer, str):
+            # "default" or, from the command line, "DIIS_80(m)" (DFTBaby evaluates that text, DFTB2.py:966-968)
+            m = re.fullmatch(r"\s*DIIS_80\(\s*(\d+)\s*\)\s*", density_mixer)
+            if density_mixer == "default":
+                density_mixer = DIIS_80(5)
+            elif m:
+                density_mixer = DIIS_80(int(m.group(1)))
+            else:
+                raise ValueError("density_mixer must be a DIIS_80 instance, 'DIIS_80(m)' or None")
         nat, norb, dev = len(self.atomlist), self.dim, self.device
         st, P = native.stream(), native.ptr
         if getattr(self, "charge_guess", None) is not None:

@@ -22,19 +22,7 @@ import numpy as np
 
 from .exceptions import ExcitedStatesError, ExcitedStatesNotConverged, SCFNotConverged
 from .params import ELEMENT_NAMES, raw_params
-
-
-def atomic_number(atom):
-    """AtomicData.atomic_number (AtomicData.py:32-40): a number stands for a point charge; otherwise the
-    element symbol with any digits removed ("C12" -> carbon), case-insensitive."""
-    try:
-        return float(atom)
-    except ValueError:
-        elem = "".join(ch for ch in atom.lower() if not ch.isdigit())
-        for Z, name in ELEMENT_NAMES.items():
-            if name == elem:
-                return Z
-        raise ValueError("no parameters for element %r" % atom)
+from .xyz import atomic_number
 
 
 def atomlist2masses(atomlist):

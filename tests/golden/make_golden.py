@@ -32,7 +32,7 @@ rotation) on stand-in objects, through the same shim.
 
 Usage::
 
-    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda|repulsive|lr_e2e|particle_hole|handler|dftb2_props]
+    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda|repulsive|lr_e2e|particle_hole|handler|dftb2_props|xyz]
 """
 import io
 import os
@@ -1047,6 +1047,51 @@ def make_dftb2_props(ref_root, rng):
     np.savez_compressed(os.path.join(HERE, "dftb2_props.npz"), **out)
 
 
+XYZ_TEXT = """6
+charge=+1 name=ethene tags=[1,2] note=C2H4
+C      0.000000    0.000000    0.667480
+C      0.000000    0.000000   -0.667480
+H      0.000000    0.922832    1.237695
+H      0.000000   -0.922832    1.237695
+H1     0.000000    0.922832   -1.237695
+h      0.000000   -0.922832   -1.237695
+Tv     2.5  0.0  0.0
+6
+second frame
+C      0.010000    0.000000    0.667480
+C      0.000000    0.020000   -0.667480
+H      0.000000    0.922832    1.237695
+H      0.000000   -0.922832    1.237695
+H      0.000000    0.922832   -1.237695
+H      0.000000   -0.922832   -1.237695
+"""
+
+
+def make_xyz(ref_root, rng):
+    """XYZ.read_xyz (through read_xyz_it), extract_keywords_xyz and xyz2txt (XYZ.py:15-195) run from DFTBaby's text,
+    with AtomicData.atomic_number and bohr_to_angs, on a two-frame C2H4 file with a lattice-vector line,
+    numbered and lower-case element labels and key=value pairs on the title line."""
+    ad = _reference_atomic_data(ref_root)
+    ns = {"np": np, "zeros": np.zeros, "la": np.linalg, "atom_names": ad.atom_names, "atomic_number": ad.atomic_number,
+          "bohr_to_angs": ad.bohr_to_angs, "covalent_radii": ad.covalent_radii}
+    src = os.path.join(ref_root, "DFTB", "XYZ.py")
+    for n in ("read_xyz_it", "read_xyz", "extract_keywords_xyz", "xyz2txt", "_append_xyz2txt"):
+        exec(compile(method_source(src, n), "XYZ.py", "exec"), ns)
+    tmp = tempfile.mkdtemp(prefix="dftbaby_xyz_")
+    fn = os.path.join(tmp, "mol.xyz")
+    open(fn, "w").write(XYZ_TEXT)
+    geoms = ns["read_xyz"](fn)
+    bohr = ns["read_xyz"](fn, units="bohr")
+    kw = ns["extract_keywords_xyz"](fn)
+    shutil.rmtree(tmp, ignore_errors=True)
+    out = dict(Z=np.array([[Z for Z, _ in g] for g in geoms]), pos=np.array([[p for _, p in g] for g in geoms]),
+               pos_bohr_units=np.array([[p for _, p in g] for g in bohr]), keywords=np.array(repr(sorted(kw.items()))),
+               text_one=np.array(ns["xyz2txt"](geoms[:1], title="one title")),
+               text_list=np.array(ns["xyz2txt"](geoms, title=["first"])),
+               text_bohr=np.array(ns["xyz2txt"](geoms[1:], units="bohr")))
+    np.savez_compressed(os.path.join(HERE, "xyz.npz"), **out)
+
+
 def make_repulsive(ref_root, rng):
     """RepulsivePotential.__init__ / getVrep (RepulsivePotential.py:17-100, as DFTB2.py:327 builds them: no
     smooth tail) on the shipped H-H, H-C and C-C tables, run from DFTBaby's text: values and first
@@ -1176,6 +1221,8 @@ def main(ref_root, only=None):
             make_handler(ref_root, np.random.default_rng(20261211))
         if only in (None, "dftb2_props"):
             make_dftb2_props(ref_root, np.random.default_rng(20261212))
+        if only in (None, "xyz"):
+            make_xyz(ref_root, None)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)

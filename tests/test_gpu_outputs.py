@@ -78,3 +78,25 @@ def test_saved_charges_seed_the_next_scc(tmp_path):
     E2 = d2.getEnergy()
     assert abs(E2 - E) < 1e-8
     assert np.abs(d2.dq.cpu().numpy() - d.dq.cpu().numpy()).max() < 1e-7
+
+
+def test_command_line(tmp_path, monkeypatch):
+    """python -m dftbaby_b200.lr_tddftb mol.xyz --nstates=3 ... (LR_TDDFTB.py:1153-1230): the spectrum file it
+    writes holds the energies and oscillator strengths of a direct LR_TDDFTB run on the same geometry."""
+    import os
+    native.load()
+    from dftbaby_b200 import lr_tddftb, xyz
+    from dftbaby_b200.lr_tddftb import LR_TDDFTB
+    monkeypatch.chdir(tmp_path)
+    xyz.write_xyz("mol.xyz", [geometry.polyene(6, sigma=0.02, seed=11)], title="charge=0")
+    argv = ["mol.xyz", "--nstates=3", "--diag_conv=1e-8", "--spectrum_file=spec.dat", "--particle_hole_states=[1]",
+            "--particle_hole_dir=."]
+    assert lr_tddftb.main(argv) == 0
+    al = xyz.read_xyz("mol.xyz")[0]
+    td = LR_TDDFTB(al, long_range_correction=1)
+    td.setGeometry(al)
+    Om, f = td.getEnergies(nstates=3, diag_conv=1e-8)
+    spec = np.loadtxt("spec.dat")
+    assert np.allclose(spec[:, 0], Om, atol=1e-6) and np.allclose(spec[:, 1], f, atol=1e-6)
+    assert np.loadtxt("particle_hole_charges_1.chrg").shape == (len(al), 2)
+    assert not os.path.exists("transition_charges.dat")
