@@ -90,7 +90,7 @@ def test_command_line(tmp_path, monkeypatch):
     monkeypatch.chdir(tmp_path)
     xyz.write_xyz("mol.xyz", [geometry.polyene(6, sigma=0.02, seed=11)], title="charge=0")
     argv = ["mol.xyz", "--nstates=3", "--diag_conv=1e-8", "--spectrum_file=spec.dat", "--particle_hole_states=[1]",
-            "--particle_hole_dir=."]
+            "--particle_hole_dir=.", "--gradient_state=1", "--gradient_file=grad.xyz"]
     assert lr_tddftb.main(argv) == 0
     al = xyz.read_xyz("mol.xyz")[0]
     td = LR_TDDFTB(al, long_range_correction=1)
@@ -100,3 +100,4 @@ def test_command_line(tmp_path, monkeypatch):
     assert np.allclose(spec[:, 0], Om, atol=1e-6) and np.allclose(spec[:, 1], f, atol=1e-6)
     assert np.loadtxt("particle_hole_charges_1.chrg").shape == (len(al), 2)
     assert not os.path.exists("transition_charges.dat")
+    assert os.path.exists("grad.xyz")

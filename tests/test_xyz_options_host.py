@@ -77,3 +77,7 @@ def test_lr_tddftb_command_line_options(tmp_path, monkeypatch, capsys):
     assert scf["scf_conv"] == 1e-9 and scf["density_mixer"] == "DIIS_80(3)"
     ph, _ = p.parse_args(LR_TDDFTB.analyseParticleHole, argv)
     assert ph == dict(particle_hole_states=[1, 2], particle_hole_dir=None)
+    from dftbaby_b200.gradients import Gradients
+    p = OptionParserFuncWrapper([LR_TDDFTB.getEnergies, Gradients.getGradients], "usage")
+    g, _ = p.parse_args(Gradients.getGradients, ["--gradient_state=1", "--gradient_file=grad.xyz"])
+    assert g == dict(gradient_state=1, gradient_file="grad.xyz", gradient_check=0)
