@@ -25,8 +25,6 @@ import torch
 
 from . import native
 
-ELEMENT_NAMES = {1: "h", 6: "c"}
-
 
 def _block_sum(Y, ind, nat):
     """Atom-block sums A[I][J] = sum_{a on I, b on J} Y[a][b]."""
@@ -330,15 +328,13 @@ class Gradients:
             return None
         if gradient_check:
             raise ValueError("gradient_check is not implemented; compare against finite differences instead")
+        from .xyz import write_xyz
         gradVrep, gradE0, gradExc = self.gradient(I=gradient_state)
         gradEtot = gradVrep + gradE0 + gradExc
-        atoms = self.dftb.getGeometry()
-        lines = ["%d" % len(atoms), "Gradient of total energy of state %d" % gradient_state]
-        for k, (Z, _) in enumerate(atoms):
-            g = gradEtot[3 * k:3 * k + 3]
-            lines.append("%4s %10.15f %10.15f %10.15f" % (ELEMENT_NAMES.get(Z, str(Z)).capitalize(), g[0], g[1], g[2]))
-        with open(gradient_file, "w") as fh:
-            fh.write("\n".join(lines) + "\n")
+        grad_atomlist = [(Z, tuple(gradEtot[3 * k:3 * k + 3])) for k, (Z, _) in enumerate(self.dftb.getGeometry())]
+        write_xyz(gradient_file, [grad_atomlist], title="Gradient of total energy of state %d" % gradient_state,
+                  units="au")
+        print("Gradient of state %d written to file %s" % (gradient_state, gradient_file))
         return gradEtot
 
 
