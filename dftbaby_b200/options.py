@@ -2,7 +2,7 @@
 (DFTB/optparse.py:1783-1935, OptionParserFuncWrapper).
 
 * Every keyword parameter with a default becomes an option ``--name`` (``--name=value`` or ``--name value``);
-  list-valued defaults are not options.
+  list-valued defaults and keyword-only parameters (programmatic arguments) are not options.
 * Defaults come from the function, then from the ``[DFTBaby]`` section of ``dftbaby.cfg`` in the working
   directory, then from the command line.
 * Values of options whose default is an int or a float are converted to that type; the others are read
@@ -41,7 +41,8 @@ class OptionParserFuncWrapper:
         for func in funcs:
             names = []
             for p in inspect.signature(func).parameters.values():
-                if p.default is inspect.Parameter.empty or p.kind in (p.VAR_KEYWORD, p.VAR_POSITIONAL):
+                if p.default is inspect.Parameter.empty or p.kind in (p.VAR_KEYWORD, p.VAR_POSITIONAL,
+                                                                       p.KEYWORD_ONLY):
                     continue
                 default = p.default
                 if isinstance(default, list):

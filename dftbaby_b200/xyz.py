@@ -102,3 +102,27 @@ def write_xyz(filename, geometries, title=" ", units="Angstrom", mode="w"):
     """XYZ.write_xyz (XYZ.py:132-150)."""
     with open(filename, mode) as fh:
         fh.write(xyz2txt(geometries, title, units))
+
+
+def read_initial_conditions(filename, units="Angstrom", fragment_id=atomic_number):
+    """XYZ.read_initial_conditions (XYZ.py:235-274): positions, then one velocity line per atom, as
+    ([(Z, (x, y, z)), ...], [(Z, (vx, vy, vz)), ...]); with units="Angstrom" both are divided by the bohr
+    length, as the reference does."""
+    if units not in ("bohr", "Angstrom", "hartree/bohr", ""):
+        raise ValueError("units must be 'Angstrom' or 'bohr', not %r" % units)
+    angs = _bohr_to_angs() if units == "Angstrom" else 1.0
+    with open(filename) as fh:
+        line = fh.readline()
+        try:
+            nat = int(line.split()[0])
+        except (ValueError, IndexError):
+            raise ValueError("Error while reading initial conditions from '%s'" % filename)
+        coords = []
+        for _ in range(nat):
+            w = fh.readline().split()
+            coords.append((fragment_id(w[0]), tuple(float(c) / angs for c in w[1:4])))
+        vels = []
+        for i in range(nat):
+            w = fh.readline().split()
+            vels.append((coords[i][0], tuple(float(c) / angs for c in w[:3])))
+    return coords, vels

@@ -32,7 +32,7 @@ rotation) on stand-in objects, through the same shim.
 
 Usage::
 
-    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda|repulsive|lr_e2e|particle_hole|handler|dftb2_props|xyz]
+    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda|repulsive|lr_e2e|particle_hole|handler|dftb2_props|xyz|md]
 """
 import io
 import os
@@ -329,21 +329,26 @@ def method_source(path, name, after=None):
     """The text of method ``name`` of a DFTBaby source file, dedented and passed through the shim.
     Tabs are expanded to 8 columns (Python 2's rule for mixed indentation) and ``<>`` becomes ``!=``.
     With ``after`` (a regular expression) the search starts at the first line matching it."""
-    import textwrap
     lines = open(path).read().expandtabs(8).splitlines(keepends=True)
     first = 0 if after is None else next(i for i, ln in enumerate(lines) if re.match(after, ln))
     start = next(i for i in range(first, len(lines)) if re.match(r"\s*def %s\(" % name, lines[i]))
     indent = len(lines[start]) - len(lines[start].lstrip())
     end = start + 1
+    in_string = False  # inside a triple-quoted string, whose lines may start at any column
+    body = [lines[start]]
     while end < len(lines):
         ln = lines[end]
-        if ln.strip() and not ln.lstrip().startswith("#") and len(ln) - len(ln.lstrip()) <= indent:
+        if not in_string and ln.strip() and not ln.lstrip().startswith("#") and len(ln) - len(ln.lstrip()) <= indent:
             break
+        # comment lines indented less than the def (trailing section headers) are not part of the method
+        if in_string or not (ln.lstrip().startswith("#") and len(ln) - len(ln.lstrip()) < indent):
+            body.append(ln)
+        if (ln.count('"""') + ln.count("\'\'\'")) % 2 == 1:
+            in_string = not in_string
         end += 1
-    # comment lines indented less than the def (trailing section headers) are not part of the method
-    body = [ln for ln in lines[start:end]
-            if not (ln.lstrip().startswith("#") and len(ln) - len(ln.lstrip()) < indent)]
-    return py2to3(textwrap.dedent("".join(body)).replace("<>", "!="))
+    # remove the def's indentation from every line that has it (string lines may have less)
+    text = "".join(ln[indent:] if ln[:indent].strip() == "" else ln for ln in body)
+    return py2to3(text.replace("<>", "!="))
 
 
 def _reference_methods(path, names, namespace):
@@ -1092,6 +1097,121 @@ def make_xyz(ref_root, rng):
     np.savez_compressed(os.path.join(HERE, "xyz.npz"), **out)
 
 
+DYNAMICS_IN = """5
+C      0.10   -0.05    1.26
+C     -0.02    0.03   -1.27
+H      0.00    1.74    2.34
+H      0.05   -1.75    2.30
+H     -0.04    1.70   -2.36
+  1.0e-4   -2.0e-4    0.5e-4
+ -1.5e-4    1.0e-4   -0.5e-4
+  3.0e-4    0.0e-4    2.0e-4
+ -2.0e-4    1.0e-4    1.0e-4
+  1.0e-4   -3.0e-4   -2.0e-4
+"""
+MD_DRAWS = (0.02, 0.7, 0.01, 0.3, 0.001, 0.9, 0.05, 0.2, 0.4, 0.003, 0.6, 0.08)
+MD_SCENARIOS = {
+    # tag: (MolecularDynamics options, number of states of the scripted PES, restart of the previous run)
+    "E": (dict(initial_state="2", nstates=3, nstep=5, output_step=1, decoherence_correction=1,
+               time_series=["particle-hole charges", "particle-hole charges current", "Lambda2 current", "Lambda2",
+                            "transition charges current"]), 4, False),
+    "E_restart": (dict(initial_state="2", nstates=3, nstep=2, output_step=1, decoherence_correction=1), 4, True),
+    "T": (dict(initial_state="brightest", fragment_excitation=(1, 0, 1, 0), nstates=3, nstep=4, output_step=2,
+               dyn_mode="T", temp=500.0, timecoupling=2.0), 4, False),
+    "S0": (dict(initial_state="0", nstates=0, nstep=3), 2, False),
+}
+
+
+class ScriptedRandom:
+    """The draws of Python's random module (or of a numpy generator) replaced by a fixed list."""
+
+    def __init__(self, draws):
+        self.draws = list(draws)
+
+    def seed(self, *args):
+        pass
+
+    def random(self):
+        return self.draws.pop(0)
+
+
+def make_md(ref_root, rng):
+    """SurfaceHopping.MolecularDynamics (Dynamics/SurfaceHopping.py:23-760) run from DFTBaby's text through the
+    handler methods of Dynamics/dftbaby_handler.py on the scripted PES of tests/golden/fake_pes.py, with scripted
+    hop draws, from the dynamics.in above: every output file and the printed text of four runs (constant energy
+    with decoherence and all time series; its restart; Berendsen thermostat from the brightest state; ground
+    state).  DFTBaby asks for a fragment_excitation tuple also for initial_state='brightest'; the run passes one."""
+    import contextlib
+    sys.path.insert(0, HERE)
+    from fake_pes import FakePES
+    ad = _reference_atomic_data(ref_root)
+    errors = {n: type(n, (Exception,), {}) for n in ("SCFNotConverged", "SCFChargeInconsistency",
+                                                      "ExcitedStatesNotConverged", "ExcitedStatesError")}
+    xyz_ns = {"np": np, "zeros": np.zeros, "atomic_number": ad.atomic_number, "bohr_to_angs": ad.bohr_to_angs}
+    exec(compile(method_source(os.path.join(ref_root, "DFTB", "XYZ.py"), "read_initial_conditions"), "XYZ.py", "exec"),
+         xyz_ns)
+    hsrc = os.path.join(ref_root, "DFTB", "Dynamics", "dftbaby_handler.py")
+    hnames = ("getBrightestState", "getAll_S0", "getAll", "writeTimeSeries", "getAvgParticleHoleCharges",
+              "getParticleHoleChargesSuperposition")
+    hns = dict(np=np, os=os, AtomicData=ad, **errors,
+               XYZ=types.SimpleNamespace(atomlist2vector=lambda al: np.hstack([np.asarray(p, float) for _, p in al])))
+    for n in hnames:
+        exec(compile(method_source(hsrc, n, after=r"class dftbaby_handler"), "dftbaby_handler.py", "exec"), hns)
+    RefHandler = type("dftbaby_handler", (), {n: hns[n] for n in hnames})
+    src = os.path.join(ref_root, "DFTB", "Dynamics", "SurfaceHopping.py")
+    names = ("__init__", "getCenterOfMass", "shiftToCenterOfMass", "momentum", "eliminateTranslation",
+             "myCrossProduct", "angularMomentum", "momentOfInertia", "getAngularVelocity", "eliminateRotation",
+             "getKineticEnergy", "getCoordVerlet", "getVelVerlet", "initializeInterface", "getData",
+             "getLocalDiabatization", "getNewState", "normalizeCoeff", "getUniformlyRescaledVelocities",
+             "getDecoherenceE", "eliminateTransRot", "scaleVelocitiesT", "scaleVelocitiesEconst", "initiateTrajectory",
+             "verlet", "readCoordVel", "restartTrajectory", "writeStep", "writeXYZ", "writeRestart",
+             "writeNACoupling", "writeEnergies", "writeActualEnergies", "writeCoefficients", "writeState",
+             "writeLocalDiabaticEnergies", "writeLocalDiabaticCouplings", "writeTimeSeries")
+    import scipy.linalg as sla
+    out = {"dynamics_in": np.array(DYNAMICS_IN), "draws": np.array(MD_DRAWS)}
+    datas = {nst: handler_data(np.random.default_rng(20261213 + nst), nst=nst) for nst in (2, 4)}
+    for nst, d in datas.items():
+        out.update({"data%d_%s" % (nst, k): v for k, v in d.items()})
+    tmp = tempfile.mkdtemp(prefix="dftbaby_md_")
+    cwd = os.getcwd()
+    try:
+        for tag, (opts, nst, restart) in MD_SCENARIOS.items():
+            run_dir = os.path.join(tmp, tag.split("_")[0])
+            if not restart:
+                os.makedirs(run_dir)
+                open(os.path.join(run_dir, "dynamics.in"), "w").write(DYNAMICS_IN)
+            os.chdir(run_dir)
+            draws = ScriptedRandom(MD_DRAWS)
+            ns = dict(np=np, la=np.linalg, sla=sla, random=draws, AtomicData=ad,
+                      os=types.SimpleNamespace(path=os.path, system=lambda cmd: 0),
+                      XYZ=types.SimpleNamespace(read_initial_conditions=xyz_ns["read_initial_conditions"]))
+
+            def factory(symbols, coordinates, tstep, nstates, charge, sc_threshold=0.001, nst=nst):
+                h = RefHandler()
+                atomlist = [(ad.atomic_number(sy), tuple(x)) for sy, x in zip(symbols, coordinates)]
+                h.dt_nuc, h.nstates, h.sc_threshold, h.Nat = tstep, nstates, sc_threshold, len(atomlist)
+                h.masses, h.pes, h.last_step = np.array(ad.atomlist2masses(atomlist)), FakePES(datas[nst], errors), None
+                return h
+
+            ns["dftbaby_handler"] = types.SimpleNamespace(dftbaby_handler=factory)
+            for n in names:
+                exec(compile(method_source(src, n, after=r"class MolecularDynamics"), "SurfaceHopping.py", "exec"), ns)
+            MD = type("MolecularDynamics", (), {n: ns[n] for n in names})
+            buf = io.StringIO()
+            with contextlib.redirect_stdout(buf):
+                md = MD(**opts)
+                md.verlet()
+            out["md_%s_stdout" % tag] = np.array(buf.getvalue())
+            out["md_%s_files" % tag] = np.array(sorted(os.listdir(".")))
+            for fn in os.listdir("."):
+                out["md_%s_file_%s" % (tag, fn)] = np.array(open(fn).read())
+            os.chdir(cwd)
+    finally:
+        os.chdir(cwd)
+        shutil.rmtree(tmp, ignore_errors=True)
+    np.savez_compressed(os.path.join(HERE, "md.npz"), **out)
+
+
 def make_repulsive(ref_root, rng):
     """RepulsivePotential.__init__ / getVrep (RepulsivePotential.py:17-100, as DFTB2.py:327 builds them: no
     smooth tail) on the shipped H-H, H-C and C-C tables, run from DFTBaby's text: values and first
@@ -1223,6 +1343,8 @@ def main(ref_root, only=None):
             make_dftb2_props(ref_root, np.random.default_rng(20261212))
         if only in (None, "xyz"):
             make_xyz(ref_root, None)
+        if only in (None, "md"):
+            make_md(ref_root, None)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)

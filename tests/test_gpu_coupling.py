@@ -137,3 +137,32 @@ def test_handler_steps_and_ground_state_fallback():
         E2, accel2, coupl2, tdip2, olap2 = h.getAll(x2, 1)
     assert E2[1] > E2[0] and np.allclose(coupl2, -coupl2.T)
     assert np.all(np.abs(np.diag(olap2)) > 0.8)
+
+
+def test_surface_hopping_program(tmp_path, monkeypatch):
+    """MolecularDynamics, DFTBaby's surface-hopping program, for three steps on the device handler: the input
+    file is read, every step writes its lines, the electronic populations stay normalised and the restart file
+    holds the last geometry."""
+    import contextlib
+    import io
+    native.load()
+    from dftbaby_b200.surface_hopping import MolecularDynamics
+    monkeypatch.chdir(tmp_path)
+    al = geometry.polyene(6, sigma=0.03, seed=2)
+    v = 2.0e-4 * np.random.default_rng(3).standard_normal((len(al), 3))
+    with open("dynamics.in", "w") as fh:
+        fh.write("%d\n" % len(al))
+        for Z, p in al:
+            fh.write("%s %.10f %.10f %.10f\n" % ({6: "C", 1: "H"}[Z], *p))
+        for row in v:
+            fh.write("%.10e %.10e %.10e\n" % tuple(row))
+    md = MolecularDynamics(initial_state="1", nstates=2, nstep=3, nuclear_step=0.2, rng=np.random.default_rng(0),
+                           pes_options=dict(long_range_correction=1, diag_conv=1e-8))
+    with contextlib.redirect_stdout(io.StringIO()):
+        md.verlet()
+    state = np.loadtxt("state.dat")
+    assert state.shape == (4, 2) and set(state[:, 1]) <= {0.0, 1.0, 2.0}
+    assert np.allclose(np.loadtxt("coeff_norm.dat")[:, 1], 1.0, atol=1e-6)
+    E = np.loadtxt("curr_energy.dat")
+    assert np.all(np.isfinite(E)) and np.abs(E[:, 3] - E[0, 3]).max() < 5e-3
+    assert open("dynamics.in0").readline().strip() == str(len(al))
