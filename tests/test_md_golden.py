@@ -97,3 +97,22 @@ def test_options_checked():
         MolecularDynamics(initial_state="bright")
     md = MolecularDynamics(initial_state="brightest", nstates=2)  # no fragment tuple needed here
     assert md.state == "brightest" and md.nstates == 3
+
+
+def test_program_options(tmp_path, monkeypatch):
+    """python -m dftbaby_b200.surface_hopping: MolecularDynamics options from [SurfaceHopping] and the command
+    line, electronic-structure options from [DFTBaby] passed on to the PES."""
+    from dftbaby_b200 import surface_hopping
+    monkeypatch.chdir(tmp_path)
+    (tmp_path / "dftbaby.cfg").write_text("[SurfaceHopping]\nnstates = 4\nnstep = 50\n"
+                                          "[DFTBaby]\nlong_range_correction = 0\nscf_conv = 1e-9\n")
+    seen = {}
+    monkeypatch.setattr(surface_hopping.MolecularDynamics, "verlet", lambda self: seen.setdefault("md", self))
+    assert surface_hopping.main(["--nuclear_step=0.25", "--initial_state=brightest", "--dyn_mode=T",
+                                 "--diag_conv=1e-7"]) == 0
+    md = seen["md"]
+    assert (md.nstates, md.nstep, md.state, md.mode) == (5, 50, "brightest", "T")
+    assert abs(md.tstep - 0.25 * md.fs_to_au) < 1e-12
+    po = md.pes_options
+    assert po["long_range_correction"] == 0 and po["scf_conv"] == 1e-9 and po["diag_conv"] == 1e-7
+    assert "nstates" not in po and "device" not in po
