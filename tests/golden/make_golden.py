@@ -1209,6 +1209,19 @@ def make_md(ref_root, rng):
     finally:
         os.chdir(cwd)
         shutil.rmtree(tmp, ignore_errors=True)
+    # HarmonicApproximation.dynamics_in_format (Dynamics/HarmonicApproximation.py:239-253), the writer of
+    # random_velocities.py, on the atoms of dynamics.in with random momenta
+    fns = {"XYZ": types.SimpleNamespace(vector2atomlist=lambda x, al: [(Z, tuple(x[3 * i:3 * i + 3]))
+                                                                       for i, (Z, _) in enumerate(al)]),
+           "AtomicData": ad}
+    exec(compile(method_source(os.path.join(ref_root, "DFTB", "Dynamics", "HarmonicApproximation.py"),
+                               "dynamics_in_format"), "HarmonicApproximation.py", "exec"), fns)
+    lines = DYNAMICS_IN.splitlines()
+    atomlist = [(ad.atomic_number(w.split()[0]), tuple(float(c) for c in w.split()[1:4])) for w in lines[1:6]]
+    q = np.hstack([p for _, p in atomlist]) + 0.01
+    mom = np.random.default_rng(20261214).random(3 * len(atomlist)) - 0.5
+    out.update(dyn_in_Z=np.array([Z for Z, _ in atomlist]), dyn_in_q=q, dyn_in_p=mom,
+               dyn_in_text=np.array(fns["dynamics_in_format"](atomlist, q, mom, "")))
     np.savez_compressed(os.path.join(HERE, "md.npz"), **out)
 
 

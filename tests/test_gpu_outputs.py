@@ -101,3 +101,22 @@ def test_command_line(tmp_path, monkeypatch):
     assert np.loadtxt("particle_hole_charges_1.chrg").shape == (len(al), 2)
     assert not os.path.exists("transition_charges.dat")
     assert os.path.exists("grad.xyz")
+
+
+def test_dftb2_program(tmp_path, monkeypatch, capsys):
+    """python -m dftbaby_b200.dftb2 mol.xyz (DFTB2.py:2635-2700): one total energy per geometry."""
+    native.load()
+    from dftbaby_b200 import xyz
+    from dftbaby_b200.dftb2 import DFTB2, main
+    monkeypatch.chdir(tmp_path)
+    geoms = [geometry.polyene(4, sigma=0.02, seed=s) for s in (1, 2)]
+    xyz.write_xyz("mol.xyz", geoms, title="charge=0")
+    assert main(["mol.xyz", "--long_range_correction=0"]) == 0
+    lines = [ln for ln in capsys.readouterr().out.splitlines() if ln.startswith("TOTAL ENERGY")]
+    got = [float(ln.split(":")[1].split()[0]) for ln in lines]
+    ref = []
+    for al in xyz.read_xyz("mol.xyz"):
+        d = DFTB2(al, long_range_correction=0)
+        d.setGeometry(al)
+        ref.append(d.getEnergy())
+    assert len(got) == 2 and np.allclose(got, ref, atol=2e-7)

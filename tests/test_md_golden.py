@@ -116,3 +116,31 @@ def test_program_options(tmp_path, monkeypatch):
     po = md.pes_options
     assert po["long_range_correction"] == 0 and po["scf_conv"] == 1e-9 and po["diag_conv"] == 1e-7
     assert "nstates" not in po and "device" not in po
+
+
+def test_dynamics_in_writer_against_reference():
+    from dftbaby_b200.random_velocities import dynamics_in_format
+    atomlist = [(int(Z), (0.0, 0.0, 0.0)) for Z in G["dyn_in_Z"]]
+    assert dynamics_in_format(atomlist, G["dyn_in_q"], G["dyn_in_p"]) == str(G["dyn_in_text"])
+
+
+def test_random_velocities_program(tmp_path, capsys):
+    """random_velocities.py: the last geometry of the xyz file, velocities whose kinetic energy is
+    1/2 nvib kB T, in the dynamics.in format the surface-hopping program reads."""
+    from dftbaby_b200 import random_velocities, xyz
+    from dftbaby_b200.params import raw_params
+    open(tmp_path / "mol.xyz", "w").write("2\nfirst\nH 0 0 0\nH 0 0 0.74\n"
+                                          "5\nsecond\nC 0 0 0\nH 0.63 0.63 0.63\nH -0.63 -0.63 0.63\n"
+                                          "H -0.63 0.63 -0.63\nH 0.63 -0.63 -0.63\n")
+    assert random_velocities.main([str(tmp_path / "mol.xyz"), str(tmp_path / "dynamics.in"), "--temperature=300",
+                                   "--seed=4"]) == 0
+    assert "temperature: 300.00000 K" in capsys.readouterr().out
+    coords, vels = xyz.read_initial_conditions(str(tmp_path / "dynamics.in"), units="bohr")
+    last = xyz.read_xyz(str(tmp_path / "mol.xyz"))[-1]
+    assert [Z for Z, _ in coords] == [Z for Z, _ in last]
+    assert np.allclose([p for _, p in coords], [p for _, p in last], atol=1e-14)
+    raw = raw_params()
+    m = np.array([float(raw["atom/%d/mass" % Z]) for Z, _ in coords])
+    v = np.array([v for _, v in vels])
+    ekin = 0.5 * np.sum(m[:, None] * v ** 2)
+    assert abs(ekin / (0.5 * (3 * 5 - 6) * float(raw["const/kBoltzmann"])) - 300.0) < 1e-6
