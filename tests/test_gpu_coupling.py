@@ -99,70 +99,3 @@ def test_pes_interface():
     coupl, olap = pes.getScalarCouplings()
     assert np.all(np.diag(olap) > 0.9) and np.allclose(coupl, -coupl.T)
     assert np.allclose(pes.getEnergy_S0(x1)[0], pes.getEnergies(x1)[0], atol=1e-8)
-
-
-def test_handler_steps_and_ground_state_fallback():
-    """dftbaby_handler on the device PES: a good step, then an excited-state solve that cannot converge
-    (one Davidson iteration at 1e-14), which sends the step to the ground state with the ground-state
-    gradient of the converged SCC (dftbaby_handler.py:106-143), then a good step again."""
-    import contextlib
-    import io
-    native.load()
-    from dftbaby_b200.gradients import Gradients
-    from dftbaby_b200.handler import dftbaby_handler
-    from dftbaby_b200.lr_tddftb import LR_TDDFTB
-    al = geometry.polyene(6, sigma=0.03, seed=2)
-    symbols = ["C" if Z == 6 else "H" for Z, _ in al]
-    x0 = np.array([p for _, p in al])
-    rng = np.random.default_rng(5)
-    x1 = x0 + 0.005 * rng.standard_normal(x0.shape)
-    x2 = x1 + 0.005 * rng.standard_normal(x0.shape)
-    h = dftbaby_handler(symbols, x0, 20.0, 3, 0.0, long_range_correction=1, diag_conv=1e-8)
-    with contextlib.redirect_stdout(io.StringIO()):
-        assert h.getBrightestState(x0) in (1, 2)
-        E, accel, coupl, tdip, olap = h.getAll(x0, 1)
-        assert accel.shape == (len(al), 3) and np.allclose(coupl, -coupl.T) and tdip.shape == (3, 3, 3)
-        h.pes.options.update(diag_maxiter=1, diag_conv=1e-14)
-        E1, accel1, coupl1, tdip1, olap1 = h.getAll(x1, 1)
-    assert np.all(E1 == E1[0]) and not coupl1.any() and not tdip1.any() and np.array_equal(olap1, np.eye(3))
-    assert h.pes.tddftb.XmY is None
-    td = LR_TDDFTB([(Z, tuple(p)) for (Z, _), p in zip(al, x1)], long_range_correction=1)
-    td.setGeometry([(Z, tuple(p)) for (Z, _), p in zip(al, x1)])
-    E0 = float(td.dftb2.getEnergy())
-    g0 = np.sum(Gradients(td).gradient(I=0), axis=0)
-    assert abs(E1[0] - E0) < 1e-8
-    assert np.abs(-accel1.reshape(-1) * h.masses - g0).max() < 1e-7
-    h.pes.options.update(diag_maxiter=50, diag_conv=1e-8)
-    with contextlib.redirect_stdout(io.StringIO()):
-        E2, accel2, coupl2, tdip2, olap2 = h.getAll(x2, 1)
-    assert E2[1] > E2[0] and np.allclose(coupl2, -coupl2.T)
-    assert np.all(np.abs(np.diag(olap2)) > 0.8)
-
-
-def test_surface_hopping_program(tmp_path, monkeypatch):
-    """MolecularDynamics, DFTBaby's surface-hopping program, for three steps on the device handler: the input
-    file is read, every step writes its lines, the electronic populations stay normalised and the restart file
-    holds the last geometry."""
-    import contextlib
-    import io
-    native.load()
-    from dftbaby_b200.surface_hopping import MolecularDynamics
-    monkeypatch.chdir(tmp_path)
-    al = geometry.polyene(6, sigma=0.03, seed=2)
-    v = 2.0e-4 * np.random.default_rng(3).standard_normal((len(al), 3))
-    with open("dynamics.in", "w") as fh:
-        fh.write("%d\n" % len(al))
-        for Z, p in al:
-            fh.write("%s %.10f %.10f %.10f\n" % ({6: "C", 1: "H"}[Z], *p))
-        for row in v:
-            fh.write("%.10e %.10e %.10e\n" % tuple(row))
-    md = MolecularDynamics(initial_state="1", nstates=2, nstep=3, nuclear_step=0.2, rng=np.random.default_rng(0),
-                           pes_options=dict(long_range_correction=1, diag_conv=1e-8))
-    with contextlib.redirect_stdout(io.StringIO()):
-        md.verlet()
-    state = np.loadtxt("state.dat")
-    assert state.shape == (4, 2) and set(state[:, 1]) <= {0.0, 1.0, 2.0}
-    assert np.allclose(np.loadtxt("coeff_norm.dat")[:, 1], 1.0, atol=1e-6)
-    E = np.loadtxt("curr_energy.dat")
-    assert np.all(np.isfinite(E)) and np.abs(E[:, 3] - E[0, 3]).max() < 5e-3
-    assert open("dynamics.in0").readline().strip() == str(len(al))
