@@ -835,12 +835,34 @@ class LR_TDDFTB:
         self.active_virtual_orbs = self.virtual_orbs[np.argsort(orbe[self.virtual_orbs])[:nr_active_virt]]
         self.nocc, self.nvirt = len(self.active_occupied_orbs), len(self.active_virtual_orbs)
 
-    def getEnergies(self, nr_active_occ=None, nr_active_virt=None, oszis="Dipoles", response_method="Casida",
-                    multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5, diag_maxiter=50,
-                    diag_check=0, diag_L2threshold=0.0, **scf_opts):
+    def setActiveLMOrbitals(self, nr_active_occ=1000, nr_active_virt=1000, select_lm=((1, 0),)):
+        """LR_TDDFTB.py:125-166: only molecular orbitals with weight (sum of squared coefficients above 1e-15)
+        on atomic orbitals whose (l, m) is in select_lm, then the energy window within them."""
+        d = self.dftb2
+        lm_idx, iao = [], 0
+        for Z, _ in d.atomlist:
+            for (n, l, m) in d.valorbs[Z]:
+                if (l, m) in select_lm:
+                    lm_idx.append(iao)
+                iao += 1
+        orbs = d.getKSCoefficients()
+        is_lm = np.sum(np.abs(orbs[np.array(lm_idx, dtype=int), :]) ** 2, axis=0) > 1.0e-15
+        f, orbe = d.getOccupation(), d.getKSEnergies()
+        self.occupied_orbs = np.where((f > 0.1) & is_lm)[0]
+        self.virtual_orbs = np.where((f <= 0.1) & is_lm)[0]
+        self.active_occupied_orbs = self.occupied_orbs[np.argsort(orbe[self.occupied_orbs])[::-1][:nr_active_occ][::-1]]
+        self.active_virtual_orbs = self.virtual_orbs[np.argsort(orbe[self.virtual_orbs])[:nr_active_virt]]
+        self.nocc, self.nvirt = len(self.active_occupied_orbs), len(self.active_virtual_orbs)
+
+    def getEnergies(self, nr_active_occ=None, nr_active_virt=None, select_lm=None, oszis="Dipoles",
+                    response_method="Casida", multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5,
+                    diag_maxiter=50, diag_check=0, diag_L2threshold=0.0, **scf_opts):
         d = self.dftb2
         self.en0 = d.getEnergy(**scf_opts)
-        self.setActiveOrbitals(nr_active_occ, nr_active_virt)
+        if select_lm is not None:
+            self.setActiveLMOrbitals(nr_active_occ, nr_active_virt, select_lm=[tuple(lm) for lm in select_lm])
+        else:
+            self.setActiveOrbitals(nr_active_occ, nr_active_virt)
         self.multiplicity = multiplicity
         orbs, S = d.getKSCoefficients(), d.getOverlapMatrix()
         co, cv = orbs[:, self.active_occupied_orbs], orbs[:, self.active_virtual_orbs]

@@ -105,6 +105,14 @@ def test_select_lm_active_space():
     sel = np.r_[td_pi.active_occupied_orbs, td_pi.active_virtual_orbs]
     assert np.all(w[sel] > 1e-3) and np.all(np.delete(w, sel) < 1e-15)
     assert np.all(np.isfinite(Om_pi)) and np.all(Om_pi > 0) and np.all(np.isfinite(f_pi))
+    # the same pi-only Casida problem on the CPU oracle
+    from oracle import dftb_oracle as O
+    o = O.LR_TDDFTB(al, long_range_correction=1)
+    o.setGeometry(al)
+    Om_o, f_o = o.getEnergies(select_lm=[(1, 0)])
+    assert np.array_equal(o.active_occupied_orbs, td_pi.active_occupied_orbs)
+    assert np.abs(np.sort(Om_pi) - np.sort(Om_o)).max() < 1e-8
+    assert np.abs(np.sum(f_pi) - np.sum(f_o)) < 1e-6
 
 
 def test_saved_charges_seed_the_next_scc(tmp_path):

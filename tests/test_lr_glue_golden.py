@@ -106,3 +106,30 @@ def test_has_active_space():
     assert td.hasActiveSpace()
     td.setActiveOrbitals()
     assert not td.hasActiveSpace()
+
+
+def test_oracle_lm_active_orbitals_against_reference():
+    """The oracle's restatement of setActiveLMOrbitals, pinned to the same DFTBaby run."""
+    from oracle import dftb_oracle as O
+    d = types.SimpleNamespace(atomlist=[(int(Z), tuple(p)) for Z, p in zip(G["lm_Z"], G["lm_pos"])],
+                              valorbs=O.Parametrization([1, 6]).valorbs, getKSCoefficients=lambda: G["lm_orbs"],
+                              getOccupation=lambda: G["f"], getKSEnergies=lambda: G["orbe"])
+    for tag, sel in (("pz", [(1, 0)]), ("s_pz", [(0, 0), (1, 0)])):
+        o = O.LR_TDDFTB.__new__(O.LR_TDDFTB)
+        o.dftb2 = d
+        o.setActiveLMOrbitals(nr_active_occ=2, nr_active_virt=3, select_lm=sel)
+        assert np.array_equal(o.active_occupied_orbs, G["lm_%s_active_occ" % tag])
+        assert np.array_equal(o.active_virtual_orbs, G["lm_%s_active_virt" % tag])
+        assert np.array_equal(o.occupied_orbs, G["lm_%s_occupied" % tag])
+
+
+def test_oracle_pi_only_casida_on_a_planar_polyene():
+    """select_lm=[(1,0)] on planar C8H10 keeps the 4 + 4 pi orbitals; the full Casida matrix of the
+    16 pi -> pi* excitations has positive roots."""
+    from dftbaby_b200 import geometry
+    from oracle import dftb_oracle as O
+    al = geometry.polyene(8)
+    o = O.LR_TDDFTB(al, long_range_correction=1)
+    o.setGeometry(al)
+    Om, f = o.getEnergies(select_lm=[(1, 0)])
+    assert (o.nocc, o.nvirt) == (4, 4) and len(Om) == 16 and np.all(Om > 0)
