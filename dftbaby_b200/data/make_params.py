@@ -65,6 +65,9 @@ def main(ref_root):
     ea = _dict_literal(atomic, "electron_affinities_eV")
     hartree_to_eV = float(re.search(r"^hartree_to_eV\s*=\s*([0-9.eE+-]+)", atomic, re.M).group(1))
     out["const/hartree_to_eV"] = np.array(hartree_to_eV)
+    # wavenumbers (cm^-1) = energy in Hartree * hartree_to_wavenumbers (AtomicData.py:4)
+    out["const/hartree_to_wavenumbers"] = np.array(
+        float(re.search(r"^hartree_to_wavenumbers\s*=\s*([0-9.eE+-]+)", atomic, re.M).group(1)))
     # wavelength in nm = hartree_to_nm / energy in Hartree (AtomicData.py:3)
     out["const/hartree_to_nm"] = np.array(
         float(re.search(r"^hartree_to_nm\s*=\s*([0-9.eE+-]+)", atomic, re.M).group(1)))

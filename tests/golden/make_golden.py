@@ -32,7 +32,7 @@ rotation) on stand-in objects, through the same shim.
 
 Usage::
 
-    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda|repulsive|lr_e2e|particle_hole|handler|dftb2_props|xyz|md]
+    python tests/golden/make_golden.py /path/to/DFTBaby [--only=core|couplings|mulliken|sk_python|scc|lr_glue|lambda|repulsive|lr_e2e|particle_hole|handler|dftb2_props|xyz|md|initial_conditions]
 """
 import io
 import os
@@ -1225,6 +1225,123 @@ def make_md(ref_root, rng):
     np.savez_compressed(os.path.join(HERE, "md.npz"), **out)
 
 
+IC_XYZ = """6
+ethene
+C      0.000000    0.000000    0.667480
+C      0.000000    0.000000   -0.667480
+H      0.000000    0.922832    1.237695
+H      0.000000   -0.922832    1.237695
+H      0.000000    0.922832   -1.237695
+H      0.000000   -0.922832   -1.237695
+"""
+IC_SEED = 20261215
+
+
+def spring_hessian(x, k=0.5):
+    """Cartesian Hessian of pair springs k/2 (r_ij - r_ij(0))^2 at their rest lengths: sum of k u u^T blocks,
+    with exactly the translations and rotations as zero modes."""
+    r = np.asarray(x, dtype=np.float64).reshape(-1, 3)
+    n = len(r)
+    H = np.zeros((3 * n, 3 * n))
+    for i in range(n):
+        for j in range(i + 1, n):
+            u = r[i] - r[j]
+            u /= np.linalg.norm(u)
+            b = k * np.outer(u, u)
+            H[3 * i:3 * i + 3, 3 * i:3 * i + 3] += b
+            H[3 * j:3 * j + 3, 3 * j:3 * j + 3] += b
+            H[3 * i:3 * i + 3, 3 * j:3 * j + 3] -= b
+            H[3 * j:3 * j + 3, 3 * i:3 * i + 3] -= b
+    return H
+
+
+def spring_gradient(x, x_rest, k=0.5):
+    """Gradient of sum_ij k/2 (r_ij - r_ij(rest))^2 at the flat coordinates x."""
+    r, r0 = np.asarray(x, float).reshape(-1, 3), np.asarray(x_rest, float).reshape(-1, 3)
+    diff = r[:, None] - r[None]
+    d = np.linalg.norm(diff, axis=-1) + np.eye(len(r))
+    d0 = np.linalg.norm(r0[:, None] - r0[None], axis=-1) + np.eye(len(r))
+    return (k * ((d - d0) / d)[..., None] * diff).sum(axis=1).reshape(-1)
+
+
+def make_initial_conditions(ref_root, rng):
+    """The initial_conditions.py program (Dynamics/initial_conditions.py) run from DFTBaby's text with the
+    functions of HarmonicApproximation.py, GaussianWavepacket.Gaussian.sample_wigner and MolecularCoords
+    (their Python 2 integer divisions made explicit), on ethene with a pair-spring Hessian; the sampler is
+    numpy's legacy generator, reseeded with a fixed seed where DFTBaby uses the clock.  Also
+    numerical_hessian_G on the spring energy's analytic gradient."""
+    import contextlib
+    ad = _reference_atomic_data(ref_root)
+    dyn = os.path.join(ref_root, "DFTB", "Dynamics")
+    xyz_ns = {"np": np, "zeros": np.zeros, "atom_names": ad.atom_names, "atomic_number": ad.atomic_number,
+              "bohr_to_angs": ad.bohr_to_angs}
+    for n in ("read_xyz_it", "read_xyz", "write_xyz", "xyz2txt", "_append_xyz2txt", "atomlist2vector",
+              "vector2atomlist"):
+        exec(compile(method_source(os.path.join(ref_root, "DFTB", "XYZ.py"), n), "XYZ.py", "exec"), xyz_ns)
+    mol_ns = {"np": np, "zeros": np.zeros}
+    for n in ("center_of_mass", "shift_to_com", "inertial_tensor"):
+        src = method_source(os.path.join(ref_root, "DFTB", "Modeling", "MolecularCoords.py"), n)
+        exec(compile(src.replace("len(pos)/3", "len(pos)//3"), "MolecularCoords.py", "exec"), mol_ns)
+
+    class FixedSeedRandom:
+        def seed(self, _):
+            np.random.seed(IC_SEED)
+
+        def multivariate_normal(self, *args):
+            return np.random.multivariate_normal(*args)
+
+    ha_ns = {"np": np, "la": np.linalg, "AtomicData": ad, "join": os.path.join,
+             "XYZ": types.SimpleNamespace(**{k: xyz_ns[k] for k in ("vector2atomlist",)}),
+             "MolCo": types.SimpleNamespace(**{k: mol_ns[k] for k in ("shift_to_com", "inertial_tensor")})}
+    gw_ns = {"np": np, "la": np.linalg, "random": FixedSeedRandom(), "time": types.SimpleNamespace(time=lambda: 0.0)}
+    exec(compile(method_source(os.path.join(dyn, "GaussianWavepacket.py"), "sample_wigner", after=r"class Gaussian")
+                 .replace("dim = N/2", "dim = N//2"), "GaussianWavepacket.py", "exec"), gw_ns)
+
+    class Gaussian:
+        def __init__(self, A, B):
+            self.A, self.B = A, B
+
+        sample_wigner = gw_ns["sample_wigner"]
+
+    ha_ns["GaussianWavepacket"] = types.SimpleNamespace(Gaussian=Gaussian)
+    for n in ("numerical_hessian_G", "expected_zero_modes", "vibrational_analysis", "wigner_distribution",
+              "initial_conditions_wigner", "dynamics_in_format", "qmf3_in_format", "save_initial_conditions"):
+        src = method_source(os.path.join(dyn, "HarmonicApproximation.py"), n)
+        exec(compile(src.replace("Nat = len(x0) / 3", "Nat = len(x0) // 3"), "HarmonicApproximation.py", "exec"),
+             ha_ns)
+    # the program: the block under `if __name__ == "__main__":`
+    import textwrap
+    lines = open(os.path.join(dyn, "initial_conditions.py")).read().expandtabs(8).splitlines(keepends=True)
+    start = next(i for i, ln in enumerate(lines) if ln.startswith("if __name__"))
+    block = py2to3(textwrap.dedent("".join(lines[start + 1:])))
+    tmp = tempfile.mkdtemp(prefix="dftbaby_ic_")
+    open(os.path.join(tmp, "mol.xyz"), "w").write(IC_XYZ)
+    atomlist = xyz_ns["read_xyz"](os.path.join(tmp, "mol.xyz"))[-1]
+    x0 = xyz_ns["atomlist2vector"](atomlist)
+    hess = spring_hessian(x0)
+    np.savetxt(os.path.join(tmp, "hessian.dat"), hess)
+    os.makedirs(os.path.join(tmp, "out"))
+    prog_ns = {"HarmonicApproximation": types.SimpleNamespace(**ha_ns), "AtomicData": ad, "np": np,
+               "XYZ": types.SimpleNamespace(**xyz_ns), "__name__": "__main__"}
+    argv = sys.argv
+    sys.argv = ["initial_conditions.py", os.path.join(tmp, "mol.xyz"), os.path.join(tmp, "hessian.dat"),
+                "--Nsample=4", "--outdir=" + os.path.join(tmp, "out"), "--power_wigner=0.8"]
+    buf = io.StringIO()
+    try:
+        with contextlib.redirect_stdout(buf):
+            exec(compile(block, "initial_conditions.py", "exec"), prog_ns)
+    finally:
+        sys.argv = argv
+    out = {"hess": hess, "stdout": np.array(buf.getvalue().replace(tmp, "<tmp>"))}
+    for fn in sorted(os.listdir(os.path.join(tmp, "out"))):
+        out["file_" + fn] = np.array(open(os.path.join(tmp, "out", fn)).read())
+    # numerical Hessian of the spring energy from its analytic gradient, away from the rest geometry
+    with contextlib.redirect_stdout(io.StringIO()):
+        out["numerical_hessian"] = ha_ns["numerical_hessian_G"](lambda x: spring_gradient(x, x0), x0 + 0.01)
+    shutil.rmtree(tmp, ignore_errors=True)
+    np.savez_compressed(os.path.join(HERE, "initial_conditions.npz"), **out)
+
+
 def make_repulsive(ref_root, rng):
     """RepulsivePotential.__init__ / getVrep (RepulsivePotential.py:17-100, as DFTB2.py:327 builds them: no
     smooth tail) on the shipped H-H, H-C and C-C tables, run from DFTBaby's text: values and first
@@ -1358,6 +1475,8 @@ def main(ref_root, only=None):
             make_xyz(ref_root, None)
         if only in (None, "md"):
             make_md(ref_root, None)
+        if only in (None, "initial_conditions"):
+            make_initial_conditions(ref_root, None)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)

@@ -173,3 +173,22 @@ def test_dftb2_program(tmp_path, monkeypatch, capsys):
         d.setGeometry(al)
         ref.append(d.getEnergy())
     assert len(got) == 2 and np.allclose(got, ref, atol=2e-7)
+
+
+def test_ground_state_hessian():
+    """Central differences of the analytic ground-state gradient (HarmonicApproximation.numerical_hessian_G):
+    symmetric, and a rigid translation of the molecule changes no force (rows sum to zero per direction)."""
+    import contextlib
+    import io
+    native.load()
+    from dftbaby_b200.initial_conditions import ground_state_hessian
+    al = geometry.polyene(2, sigma=0.02, seed=9)
+    with contextlib.redirect_stdout(io.StringIO()):
+        H = ground_state_hessian(al, h=1.0e-4, long_range_correction=1)
+    n = 3 * len(al)
+    assert H.shape == (n, n) and np.allclose(H, H.T)
+    for c in range(3):
+        t = np.zeros(n)
+        t[c::3] = 1.0
+        assert np.abs(H @ t).max() < 1e-3
+    assert np.abs(H).max() > 0.1  # bond stretches are stiff
