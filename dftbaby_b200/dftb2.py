@@ -503,7 +503,6 @@ def main(argv=None):
     if len(args) < 1:
         print(usage)
         return -1
-    options.pop("device", None)
     kwds = extract_keywords_xyz(args[0])
     structures = read_xyz(args[0])
     dftb2 = DFTB2(structures[0], **options)

@@ -794,7 +794,6 @@ def main(argv=None):
     if len(args) < 1:
         print(USAGE)
         return -1
-    options.pop("device", None)
     xyz_file = args[0]
     atomlist = read_xyz(xyz_file)[0]
     kwds = extract_keywords_xyz(xyz_file)

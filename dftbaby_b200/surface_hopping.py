@@ -631,8 +631,7 @@ def main(argv=None):
     pes_options = {}
     for f in (DFTB2.__init__, DFTB2.runSCC, LR_TDDFTB.getEnergies):
         pes_options.update(parser.parse_args(f, argv)[0])
-    for k in ("device", "nstates"):
-        pes_options.pop(k, None)
+    pes_options.pop("nstates", None)  # the number of states is the program's own option
     md = MolecularDynamics(**md_options, pes_options=pes_options)
     md.verlet()
     return 0

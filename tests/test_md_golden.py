@@ -115,7 +115,7 @@ def test_program_options(tmp_path, monkeypatch):
     assert abs(md.tstep - 0.25 * md.fs_to_au) < 1e-12
     po = md.pes_options
     assert po["long_range_correction"] == 0 and po["scf_conv"] == 1e-9 and po["diag_conv"] == 1e-7
-    assert "nstates" not in po and "device" not in po
+    assert "nstates" not in po and po["device"] is None
 
 
 def test_dynamics_in_writer_against_reference():
