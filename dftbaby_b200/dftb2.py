@@ -101,6 +101,25 @@ class DFTB2(object):
             raise ValueError("only erf switching is implemented")
         if nr_unpaired_electrons != 0:
             raise ValueError("open-shell singlets are not implemented")
+        if use_symmetry:
+            raise ValueError("point-group symmetry (use_symmetry > 0) is not supported here")
+        # DFTBaby's other constructor options (DFTB2.py:62-71): those that change the result are accepted at
+        # their defaults only; scratch_dir, cpks_solver and the cavity / QM-MM / tuning companions have no
+        # effect without them.  Unknown names are an error, as for DFTBaby's constructor.
+        off = dict(point_charges_xyz=None, onsite_correction=0, tune_range_radius=0, reppot_scaling=1.0,
+                   mulliken_dipoles=0, dispersion_correction=None, qmmm_partitioning=None,
+                   periodic_force_field=None, cavity_radius=0.0)
+        inert = {"qmmm_embedding", "cavity_force_constant", "save_tuning_curve", "scratch_dir", "cpks_solver",
+                 "reppot_paths"}
+        for k, v in opts.items():
+            if k in off:
+                if v != off[k]:
+                    raise ValueError("%s=%r is not supported here (only %r)" % (k, v, off[k]))
+            elif k == "reppot_paths":
+                if v not in (None, "[]", [], ()):
+                    raise ValueError("additional repulsive potentials (reppot_paths) are not supported here")
+            elif k not in inert:
+                raise TypeError("DFTB2() got an unexpected keyword argument %r" % k)
         self.parameter_set = parameter_set
         self.verbose = verbose
         self.distance_cutoff = distance_cutoff

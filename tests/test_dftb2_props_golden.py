@@ -47,3 +47,20 @@ def test_charge_guess_balancing_and_set_charge_against_reference(capsys):
     assert d.Nelec_val == float(G["nelec_empty"])
     assert capsys.readouterr().out == str(G["setcharge_text_empty"])
 
+
+
+def test_options_off_the_path_are_refused():
+    """DFTBaby's constructor options that would change the result are accepted at their defaults only; unknown
+    names raise TypeError as DFTBaby's constructor does.  All checks come before the device is touched."""
+    import pytest
+    from dftbaby_b200.native import NativeUnavailable
+    al = [(1, (0.0, 0.0, 0.0)), (1, (0.0, 0.0, 1.4))]
+    for bad in (dict(mulliken_dipoles=1), dict(point_charges_xyz="pc.xyz"), dict(dispersion_correction=1),
+                dict(use_symmetry=1), dict(reppot_paths="['x.py']"), dict(reppot_scaling=0.9)):
+        with pytest.raises(ValueError):
+            DFTB2(al, **bad)
+    with pytest.raises(TypeError):
+        DFTB2(al, mulliken_dipole=0)
+    # defaults and inert options get as far as the device
+    with pytest.raises(NativeUnavailable):
+        DFTB2(al, mulliken_dipoles=0, scratch_dir="/tmp", cpks_solver="iterative", reppot_paths="[]")
