@@ -368,6 +368,10 @@ class LR_TDDFTB:
         self.Irreps = [""] * len(self.Omega)
         ev[3].record()
         if getattr(d, "verbose", 0) > 0:
+            # DFTBaby calls determineActiveSpace after every iterative solve; without verbose output it has
+            # no effect, so it runs here only to print its report
+            if nstates is not None:
+                self.determineActiveSpace()
             self._writeExcitations()
         return self.Omega, self.oscillator_strength
 
@@ -602,7 +606,24 @@ class LR_TDDFTB:
             occ_mins.append(self.active_occupied_orbs[np.min(occ)])
             virt_maxs.append(self.active_virtual_orbs[np.max(virt)])
         HOMO = self.occupied_orbs.max()
-        return int(HOMO - min(occ_mins) + 1), int(max(virt_maxs) - HOMO)
+        nr_active_occ, nr_active_virt = int(HOMO - min(occ_mins) + 1), int(max(virt_maxs) - HOMO)
+        if getattr(self.dftb2, "verbose", 0) > 0:
+            Nst = C.shape[0]
+            print("")
+            print("Active Space")
+            print("============")
+            for n in range(Nst):
+                print("State %3d: contains excitations from window  occ %3d - virt %3d" % (n + 1, occ_mins[n],
+                                                                                          virt_maxs[n]))
+            print("")
+            print("The suggested active space for describing the lowest %d states consists of" % Nst)
+            print("the highest %d occupied and the lowest %d virtual orbitals." % (nr_active_occ, nr_active_virt))
+            print("This active space accounts for %2.7f of the total probability for each state." % (1.0 - threshold))
+            print("You should check that the active space contains all neighbouring (almost) degenerate orbitals.")
+            print("Dimension of active space: %d" % (nr_active_occ * nr_active_virt))
+            print("Dimension of  full  space: %d" % (len(self.occupied_orbs) * len(self.virtual_orbs)))
+            print("")
+        return nr_active_occ, nr_active_virt
 
     def TransitionChargesState(self, I):
         """LR_TDDFTB.TransitionChargesState (LR_TDDFTB.py:900-908): q_A = sum_ia C_I,ia q_A^ia (numpy, Nat)."""

@@ -728,6 +728,13 @@ def make_lr_glue(ref_root, rng):
     out["osc"] = r.getOscillatorStrengths()
     out["active_space_1e-5"] = np.array(r.determineActiveSpace())
     out["active_space_1e-2"] = np.array(r.determineActiveSpace(threshold=1e-2))
+    import contextlib
+    dftb2.verbose = 1
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        r.determineActiveSpace(threshold=1e-2)
+    dftb2.verbose = 0
+    out["active_space_text"] = np.array(buf.getvalue())
     out["tq_state_1"] = r.TransitionChargesState(1)
     # setActiveLMOrbitals on a planar-like C3H2 layout: the MO coefficients split into blocks over the p_z, the
     # s and the in-plane p atomic orbitals, so a selection of (l, m) keeps exactly the MOs of its blocks

@@ -133,3 +133,10 @@ def test_oracle_pi_only_casida_on_a_planar_polyene():
     o.setGeometry(al)
     Om, f = o.getEnergies(select_lm=[(1, 0)])
     assert (o.nocc, o.nvirt) == (4, 4) and len(Om) == 16 and np.all(Om > 0)
+
+
+def test_active_space_report_against_reference(capsys):
+    td = _solved()
+    td.dftb2.verbose = 1
+    assert tuple(td.determineActiveSpace(threshold=1e-2)) == tuple(G["active_space_1e-2"])
+    assert capsys.readouterr().out == str(G["active_space_text"])
