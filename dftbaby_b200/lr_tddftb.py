@@ -651,10 +651,35 @@ class LR_TDDFTB:
         hole = -torch.zeros(nat, dtype=torch.float64, device=Co.device).index_add_(0, ind, hw)
         return particle.cpu().numpy(), hole.cpu().numpy()
 
+    def _exciton_report(self, title, particle, hole):
+        """The exciton report DFTBaby prints at verbose > 0 (LR_TDDFTB.py:924-945): particle and hole centres,
+        their distance and the charges per atom."""
+        from .params import ELEMENT_NAMES
+        p_pos, h_pos = np.zeros(3), np.zeros(3)
+        for A, (ZA, posA) in enumerate(self.dftb2.atomlist):
+            p_pos += np.array(posA) * particle[A]
+            h_pos += np.array(posA) * hole[A]
+        p_pos /= float(np.sum(particle))
+        h_pos /= float(np.sum(hole))
+        txt = title
+        txt += "===================\n"
+        txt += "Particle position: %s bohr\n" % p_pos
+        txt += "Hole     position: %s bohr\n" % h_pos
+        txt += "P-H distance     : %3.7f bohr\n" % np.linalg.norm(p_pos - h_pos)
+        txt += "Particle-Hole Charges\n"
+        txt += "======================\n"
+        for A, (ZA, _) in enumerate(self.dftb2.atomlist):
+            txt += "%s: %3.7f (p) \t %3.7f (h)\n" % (("%s-%s" % (ELEMENT_NAMES[ZA], A)).center(12), particle[A],
+                                                      hole[A])
+        print(txt)
+
     def ParticleHoleCharges(self, I):
         """LR_TDDFTB.ParticleHoleCharges (LR_TDDFTB.py:910-947): the density difference between excited state
         I (0-based) and the ground state as particle and hole charges on the atoms (numpy, Nat each)."""
-        return self._particle_hole(self.Cij[I])
+        particle, hole = self._particle_hole(self.Cij[I])
+        if getattr(self.dftb2, "verbose", 0) > 0:
+            self._exciton_report("Exciton: State %d\n" % I, particle, hole)
+        return particle, hole
 
     def ParticleHoleChargesSuperposition(self, coeffs):
         """LR_TDDFTB.ParticleHoleChargesSuperposition (LR_TDDFTB.py:948-1006): particle and hole charges of the
@@ -662,7 +687,10 @@ class LR_TDDFTB:
         n = len(self.Omega)
         c = torch.as_tensor(np.asarray(coeffs)[:n], dtype=torch.complex128, device=self.Cij.device)
         Csuper = torch.einsum("I,Iia->ia", c, self.Cij[:n].to(torch.complex128))
-        return self._particle_hole(Csuper)
+        particle, hole = self._particle_hole(Csuper)
+        if getattr(self.dftb2, "verbose", 0) > 0:
+            self._exciton_report("Exciton: \n", particle, hole)
+        return particle, hole
 
     def analyseParticleHole(self, particle_hole_states=(), particle_hole_dir=None):
         """LR_TDDFTB.analyseParticleHole (LR_TDDFTB.py:997-1007): for each excited state I (1-based) in

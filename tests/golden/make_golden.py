@@ -859,7 +859,6 @@ def make_particle_hole(ref_root, rng):
     (LR_TDDFTB.py:910-1007) run from DFTBaby's text on the C4H6 layout of make_mulliken_trans_charges,
     with the Mulliken transition charges q_oo, q_vv made by DFTBaby's own Python loop
     (LR_TDDFTB.py:267-296) from the stored S and orbitals."""
-    import string
     import textwrap
     Zs = [6, 6, 6, 6, 1, 1, 1, 1, 1, 1]
     valorbs = {1: [(1, 0, 0)], 6: [(2, 0, 0), (2, 1, -1), (2, 1, 0), (2, 1, 1)]}
@@ -883,7 +882,8 @@ def make_particle_hole(ref_root, rng):
     ns = {"zeros": np.zeros, "dot": np.dot, "self": r, "atomlist": atomlist, "valorbs": valorbs, "orbs": orbs,
           "S": S}
     exec(compile(block, "LR_TDDFTB.py:_MullikenTransitionCharges", "exec"), ns)
-    ns = {"np": np, "la": np.linalg, "string": string, "path": os.path, "atom_names": ["h", "he", "li", "be", "b", "c"]}
+    ns = {"np": np, "la": np.linalg, "path": os.path, "atom_names": ["h", "he", "li", "be", "b", "c"],
+          "string": types.SimpleNamespace(center=lambda text, width: text.center(width))}
     for n in ("ParticleHoleCharges", "ParticleHoleChargesSuperposition", "analyseParticleHole"):
         exec(compile(method_source(os.path.join(ref_root, "DFTB", "LR_TDDFTB.py"), n, after=r"class LR_TDDFTB"),
                      "LR_TDDFTB.py", "exec"), ns)
@@ -893,11 +893,20 @@ def make_particle_hole(ref_root, rng):
     tmp = tempfile.mkdtemp(prefix="dftbaby_ph_")
     ns["analyseParticleHole"](r, particle_hole_states=[1, 3], particle_hole_dir=tmp)
     chrg = [open(os.path.join(tmp, "particle_hole_charges_%d.chrg" % I)).read() for I in (1, 3)]
+    # the exciton reports printed at verbose > 0
+    import contextlib
+    r.dftb2.verbose = 1
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        ns["ParticleHoleCharges"](r, 1)
+        ns["ParticleHoleChargesSuperposition"](r, coeffs)
+    r.dftb2.verbose = 0
+    report = buf.getvalue()
     shutil.rmtree(tmp, ignore_errors=True)
     np.savez_compressed(os.path.join(HERE, "particle_hole.npz"), Z=np.array(Zs), pos=pos, S=S, orbs=orbs, occ=occ,
                         virt=virt, C=C, coeffs=coeffs, ph_p=np.array([p for p, _ in ph]),
                         ph_h=np.array([h for _, h in ph]), sup_p=sup_p, sup_h=sup_h, chrg_1=np.array(chrg[0]),
-                        chrg_3=np.array(chrg[1]))
+                        chrg_3=np.array(chrg[1]), report=np.array(report))
 
 
 def handler_data(rng, nst=4, Zs=(6, 6, 1, 1, 1)):

@@ -47,3 +47,21 @@ def test_particle_hole_files_against_reference(tmp_path):
         ref = np.loadtxt(io.StringIO(str(G["chrg_%d" % I])))
         assert np.abs(got - ref).max() < 1e-14
 
+
+
+def test_exciton_report_against_reference(capsys):
+    """The report printed at verbose > 0 (LR_TDDFTB.py:924-945, 983-996): text identical, numbers to 1e-12."""
+    td = _solved()
+    td.dftb2.verbose = 1
+    td.ParticleHoleCharges(1)
+    td.ParticleHoleChargesSuperposition(G["coeffs"])
+    got, ref = capsys.readouterr().out.splitlines(), str(G["report"]).splitlines()
+    assert len(got) == len(ref)
+    for a, b in zip(got, ref):
+        ta, tb = a.replace("[", " ").replace("]", " ").split(), b.replace("[", " ").replace("]", " ").split()
+        assert len(ta) == len(tb), (a, b)
+        for x, y in zip(ta, tb):
+            try:
+                assert abs(float(x) - float(y)) < 1e-12 * max(1.0, abs(float(y))), (a, b)
+            except ValueError:
+                assert x == y, (a, b)
