@@ -201,6 +201,46 @@ class Gradients:
         raise RuntimeError("Z-vector equations: Krylov solver for linear system did not converge after %d "
                            "iterations (threshold: %e) !!!" % (maxiter, conv))
 
+    def _gradient_check(self, gradient_state, gradVrep, gradE0, gradExc):
+        """ExcGradients.getGradients with gradient_check=1 (ExcGradients.py:1011-1054)."""
+        d, td = self.dftb, self.tddftb
+        atomlist = list(d.atomlist)
+        x0 = np.hstack([np.asarray(p, dtype=np.float64) for _, p in atomlist])
+        gradVrepNum = numerical_gradient(lambda x: d._energy_func(x, atomlist, "Enuc"), x0)
+        print("REPULSIVE POTENTIAL")
+        print("ANALYTICAL GRADIENT")
+        print(gradVrep)
+        print("NUMERICAL GRADIENT")
+        print(gradVrepNum)
+        err_vrep = np.linalg.norm(gradVrep - gradVrepNum)
+        gradE0Num = numerical_gradient(lambda x: d._energy_func(x, atomlist, "Eelec"), x0)
+        print("GROUND STATE")
+        print("ANALYTICAL GRADIENT")
+        print(gradE0)
+        print("NUMERICAL GRADIENT")
+        print(gradE0Num)
+        err_e0 = np.linalg.norm(gradE0 - gradE0Num)
+        if gradient_state > 0:
+            gradExcNum = numerical_gradient(lambda x: td.energy_func(x, atomlist, gradient_state - 1), x0)
+            print("STATE %d" % gradient_state)
+            print("ANALYTICAL GRADIENT")
+            print(gradExc)
+            print("NUMERICAL GRADIENT")
+            print(gradExcNum)
+            err_exc = np.linalg.norm(gradExc - gradExcNum)
+        else:
+            err_exc = 0.0
+        print("ERROR REPULSIVE: %s" % err_vrep)
+        print("ERROR E0: %s" % err_e0)
+        print("ERROR EXCITATION: %s" % err_exc)
+        print("NOTE: To check the gradients you should tighten the SCF convergence setting (using "
+              "--scf_conv=1.0e-14) and disable the density mixer (using --density_mixer=None). If the space of "
+              "excitations has been restricted to those between active occupied and virtual orbitals, the gradients "
+              "will be wrong unless the state of interest is contained fully in the active space.")
+        for name, err in (("gradient vrep", err_vrep), ("E0", err_e0), ("E_exc", err_exc)):
+            if not err < 1.0e-4:
+                raise AssertionError("err(%s) = %s" % (name, err))
+
     # ------------------------------------------------------------ public API
     def gradient(self, I=0, check_zvector=0, save_intermediates_CPKS=0):
         """Returns (gradVrep, gradE0, gradExc), numpy arrays of length 3 Nat; I = 0 is the ground
@@ -323,19 +363,38 @@ class Gradients:
     def getGradients(self, gradient_state=2, gradient_file=None, gradient_check=0):
         """Total gradient of state gradient_state written to gradient_file in xyz format (atomic units);
         returns it, or None without a file, as ExcGradients.getGradients does (ExcGradients.py:982-1078).
-        gradient_check is not supported here: finite differences are the test suite's job."""
+
+        gradient_check=1 also differentiates the repulsive, electronic ground-state and excitation energies
+        numerically (central differences, h = 1e-5 bohr; the excited state with the options of the last
+        getEnergies), prints both and raises AssertionError when a difference norm reaches 1e-4, as DFTBaby
+        does.  The objects are left at the last displaced geometry, as in DFTBaby.  DFTBaby's analytic
+        gradients follow its Fortran spline and orbital-order conventions while its energies do too, and
+        the two disagree by about 1e-3 Ha/bohr, so the check can fail for DFTBaby and here alike."""
         if gradient_file is None:
             return None
-        if gradient_check:
-            raise ValueError("gradient_check is not implemented; compare against finite differences instead")
         from .xyz import write_xyz
         gradVrep, gradE0, gradExc = self.gradient(I=gradient_state)
+        if gradient_check == 1:
+            self._gradient_check(gradient_state, gradVrep, gradE0, gradExc)
         gradEtot = gradVrep + gradE0 + gradExc
         grad_atomlist = [(Z, tuple(gradEtot[3 * k:3 * k + 3])) for k, (Z, _) in enumerate(self.dftb.getGeometry())]
         write_xyz(gradient_file, [grad_atomlist], title="Gradient of total energy of state %d" % gradient_state,
                   units="au")
         print("Gradient of state %d written to file %s" % (gradient_state, gradient_file))
         return gradEtot
+
+
+def numerical_gradient(f, x0, h=1.0e-5):
+    """utils.numerical_gradient (utils.py:176-210): central differences of the scalar function f at x0."""
+    x0 = np.asarray(x0, dtype=np.float64)
+    n = len(x0)
+    dfdx = np.zeros(n)
+    for i in range(n):
+        print("numerical gradient: %d of %d" % (i, n))
+        ei = np.zeros(n)
+        ei[i] = 1.0
+        dfdx[i] = (f(x0 + h * ei) - f(x0 - h * ei)) / (2.0 * h)
+    return dfdx
 
 
 def _trans_charges_full(d, Co, Cv):

@@ -332,6 +332,9 @@ class LR_TDDFTB:
         preconditioner when no warm start is available; the solve runs to the
         same residual threshold, and the plain start is used if it fails.
         """
+        # kept for energy_func, which repeats this calculation at other geometries
+        self._last_options = {k: v for k, v in locals().items() if k not in ("self", "scf_opts")}
+        self._last_options.update(scf_opts)
         if response_method == "Tamm-Dancoff":
             # DFTBaby's own Solver.TDA raises before doing anything ("Revise the TDA code", Solver.py:194)
             raise ValueError("response_method='Tamm-Dancoff' is disabled in DFTBaby itself (Solver.TDA)")
@@ -607,7 +610,7 @@ class LR_TDDFTB:
             virt_maxs.append(self.active_virtual_orbs[np.max(virt)])
         HOMO = self.occupied_orbs.max()
         nr_active_occ, nr_active_virt = int(HOMO - min(occ_mins) + 1), int(max(virt_maxs) - HOMO)
-        if getattr(self.dftb2, "verbose", 0) > 0:
+        if getattr(getattr(self, "dftb2", None), "verbose", 0) > 0:
             Nst = C.shape[0]
             print("")
             print("Active Space")
@@ -789,9 +792,11 @@ class LR_TDDFTB:
 
     def energy_func(self, x, atomlist, I, **options):
         """LR_TDDFTB.energy_func (LR_TDDFTB.py:115-124): the excitation energy of state I (0-based) at the flat
-        coordinates x (bohr), for numerical differentiation; getEnergies and SCC options as keywords
-        (the reference reads them from its command line)."""
+        coordinates x (bohr), for numerical differentiation; getEnergies and SCC options as keywords, by
+        default those of the last getEnergies call (the reference reads them from its command line)."""
         x = np.asarray(x, dtype=np.float64).reshape(-1)
+        if not options:
+            options = dict(getattr(self, "_last_options", {}))
         self.setGeometry([(Z, tuple(x[3 * i:3 * i + 3])) for i, (Z, _) in enumerate(atomlist)])
         self.getEnergies(**options)
         return self.Omega[I]
