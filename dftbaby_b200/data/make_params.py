@@ -65,6 +65,9 @@ def main(ref_root):
     ea = _dict_literal(atomic, "electron_affinities_eV")
     hartree_to_eV = float(re.search(r"^hartree_to_eV\s*=\s*([0-9.eE+-]+)", atomic, re.M).group(1))
     out["const/hartree_to_eV"] = np.array(hartree_to_eV)
+    # dipoles in Debye = dipoles in e*bohr * ebohr_to_debye (AtomicData.py:9, written there as 1.0/0.393430307)
+    out["const/ebohr_to_debye"] = np.array(float(eval(re.search(r"^ebohr_to_debye\s*=\s*([^#\n]+)", atomic,
+                                                                re.M).group(1))))
     # wavenumbers (cm^-1) = energy in Hartree * hartree_to_wavenumbers (AtomicData.py:4)
     out["const/hartree_to_wavenumbers"] = np.array(
         float(re.search(r"^hartree_to_wavenumbers\s*=\s*([0-9.eE+-]+)", atomic, re.M).group(1)))

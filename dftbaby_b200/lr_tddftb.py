@@ -361,16 +361,24 @@ class LR_TDDFTB:
                                  diag_L2threshold=diag_L2threshold, precision=precision, refine_fp64=refine_fp64,
                                  guess_model=guess_model)
         ev[2].record()
+        verbose = getattr(d, "verbose", 0) > 0
         if oszis == "Dipoles":
+            if verbose:
+                print("compute transition dipoles from Slater-Koster tables")
             self._TransitionDipoles()
+            if verbose:
+                # DFTBaby evaluates the dipole matrix elements here for their printed report only
+                self.getTransitionDipolesExc(len(self.Omega))
         else:
+            if verbose:
+                print("compute transition dipoles using Mulliken approximation (ZDO)")
             self._TransitionDipolesMulliken()
         self.getOscillatorStrengths()
         self.Lambda2 = torch.sum(self.Cij ** 2 * self.Oia[None], dim=(1, 2))
         # states are not classified by symmetry: empty labels, as DFTBaby without use_symmetry
         self.Irreps = [""] * len(self.Omega)
         ev[3].record()
-        if getattr(d, "verbose", 0) > 0:
+        if verbose:
             # DFTBaby calls determineActiveSpace after every iterative solve; without verbose output it has
             # no effect, so it runs here only to print its report
             if nstates is not None:
@@ -561,10 +569,15 @@ class LR_TDDFTB:
             raise ValueError("transition dipoles between excited states need a closed-shell ground state")
         t_oo, t_ov, t_vv = mo_dipoles(occ, occ), mo_dipoles(occ, virt), mo_dipoles(virt, virt)
         t_all = mo_dipoles(occ_all, occ_all)
-        d0 = 2.0 * torch.einsum("kkc->c", t_all)  # inactive and active occupied orbitals together
+        d0_elec = 2.0 * torch.einsum("kkc->c", t_all)  # inactive and active occupied orbitals together
         Z = torch.as_tensor([float(d.ne_val[Zat]) for Zat, _ in d.atomlist], dtype=torch.float64, device=dev)
         pos = torch.as_tensor(np.array([p for _, p in d.atomlist], dtype=np.float64), device=dev)
-        d0 = d0 - (Z[:, None] * pos).sum(0)
+        d0_nuc = -(Z[:, None] * pos).sum(0)
+        verbose = getattr(d, "verbose", 0) > 0
+        if verbose:
+            print("electronic dipole moment (in e*bohr): %s" % d0_elec.cpu().numpy())
+            print("nuclear dipole moment (in e*bohr):    %s" % d0_nuc.cpu().numpy())
+        d0 = d0_elec + d0_nuc
         C = self.Cij[:Nst - 1].to(torch.float64)
         tdip = torch.zeros((Nst, Nst, 3), dtype=torch.float64, device=dev)
         tdip[0, 0] = d0
@@ -575,7 +588,23 @@ class LR_TDDFTB:
         oo = torch.einsum("Aia,Bja,ijc->ABc", C, C, t_oo)
         vv = torch.einsum("Aia,Bib,abc->ABc", C, C, t_vv)
         tdip[1:, 1:] = d0[None, None, :] * P0[:, :, None] - oo + vv
-        return tdip.cpu().numpy()
+        tdip = tdip.cpu().numpy()
+        if verbose:
+            # electrons count positive in these matrix elements: the sign flips for the dipole in Debye
+            debye = float(raw_params()["const/ebohr_to_debye"])
+            txt = "\n"
+            txt += "                   Dipole Matrix Elements (in Debye)\n"
+            txt += "                   =================================\n"
+            txt += "  Bra <i|    Ket |j>         <i|mu(X)|j>       <i|mu(Y)|j>      <i|mu(Z)|j>      |<i|mu|j>|\n"
+            txt += "-------------------------------------------------------------------------------------------\n"
+            for i in range(Nst):
+                for j in range(i, Nst):
+                    dvec = tdip[i, j, :] * (-debye)
+                    txt += "  %4.1d       %4.1d          %+12.6e     %+12.6e    %+12.6e    %+12.6e        \n" % (
+                        i, j, dvec[0], dvec[1], dvec[2], np.linalg.norm(dvec))
+            txt += "\n"
+            print(txt)
+        return tdip
 
     def getOscillatorStrengths(self):
         """f = 2/3 Omega |t|^2 for singlets, 0 for triplets (LR_TDDFTB.py:698-705)."""

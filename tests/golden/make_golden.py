@@ -766,6 +766,16 @@ def make_lr_glue(ref_root, rng):
                     "lm_%s_active_occ" % tag: lm_r.active_occupied_orbs,
                     "lm_%s_active_virt" % tag: lm_r.active_virtual_orbs})
     out["tdip_exc"] = r.getTransitionDipolesExc(4)
+    # the report printed at verbose > 0, with DFTBaby's AtomicData constants
+    import contextlib
+    ns["AtomicData"] = _reference_atomic_data(ref_root)
+    dftb2.verbose = 1
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        r.getTransitionDipolesExc(4)
+    dftb2.verbose = 0
+    ns["AtomicData"] = atomic
+    out["tdip_exc_report"] = np.array(buf.getvalue())
     tmp = tempfile.mkdtemp(prefix="dftbaby_lr_")
     real_string = sys.modules.get("string")
     sys.modules["string"] = types.SimpleNamespace(rjust=lambda text, width: text.rjust(width))

@@ -140,3 +140,28 @@ def test_active_space_report_against_reference(capsys):
     td.dftb2.verbose = 1
     assert tuple(td.determineActiveSpace(threshold=1e-2)) == tuple(G["active_space_1e-2"])
     assert capsys.readouterr().out == str(G["active_space_text"])
+
+
+def _same_report(got, ref, rtol):
+    gl, rl = got.splitlines(), ref.splitlines()
+    assert len(gl) == len(rl)
+    for a, b in zip(gl, rl):
+        ta, tb = a.replace("[", " ").replace("]", " ").split(), b.replace("[", " ").replace("]", " ").split()
+        assert len(ta) == len(tb), (a, b)
+        for x, y in zip(ta, tb):
+            try:
+                fx, fy = float(x), float(y)
+            except ValueError:
+                assert x == y, (a, b)
+                continue
+            assert abs(fx - fy) <= rtol * max(1.0, abs(fy)), (a, b)
+
+
+def test_dipole_report_against_reference(capsys):
+    """The dipole report of getTransitionDipolesExc at verbose > 0 (LR_TDDFTB.py:648-697), in Debye with
+    DFTBaby's conversion factor; printed with 7 significant digits."""
+    td = _solved()
+    td._TransitionDipoles()
+    td.dftb2.verbose = 1
+    td.getTransitionDipolesExc(4)
+    _same_report(capsys.readouterr().out, str(G["tdip_exc_report"]), 1e-6)
