@@ -268,6 +268,7 @@ class DFTB2(object):
             self.E_HF_x = self.lc_exchange_energy().item()
             self.E_elec += self.E_HF_x
         self.E_nuc = self.getRepulsiveEnergy()
+        self.E_rep = self.E_nuc  # DFTBaby's reports call it E_rep
         self.E_tot = self.E_elec + self.E_nuc
         return self.E_bs, self.E_coulomb, self.E_elec, self.E_nuc, self.E_tot
 
@@ -397,7 +398,13 @@ class DFTB2(object):
             self.relative_change, sum_dq, self.HLgap = float(host[0]), float(host[1]), float(host[2])
             if abs(sum_dq + self.charge) > 1.0e-5:
                 raise SCFChargeInconsistency("Mulliken charges do not add up to total charge, sum dq = %s" % -sum_dq)
+            if self.verbose > 0:
+                self.getEnergies()
+                self.writeIteration()
             if converged:
+                if self.verbose > 0:
+                    print("!!! CONVERGED after %s iterations (relative change = %.2e < %.2e = threshold)!!!"
+                          % (self.i + 1, self.relative_change, scf_conv))
                 break
             if self.relative_change < scf_conv:
                 converged = True
@@ -417,6 +424,51 @@ class DFTB2(object):
         if self.Nelec_val < 0.5:
             print("\nWARNING: There are no valence electrons in this molecule, \n         charge = %+d,  nr. valence "
                   "electrons = %s !\n" % (self.charge, self.Nelec_val))
+
+    def writeIteration(self, info=("convergence", "energies", "orbitals", "charges")):
+        """DFTB2.writeIteration (DFTB2.py:2146-2233): the report of one SCC iteration printed at verbose > 0
+        (the MO coefficients of verbose > 1 are not printed)."""
+        h2ev = float(raw_params()["const/hartree_to_eV"])
+        num = lambda a: a.cpu().numpy() if torch.is_tensor(a) else np.asarray(a)
+        def line(label, e):
+            return "%s: %s %s\n" % (label, ("%.7f hartree" % e).rjust(20), ("%.7f eV" % (e * h2ev)).rjust(20))
+
+        txt = "      *******************\n"
+        txt += "      * Iteration: %.2d *\n" % self.i
+        txt += "      *******************\n"
+        if "convergence" in info:
+            txt += "  Convergence\n"
+            txt += "  ===========\n"
+            txt += "relative change: %.6e\n" % self.relative_change
+        if "energies" in info:
+            txt += "  Electronic Energies\n"
+            txt += "  ===================\n"
+            txt += line("band structure energy E_bs", self.E_bs)
+            txt += line("Coulomb energy E_coulomb  ", self.E_coulomb)
+            if hasattr(self, "E_HF_x"):
+                txt += line("long range HF-x E_x       ", self.E_HF_x)
+            txt += line("total electronic energy   ", self.E_elec)
+            txt += line("repulsion energy          ", self.E_rep)
+            txt += line("total energy              ", self.E_tot)
+        if "orbitals" in info:
+            txt += line("HOMO-LUMO gap             ", self.HLgap)
+            txt += "  Orbital Energies\n"
+            txt += "  ================\n"
+            orbe, f = num(self.orbe), num(self.f)
+            for i, a in enumerate(np.argsort(orbe)):
+                txt += "%s: %s %s  (%.3f e)\n" % (str(i + 1).rjust(6), ("%.7f hartree" % orbe[a]).rjust(20),
+                                                ("%.7f eV" % (orbe[a] * h2ev)).rjust(20), f[a])
+        if "charges" in info:
+            q, dq = num(self.q), num(self.dq)
+            txt += "  Mulliken Charges   (Partial Charges)\n"
+            txt += "  NOTE: charges are in units of e-!\n"
+            txt += "  =========================================================================\n"
+            for i, (Zi, _) in enumerate(self.atomlist):
+                txt += "%s: %.3f\t(%+.3f)\n" % (("%s-%s" % (ELEMENT_NAMES[Zi], i)).center(12), q[i], dq[i])
+            txt += "  =========================================================================\n"
+            txt += "  sum of charges        : %+.3f\n" % np.sum(q)
+            txt += "  sum of partial charges: %+.3f\n" % np.sum(dq)
+        print(txt)
 
     def _balance_partial_charges(self, dq):
         """DFTB2._balance_partial_charges (DFTB2.py:839-848): dq shifted evenly so that the partial charges add

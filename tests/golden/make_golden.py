@@ -1075,6 +1075,24 @@ def make_dftb2_props(ref_root, rng):
     with contextlib.redirect_stdout(buf):
         r.setCharge(12.0)  # no valence electrons left: the reference warns
     out["nelec_empty"], out["setcharge_text_empty"] = r.Nelec_val, np.array(buf.getvalue())
+    # the report of one SCC iteration printed at verbose > 0 (DFTB2.writeIteration, DFTB2.py:2146-2233)
+    exec(compile(method_source(os.path.join(ref_root, "DFTB", "DFTB2.py"), "writeIteration", after=r"class DFTB2"),
+                 "DFTB2.py", "exec"), ns)
+    ns.update(hartree_to_eV=_reference_atomic_data(ref_root).hartree_to_eV, argsort=np.argsort)
+    orbe = np.sort(rng.standard_normal(12))[rng.permutation(12)]
+    it = types.SimpleNamespace(i=7, relative_change=3.25e-6, E_bs=-11.1, E_coulomb=0.05, E_HF_x=-0.02,
+                               E_elec=-11.07, E_rep=0.8, E_tot=-10.27, HLgap=0.31, orbe=orbe,
+                               f=np.where(orbe < np.sort(orbe)[6], 2.0, 0.0), q=q0 - dq, dq=dq, verbose=1,
+                               mulliken_dipoles=0, qmmm=None, cavity=None, atomlist=r.atomlist)
+    sys.modules["string"] = types.SimpleNamespace(center=lambda text, width: text.center(width),
+                                                  rjust=lambda text, width: text.rjust(width))
+    buf = io.StringIO()
+    try:
+        with contextlib.redirect_stdout(buf):
+            ns["writeIteration"](it)
+    finally:
+        sys.modules["string"] = real_string
+    out.update(it_orbe=orbe, it_f=it.f, iteration_text=np.array(buf.getvalue()))
     np.savez_compressed(os.path.join(HERE, "dftb2_props.npz"), **out)
 
 

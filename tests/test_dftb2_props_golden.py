@@ -64,3 +64,13 @@ def test_options_off_the_path_are_refused():
     # defaults and inert options get as far as the device
     with pytest.raises(NativeUnavailable):
         DFTB2(al, mulliken_dipoles=0, scratch_dir="/tmp", cpks_solver="iterative", reppot_paths="[]")
+
+
+def test_scc_iteration_report_against_reference(capsys):
+    """DFTB2.writeIteration (DFTB2.py:2146-2233), the report printed for each SCC iteration at verbose > 0."""
+    d = _ground_state()
+    d.i, d.relative_change = 7, 3.25e-6
+    d.E_bs, d.E_coulomb, d.E_HF_x, d.E_elec, d.E_rep, d.E_tot, d.HLgap = -11.1, 0.05, -0.02, -11.07, 0.8, -10.27, 0.31
+    d.orbe, d.f = torch.tensor(G["it_orbe"]), torch.tensor(G["it_f"])
+    d.writeIteration()
+    assert capsys.readouterr().out == str(G["iteration_text"])
