@@ -400,9 +400,14 @@ class LR_TDDFTB:
         """LR_TDDFTB._solve_lr_equations (LR_TDDFTB.py:403-527)."""
         d = self.dftb2
         dev = d.device
+        verbose = getattr(d, "verbose", 0) > 0
+        if verbose:
+            print("compute transition charges")
         self.qtrans_oo = self.qtrans_vv = None
         _, self.qtrans_ov, _ = self._trans_charges(("ov",))
         self._Lambda2_calcOia()
+        if verbose:
+            print("build gamma matrices")
         orbe = d.orbe
         occ = torch.as_tensor(self.active_occupied_orbs, device=dev)
         virt = torch.as_tensor(self.active_virtual_orbs, device=dev)
@@ -427,6 +432,9 @@ class LR_TDDFTB:
             from . import learned as _learned
             learned["guess_key"], learned["precond_diag"] = _learned.guess_inputs(guess_model, self)
         self.stats["learned_start"] = bool(learned)
+        if verbose:
+            print("construct and diagonalize full TD-DFTB matrix with dimension %d" % (self.nocc * self.nvirt)
+                  if nstates is None else "solve eigenvalue problem iteratively")
         if nstates is None:
             Om, C, XmY, XpY = self._casida(multiplicity)
         elif not lc:
