@@ -1100,8 +1100,11 @@ int dftb_dgemm(int transa, int transb, int m, int n, int k, double alpha, const 
 // until the process exits.  On the host its name is only a stand-in symbol,
 // so its device address is looked up with cudaGetSymbolAddress, once per
 // device, the first time the entry point runs with that device current (the
-// first call should therefore come before any stream capture).  All calls on
-// one device share the array: calls that can run at the same time on the GPU
+// first call should therefore come before any stream capture).  Under lazy
+// module loading the array is committed when this module is first used on a
+// device, possibly by that first call.  The cached address belongs to the
+// device's primary context; it is not looked up again after cudaDeviceReset.
+// All calls on one device share the array: calls that can run at the same time on the GPU
 // (unordered streams, concurrent host threads) race on it and must be
 // serialised by the caller.  Every call rewrites the parts of the scratch it
 // reads, so nothing has to be cleared between calls.
@@ -1148,6 +1151,8 @@ extern "C" int dftb_trans_charges_noalloc(int norb, int nat, int nocc, int nvirt
                                           double *q_vv, void *stream) {
     if (norb <= 0 || nat <= 0 || nocc < 0 || nvirt < 0 || nat > norb)
         return fail(DFTB_ERR_BAD_SIZE, "trans_charges_noalloc: sizes");
+    // the atom index is the grid's z extent; refuse before anything is launched
+    if (nat > 65535) return fail(DFTB_ERR_BAD_SIZE, "trans_charges_noalloc: nat > 65535");
     const size_t need = dftb_trans_charges_workspace_size(norb, nocc, nvirt);
     if (need > kNoAllocScratchBytes) {
         snprintf(g_last_error, sizeof(g_last_error),
@@ -1174,7 +1179,6 @@ extern "C" int dftb_trans_charges_noalloc(int norb, int nat, int nocc, int nvirt
                  {q_vv, cv, scv, cv, scv, nvirt, nvirt}};
     for (auto &b : blks) {
         if (!b.out || b.n1 == 0 || b.n2 == 0) continue;
-        if (nat > 65535) return fail(DFTB_ERR_BAD_SIZE, "trans_charges_noalloc: nat > 65535");
         dim3 grid(cdiv(b.n2, 32), cdiv(b.n1, 32), nat);
         tc_kernel<<<grid, dim3(32, 8), 0, st>>>(b.n1, b.n2, first, b.c1, b.s1, b.c2, b.s2, b.out);
         if ((rc = check_launch("tc_kernel (noalloc)"))) return rc;

@@ -557,36 +557,3 @@ class DFTB2(object):
 
     def getGaussianOverlap(self):
         return self.gaussOmega
-
-
-def main(argv=None):
-    """The DFTB2.py program (DFTB2.py:2635-2700): the total energy of every geometry in an xyz file, with
-    DFTB2 and runSCC options from dftbaby.cfg and the command line and the charge from the title line.
-    Orbital localisation, Molden and cube exports are not provided."""
-    from .options import OptionParserFuncWrapper
-    from .xyz import extract_keywords_xyz, read_xyz
-    usage = ("Usage: python -m dftbaby_b200.dftb2 <xyz-file>\n"
-             "   options can be passed on the command line or\n"
-             "   in a configuration file called 'dftbaby.cfg'\n"
-             "   --help option will provide more information\n")
-    parser = OptionParserFuncWrapper([DFTB2.__init__, DFTB2.runSCC], usage)
-    options, args = parser.parse_args(DFTB2.__init__, argv)
-    if len(args) < 1:
-        print(usage)
-        return -1
-    kwds = extract_keywords_xyz(args[0])
-    structures = read_xyz(args[0])
-    dftb2 = DFTB2(structures[0], **options)
-    scf_options, _ = parser.parse_args(DFTB2.runSCC, argv)
-    h2ev = float(raw_params()["const/hartree_to_eV"])
-    for i, atomlist in enumerate(structures):
-        dftb2.setGeometry(atomlist, kwds.get("charge", 0.0))
-        dftb2.getEnergy(**scf_options)
-        print("TOTAL ENERGY OF STRUCTURE %d              : %s %s\n" % (i, ("%.7f hartree" % dftb2.E_tot).rjust(20),
-                                                                       ("%.7f eV" % (dftb2.E_tot * h2ev)).rjust(20)))
-    print("FINISHED")
-    return 0
-
-
-if __name__ == "__main__":
-    raise SystemExit(main())

@@ -372,16 +372,23 @@ class Gradients:
         the two disagree by about 1e-3 Ha/bohr, so the check can fail for DFTBaby and here alike."""
         if gradient_file is None:
             return None
-        from .xyz import write_xyz
         gradVrep, gradE0, gradExc = self.gradient(I=gradient_state)
         if gradient_check == 1:
             self._gradient_check(gradient_state, gradVrep, gradE0, gradExc)
         gradEtot = gradVrep + gradE0 + gradExc
-        grad_atomlist = [(Z, tuple(gradEtot[3 * k:3 * k + 3])) for k, (Z, _) in enumerate(self.dftb.getGeometry())]
-        write_xyz(gradient_file, [grad_atomlist], title="Gradient of total energy of state %d" % gradient_state,
-                  units="au")
+        _write_gradient_xyz(gradient_file, [Z for Z, _ in self.dftb.getGeometry()], gradEtot.reshape(-1, 3),
+                            "Gradient of total energy of state %d" % gradient_state)
         print("Gradient of state %d written to file %s" % (gradient_state, gradient_file))
         return gradEtot
+
+
+def _write_gradient_xyz(path, Zs, g, title):
+    """One frame in xyz layout (atom count, title, element and three numbers per atom), atomic units."""
+    from .params import ELEMENT_NAMES
+    with open(path, "w") as fh:
+        fh.write("%d\n%s\n" % (len(Zs), title))
+        for Z, row in zip(Zs, g):
+            fh.write("%4s  %+.15e  %+.15e  %+.15e\n" % (ELEMENT_NAMES[Z].capitalize(), *row))
 
 
 def numerical_gradient(f, x0, h=1.0e-5):

@@ -863,43 +863,3 @@ class LR_TDDFTB:
 
     def getXY(self):
         return self.XmY, self.XpY
-
-
-USAGE = "Usage: python -m dftbaby_b200.lr_tddftb <xyz-file> [--option=value ...]\n   --help lists the options"
-
-
-def main(argv=None):
-    """The LR_TDDFTB.py command line (LR_TDDFTB.py:1153-1230) for the options of this package: the geometry
-    (Angstrom) and the total charge (``charge=`` on the xyz title line) from the xyz file; DFTB2, runSCC,
-    getEnergies, saveAbsorptionSpectrum, saveTransitionCharges, analyseParticleHole and getGradients options
-    from ``dftbaby.cfg`` and the command line.  Prints the excitation table when --verbose is above 0, writes
-    absorption_spectrum.dat (or --spectrum_file) and, with --gradient_file, the gradient of --gradient_state.
-    Molden, cube, NTO and NAC exports are not provided."""
-    from .gradients import Gradients
-    from .options import OptionParserFuncWrapper
-    from .xyz import extract_keywords_xyz, read_xyz
-    parser = OptionParserFuncWrapper([DFTB2.__init__, DFTB2.runSCC, LR_TDDFTB.getEnergies,
-                                      LR_TDDFTB.saveAbsorptionSpectrum, LR_TDDFTB.saveTransitionCharges,
-                                      LR_TDDFTB.analyseParticleHole, Gradients.getGradients], USAGE)
-    options, args = parser.parse_args(DFTB2.__init__, argv)
-    if len(args) < 1:
-        print(USAGE)
-        return -1
-    xyz_file = args[0]
-    atomlist = read_xyz(xyz_file)[0]
-    kwds = extract_keywords_xyz(xyz_file)
-    tddftb = LR_TDDFTB(atomlist, **options)
-    options, _ = parser.parse_args(LR_TDDFTB.getEnergies, argv)
-    scf_options, _ = parser.parse_args(DFTB2.runSCC, argv)
-    options.update(scf_options)
-    tddftb.setGeometry(atomlist, charge=kwds.get("charge", 0.0))
-    tddftb.getEnergies(**options)
-    tddftb.saveAbsorptionSpectrum(**parser.parse_args(LR_TDDFTB.saveAbsorptionSpectrum, argv)[0])
-    tddftb.saveTransitionCharges(**parser.parse_args(LR_TDDFTB.saveTransitionCharges, argv)[0])
-    tddftb.analyseParticleHole(**parser.parse_args(LR_TDDFTB.analyseParticleHole, argv)[0])
-    Gradients(tddftb).getGradients(**parser.parse_args(Gradients.getGradients, argv)[0])
-    return 0
-
-
-if __name__ == "__main__":
-    raise SystemExit(main())

@@ -131,11 +131,16 @@ int dftb_trans_charges(int norb, int nat, int nocc, int nvirt, const double *orb
  * fixed 8 MiB device array that each GPU loading the library holds until the
  * process exits.  Requests needing more than dftb_trans_charges_noalloc_max_bytes()
  * of scratch (dftb_trans_charges_workspace_size() > 8 MiB) return
- * DFTB_ERR_WORKSPACE and launch nothing.  The first call on a device looks up
- * the array's address for that device (cudaGetSymbolAddress), so make it
- * before any stream capture.  All calls on one device share the array: calls
- * that may run concurrently on the GPU race and must be serialised.  No
- * device memory is allocated or freed. */
+ * DFTB_ERR_WORKSPACE and launch nothing, as do more than 65535 atoms.  The
+ * first call on a device looks up the array's address for that device
+ * (cudaGetSymbolAddress), so make it before any stream capture.  With CUDA's
+ * lazy module loading (the default) the array is also committed on that device
+ * only when this library's kernels are first used there, which may be this
+ * first call: a host that reserves the GPU's memory for its own pool should
+ * make one call (any size) before reserving it.  The cached address belongs
+ * to the device's primary context and does not survive cudaDeviceReset.  All
+ * calls on one device share the array: calls that may run concurrently on the
+ * GPU race and must be serialised.  No device memory is allocated or freed. */
 size_t dftb_trans_charges_noalloc_max_bytes(void);
 int dftb_trans_charges_noalloc(int norb, int nat, int nocc, int nvirt, const double *orbs_occ,
                                const double *orbs_virt, const double *S, const int *orbs_per_atom, double *q_oo,

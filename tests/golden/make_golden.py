@@ -919,109 +919,6 @@ def make_particle_hole(ref_root, rng):
                         chrg_3=np.array(chrg[1]), report=np.array(report))
 
 
-def handler_data(rng, nst=4, Zs=(6, 6, 1, 1, 1)):
-    """The arrays the scripted PES of tests/golden/fake_pes.py returns."""
-    nat = len(Zs)
-    A = rng.standard_normal((nst, nst))
-    P = np.diag(rng.choice([-1.0, 1.0], nst))
-    ph_p = rng.random((nst - 1, nat))
-    return dict(Z=np.array(Zs), pos=rng.standard_normal((nat, 3)),
-                E=np.sort(rng.standard_normal((3, nst)), axis=1) - 40.0,
-                grad=rng.standard_normal((3, nst, 3 * nat)), E0=rng.standard_normal(2) - 40.0,
-                grad0=rng.standard_normal((2, 3 * nat)), coupl=A - A.T, olap=np.eye(nst) + 0.05 * A,
-                tdip=rng.standard_normal((nst, nst, 3)), P=P, ph_p=ph_p, ph_h=-ph_p[:, ::-1],
-                lambda2=rng.random(nst - 1), tq=rng.standard_normal((nst - 1, nat)))
-
-
-def make_handler(ref_root, rng):
-    """dftbaby_handler.getBrightestState, getAll_S0, getAll, writeTimeSeries, getAvgParticleHoleCharges and
-    getParticleHoleChargesSuperposition (Dynamics/dftbaby_handler.py:30-319) run from DFTBaby's text on the
-    scripted PES of tests/golden/fake_pes.py: returned arrays, PES call sequences, printed text, time-series
-    files, and which failures propagate."""
-    import contextlib
-    sys.path.insert(0, HERE)
-    from fake_pes import FakePES
-    src = os.path.join(ref_root, "DFTB", "Dynamics", "dftbaby_handler.py")
-    names = ("getBrightestState", "getAll_S0", "getAll", "writeTimeSeries", "getAvgParticleHoleCharges",
-             "getParticleHoleChargesSuperposition")
-    errors = {n: type(n, (Exception,), {}) for n in ("SCFNotConverged", "SCFChargeInconsistency",
-                                                      "ExcitedStatesNotConverged", "ExcitedStatesError")}
-    atomic = _reference_atomic_data(ref_root)
-    xyz = types.SimpleNamespace(atomlist2vector=lambda al: np.hstack([np.asarray(p, dtype=float) for _, p in al]))
-    ns = dict(np=np, os=os, XYZ=xyz, AtomicData=atomic, **errors)
-    for n in names:
-        exec(compile(method_source(src, n, after=r"class dftbaby_handler"), "dftbaby_handler.py", "exec"), ns)
-    Ref = type("dftbaby_handler", (), {n: ns[n] for n in names})
-    data = handler_data(rng)
-    nst, nat = data["E"].shape[1], len(data["Z"])
-    atomlist = [(int(Z), tuple(p)) for Z, p in zip(data["Z"], data["pos"])]
-    masses = np.array(atomic.atomlist2masses(atomlist))
-    coords = [data["pos"] + 0.01 * k for k in range(4)]
-
-    def handler(pes):
-        h = Ref()
-        h.dt_nuc, h.nstates, h.sc_threshold, h.Nat, h.masses, h.pes, h.last_step = 20.0, nst, 0.002, nat, masses, pes, None
-        return h
-
-    out = dict(masses=masses, dt_nuc=20.0, sc_threshold=0.002, **{"data_" + k: v for k, v in data.items()})
-    # A: a good step, an excited-state failure (ground-state fallback), an excited-state failure whose
-    # ground-state fallback fails too (last step reused), a good step
-    pes = FakePES(data, errors, fail_exc={1: "ExcitedStatesNotConverged", 2: "ExcitedStatesError"},
-                  fail_s0={1: "SCFNotConverged"})
-    h = handler(pes)
-    buf = io.StringIO()
-    with contextlib.redirect_stdout(buf):
-        out["brightest"] = h.getBrightestState(coords[0])
-        for k, st in enumerate((2, 2, 2, 1)):
-            res = h.getAll(coords[k], st)
-            for name, a in zip(("energies", "accel", "coupl", "tdip", "olap"), res):
-                out["A%d_%s" % (k, name)] = np.asarray(a)
-        fish = types.SimpleNamespace(c=np.array([0.1 + 0.2j, 0.5 - 0.1j, 0.3j, 0.7]), time=413.4, fs_to_au=41.341,
-                                     au_to_ang=0.529177, state=2)
-        series = ["particle-hole charges", "particle-hole charges current", "Lambda2 current", "Lambda2",
-                  "transition charges current"]
-        tmp = tempfile.mkdtemp(prefix="dftbaby_ts_")
-        cwd = os.getcwd()
-        os.chdir(tmp)
-        try:
-            h.writeTimeSeries(fish, series)
-            fish.state, fish.time = 0, 434.1
-            h.writeTimeSeries(fish, series)
-            for fn in sorted(os.listdir(tmp)):
-                out["file_" + fn] = np.array(open(fn).read())
-        finally:
-            os.chdir(cwd)
-            shutil.rmtree(tmp, ignore_errors=True)
-        out["avg_p"], out["avg_h"] = h.getAvgParticleHoleCharges(fish.c)
-        out["fish_c"] = fish.c
-    out["A_stdout"] = np.array(buf.getvalue())
-    out["A_log"] = np.array(pes.log)
-    # B: a failed first step on an excited state propagates; C: on the ground state it falls back;
-    # D: getAll_S0 without a previous step propagates the SCF failure; E: a charge inconsistency is not caught
-    scen = {"B": (dict(fail_exc={0: "ExcitedStatesError"}), [(0, 2)]),
-            "C": (dict(fail_exc={0: "SCFNotConverged"}), [(0, 0)]),
-            "D": (dict(fail_s0={0: "SCFNotConverged"}), None),
-            "E": (dict(fail_exc={1: "SCFChargeInconsistency"}), [(0, 1), (1, 1)])}
-    for tag, (script, steps) in scen.items():
-        pes = FakePES(data, errors, **script)
-        h = handler(pes)
-        raised = ""
-        with contextlib.redirect_stdout(io.StringIO()):
-            try:
-                if steps is None:
-                    h.getAll_S0(coords[0])
-                else:
-                    for k, st in steps:
-                        res = h.getAll(coords[k], st)
-                        for name, a in zip(("energies", "accel", "coupl", "tdip", "olap"), res):
-                            out["%s%d_%s" % (tag, k, name)] = np.asarray(a)
-            except Exception as e:  # the class name is what the test compares
-                raised = type(e).__name__
-        out[tag + "_raised"] = np.array(raised)
-        out[tag + "_log"] = np.array(pes.log)
-    np.savez_compressed(os.path.join(HERE, "handler.npz"), **out)
-
-
 def make_dftb2_props(ref_root, rng):
     """DFTB2.getDipoleMoment, getMullikenDipoleMoment (with _center_of_nuclear_charge), write_Mulliken_charges,
     _balance_partial_charges and setCharge (DFTB2.py:429-435, 839-860, 1712-1721, 2456-2486) run from DFTBaby's
@@ -1114,276 +1011,6 @@ H      0.000000   -0.922832    1.237695
 H      0.000000    0.922832   -1.237695
 H      0.000000   -0.922832   -1.237695
 """
-
-
-def make_xyz(ref_root, rng):
-    """XYZ.read_xyz (through read_xyz_it), extract_keywords_xyz and xyz2txt (XYZ.py:15-195) run from DFTBaby's text,
-    with AtomicData.atomic_number and bohr_to_angs, on a two-frame C2H4 file with a lattice-vector line,
-    numbered and lower-case element labels and key=value pairs on the title line."""
-    ad = _reference_atomic_data(ref_root)
-    ns = {"np": np, "zeros": np.zeros, "la": np.linalg, "atom_names": ad.atom_names, "atomic_number": ad.atomic_number,
-          "bohr_to_angs": ad.bohr_to_angs, "covalent_radii": ad.covalent_radii}
-    src = os.path.join(ref_root, "DFTB", "XYZ.py")
-    for n in ("read_xyz_it", "read_xyz", "extract_keywords_xyz", "xyz2txt", "_append_xyz2txt"):
-        exec(compile(method_source(src, n), "XYZ.py", "exec"), ns)
-    tmp = tempfile.mkdtemp(prefix="dftbaby_xyz_")
-    fn = os.path.join(tmp, "mol.xyz")
-    open(fn, "w").write(XYZ_TEXT)
-    geoms = ns["read_xyz"](fn)
-    bohr = ns["read_xyz"](fn, units="bohr")
-    kw = ns["extract_keywords_xyz"](fn)
-    shutil.rmtree(tmp, ignore_errors=True)
-    out = dict(Z=np.array([[Z for Z, _ in g] for g in geoms]), pos=np.array([[p for _, p in g] for g in geoms]),
-               pos_bohr_units=np.array([[p for _, p in g] for g in bohr]), keywords=np.array(repr(sorted(kw.items()))),
-               text_one=np.array(ns["xyz2txt"](geoms[:1], title="one title")),
-               text_list=np.array(ns["xyz2txt"](geoms, title=["first"])),
-               text_bohr=np.array(ns["xyz2txt"](geoms[1:], units="bohr")))
-    np.savez_compressed(os.path.join(HERE, "xyz.npz"), **out)
-
-
-DYNAMICS_IN = """5
-C      0.10   -0.05    1.26
-C     -0.02    0.03   -1.27
-H      0.00    1.74    2.34
-H      0.05   -1.75    2.30
-H     -0.04    1.70   -2.36
-  1.0e-4   -2.0e-4    0.5e-4
- -1.5e-4    1.0e-4   -0.5e-4
-  3.0e-4    0.0e-4    2.0e-4
- -2.0e-4    1.0e-4    1.0e-4
-  1.0e-4   -3.0e-4   -2.0e-4
-"""
-MD_DRAWS = (0.02, 0.7, 0.01, 0.3, 0.001, 0.9, 0.05, 0.2, 0.4, 0.003, 0.6, 0.08)
-MD_SCENARIOS = {
-    # tag: (MolecularDynamics options, number of states of the scripted PES, restart of the previous run)
-    "E": (dict(initial_state="2", nstates=3, nstep=5, output_step=1, decoherence_correction=1,
-               time_series=["particle-hole charges", "particle-hole charges current", "Lambda2 current", "Lambda2",
-                            "transition charges current"]), 4, False),
-    "E_restart": (dict(initial_state="2", nstates=3, nstep=2, output_step=1, decoherence_correction=1), 4, True),
-    "T": (dict(initial_state="brightest", fragment_excitation=(1, 0, 1, 0), nstates=3, nstep=4, output_step=2,
-               dyn_mode="T", temp=500.0, timecoupling=2.0), 4, False),
-    "S0": (dict(initial_state="0", nstates=0, nstep=3), 2, False),
-}
-
-
-class ScriptedRandom:
-    """The draws of Python's random module (or of a numpy generator) replaced by a fixed list."""
-
-    def __init__(self, draws):
-        self.draws = list(draws)
-
-    def seed(self, *args):
-        pass
-
-    def random(self):
-        return self.draws.pop(0)
-
-
-def make_md(ref_root, rng):
-    """SurfaceHopping.MolecularDynamics (Dynamics/SurfaceHopping.py:23-760) run from DFTBaby's text through the
-    handler methods of Dynamics/dftbaby_handler.py on the scripted PES of tests/golden/fake_pes.py, with scripted
-    hop draws, from the dynamics.in above: every output file and the printed text of four runs (constant energy
-    with decoherence and all time series; its restart; Berendsen thermostat from the brightest state; ground
-    state).  DFTBaby asks for a fragment_excitation tuple also for initial_state='brightest'; the run passes one."""
-    import contextlib
-    sys.path.insert(0, HERE)
-    from fake_pes import FakePES
-    ad = _reference_atomic_data(ref_root)
-    errors = {n: type(n, (Exception,), {}) for n in ("SCFNotConverged", "SCFChargeInconsistency",
-                                                      "ExcitedStatesNotConverged", "ExcitedStatesError")}
-    xyz_ns = {"np": np, "zeros": np.zeros, "atomic_number": ad.atomic_number, "bohr_to_angs": ad.bohr_to_angs}
-    exec(compile(method_source(os.path.join(ref_root, "DFTB", "XYZ.py"), "read_initial_conditions"), "XYZ.py", "exec"),
-         xyz_ns)
-    hsrc = os.path.join(ref_root, "DFTB", "Dynamics", "dftbaby_handler.py")
-    hnames = ("getBrightestState", "getAll_S0", "getAll", "writeTimeSeries", "getAvgParticleHoleCharges",
-              "getParticleHoleChargesSuperposition")
-    hns = dict(np=np, os=os, AtomicData=ad, **errors,
-               XYZ=types.SimpleNamespace(atomlist2vector=lambda al: np.hstack([np.asarray(p, float) for _, p in al])))
-    for n in hnames:
-        exec(compile(method_source(hsrc, n, after=r"class dftbaby_handler"), "dftbaby_handler.py", "exec"), hns)
-    RefHandler = type("dftbaby_handler", (), {n: hns[n] for n in hnames})
-    src = os.path.join(ref_root, "DFTB", "Dynamics", "SurfaceHopping.py")
-    names = ("__init__", "getCenterOfMass", "shiftToCenterOfMass", "momentum", "eliminateTranslation",
-             "myCrossProduct", "angularMomentum", "momentOfInertia", "getAngularVelocity", "eliminateRotation",
-             "getKineticEnergy", "getCoordVerlet", "getVelVerlet", "initializeInterface", "getData",
-             "getLocalDiabatization", "getNewState", "normalizeCoeff", "getUniformlyRescaledVelocities",
-             "getDecoherenceE", "eliminateTransRot", "scaleVelocitiesT", "scaleVelocitiesEconst", "initiateTrajectory",
-             "verlet", "readCoordVel", "restartTrajectory", "writeStep", "writeXYZ", "writeRestart",
-             "writeNACoupling", "writeEnergies", "writeActualEnergies", "writeCoefficients", "writeState",
-             "writeLocalDiabaticEnergies", "writeLocalDiabaticCouplings", "writeTimeSeries")
-    import scipy.linalg as sla
-    out = {"dynamics_in": np.array(DYNAMICS_IN), "draws": np.array(MD_DRAWS)}
-    datas = {nst: handler_data(np.random.default_rng(20261213 + nst), nst=nst) for nst in (2, 4)}
-    for nst, d in datas.items():
-        out.update({"data%d_%s" % (nst, k): v for k, v in d.items()})
-    tmp = tempfile.mkdtemp(prefix="dftbaby_md_")
-    cwd = os.getcwd()
-    try:
-        for tag, (opts, nst, restart) in MD_SCENARIOS.items():
-            run_dir = os.path.join(tmp, tag.split("_")[0])
-            if not restart:
-                os.makedirs(run_dir)
-                open(os.path.join(run_dir, "dynamics.in"), "w").write(DYNAMICS_IN)
-            os.chdir(run_dir)
-            draws = ScriptedRandom(MD_DRAWS)
-            ns = dict(np=np, la=np.linalg, sla=sla, random=draws, AtomicData=ad,
-                      os=types.SimpleNamespace(path=os.path, system=lambda cmd: 0),
-                      XYZ=types.SimpleNamespace(read_initial_conditions=xyz_ns["read_initial_conditions"]))
-
-            def factory(symbols, coordinates, tstep, nstates, charge, sc_threshold=0.001, nst=nst):
-                h = RefHandler()
-                atomlist = [(ad.atomic_number(sy), tuple(x)) for sy, x in zip(symbols, coordinates)]
-                h.dt_nuc, h.nstates, h.sc_threshold, h.Nat = tstep, nstates, sc_threshold, len(atomlist)
-                h.masses, h.pes, h.last_step = np.array(ad.atomlist2masses(atomlist)), FakePES(datas[nst], errors), None
-                return h
-
-            ns["dftbaby_handler"] = types.SimpleNamespace(dftbaby_handler=factory)
-            for n in names:
-                exec(compile(method_source(src, n, after=r"class MolecularDynamics"), "SurfaceHopping.py", "exec"), ns)
-            MD = type("MolecularDynamics", (), {n: ns[n] for n in names})
-            buf = io.StringIO()
-            with contextlib.redirect_stdout(buf):
-                md = MD(**opts)
-                md.verlet()
-            out["md_%s_stdout" % tag] = np.array(buf.getvalue())
-            out["md_%s_files" % tag] = np.array(sorted(os.listdir(".")))
-            for fn in os.listdir("."):
-                out["md_%s_file_%s" % (tag, fn)] = np.array(open(fn).read())
-            os.chdir(cwd)
-    finally:
-        os.chdir(cwd)
-        shutil.rmtree(tmp, ignore_errors=True)
-    # HarmonicApproximation.dynamics_in_format (Dynamics/HarmonicApproximation.py:239-253), the writer of
-    # random_velocities.py, on the atoms of dynamics.in with random momenta
-    fns = {"XYZ": types.SimpleNamespace(vector2atomlist=lambda x, al: [(Z, tuple(x[3 * i:3 * i + 3]))
-                                                                       for i, (Z, _) in enumerate(al)]),
-           "AtomicData": ad}
-    exec(compile(method_source(os.path.join(ref_root, "DFTB", "Dynamics", "HarmonicApproximation.py"),
-                               "dynamics_in_format"), "HarmonicApproximation.py", "exec"), fns)
-    lines = DYNAMICS_IN.splitlines()
-    atomlist = [(ad.atomic_number(w.split()[0]), tuple(float(c) for c in w.split()[1:4])) for w in lines[1:6]]
-    q = np.hstack([p for _, p in atomlist]) + 0.01
-    mom = np.random.default_rng(20261214).random(3 * len(atomlist)) - 0.5
-    out.update(dyn_in_Z=np.array([Z for Z, _ in atomlist]), dyn_in_q=q, dyn_in_p=mom,
-               dyn_in_text=np.array(fns["dynamics_in_format"](atomlist, q, mom, "")))
-    np.savez_compressed(os.path.join(HERE, "md.npz"), **out)
-
-
-IC_XYZ = """6
-ethene
-C      0.000000    0.000000    0.667480
-C      0.000000    0.000000   -0.667480
-H      0.000000    0.922832    1.237695
-H      0.000000   -0.922832    1.237695
-H      0.000000    0.922832   -1.237695
-H      0.000000   -0.922832   -1.237695
-"""
-IC_SEED = 20261215
-
-
-def spring_hessian(x, k=0.5):
-    """Cartesian Hessian of pair springs k/2 (r_ij - r_ij(0))^2 at their rest lengths: sum of k u u^T blocks,
-    with exactly the translations and rotations as zero modes."""
-    r = np.asarray(x, dtype=np.float64).reshape(-1, 3)
-    n = len(r)
-    H = np.zeros((3 * n, 3 * n))
-    for i in range(n):
-        for j in range(i + 1, n):
-            u = r[i] - r[j]
-            u /= np.linalg.norm(u)
-            b = k * np.outer(u, u)
-            H[3 * i:3 * i + 3, 3 * i:3 * i + 3] += b
-            H[3 * j:3 * j + 3, 3 * j:3 * j + 3] += b
-            H[3 * i:3 * i + 3, 3 * j:3 * j + 3] -= b
-            H[3 * j:3 * j + 3, 3 * i:3 * i + 3] -= b
-    return H
-
-
-def spring_gradient(x, x_rest, k=0.5):
-    """Gradient of sum_ij k/2 (r_ij - r_ij(rest))^2 at the flat coordinates x."""
-    r, r0 = np.asarray(x, float).reshape(-1, 3), np.asarray(x_rest, float).reshape(-1, 3)
-    diff = r[:, None] - r[None]
-    d = np.linalg.norm(diff, axis=-1) + np.eye(len(r))
-    d0 = np.linalg.norm(r0[:, None] - r0[None], axis=-1) + np.eye(len(r))
-    return (k * ((d - d0) / d)[..., None] * diff).sum(axis=1).reshape(-1)
-
-
-def make_initial_conditions(ref_root, rng):
-    """The initial_conditions.py program (Dynamics/initial_conditions.py) run from DFTBaby's text with the
-    functions of HarmonicApproximation.py, GaussianWavepacket.Gaussian.sample_wigner and MolecularCoords
-    (their Python 2 integer divisions made explicit), on ethene with a pair-spring Hessian; the sampler is
-    numpy's legacy generator, reseeded with a fixed seed where DFTBaby uses the clock.  Also
-    numerical_hessian_G on the spring energy's analytic gradient."""
-    import contextlib
-    ad = _reference_atomic_data(ref_root)
-    dyn = os.path.join(ref_root, "DFTB", "Dynamics")
-    xyz_ns = {"np": np, "zeros": np.zeros, "atom_names": ad.atom_names, "atomic_number": ad.atomic_number,
-              "bohr_to_angs": ad.bohr_to_angs}
-    for n in ("read_xyz_it", "read_xyz", "write_xyz", "xyz2txt", "_append_xyz2txt", "atomlist2vector",
-              "vector2atomlist"):
-        exec(compile(method_source(os.path.join(ref_root, "DFTB", "XYZ.py"), n), "XYZ.py", "exec"), xyz_ns)
-    mol_ns = {"np": np, "zeros": np.zeros}
-    for n in ("center_of_mass", "shift_to_com", "inertial_tensor"):
-        src = method_source(os.path.join(ref_root, "DFTB", "Modeling", "MolecularCoords.py"), n)
-        exec(compile(src.replace("len(pos)/3", "len(pos)//3"), "MolecularCoords.py", "exec"), mol_ns)
-
-    class FixedSeedRandom:
-        def seed(self, _):
-            np.random.seed(IC_SEED)
-
-        def multivariate_normal(self, *args):
-            return np.random.multivariate_normal(*args)
-
-    ha_ns = {"np": np, "la": np.linalg, "AtomicData": ad, "join": os.path.join,
-             "XYZ": types.SimpleNamespace(**{k: xyz_ns[k] for k in ("vector2atomlist",)}),
-             "MolCo": types.SimpleNamespace(**{k: mol_ns[k] for k in ("shift_to_com", "inertial_tensor")})}
-    gw_ns = {"np": np, "la": np.linalg, "random": FixedSeedRandom(), "time": types.SimpleNamespace(time=lambda: 0.0)}
-    exec(compile(method_source(os.path.join(dyn, "GaussianWavepacket.py"), "sample_wigner", after=r"class Gaussian")
-                 .replace("dim = N/2", "dim = N//2"), "GaussianWavepacket.py", "exec"), gw_ns)
-
-    class Gaussian:
-        def __init__(self, A, B):
-            self.A, self.B = A, B
-
-        sample_wigner = gw_ns["sample_wigner"]
-
-    ha_ns["GaussianWavepacket"] = types.SimpleNamespace(Gaussian=Gaussian)
-    for n in ("numerical_hessian_G", "expected_zero_modes", "vibrational_analysis", "wigner_distribution",
-              "initial_conditions_wigner", "dynamics_in_format", "qmf3_in_format", "save_initial_conditions"):
-        src = method_source(os.path.join(dyn, "HarmonicApproximation.py"), n)
-        exec(compile(src.replace("Nat = len(x0) / 3", "Nat = len(x0) // 3"), "HarmonicApproximation.py", "exec"),
-             ha_ns)
-    # the program: the block under `if __name__ == "__main__":`
-    import textwrap
-    lines = open(os.path.join(dyn, "initial_conditions.py")).read().expandtabs(8).splitlines(keepends=True)
-    start = next(i for i, ln in enumerate(lines) if ln.startswith("if __name__"))
-    block = py2to3(textwrap.dedent("".join(lines[start + 1:])))
-    tmp = tempfile.mkdtemp(prefix="dftbaby_ic_")
-    open(os.path.join(tmp, "mol.xyz"), "w").write(IC_XYZ)
-    atomlist = xyz_ns["read_xyz"](os.path.join(tmp, "mol.xyz"))[-1]
-    x0 = xyz_ns["atomlist2vector"](atomlist)
-    hess = spring_hessian(x0)
-    np.savetxt(os.path.join(tmp, "hessian.dat"), hess)
-    os.makedirs(os.path.join(tmp, "out"))
-    prog_ns = {"HarmonicApproximation": types.SimpleNamespace(**ha_ns), "AtomicData": ad, "np": np,
-               "XYZ": types.SimpleNamespace(**xyz_ns), "__name__": "__main__"}
-    argv = sys.argv
-    sys.argv = ["initial_conditions.py", os.path.join(tmp, "mol.xyz"), os.path.join(tmp, "hessian.dat"),
-                "--Nsample=4", "--outdir=" + os.path.join(tmp, "out"), "--power_wigner=0.8"]
-    buf = io.StringIO()
-    try:
-        with contextlib.redirect_stdout(buf):
-            exec(compile(block, "initial_conditions.py", "exec"), prog_ns)
-    finally:
-        sys.argv = argv
-    out = {"hess": hess, "stdout": np.array(buf.getvalue().replace(tmp, "<tmp>"))}
-    for fn in sorted(os.listdir(os.path.join(tmp, "out"))):
-        out["file_" + fn] = np.array(open(os.path.join(tmp, "out", fn)).read())
-    # numerical Hessian of the spring energy from its analytic gradient, away from the rest geometry
-    with contextlib.redirect_stdout(io.StringIO()):
-        out["numerical_hessian"] = ha_ns["numerical_hessian_G"](lambda x: spring_gradient(x, x0), x0 + 0.01)
-    shutil.rmtree(tmp, ignore_errors=True)
-    np.savez_compressed(os.path.join(HERE, "initial_conditions.npz"), **out)
 
 
 def make_repulsive(ref_root, rng):
@@ -1511,16 +1138,8 @@ def main(ref_root, only=None):
             make_lr_e2e(ref_root, mods)
         if only in (None, "particle_hole"):
             make_particle_hole(ref_root, np.random.default_rng(20261210))
-        if only in (None, "handler"):
-            make_handler(ref_root, np.random.default_rng(20261211))
         if only in (None, "dftb2_props"):
             make_dftb2_props(ref_root, np.random.default_rng(20261212))
-        if only in (None, "xyz"):
-            make_xyz(ref_root, None)
-        if only in (None, "md"):
-            make_md(ref_root, None)
-        if only in (None, "initial_conditions"):
-            make_initial_conditions(ref_root, None)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     print("golden fixtures written to", HERE)
@@ -1529,4 +1148,6 @@ def main(ref_root, only=None):
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--only=")]
     only = next((a.split("=", 1)[1] for a in sys.argv[1:] if a.startswith("--only=")), None)
-    main(args[0] if args else "/root/reference", only)
+    if len(args) != 1:
+        sys.exit("usage: python make_golden.py REFERENCE_ROOT [--only=PART]  (REFERENCE_ROOT: the DFTBaby checkout)")
+    main(args[0], only)

@@ -88,5 +88,11 @@ def test_noalloc_refuses_requests_beyond_the_static_scratch():
                                       P(out), native.stream())
     assert rc == native.DFTB_ERR_WORKSPACE if hasattr(native, "DFTB_ERR_WORKSPACE") else rc == -4
     assert b"static array" in L.dftb_last_error()
+    # more atoms than the grid's z extent holds: refused before any launch (no orbital blocks, so the
+    # scratch itself would fit); the dummy orbitals-per-atom pointer is never read
+    assert L.dftb_trans_charges_workspace_size(70000, 0, 0) < limit
+    rc = L.dftb_trans_charges_noalloc(70000, 66000, 0, 0, P(dummy), P(dummy), P(dummy), P(dummy), P(out), P(out),
+                                      P(out), native.stream())
+    assert rc == -1 and b"65535" in L.dftb_last_error()  # DFTB_ERR_BAD_SIZE
     torch.cuda.synchronize()
     assert (out.cpu().numpy() == 0.0).all()
