@@ -403,28 +403,107 @@ __global__ void prefix_kernel(int nat, const int *opa, int *first) {
     }
 }
 
-// q[A][p][q] = 1/2 sum_{mu in A} (C1[mu][p] Sc2[mu][q] + C2[mu][q] Sc1[mu][p]); each thread 4 rows p.
-__global__ void tc_kernel(int n1, int n2, const int *first, const double *C1, const double *Sc1, const double *C2,
-                          const double *Sc2, double *q) {
-    const int qi = blockIdx.x * 32 + threadIdx.x;
-    const int p0 = blockIdx.y * 32 + threadIdx.y * 4;
-    const int A = blockIdx.z;
-    if (qi >= n2) return;
-    const int f0 = first[A], f1 = first[A + 1];
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int mu = f0; mu < f1; ++mu) {
-        const double c2 = C2[(size_t)mu * n2 + qi], s2 = Sc2[(size_t)mu * n2 + qi];
+// q[A][p][q] = 1/2 sum_{mu in A} (C1[mu][p] Sc2[mu][q] + C2[mu][q] Sc1[mu][p]).
+// The output (nat x n1 x n2 doubles) is the only large stream, so the kernel is built around writing it at
+// HBM speed: a CTA owns a TC_TP x TC_TQ tile of (p, q) for a run of TC_ATOMS atoms; per atom the rows mu of
+// C1, Sc1 (TC_TP wide) and C2, Sc2 (TC_TQ wide) are staged once in shared memory, and every thread writes
+// adjacent pairs of q with 16-byte stores (each warp stores 512 contiguous bytes of one row p).  Atoms with
+// up to TC_MAXO orbitals (s, p, d shells) take the staged path; larger ones read their rows from global
+// memory directly.
+constexpr int TC_TP = 64, TC_TQ = 128, TC_THREADS = 256, TC_MAXO = 9, TC_ATOMS = 8, TC_ROWS = 8;
+
+template <bool VEC>
+__global__ void __launch_bounds__(TC_THREADS) tc_tile_kernel(int nat, int n1, int n2, const int *first,
+                                                             const double *__restrict__ C1,
+                                                             const double *__restrict__ Sc1,
+                                                             const double *__restrict__ C2,
+                                                             const double *__restrict__ Sc2, double *q) {
+    __shared__ double sC1[TC_MAXO][TC_TP], sS1[TC_MAXO][TC_TP];
+    __shared__ __align__(16) double sC2[TC_MAXO][TC_TQ], sS2[TC_MAXO][TC_TQ];
+    const int tid = threadIdx.x;
+    const int qp = tid & 63, pg = tid >> 6;  // q pair within the tile; row group
+    const int q0 = blockIdx.x * TC_TQ, p0 = blockIdx.y * TC_TP;
+    const int qg = q0 + 2 * qp;
+    const int A0 = blockIdx.z * TC_ATOMS;
+    const int A1 = min(nat, A0 + TC_ATOMS);
+    for (int A = A0; A < A1; ++A) {
+        const int f0 = first[A], nA = first[A + 1] - f0;
+        const bool staged = nA <= TC_MAXO;
+        if (staged) {
+            __syncthreads();  // the previous atom's readers are done with the buffers
+            for (int i = tid; i < nA * TC_TP; i += TC_THREADS) {
+                const int j = i / TC_TP, pp = i % TC_TP, p = p0 + pp;
+                const size_t o = (size_t)(f0 + j) * n1 + p;
+                sC1[j][pp] = p < n1 ? C1[o] : 0.0;
+                sS1[j][pp] = p < n1 ? Sc1[o] : 0.0;
+            }
+            for (int i = tid; i < nA * TC_TQ; i += TC_THREADS) {
+                const int j = i / TC_TQ, qq = i % TC_TQ, qi = q0 + qq;
+                const size_t o = (size_t)(f0 + j) * n2 + qi;
+                sC2[j][qq] = qi < n2 ? C2[o] : 0.0;
+                sS2[j][qq] = qi < n2 ? Sc2[o] : 0.0;
+            }
+            __syncthreads();
+        }
+        for (int batch = 0; batch < TC_TP / (4 * TC_ROWS); ++batch) {
+            double acc0[TC_ROWS], acc1[TC_ROWS];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int p = p0 + r;
-            if (p < n1) acc[r] += C1[(size_t)mu * n1 + p] * s2 + c2 * Sc1[(size_t)mu * n1 + p];
+            for (int r = 0; r < TC_ROWS; ++r) acc0[r] = acc1[r] = 0.0;
+            const int pl0 = pg + 4 * batch * TC_ROWS;  // local row of r = 0; rows step by 4
+            if (staged) {
+                for (int j = 0; j < nA; ++j) {
+                    const double c2a = sC2[j][2 * qp], c2b = sC2[j][2 * qp + 1];
+                    const double s2a = sS2[j][2 * qp], s2b = sS2[j][2 * qp + 1];
+#pragma unroll
+                    for (int r = 0; r < TC_ROWS; ++r) {
+                        const double a1 = sC1[j][pl0 + 4 * r], b1 = sS1[j][pl0 + 4 * r];
+                        acc0[r] += a1 * s2a + c2a * b1;
+                        acc1[r] += a1 * s2b + c2b * b1;
+                    }
+                }
+            } else {
+                for (int j = 0; j < nA; ++j) {
+                    const size_t r2 = (size_t)(f0 + j) * n2;
+                    const double c2a = qg < n2 ? C2[r2 + qg] : 0.0, s2a = qg < n2 ? Sc2[r2 + qg] : 0.0;
+                    const double c2b = qg + 1 < n2 ? C2[r2 + qg + 1] : 0.0;
+                    const double s2b = qg + 1 < n2 ? Sc2[r2 + qg + 1] : 0.0;
+#pragma unroll
+                    for (int r = 0; r < TC_ROWS; ++r) {
+                        const int p = p0 + pl0 + 4 * r;
+                        const size_t r1 = (size_t)(f0 + j) * n1 + p;
+                        const double a1 = p < n1 ? C1[r1] : 0.0, b1 = p < n1 ? Sc1[r1] : 0.0;
+                        acc0[r] += a1 * s2a + c2a * b1;
+                        acc1[r] += a1 * s2b + c2b * b1;
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < TC_ROWS; ++r) {
+                const int p = p0 + pl0 + 4 * r;
+                if (p >= n1 || qg >= n2) continue;
+                double *row = q + ((size_t)A * n1 + p) * n2;
+                if (VEC && qg + 1 < n2) {
+                    *reinterpret_cast<double2 *>(row + qg) = make_double2(0.5 * acc0[r], 0.5 * acc1[r]);
+                } else {
+                    row[qg] = 0.5 * acc0[r];
+                    if (qg + 1 < n2) row[qg + 1] = 0.5 * acc1[r];
+                }
+            }
         }
     }
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const int p = p0 + r;
-        if (p < n1) q[((size_t)A * n1 + p) * n2 + qi] = 0.5 * acc[r];
-    }
+}
+
+// one (n1 x n2) block of transition charges for all atoms
+int launch_tc(int nat, int n1, int n2, const int *first, const double *C1, const double *Sc1, const double *C2,
+              const double *Sc2, double *out, cudaStream_t st, const char *where) {
+    dim3 grid(cdiv(n2, TC_TQ), cdiv(n1, TC_TP), cdiv(nat, TC_ATOMS));
+    if (grid.y > 65535u || grid.z > 65535u) return fail(DFTB_ERR_BAD_SIZE, "trans_charges: grid too large");
+    // 16-byte stores need every row of the output to start on an even index (and an aligned base)
+    if (n2 % 2 == 0 && ((uintptr_t)out & 15) == 0)
+        tc_tile_kernel<true><<<grid, TC_THREADS, 0, st>>>(nat, n1, n2, first, C1, Sc1, C2, Sc2, out);
+    else
+        tc_tile_kernel<false><<<grid, TC_THREADS, 0, st>>>(nat, n1, n2, first, C1, Sc1, C2, Sc2, out);
+    return check_launch(where);
 }
 
 // diagonal q^{pp}_A
@@ -929,6 +1008,7 @@ int dftb_trans_charges(int norb, int nat, int nocc, int nvirt, const double *co,
     double *sco, *scv;
     int *first;
     if (nat > norb) return fail(DFTB_ERR_BAD_SIZE, "trans_charges: nat > norb");
+    if (nat > 65535) return fail(DFTB_ERR_BAD_SIZE, "trans_charges: nat > 65535");
     int rc = trans_charges_common(norb, nat, nocc, nvirt, co, cv, Sm, opa, work, work_bytes, st, &sco, &scv, &first);
     if (rc) return rc;
     struct Blk {
@@ -940,10 +1020,8 @@ int dftb_trans_charges(int norb, int nat, int nocc, int nvirt, const double *co,
                  {q_vv, cv, scv, cv, scv, nvirt, nvirt}};
     for (auto &b : blks) {
         if (!b.out || b.n1 == 0 || b.n2 == 0) continue;
-        if (nat > 65535) return fail(DFTB_ERR_BAD_SIZE, "trans_charges: nat > 65535");
-        dim3 grid(cdiv(b.n2, 32), cdiv(b.n1, 32), nat);
-        tc_kernel<<<grid, dim3(32, 8), 0, st>>>(b.n1, b.n2, first, b.c1, b.s1, b.c2, b.s2, b.out);
-        if ((rc = check_launch("tc_kernel"))) return rc;
+        if ((rc = launch_tc(nat, b.n1, b.n2, first, b.c1, b.s1, b.c2, b.s2, b.out, st, "tc_tile_kernel")))
+            return rc;
     }
     return DFTB_OK;
 }
@@ -1179,9 +1257,8 @@ extern "C" int dftb_trans_charges_noalloc(int norb, int nat, int nocc, int nvirt
                  {q_vv, cv, scv, cv, scv, nvirt, nvirt}};
     for (auto &b : blks) {
         if (!b.out || b.n1 == 0 || b.n2 == 0) continue;
-        dim3 grid(cdiv(b.n2, 32), cdiv(b.n1, 32), nat);
-        tc_kernel<<<grid, dim3(32, 8), 0, st>>>(b.n1, b.n2, first, b.c1, b.s1, b.c2, b.s2, b.out);
-        if ((rc = check_launch("tc_kernel (noalloc)"))) return rc;
+        if ((rc = launch_tc(nat, b.n1, b.n2, first, b.c1, b.s1, b.c2, b.s2, b.out, st, "tc_tile_kernel (noalloc)")))
+            return rc;
     }
     return DFTB_OK;
 }

@@ -302,8 +302,17 @@ class DFTB2(object):
 
     def runSCC(self, maxiter=1000, scf_conv=1.0e-10, start_from_previous=1, mixing_threshold=1.0e-3,
                density_mixer="default", fock_interpolator=None, level_shift=0.1, HOMO_LUMO_tol=0.05,
-               linear_mixing_coefficient=0.33):
-        """Self-consistent charges (DFTB2.runSCC, DFTB2.py:940-1160), T = 0."""
+               linear_mixing_coefficient=0.33, eigensolver="full", subspace_start=0.1):
+        """Self-consistent charges (DFTB2.runSCC, DFTB2.py:940-1160), T = 0.
+
+        eigensolver (not in DFTBaby): "full" solves H C = S C e in every iteration, as DFTBaby does.
+        "subspace" does so only until the relative change drops below subspace_start; after that each
+        iteration moves the occupied space of the previous iteration onto the new Hamiltonian by a few
+        Jacobi-type rotations (``_track_occupied``, a handful of Norb^2 Nocc GEMMs instead of a dense
+        eigensolve), and the last, converged iteration solves the full problem again, so the orbitals
+        and energies handed on are exact eigenpairs.  The density of a T = 0 closed shell depends on the
+        occupied space only, so the mixing schedule, the convergence test and the fixed point are
+        DFTBaby's; iterates differ by the rotations' residual (below 1e-6 of the last relative change)."""
         if fock_interpolator is not None:
             raise ValueError("Fock interpolation is not implemented")
         if isinstance(density_mixer, str):
@@ -341,6 +350,12 @@ class DFTB2(object):
         dq = torch.empty(nat, dtype=torch.float64, device=dev)
         nfull = int(self.Nelec_val // 2)
         HOMO = nfull - 1 if self.Nelec_val - 2 * nfull == 0 else nfull
+        if eigensolver not in ("full", "subspace"):
+            raise ValueError("eigensolver must be 'full' or 'subspace'")
+        # occupied-space tracking needs a closed shell with at least one empty orbital
+        track = eigensolver == "subspace" and self.Nelec_val == 2 * nfull and 0 < nfull < norb
+        self.subspace_iterations = 0
+        tracked = None
         for self.i in range(maxiter):
             native.call("dftb_scc_hamiltonian", norb, nat, P(self._ind), P(self.H0), P(self.S), P(self.gamma),
                         P(self.dq), P(estat), P(H), st)
@@ -355,26 +370,40 @@ class DFTB2(object):
                     b *= 0.5
                 if self.relative_change < 1.0e3 * scf_conv:
                     b = 0.0
-            if shift_flag and b > 0.0:
-                # level shift of the virtual block in the basis of the last MOs (DFTB2.py:1059-1081)
-                B = self.orbs
-                Hm = B.T @ Hk @ B
-                virt = torch.nonzero(self.f == 0.0).flatten()
-                Hm[virt, virt] += b
-                self.orbe, Cp = torch.linalg.eigh(Hm)
-                self.orbs = B @ Cp
+            step_tracked = False
+            if (track and tracked is not None and not converged and not shift_flag
+                    and self.relative_change < subspace_start):
+                moved = self._track_occupied(Hk, tracked, self.relative_change)
+                if moved is not None:
+                    tracked, step_tracked = moved, True
+            if step_tracked:
+                Co = tracked[0]
+                Pnew = 2.0 * (Co @ Co.T)
+                self.subspace_iterations += 1
             else:
-                # L^-1 Hk L^-T and L^-T C' by triangular solves (n^3 FLOPs each instead of the
-                # 2 n^3 of a product with an explicit inverse); eigh reads the lower triangle
-                Y = torch.linalg.solve_triangular(self._L, Hk, upper=False)
-                Hp = torch.linalg.solve_triangular(self._L, Y.mT, upper=False).mT
-                self.orbe, Cp = torch.linalg.eigh(Hp)
-                self.orbs = torch.linalg.solve_triangular(self._L.mT, Cp, upper=True)
-            have_orbe = True
-            self.f = self._occupation(self.orbe)
-            occ = self.f > 0.0
-            Cocc = self.orbs[:, occ]
-            Pnew = (Cocc * self.f[occ]) @ Cocc.T
+                if shift_flag and b > 0.0:
+                    # level shift of the virtual block in the basis of the last MOs (DFTB2.py:1059-1081)
+                    B = self.orbs
+                    Hm = B.T @ Hk @ B
+                    virt = torch.nonzero(self.f == 0.0).flatten()
+                    Hm[virt, virt] += b
+                    self.orbe, Cp = torch.linalg.eigh(Hm)
+                    self.orbs = B @ Cp
+                else:
+                    # L^-1 Hk L^-T and L^-T C' by triangular solves (n^3 FLOPs each instead of the
+                    # 2 n^3 of a product with an explicit inverse); eigh reads the lower triangle
+                    Y = torch.linalg.solve_triangular(self._L, Hk, upper=False)
+                    Hp = torch.linalg.solve_triangular(self._L, Y.mT, upper=False).mT
+                    self.orbe, Cp = torch.linalg.eigh(Hp)
+                    self.orbs = torch.linalg.solve_triangular(self._L.mT, Cp, upper=True)
+                have_orbe = True
+                self.f = self._occupation(self.orbe)
+                occ = self.f > 0.0
+                Cocc = self.orbs[:, occ]
+                Pnew = (Cocc * self.f[occ]) @ Cocc.T
+                if track and not shift_flag:
+                    # eigh returns ascending energies: the occupied space is the first nfull columns
+                    tracked = (self.orbs[:, :nfull], self.orbs[:, nfull:], self.orbe[:nfull], self.orbe[nfull:])
             if density_mixer is not None and not converged and mixing_flag:
                 Pnew = density_mixer.next_approximation(Pnew)
             elif not converged:
@@ -392,8 +421,13 @@ class DFTB2(object):
                 rel = torch.linalg.norm(P_last - self.P) / torch.linalg.norm(self.P)
             else:
                 rel = torch.tensor(self.relative_change, dtype=torch.float64, device=dev)
-            gap = self.orbe[HOMO + 1] - self.orbe[HOMO] if HOMO + 1 < norb else torch.zeros((), device=dev,
-                                                                                           dtype=torch.float64)
+            if step_tracked:
+                # diagonal estimates of the occupied and virtual levels
+                gap = tracked[3].min() - tracked[2].max()
+            elif HOMO + 1 < norb:
+                gap = self.orbe[HOMO + 1] - self.orbe[HOMO]
+            else:
+                gap = torch.zeros((), device=dev, dtype=torch.float64)
             host = torch.stack([rel.reshape(()), self.dq.sum(), gap.reshape(())]).cpu().numpy()
             self.relative_change, sum_dq, self.HLgap = float(host[0]), float(host[1]), float(host[2])
             if abs(sum_dq + self.charge) > 1.0e-5:
@@ -416,6 +450,40 @@ class DFTB2(object):
         self.scc_iterations = self.i + 1
         if getattr(self, "save_converged_charges", None) is not None:
             np.savetxt(os.path.expandvars(os.path.expanduser(self.save_converged_charges)), self.dq.cpu().numpy())
+
+    def _track_occupied(self, H, tracked, rel, max_steps=8):
+        """Move an S-orthonormal occupied/virtual split (Co, Cv) onto the invariant subspaces of H.
+
+        Each step forms the coupling block F = Cv^T H Co and rotates the two spaces by the first-order
+        (Jacobi) correction Y_ai = F_ai / (e_i - e_a), with e_i = diag(Co^T H Co) and e_a the virtual
+        levels of the last full solve: Co + Cv Y and Cv - Co Y^T stay exactly S-orthogonal to each other,
+        and their Gram matrices I + Y^T Y and I + Y Y^T renormalise them (Cholesky).  Steps repeat until
+        max |F| < max(1e-13, 1e-6 rel), rel being the last relative density change.  Returns the new
+        (Co, Cv, e_o, e_v), or None when an occupied level is not below every virtual one or the rotations
+        have not converged after max_steps; the caller then solves the full eigenproblem."""
+        Co, Cv, eo, ev = tracked
+        tol = max(1.0e-13, 1.0e-6 * rel)
+        no, nv = Co.shape[1], Cv.shape[1]
+        for step in range(max_steps + 1):
+            HCo = H @ Co
+            F = Cv.T @ HCo
+            eo = torch.sum(Co * HCo, dim=0)
+            den = eo[None, :] - ev[:, None]
+            fmax, dmax = torch.stack([torch.max(torch.abs(F)), torch.max(den)]).cpu().numpy()
+            if not np.isfinite(fmax) or dmax >= 0.0:
+                return None
+            if fmax < tol:
+                return Co, Cv, eo, ev
+            if step == max_steps:
+                return None
+            Y = F / den
+            Con = torch.addmm(Co, Cv, Y)
+            Cvn = torch.addmm(Cv, Co, Y.T, alpha=-1.0)
+            Lo, io = torch.linalg.cholesky_ex(torch.addmm(torch.eye(no, dtype=Y.dtype, device=Y.device), Y.T, Y))
+            Lv, iv = torch.linalg.cholesky_ex(torch.addmm(torch.eye(nv, dtype=Y.dtype, device=Y.device), Y, Y.T))
+            Co = torch.linalg.solve_triangular(Lo.mT, Con, upper=True, left=False)
+            Cv = torch.linalg.solve_triangular(Lv.mT, Cvn, upper=True, left=False)
+        return None
 
     def setCharge(self, charge):
         """DFTB2.setCharge (DFTB2.py:429-435): net charge (units of e) and the valence electron count."""

@@ -320,13 +320,20 @@ class LR_TDDFTB:
     def getEnergies(self, nr_active_occ=None, nr_active_virt=None, select_lm=None, oszis="Dipoles",
                     response_method="Casida", multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5,
                     diag_maxiter=50, diag_check=0, diag_L2threshold=0.0, diag_selected_irreps=None,
-                    ct_correction=0, stability=0, precision="fp64", refine_fp64=True, guess_model=None, **scf_opts):
+                    ct_correction=0, stability=0, precision="fp64", refine_fp64=True, refine_iterations=None,
+                    guess_model=None, **scf_opts):
         """LR_TDDFTB.getEnergies (LR_TDDFTB.py:37-114); returns (Omega, f) in Hartree.
 
         precision="mixed" (not in DFTBaby) evaluates the long-range exchange of
         the Davidson products with split-precision BF16 tensor-core GEMMs; with
-        refine_fp64 the mixed result then seeds the FP64 solver, whose residual
-        test (diag_conv) decides convergence as in the plain path.
+        refine_fp64 the mixed result then seeds the FP64 solver.  With
+        refine_iterations=None that solver iterates until its residual test
+        (diag_conv) passes, as in the plain path; with refine_iterations=n it
+        re-projects the operator, with FP64 products, onto the converged vectors
+        (and, for n > 0, onto n rounds of FP64 residual corrections) and returns
+        those Ritz pairs: FP64 corrections of the mixed-precision products at the
+        cost of 2 nstates (n + 1) FP64 product columns.  Its FP64 residual norms
+        are in stats["refine_residual"].
         guess_model (not in DFTBaby): a learned.GuessNet whose pair scores choose
         the initial Davidson vectors and whose shifts correct the diagonal
         preconditioner when no warm start is available; the solve runs to the
@@ -359,7 +366,7 @@ class LR_TDDFTB:
         self._solve_lr_equations(multiplicity=multiplicity, nstates=nstates, diag_ifact=diag_ifact,
                                  diag_conv=diag_conv, diag_maxiter=diag_maxiter, diag_check=diag_check,
                                  diag_L2threshold=diag_L2threshold, precision=precision, refine_fp64=refine_fp64,
-                                 guess_model=guess_model)
+                                 refine_iterations=refine_iterations, guess_model=guess_model)
         ev[2].record()
         verbose = getattr(d, "verbose", 0) > 0
         if oszis == "Dipoles":
@@ -396,7 +403,7 @@ class LR_TDDFTB:
 
     def _solve_lr_equations(self, multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5, diag_maxiter=50,
                             diag_check=0, diag_L2threshold=0.0, precision="fp64", refine_fp64=True,
-                            guess_model=None):
+                            refine_iterations=None, guess_model=None):
         """LR_TDDFTB._solve_lr_equations (LR_TDDFTB.py:403-527)."""
         d = self.dftb2
         dev = d.device
@@ -474,7 +481,16 @@ class LR_TDDFTB:
                 self.stats["mixed_products"] = mixed.products_applied
                 XmY0, XpY0, Om0, C0 = XmY, XpY, Om, C
                 del mixed
-            if precision != "mixed" or refine_fp64:
+            if precision == "mixed" and refine_fp64 and refine_iterations is not None:
+                # FP64 corrections of the converged mixed-precision block: Rayleigh-Ritz with FP64 products
+                rstats = {}
+                Om, C, XmY, XpY = nonhermitian_davidson(prod, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
+                                                        maxiter=int(refine_iterations) + 1, XmYguess=XmY0,
+                                                        XpYguess=XpY0, w_guess=Om0, stats=rstats,
+                                                        ritz_on_guess=True, raise_on_maxiter=False)
+                self.stats["refine_iterations"] = rstats.get("iterations")
+                self.stats["refine_residual"] = float(np.max(rstats["residual_norms"][-1]))
+            elif precision != "mixed" or refine_fp64:
                 def run(extra):
                     return nonhermitian_davidson(prod, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
                                                  maxiter=diag_maxiter, XmYguess=XmY0, XpYguess=XpY0, w_guess=Om0,
@@ -622,6 +638,19 @@ class LR_TDDFTB:
         else:
             self.oscillator_strength = 0.0 * self.Omega
         return self.oscillator_strength
+
+    def oscillatorStrengthsXpY(self):
+        """f_XY = 2/3 Omega |sum_ia t_ia (X+Y)_ia|^2 (not in DFTBaby), with (X+Y).(X-Y) = 1 per state.
+
+        DFTBaby's f (getOscillatorStrengths) contracts the dipoles with C; with the long-range correction
+        the solver's C = b.Tb (Solver.py:910-911) depends on the whole expansion space and keeps changing
+        after Omega and X+/-Y have converged.  X+Y is a right eigenvector of the problem and converges with
+        the residual, so f_XY compares two solvers (or precisions) by their converged states alone.
+        Needs oszis="Dipoles" (the active-block dipoles t_ia of the last getEnergies)."""
+        t = self.tdip_ov  # (3, nocc, nvirt)
+        tx = torch.einsum("kia,cia->ck", self.XpY.to(torch.float64), t)
+        Om = torch.as_tensor(self.Omega, device=tx.device)
+        return (2.0 / 3.0 * Om * torch.sum(tx * tx, dim=0)).cpu().numpy()
 
     def getExcEnergies(self):
         return self.Omega

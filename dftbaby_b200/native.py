@@ -15,7 +15,9 @@ LIB_PATH = os.path.join(HERE, "lib", "libdftbaby_b200.so")
 DFTB_OK = 0
 DFTB_ERR_WORKSPACE = -4
 DFTB_ERR_UNSUPPORTED = -5
-_ERRORS = {-1: "bad size", -2: "null pointer", -3: "CUDA error", -4: "workspace too small", -5: "unsupported"}
+DFTB_ERR_NOT_CONVERGED = -6
+_ERRORS = {-1: "bad size", -2: "null pointer", -3: "CUDA error", -4: "workspace too small", -5: "unsupported",
+           -6: "not converged"}
 
 
 class NativeUnavailable(RuntimeError):
@@ -81,6 +83,12 @@ _SIGNATURES = {
     "dftb_batched_eigh_workspace_size": (_I, [_I, _I, ctypes.POINTER(_Z)]),
     "dftb_batched_eigh": (_I, [_I, _I, _P, _P, _P, _Z, _P, _P]),
     "dftb_eigh_last_error": (ctypes.c_char_p, []),
+    "dftb_solver_workspace_size": (_Z, [_I, _I, _I, _I, _I]),
+    "dftb_solver_create": (_I, [_I, _I, _I, _I, _I, _P, _Z, ctypes.POINTER(_P)]),
+    "dftb_solver_solve_hermitian": (_I, [_P, _P, _P, _P, _D, _I, _I, _P, _P, _P, _P, ctypes.POINTER(_I), _P]),
+    "dftb_solver_reset": (_I, [_P]),
+    "dftb_solver_destroy": (_I, [_P]),
+    "dftb_solver_last_error": (ctypes.c_char_p, []),
 }
 
 
@@ -121,7 +129,8 @@ def check(rc, what):
         msg = ""
         if _lib is not None:
             msg = (_lib.dftb_last_error().decode() or _lib.dftb_grad_last_error().decode()
-                   or _lib.dftb_mlp_last_error().decode() or _lib.dftb_eigh_last_error().decode())
+                   or _lib.dftb_mlp_last_error().decode() or _lib.dftb_eigh_last_error().decode()
+                   or _lib.dftb_solver_last_error().decode())
         raise NativeError("%s failed (%s): %s" % (what, _ERRORS.get(rc, rc), msg))
 
 

@@ -246,7 +246,8 @@ def _sqrtm_spd(M):
 
 def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxiter=10, XmYguess=None,
                           XpYguess=None, w_guess=None, stats=None, symmetrize=False, accept_guess=False,
-                          Cguess=None, guess_key=None, precond_diag=None):
+                          Cguess=None, guess_key=None, precond_diag=None, ritz_on_guess=False,
+                          raise_on_maxiter=True):
     """Lowest nstates of the non-Hermitian TD-DFTB problem (Stratmann-Scuseria-Frisch).
 
     products(V) returns ((A+B).V, (A-B).V) for a (nov, ncol) block.
@@ -262,6 +263,11 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
     the whole basis by QR at the end of iteration 0, which spans the same space.
     guess_key and precond_diag replace omega in the choice of the initial unit
     vectors and in the preconditioner, as in hermitian_davidson.
+    ritz_on_guess=True (refinement of a solution found with other products)
+    projects the operator onto the guess block already in iteration 0 and takes
+    its Ritz pairs; raise_on_maxiter=False then returns the Ritz pairs of the
+    last iteration instead of raising when maxiter is reached (the residual
+    norms of every iteration are in stats["residual_norms"]).
     """
     nocc, nvirt = omega.shape
     om = omega.reshape(-1).contiguous()
@@ -283,7 +289,7 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
     l = lmax
     for it in range(maxiter):
         bs, AP, AM = B.bs, B.prod(0), B.prod(1)
-        if XpYguess is None or it > 0:
+        if XpYguess is None or it > 0 or ritz_on_guess:
             Mp = B.M[0]
             Mm = B.M[1]
             if symmetrize:
@@ -318,7 +324,9 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
         norms = normsL + normsR
         if stats is not None:
             stats.setdefault("residual_norms", []).append(norms.copy())
-        if (norms < conv).all() and (it > 0 or accept_guess):
+        if (norms < conv).all() and (it > 0 or accept_guess or ritz_on_guess):
+            break
+        if it == maxiter - 1 and not raise_on_maxiter:
             break
         dkmax = min(kmax - l, 2 * k)
         eps = 0.01 * conv
@@ -352,7 +360,7 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
         stats["iterations"] = it + 1
         stats["subspace"] = l
     Omega = w[:k]
-    if XpYguess is not None and it == 0:
+    if XpYguess is not None and it == 0 and not ritz_on_guess:
         if Cguess is None:
             raise ExcitedStatesError("a guess was accepted without its C vectors")
         C = Cguess.reshape(k, -1).T
@@ -360,3 +368,59 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
         C = bs @ Tb[:, :k]
     shape = (k, nocc, nvirt)
     return Omega, C.T.reshape(shape), Lk.T.reshape(shape), Rk.T.reshape(shape)
+
+
+class DeviceSolver:
+    """The fused device solve of the C ABI (dftb_solver_* in include/dftbaby_b200.h) from Python.
+
+    One handle owns the Davidson space for nstates states of an (nocc x nvirt) problem on nat atoms, in a
+    device workspace allocated here once; ``solve_hermitian`` runs Solver.HermitianDavidson
+    (DFTB/Solver.py:404-578) entirely inside the library and returns (Omega, C, XmY, XpY, iterations) like
+    ``hermitian_davidson``.  A later solve with warm_start=True starts from the previous X+Y, as DFTBaby's
+    solver does when it is handed the last solution (Solver.py:461-478)."""
+
+    def __init__(self, nat, nocc, nvirt, nstates, max_iter=50, device=None):
+        import ctypes
+        L = native.load()
+        self.nat, self.nocc, self.nvirt, self.k, self.max_iter = nat, nocc, nvirt, nstates, max_iter
+        nbytes = L.dftb_solver_workspace_size(nat, nocc, nvirt, nstates, max_iter)
+        if nbytes == 0:
+            raise native.NativeError("dftb_solver_workspace_size: sizes out of range or cuBLAS/cuSOLVER missing")
+        self.ws = torch.empty(nbytes, dtype=torch.uint8, device=device or torch.device("cuda"))
+        h = ctypes.c_void_p()
+        native.check(L.dftb_solver_create(nat, nocc, nvirt, nstates, max_iter, native.ptr(self.ws), nbytes,
+                                          ctypes.byref(h)), "dftb_solver_create")
+        self.h = h
+
+    def solve_hermitian(self, gamma, q_ov, omega, conv=1.0e-5, maxiter=None, warm_start=True):
+        import ctypes
+        L = native.load()
+        dev = self.ws.device
+        k, shape = self.k, (self.k, self.nocc, self.nvirt)
+        Om = torch.empty(k, dtype=torch.float64, device=dev)
+        C, XmY, XpY = (torch.empty(shape, dtype=torch.float64, device=dev) for _ in range(3))
+        it = ctypes.c_int(0)
+        maxiter = self.max_iter if maxiter is None else min(maxiter, self.max_iter)
+        gamma, q_ov, omega = gamma.contiguous(), q_ov.contiguous(), omega.contiguous()
+        rc = L.dftb_solver_solve_hermitian(self.h, native.ptr(gamma), native.ptr(q_ov), native.ptr(omega),
+                                           float(conv), int(maxiter), int(bool(warm_start)), native.ptr(Om),
+                                           native.ptr(C), native.ptr(XmY), native.ptr(XpY), ctypes.byref(it),
+                                           native.stream())
+        if rc == native.DFTB_ERR_NOT_CONVERGED:
+            raise ExcitedStatesNotConverged(L.dftb_solver_last_error().decode())
+        native.check(rc, "dftb_solver_solve_hermitian")
+        return Om, C, XmY, XpY, it.value
+
+    def reset(self):
+        native.check(native.load().dftb_solver_reset(self.h), "dftb_solver_reset")
+
+    def close(self):
+        if getattr(self, "h", None) is not None:
+            native.load().dftb_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -34,6 +34,7 @@ extern "C" {
 #define DFTB_ERR_CUDA -3        /* a CUDA launch or runtime call failed       */
 #define DFTB_ERR_WORKSPACE -4   /* the workspace is smaller than required     */
 #define DFTB_ERR_UNSUPPORTED -5 /* angular momentum or table layout not handled */
+#define DFTB_ERR_NOT_CONVERGED -6 /* an iterative solve hit its iteration limit */
 
 /* Library version and the CUDA error string of the last failing call on this
  * host thread (empty if none). */
@@ -337,6 +338,37 @@ const char *dftb_mlp_last_error(void);
 int dftb_batched_eigh_workspace_size(int n, int batch, size_t *bytes);
 int dftb_batched_eigh(int n, int batch, double *A, double *W, void *work, size_t work_bytes, int *info, void *stream);
 const char *dftb_eigh_last_error(void);
+
+/* ---- the fused device solve ------------------------------------------------------
+ * Replaces the Davidson branch of LR_TDDFTB._solve_lr_equations (DFTB/LR_TDDFTB.py:403-527)
+ * for the problem without long-range correction, Solver.HermitianDavidson
+ * (DFTB/Solver.py:404-578): R T = Omega^2 T with R = omega^2 + 4 sqrt(omega) q_ov^T gamma q_ov sqrt(omega).
+ * An opaque handle owns the expansion space, its products, the projected matrix and the previous
+ * solution (the warm start of the next solve, Solver.py:461-478), in device memory the caller
+ * provides once: dftb_solver_workspace_size() bytes, or 0 when the sizes are out of range or cuBLAS /
+ * cuSOLVER (resolved at run time) are missing.  The handle also holds one cuBLAS and one cuSOLVER
+ * handle; dftb_solver_destroy releases them (not the workspace).  One handle per host thread: calls
+ * on the same handle must not overlap.
+ *   max_iter bounds the Davidson iterations of every solve (the space holds nstates (max_iter + 1)
+ *   vectors at most, and at most 46340);
+ *   gamma (nat, nat), q_ov (nat, nocc, nvirt), omega (nocc, nvirt): as for dftb_hermitian_rv;
+ *   conv: the residual-norm threshold of every state (DFTBaby's diag_conv); maxiter <= max_iter;
+ *   warm_start != 0 starts from the previous solve's X+Y (ignored before the first solve or after
+ *   dftb_solver_reset);
+ *   outputs (device): Omega (nstates), C, XmY, XpY (nstates, nocc, nvirt), each but Omega may be NULL;
+ *   iterations (host, may be NULL): Davidson iterations taken.
+ * Returns DFTB_ERR_NOT_CONVERGED (DFTBaby's ExcitedStatesNotConverged) when maxiter is reached.
+ * The call synchronises the stream once per iteration to read the residual norms. */
+typedef struct dftb_solver dftb_solver;
+size_t dftb_solver_workspace_size(int nat, int nocc, int nvirt, int nstates, int max_iter);
+int dftb_solver_create(int nat, int nocc, int nvirt, int nstates, int max_iter, void *work, size_t work_bytes,
+                       dftb_solver **out);
+int dftb_solver_solve_hermitian(dftb_solver *s, const double *gamma, const double *q_ov, const double *omega,
+                                double conv, int maxiter, int warm_start, double *Omega, double *C, double *XmY,
+                                double *XpY, int *iterations, void *stream);
+int dftb_solver_reset(dftb_solver *s);
+int dftb_solver_destroy(dftb_solver *s);
+const char *dftb_solver_last_error(void);
 
 #ifdef __cplusplus
 }

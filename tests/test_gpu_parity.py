@@ -113,6 +113,36 @@ def test_trans_charges_and_monopoles_match_oracle(dev):
     assert np.abs(dq.cpu().numpy() - dqo).max() < 1e-13
 
 
+@pytest.mark.parametrize("nocc,nvirt", [(130, 258), (67, 257), (1, 3)])
+def test_trans_charges_ragged_tiles_match_oracle(dev, nocc, nvirt):
+    """Shapes that cut every tile of the transition-charge kernel (64 rows p x 128 columns q x 8 atoms):
+    partial tiles in both directions, even and odd row lengths (16-byte and scalar stores), 19 atoms (a
+    partial atom run) with 1, 4, 9 and 10 orbitals (the last one above the staged limit, read from global
+    memory).  Random coefficients and overlap: the kernel is plain algebra on them."""
+    rng = np.random.default_rng(nocc + nvirt)
+    opa = np.array([4, 1, 9, 1, 10, 4, 4, 1, 1, 4, 9, 4, 1, 1, 4, 4, 1, 4, 4], dtype=np.int32)
+    nat, norb = len(opa), int(opa.sum())
+    co = rng.standard_normal((norb, nocc))
+    cv = rng.standard_normal((norb, nvirt))
+    Sm = rng.standard_normal((norb, norb))
+    Sm = 0.5 * (Sm + Sm.T)
+    q_oo, q_ov, q_vv = O.trans_charges(co, cv, Sm, opa)
+    L = native.load()
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    Co, Cv, S, opa_d = t(co), t(cv), t(Sm), t(opa)
+    outs = [torch.full(sh, np.nan, dtype=torch.float64, device=dev)
+            for sh in ((nat, nocc, nocc), (nat, nocc, nvirt), (nat, nvirt, nvirt))]
+    nbytes = L.dftb_trans_charges_workspace_size(norb, nocc, nvirt)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    P = native.ptr
+    native.call("dftb_trans_charges", norb, nat, nocc, nvirt, P(Co), P(Cv), P(S), P(opa_d), P(outs[0]), P(outs[1]),
+                P(outs[2]), P(ws), nbytes, native.stream())
+    for a, b in zip(outs, (q_oo, q_ov, q_vv)):
+        a = a.cpu().numpy()
+        assert np.isfinite(a).all()
+        assert np.abs(a - b).max() < 1e-12 * max(1.0, np.abs(b).max())
+
+
 def test_products_match_reference_golden(dev, golden):
     """(A+B).v, (A-B).v (transition-charge form) against DFTBaby's own _ApBv/_AmBv."""
     g = golden("solvers_c10h12.npz")

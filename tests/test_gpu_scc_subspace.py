@@ -1,0 +1,38 @@
+"""The SCC with occupied-space tracking (runSCC(eigensolver="subspace"), not in DFTBaby) against the oracle's
+restatement of DFTBaby's runSCC (DFTB2.py:940-1160): the same number of iterations, the same total energy and
+charges, and, since the last iteration is a full eigensolve, orbital energies and excitation energies that
+match the full-eigensolver path."""
+import numpy as np
+import pytest
+
+from dftbaby_b200 import geometry, native
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", ["polyene20_lc", "armchair2_lc", "polyene12_nolc"])
+def test_subspace_scc_matches_oracle(name):
+    native.load()
+    from dftbaby_b200.lr_tddftb import LR_TDDFTB
+    from oracle import dftb_oracle as O
+    al, lc = {"polyene20_lc": (geometry.polyene(20, sigma=0.02, seed=0), 1),
+              "armchair2_lc": (geometry.armchair_flake(2, sigma=0.01, seed=3), 1),
+              "polyene12_nolc": (geometry.polyene(12, sigma=0.02, seed=4), 0)}[name]
+    o = O.DFTB2(al, long_range_correction=lc)
+    o.setGeometry(al)
+    E_o = o.getEnergy()
+    td = LR_TDDFTB(al, long_range_correction=lc)
+    td.setGeometry(al)
+    Om_s, f_s = td.getEnergies(nstates=6, diag_conv=1e-8, eigensolver="subspace")
+    d = td.dftb2
+    assert d.subspace_iterations > 0.5 * d.scc_iterations  # most iterations skipped the dense eigensolve
+    assert d.scc_iterations == o.scc_iterations
+    # DFTBaby's DIIS-change criterion stops within ~1e-8 Ha of the fixed point; both paths stop there
+    assert abs(d.E_tot - E_o) < 1e-8
+    assert np.abs(d.dq.cpu().numpy() - o.dq).max() < 1e-6
+    assert np.abs(d.orbe.cpu().numpy() - o.orbe).max() < 1e-7
+    tf = LR_TDDFTB(al, long_range_correction=lc)
+    tf.setGeometry(al)
+    Om_f, f_f = tf.getEnergies(nstates=6, diag_conv=1e-8)
+    assert np.abs(Om_s - Om_f).max() * 27.211 < 1e-5  # eV
+    assert np.abs(f_s - f_f).max() < 1e-5
