@@ -405,12 +405,43 @@ __global__ void prefix_kernel(int nat, const int *opa, int *first) {
 
 // q[A][p][q] = 1/2 sum_{mu in A} (C1[mu][p] Sc2[mu][q] + C2[mu][q] Sc1[mu][p]).
 // The output (nat x n1 x n2 doubles) is the only large stream, so the kernel is built around writing it at
-// HBM speed: a CTA owns a TC_TP x TC_TQ tile of (p, q) for a run of TC_ATOMS atoms; per atom the rows mu of
-// C1, Sc1 (TC_TP wide) and C2, Sc2 (TC_TQ wide) are staged once in shared memory, and every thread writes
-// adjacent pairs of q with 16-byte stores (each warp stores 512 contiguous bytes of one row p).  Atoms with
-// up to TC_MAXO orbitals (s, p, d shells) take the staged path; larger ones read their rows from global
-// memory directly.
-constexpr int TC_TP = 64, TC_TQ = 128, TC_THREADS = 256, TC_MAXO = 9, TC_ATOMS = 8, TC_ROWS = 8;
+// HBM speed: a CTA owns a TC_TP x TC_TQ tile of (p, q) for a run of TC_ATOMS atoms.  Per atom the rows mu of
+// C1, Sc1 (TC_TP wide) and C2, Sc2 (TC_TQ wide) are staged in shared memory by cp.async, one atom ahead
+// (three buffers, so one barrier per atom suffices), and the next atom's rows arrive while the current
+// atom's outputs are stored; every thread writes
+// adjacent pairs of q with 16-byte stores (each warp stores 512 contiguous bytes of one row p).  Atoms with up
+// to TC_MAXO orbitals (s and p shells) take the staged path; larger ones read their rows from global memory.
+constexpr int TC_TP = 64, TC_TQ = 128, TC_THREADS = 256, TC_MAXO = 4, TC_ATOMS = 8, TC_ROWS = 4;
+
+__device__ __forceinline__ void cp_async8(void *dst, const double *src, bool valid) {
+    // 8-byte asynchronous copy; with src-size 0 the destination is zero-filled and nothing is read
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(valid ? 8 : 0)
+                 : "memory");
+}
+
+struct TcStage {
+    double c1[TC_MAXO][TC_TP], s1[TC_MAXO][TC_TP], c2[TC_MAXO][TC_TQ], s2[TC_MAXO][TC_TQ];
+};
+
+__device__ __forceinline__ void tc_stage(TcStage &b, int f0, int nA, int n1, int n2, int p0, int q0,
+                                         const double *C1, const double *Sc1, const double *C2,
+                                         const double *Sc2) {
+    for (int i = threadIdx.x; i < nA * TC_TP; i += TC_THREADS) {
+        const int j = i / TC_TP, pp = i % TC_TP, p = p0 + pp;
+        const bool v = p < n1;
+        const size_t o = v ? (size_t)(f0 + j) * n1 + p : 0;
+        cp_async8(&b.c1[j][pp], C1 + o, v);
+        cp_async8(&b.s1[j][pp], Sc1 + o, v);
+    }
+    for (int i = threadIdx.x; i < nA * TC_TQ; i += TC_THREADS) {
+        const int j = i / TC_TQ, qq = i % TC_TQ, qi = q0 + qq;
+        const bool v = qi < n2;
+        const size_t o = v ? (size_t)(f0 + j) * n2 + qi : 0;
+        cp_async8(&b.c2[j][qq], C2 + o, v);
+        cp_async8(&b.s2[j][qq], Sc2 + o, v);
+    }
+}
 
 template <bool VEC>
 __global__ void __launch_bounds__(TC_THREADS) tc_tile_kernel(int nat, int n1, int n2, const int *first,
@@ -418,47 +449,54 @@ __global__ void __launch_bounds__(TC_THREADS) tc_tile_kernel(int nat, int n1, in
                                                              const double *__restrict__ Sc1,
                                                              const double *__restrict__ C2,
                                                              const double *__restrict__ Sc2, double *q) {
-    __shared__ double sC1[TC_MAXO][TC_TP], sS1[TC_MAXO][TC_TP];
-    __shared__ __align__(16) double sC2[TC_MAXO][TC_TQ], sS2[TC_MAXO][TC_TQ];
+    __shared__ __align__(16) TcStage buf[3];
     const int tid = threadIdx.x;
     const int qp = tid & 63, pg = tid >> 6;  // q pair within the tile; row group
     const int q0 = blockIdx.x * TC_TQ, p0 = blockIdx.y * TC_TP;
     const int qg = q0 + 2 * qp;
     const int A0 = blockIdx.z * TC_ATOMS;
     const int A1 = min(nat, A0 + TC_ATOMS);
+    // prologue: stage the first atom
+    {
+        const int f0 = first[A0], nA = first[A0 + 1] - f0;
+        if (nA <= TC_MAXO) tc_stage(buf[0], f0, nA, n1, n2, p0, q0, C1, Sc1, C2, Sc2);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     for (int A = A0; A < A1; ++A) {
+        const int k = A - A0;
         const int f0 = first[A], nA = first[A + 1] - f0;
         const bool staged = nA <= TC_MAXO;
-        if (staged) {
-            __syncthreads();  // the previous atom's readers are done with the buffers
-            for (int i = tid; i < nA * TC_TP; i += TC_THREADS) {
-                const int j = i / TC_TP, pp = i % TC_TP, p = p0 + pp;
-                const size_t o = (size_t)(f0 + j) * n1 + p;
-                sC1[j][pp] = p < n1 ? C1[o] : 0.0;
-                sS1[j][pp] = p < n1 ? Sc1[o] : 0.0;
-            }
-            for (int i = tid; i < nA * TC_TQ; i += TC_THREADS) {
-                const int j = i / TC_TQ, qq = i % TC_TQ, qi = q0 + qq;
-                const size_t o = (size_t)(f0 + j) * n2 + qi;
-                sC2[j][qq] = qi < n2 ? C2[o] : 0.0;
-                sS2[j][qq] = qi < n2 ? Sc2[o] : 0.0;
-            }
-            __syncthreads();
+        if (A + 1 < A1) {
+            // next atom's rows into buffer (k + 1) % 3, last read in iteration k - 2: every thread has
+            // passed the barrier of iteration k - 1 since, so those reads are finished
+            const int g0 = first[A + 1], nB = first[A + 2] - g0;
+            if (nB <= TC_MAXO) tc_stage(buf[(k + 1) % 3], g0, nB, n1, n2, p0, q0, C1, Sc1, C2, Sc2);
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
+        __syncthreads();
+        const TcStage &sb = buf[k % 3];
         for (int batch = 0; batch < TC_TP / (4 * TC_ROWS); ++batch) {
             double acc0[TC_ROWS], acc1[TC_ROWS];
 #pragma unroll
             for (int r = 0; r < TC_ROWS; ++r) acc0[r] = acc1[r] = 0.0;
-            const int pl0 = pg + 4 * batch * TC_ROWS;  // local row of r = 0; rows step by 4
+            // this thread's rows: TC_ROWS consecutive ones, so that the staged C1 / Sc1 values of two rows
+            // come in one 16-byte shared-memory read (the same address for the whole warp: a broadcast)
+            const int pl0 = (batch * 4 + pg) * TC_ROWS;
             if (staged) {
                 for (int j = 0; j < nA; ++j) {
-                    const double c2a = sC2[j][2 * qp], c2b = sC2[j][2 * qp + 1];
-                    const double s2a = sS2[j][2 * qp], s2b = sS2[j][2 * qp + 1];
+                    const double2 c2 = *reinterpret_cast<const double2 *>(&sb.c2[j][2 * qp]);
+                    const double2 s2 = *reinterpret_cast<const double2 *>(&sb.s2[j][2 * qp]);
 #pragma unroll
-                    for (int r = 0; r < TC_ROWS; ++r) {
-                        const double a1 = sC1[j][pl0 + 4 * r], b1 = sS1[j][pl0 + 4 * r];
-                        acc0[r] += a1 * s2a + c2a * b1;
-                        acc1[r] += a1 * s2b + c2b * b1;
+                    for (int r = 0; r < TC_ROWS; r += 2) {
+                        const double2 a1 = *reinterpret_cast<const double2 *>(&sb.c1[j][pl0 + r]);
+                        const double2 b1 = *reinterpret_cast<const double2 *>(&sb.s1[j][pl0 + r]);
+                        acc0[r] += a1.x * s2.x + c2.x * b1.x;
+                        acc1[r] += a1.x * s2.y + c2.y * b1.x;
+                        acc0[r + 1] += a1.y * s2.x + c2.x * b1.y;
+                        acc1[r + 1] += a1.y * s2.y + c2.y * b1.y;
                     }
                 }
             } else {
@@ -469,7 +507,7 @@ __global__ void __launch_bounds__(TC_THREADS) tc_tile_kernel(int nat, int n1, in
                     const double s2b = qg + 1 < n2 ? Sc2[r2 + qg + 1] : 0.0;
 #pragma unroll
                     for (int r = 0; r < TC_ROWS; ++r) {
-                        const int p = p0 + pl0 + 4 * r;
+                        const int p = p0 + pl0 + r;
                         const size_t r1 = (size_t)(f0 + j) * n1 + p;
                         const double a1 = p < n1 ? C1[r1] : 0.0, b1 = p < n1 ? Sc1[r1] : 0.0;
                         acc0[r] += a1 * s2a + c2a * b1;
@@ -479,7 +517,7 @@ __global__ void __launch_bounds__(TC_THREADS) tc_tile_kernel(int nat, int n1, in
             }
 #pragma unroll
             for (int r = 0; r < TC_ROWS; ++r) {
-                const int p = p0 + pl0 + 4 * r;
+                const int p = p0 + pl0 + r;
                 if (p >= n1 || qg >= n2) continue;
                 double *row = q + ((size_t)A * n1 + p) * n2;
                 if (VEC && qg + 1 < n2) {

@@ -371,9 +371,11 @@ class DFTB2(object):
                 if self.relative_change < 1.0e3 * scf_conv:
                     b = 0.0
             step_tracked = False
-            if (track and tracked is not None and not converged and not shift_flag
-                    and self.relative_change < subspace_start):
-                moved = self._track_occupied(Hk, tracked, self.relative_change)
+            if track and tracked is not None and not converged and self.relative_change < subspace_start:
+                # with DFTBaby's level shift the tracked spaces follow the shifted Hamiltonian, as the
+                # dense branch below does
+                moved = self._track_occupied(Hk, tracked, self.relative_change,
+                                             shift=b if (shift_flag and b > 0.0) else 0.0)
                 if moved is not None:
                     tracked, step_tracked = moved, True
             if step_tracked:
@@ -382,8 +384,9 @@ class DFTB2(object):
                 self.subspace_iterations += 1
             else:
                 if shift_flag and b > 0.0:
-                    # level shift of the virtual block in the basis of the last MOs (DFTB2.py:1059-1081)
-                    B = self.orbs
+                    # level shift of the virtual block in the basis of the last MOs (DFTB2.py:1059-1081); after
+                    # tracked iterations those are the tracked occupied and virtual spaces
+                    B = self.orbs if tracked is None else torch.cat([tracked[0], tracked[1]], dim=1)
                     Hm = B.T @ Hk @ B
                     virt = torch.nonzero(self.f == 0.0).flatten()
                     Hm[virt, virt] += b
@@ -401,9 +404,12 @@ class DFTB2(object):
                 occ = self.f > 0.0
                 Cocc = self.orbs[:, occ]
                 Pnew = (Cocc * self.f[occ]) @ Cocc.T
-                if track and not shift_flag:
-                    # eigh returns ascending energies: the occupied space is the first nfull columns
-                    tracked = (self.orbs[:, :nfull], self.orbs[:, nfull:], self.orbe[:nfull], self.orbe[nfull:])
+                if track:
+                    # eigh returns ascending energies: the occupied space is the first nfull columns; the
+                    # virtual levels are kept without the level shift this solve may have added
+                    vshift = b if (shift_flag and b > 0.0) else 0.0
+                    tracked = (self.orbs[:, :nfull], self.orbs[:, nfull:], self.orbe[:nfull],
+                               self.orbe[nfull:] - vshift)
             if density_mixer is not None and not converged and mixing_flag:
                 Pnew = density_mixer.next_approximation(Pnew)
             elif not converged:
@@ -422,8 +428,8 @@ class DFTB2(object):
             else:
                 rel = torch.tensor(self.relative_change, dtype=torch.float64, device=dev)
             if step_tracked:
-                # diagonal estimates of the occupied and virtual levels
-                gap = tracked[3].min() - tracked[2].max()
+                # diagonal estimates of the occupied and (level-shifted, as DFTBaby reports them) virtual levels
+                gap = tracked[3].min() + (b if (shift_flag and b > 0.0) else 0.0) - tracked[2].max()
             elif HOMO + 1 < norb:
                 gap = self.orbe[HOMO + 1] - self.orbe[HOMO]
             else:
@@ -451,24 +457,29 @@ class DFTB2(object):
         if getattr(self, "save_converged_charges", None) is not None:
             np.savetxt(os.path.expandvars(os.path.expanduser(self.save_converged_charges)), self.dq.cpu().numpy())
 
-    def _track_occupied(self, H, tracked, rel, max_steps=8):
+    def _track_occupied(self, H, tracked, rel, shift=0.0, max_steps=8):
         """Move an S-orthonormal occupied/virtual split (Co, Cv) onto the invariant subspaces of H.
 
         Each step forms the coupling block F = Cv^T H Co and rotates the two spaces by the first-order
         (Jacobi) correction Y_ai = F_ai / (e_i - e_a), with e_i = diag(Co^T H Co) and e_a the virtual
         levels of the last full solve: Co + Cv Y and Cv - Co Y^T stay exactly S-orthogonal to each other,
         and their Gram matrices I + Y^T Y and I + Y Y^T renormalise them (Cholesky).  Steps repeat until
-        max |F| < max(1e-13, 1e-6 rel), rel being the last relative density change.  Returns the new
+        max |F| < max(1e-13, 1e-6 rel), rel being the last relative density change.  A level shift b > 0
+        is DFTBaby's (DFTB2.py:1059-1081): b added to the virtual block in the basis of the previous
+        orbitals, i.e. H + b S Cv0 Cv0^T S with Cv0 the virtual space on entry.  Returns the new
         (Co, Cv, e_o, e_v), or None when an occupied level is not below every virtual one or the rotations
         have not converged after max_steps; the caller then solves the full eigenproblem."""
         Co, Cv, eo, ev = tracked
         tol = max(1.0e-13, 1.0e-6 * rel)
         no, nv = Co.shape[1], Cv.shape[1]
+        SCv0 = self.S @ Cv if shift > 0.0 else None
         for step in range(max_steps + 1):
             HCo = H @ Co
+            if SCv0 is not None:
+                HCo = torch.addmm(HCo, SCv0, SCv0.T @ Co, alpha=shift)
             F = Cv.T @ HCo
             eo = torch.sum(Co * HCo, dim=0)
-            den = eo[None, :] - ev[:, None]
+            den = eo[None, :] - (ev[:, None] + shift)
             fmax, dmax = torch.stack([torch.max(torch.abs(F)), torch.max(den)]).cpu().numpy()
             if not np.isfinite(fmax) or dmax >= 0.0:
                 return None

@@ -31,6 +31,7 @@ from .dftb2 import DFTB2
 from .exceptions import ExcitedStatesError, ExcitedStatesNotConverged
 from .params import raw_params
 from .solver import hermitian_davidson, nonhermitian_davidson
+from .solver import refine_fp64 as _refine_fp64
 
 
 class ExchangeAO:
@@ -472,24 +473,26 @@ class LR_TDDFTB:
                 mixed = ExchangeMixed(d.gamma, d.G_lr, self.qtrans_ov, self.omega.reshape(-1), Co, Cv, d.S,
                                       len(d.atomlist), self.nocc, self.nvirt, d.workspace, lc=1)
                 mstats = {}
-                Om, C, XmY, XpY = nonhermitian_davidson(mixed, self.omega, nstates, ifact=diag_ifact,
-                                                        conv=diag_conv, maxiter=diag_maxiter, XmYguess=XmY0,
-                                                        XpYguess=XpY0, w_guess=Om0, stats=mstats, symmetrize=True,
-                                                        **learned)
+                keep_basis = refine_fp64 and refine_iterations is not None
+                res = nonhermitian_davidson(mixed, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
+                                            maxiter=diag_maxiter, XmYguess=XmY0, XpYguess=XpY0, w_guess=Om0,
+                                            stats=mstats, symmetrize=True, return_basis=keep_basis, **learned)
+                Om, C, XmY, XpY = res[:4]
+                mixed_basis = res[4] if keep_basis else None
                 tcgemm.check_errors(dev)
                 self.stats["mixed"] = {k: v for k, v in mstats.items() if k != "residual_norms"}
                 self.stats["mixed_products"] = mixed.products_applied
                 XmY0, XpY0, Om0, C0 = XmY, XpY, Om, C
                 del mixed
             if precision == "mixed" and refine_fp64 and refine_iterations is not None:
-                # FP64 corrections of the converged mixed-precision block: Rayleigh-Ritz with FP64 products
+                # FP64 corrections of the mixed-precision projection (refine_fp64 in solver.py)
                 rstats = {}
-                Om, C, XmY, XpY = nonhermitian_davidson(prod, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
-                                                        maxiter=int(refine_iterations) + 1, XmYguess=XmY0,
-                                                        XpYguess=XpY0, w_guess=Om0, stats=rstats,
-                                                        ritz_on_guess=True, raise_on_maxiter=False)
-                self.stats["refine_iterations"] = rstats.get("iterations")
-                self.stats["refine_residual"] = float(np.max(rstats["residual_norms"][-1]))
+                Om, C, XmY, XpY = _refine_fp64(prod, mixed_basis, self.omega, nstates,
+                                               rounds=max(1, int(refine_iterations)), stats=rstats)
+                del mixed_basis
+                self.stats["refine_rounds"] = rstats["refine_rounds"]
+                self.stats["refine_residuals"] = rstats["refine_residuals"]
+                self.stats["refine_residual"] = rstats["refine_residuals"][-1]
             elif precision != "mixed" or refine_fp64:
                 def run(extra):
                     return nonhermitian_davidson(prod, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,

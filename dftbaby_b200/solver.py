@@ -247,7 +247,7 @@ def _sqrtm_spd(M):
 def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxiter=10, XmYguess=None,
                           XpYguess=None, w_guess=None, stats=None, symmetrize=False, accept_guess=False,
                           Cguess=None, guess_key=None, precond_diag=None, ritz_on_guess=False,
-                          raise_on_maxiter=True):
+                          raise_on_maxiter=True, return_basis=False):
     """Lowest nstates of the non-Hermitian TD-DFTB problem (Stratmann-Scuseria-Frisch).
 
     products(V) returns ((A+B).V, (A-B).V) for a (nov, ncol) block.
@@ -268,6 +268,8 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
     its Ritz pairs; raise_on_maxiter=False then returns the Ritz pairs of the
     last iteration instead of raising when maxiter is reached (the residual
     norms of every iteration are in stats["residual_norms"]).
+    return_basis=True appends the expansion space (a Basis with its cached
+    products) to the returned tuple, for refine_fp64.
     """
     nocc, nvirt = omega.shape
     om = omega.reshape(-1).contiguous()
@@ -367,7 +369,87 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
     else:
         C = bs @ Tb[:, :k]
     shape = (k, nocc, nvirt)
-    return Omega, C.T.reshape(shape), Lk.T.reshape(shape), Rk.T.reshape(shape)
+    out = (Omega, C.T.reshape(shape), Lk.T.reshape(shape), Rk.T.reshape(shape))
+    return out + (B,) if return_basis else out
+
+
+def _ssf_ritz(Mp, Mm):
+    """Stratmann-Scuseria-Frisch Ritz pairs of projected (A+B), (A-B) (Solver.py:757-798): w, Rb, Lb, Tb."""
+    Mp = 0.5 * (Mp + Mp.T)
+    Mmsq = _sqrtm_spd(Mm)
+    Mh = Mmsq @ Mp @ Mmsq
+    w2, Tb = torch.linalg.eigh(0.5 * (Mh + Mh.T))
+    if bool((w2 <= 0.0).any()):
+        raise ExcitedStatesError("the projected problem has a non-positive eigenvalue")
+    w = torch.sqrt(w2)
+    Rb = (Mmsq @ Tb) / torch.sqrt(w)
+    Lb = (Mp @ Rb) / w
+    return w, Rb, Lb, Tb
+
+
+def refine_fp64(products, B, omega, nstates, rounds=2, stats=None):
+    """FP64 corrections of a solution found with reduced-precision products (not in DFTBaby).
+
+    B is the expansion space V of the reduced-precision solve with its cached products A_r V (A = A+B and
+    A-B).  With E = A - A_r the precision error of the operator, the exact projection is V^T A V =
+    V^T A_r V + V^T E V.  Each round computes FP64 products A Q of the current Ritz vectors (Q: the L and R
+    vectors of the nstates states, orthonormalised against the directions of earlier rounds), so that
+    E Q = A Q - A_r V (V^T Q) is known exactly, and corrects the projected matrices on the span P of all
+    such Q:  V^T E V ~ G c^T + c G^T - c (c^T G) c^T with c = V^T Q_all, G = V^T E Q_all -- exact on P.  The
+    Ritz pairs of the corrected matrices in the whole space V are the next round's vectors.  A round costs
+    2 nstates FP64 product columns plus tall GEMMs over V.
+
+    The Ritz vectors entering each round lie in P, where A is known exactly, so their FP64 residual norms
+    ||(A+B)R - L w|| + ||(A-B)L - R w|| are exact: stats["refine_residuals"] holds the largest one per
+    round.  Returns Omega (k), C, XmY, XpY as (k, nocc, nvirt), like nonhermitian_davidson."""
+    nocc, nvirt = omega.shape
+    k = nstates
+    V, AP, AM = B.bs, B.prod(0), B.prod(1)
+    Mp0, Mm0 = B.M[0], B.M[1]
+    Mp0 = 0.5 * (Mp0 + Mp0.T)
+    Mm0 = 0.5 * (Mm0 + Mm0.T)
+    w, Rb, Lb, Tb = _ssf_ritz(Mp0, Mm0)
+    Q_all = C_all = Ep_all = Em_all = None
+    res = []
+    for r in range(rounds):
+        Rk, Lk = V @ Rb[:, :k], V @ Lb[:, :k]
+        Q = orthonormalize_new(Q_all, torch.cat([Lk, Rk], dim=1))
+        c = V.T @ Q
+        Pp, Pm = products(Q)
+        Ep = Pp - AP @ c
+        Em = Pm - AM @ c
+        if Q_all is None:
+            Q_all, C_all, Ep_all, Em_all = Q, c, Ep, Em
+        else:
+            Q_all = torch.cat([Q_all, Q], dim=1)
+            C_all = torch.cat([C_all, c], dim=1)
+            Ep_all = torch.cat([Ep_all, Ep], dim=1)
+            Em_all = torch.cat([Em_all, Em], dim=1)
+        # exact FP64 residuals of the pairs entering this round (they lie in span Q_all)
+        wk = w[:k]
+        ApR = AP @ Rb[:, :k] + Ep_all @ (Q_all.T @ Rk)
+        AmL = AM @ Lb[:, :k] + Em_all @ (Q_all.T @ Lk)
+        _, nL = _residuals(ApR, Lk, wk)
+        _, nR = _residuals(AmL, Rk, wk)
+        res.append(float(torch.max(nL + nR).item()))
+        # corrected projections on the whole space
+        Mp, Mm = Mp0, Mm0
+        for M0, E_all in ((0, Ep_all), (1, Em_all)):
+            G = V.T @ E_all
+            H = C_all.T @ G
+            corr = G @ C_all.T
+            corr = corr + corr.T - C_all @ (0.5 * (H + H.T)) @ C_all.T
+            if M0 == 0:
+                Mp = Mp0 + corr
+            else:
+                Mm = Mm0 + corr
+        w, Rb, Lb, Tb = _ssf_ritz(Mp, Mm)
+    if stats is not None:
+        stats["refine_rounds"] = rounds
+        stats["refine_residuals"] = res
+    Rk, Lk, Ck = V @ Rb[:, :k], V @ Lb[:, :k], V @ Tb[:, :k]
+    shape = (k, nocc, nvirt)
+    return w[:k], Ck.T.reshape(shape), Lk.T.reshape(shape), Rk.T.reshape(shape)
 
 
 class DeviceSolver:

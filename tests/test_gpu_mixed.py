@@ -67,3 +67,38 @@ def test_mixed_solve_within_1meV_and_refined_solve_matches_fp64():
     # C = b.Tb of the short refinement subspace, which the non-Hermitian
     # solver does not converge, so f is not compared for it.)
     assert np.abs(Or - O64).max() * HARTREE_TO_EV < 1e-6
+
+
+@pytest.mark.parametrize("rounds", [1, 2])
+def test_mixed_with_fp64_corrections_meets_the_accuracy_gate_on_a_flake(rounds):
+    """The benchmark's accuracy gate on a mid-size long-range-corrected flake (armchair C114H30, 60 x 60
+    window, 12 states): the tensor-core solve followed by FP64 corrections of its projection (refine_fp64 in
+    solver.py) against the plain FP64 path run to a residual of 1e-10.  Energies within 1 meV and X+Y
+    oscillator strengths within 1e-4 (summed over clusters of states closer than 1 meV), and the exact FP64
+    residual of the corrected states is reported and shrinks from round to round."""
+    from dftbaby_b200 import LR_TDDFTB
+    native.load()
+    al = geometry.armchair_flake(2, sigma=0.01, seed=11)
+    win = dict(nr_active_occ=60, nr_active_virt=60, nstates=12, diag_maxiter=200)
+    tp = LR_TDDFTB(al, long_range_correction=1)
+    tp.setGeometry(al)
+    O64, _ = tp.getEnergies(diag_conv=1e-10, **win)
+    fxy64 = tp.oscillatorStrengthsXpY()
+    tm = LR_TDDFTB(al, long_range_correction=1)
+    tm.setGeometry(al)
+    Om, _ = tm.getEnergies(diag_conv=1e-6, precision="mixed", refine_fp64=True, refine_iterations=rounds,
+                           eigensolver="subspace", **win)
+    fxy = tm.oscillatorStrengthsXpY()
+    assert np.abs(Om - O64).max() * HARTREE_TO_EV < 1e-3
+    worst, i, tol = 0.0, 0, 1e-3 / HARTREE_TO_EV
+    while i < len(O64):
+        j = i + 1
+        while j < len(O64) and O64[j] - O64[j - 1] < tol:
+            j += 1
+        worst = max(worst, abs(fxy[i:j].sum() - fxy64[i:j].sum()))
+        i = j
+    assert worst < 1e-4, worst
+    res = tm.stats["refine_residuals"]
+    assert len(res) == rounds and all(np.isfinite(res))
+    if rounds > 1:
+        assert res[-1] < res[0]
