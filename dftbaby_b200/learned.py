@@ -3,9 +3,10 @@
 A small network looks at every occupied-virtual pair (i, a) of a molecule and predicts two
 numbers:
 
-* a score s_ia, trained on sqrt(sum_I C_I,ia^2) over the lowest converged states I, which
-  chooses the pairs whose unit vectors start the Davidson search (DFTBaby takes the
-  lowest omega_ia, Solver.py:232-251);
+* a score s_ia, trained on sqrt(sum_I C_I,ia^2) over the lowest converged states I.  The
+  orbitals that carry most of the predicted weight form a block on which the exact TD-DFTB
+  problem is solved densely; its solutions start the Davidson search (``dense_start``; DFTBaby
+  starts from unit vectors on the lowest omega_ia, Solver.py:232-251);
 * a shift d_ia, trained on sqrt(diag(A+B) diag(A-B)) - omega_ia, so that the correction
   vectors are divided by (w - omega - d) instead of DFTBaby's (w - omega)
   (Solver.py:530-537, 863-866).
@@ -319,6 +320,64 @@ def guess_inputs(net, td):
     score, shift = net.predict(feats)
     om = td.omega.reshape(-1)
     return (-score).double(), om + shift.double().clamp(min=-0.5 * float(om.min()))
+
+
+def _top(imp, m):
+    return torch.sort(torch.topk(imp, min(m, imp.numel())).indices).values
+
+
+def dense_start(net, td, nstates, block=24, extra=8, frontier=False):
+    """Start vectors for the Davidson solve of td (an LR_TDDFTB of this package with its active space and
+    q_ov set).  An orbital block is chosen: the `block` occupied and `block` virtual orbitals nearest the gap,
+    joined by the `extra` further orbitals on each side that carry most of the network's predicted weight
+    (sum over partners of the squared pair score).  The exact TD-DFTB A matrix on that block (Solver.buildAB,
+    Solver.py:35-96, Tamm-Dancoff form) is diagonalised densely, and its lowest nstates eigenvectors,
+    embedded in the full pair space, are returned as (XmY, XpY, Omega) for the solver's warm-start path.
+    frontier=True leaves the network out (the frontier block alone, the untrained version of the start)."""
+    from . import native
+    d = td.dftb2
+    no, nv = td.nocc, td.nvirt
+    oi = torch.arange(max(0, no - block), no, device=d.device)
+    vi = torch.arange(0, min(block, nv), device=d.device)
+    if not frontier and extra > 0:
+        score, _ = net.predict(molecule_features(td))
+        W = score.double().clamp_min(0.0).reshape(no, nv) ** 2
+        wo, wv = W.sum(1), W.sum(0)
+        wo[oi], wv[vi] = -1.0, -1.0  # already in the block
+        oi = torch.sort(torch.cat([oi, torch.topk(wo, min(extra, max(0, no - oi.numel()))).indices])).values
+        vi = torch.sort(torch.cat([vi, torch.topk(wv, min(extra, max(0, nv - vi.numel()))).indices])).values
+    if oi.numel() * vi.numel() < nstates:
+        raise ValueError("the orbital block holds fewer pairs than states")
+    Co, Cv = td._active_coefficients()
+    Co, Cv = Co[:, oi].contiguous(), Cv[:, vi].contiguous()
+    nat, norb, bo, bv = len(d.atomlist), d.dim, oi.numel(), vi.numel()
+    q = [torch.empty(sh, dtype=torch.float64, device=d.device) for sh in ((nat, bo, bo), (nat, bo, bv), (nat, bv, bv))]
+    L = native.load()
+    ws = d.workspace.get(L.dftb_trans_charges_workspace_size(norb, bo, bv))
+    native.call("dftb_trans_charges", norb, nat, bo, bv, native.ptr(Co), native.ptr(Cv), native.ptr(d.S),
+                native.ptr(d._opa), native.ptr(q[0]), native.ptr(q[1]), native.ptr(q[2]), native.ptr(ws), ws.numel(),
+                native.stream())
+    q_oo, q_ov, q_vv = q
+    n = bo * bv
+    A = 2.0 * torch.einsum("Aia,AB,Bjb->iajb", q_ov, d.gamma, q_ov).reshape(n, n)
+    if d.long_range_correction == 1:
+        A = A - torch.einsum("Aij,AB,Bab->iajb", q_oo, d.gamma_lr, q_vv).reshape(n, n)
+    A = A + torch.diag(td.omega[oi][:, vi].reshape(-1))
+    Om, X = torch.linalg.eigh(0.5 * (A + A.T))
+    Om = Om[:nstates].clamp_min(1e-6)
+    T = torch.zeros((nstates, no, nv), dtype=torch.float64, device=d.device)
+    T[:, oi[:, None], vi[None, :]] = X[:, :nstates].T.reshape(nstates, bo, bv)
+    # X+Y and X-Y as the Hermitian solver relates them to its eigenvectors (sqrt(omega) T / sqrt(Omega) and
+    # sqrt(Omega) T / sqrt(omega)), so both solvers' warm-start paths get independent, well-scaled columns
+    so = torch.sqrt(td.omega)[None]
+    sO = torch.sqrt(Om)[:, None, None]
+    return sO * T / so, so * T / sO, Om
+
+
+class FrontierStart:
+    """The untrained counterpart of a GuessNet for LR_TDDFTB.getEnergies(guess_model=...): the dense start
+    on the orbital block nearest the gap, with DFTBaby's preconditioner (for comparisons)."""
+    frontier = True
 
 
 DEFAULT_MODEL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "guess_net.npz")

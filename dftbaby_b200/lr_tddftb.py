@@ -326,15 +326,14 @@ class LR_TDDFTB:
         """LR_TDDFTB.getEnergies (LR_TDDFTB.py:37-114); returns (Omega, f) in Hartree.
 
         precision="mixed" (not in DFTBaby) evaluates the long-range exchange of
-        the Davidson products with split-precision BF16 tensor-core GEMMs; with
-        refine_fp64 the mixed result then seeds the FP64 solver.  With
-        refine_iterations=None that solver iterates until its residual test
-        (diag_conv) passes, as in the plain path; with refine_iterations=n it
-        re-projects the operator, with FP64 products, onto the converged vectors
-        (and, for n > 0, onto n rounds of FP64 residual corrections) and returns
-        those Ritz pairs: FP64 corrections of the mixed-precision products at the
-        cost of 2 nstates (n + 1) FP64 product columns.  Its FP64 residual norms
-        are in stats["refine_residual"].
+        the Davidson products with split-precision BF16 tensor-core GEMMs.  With
+        refine_fp64 and refine_iterations=None the mixed result then seeds the
+        FP64 solver, which iterates until its residual test (diag_conv) passes,
+        as in the plain path.  With refine_iterations=n >= 1 the projection of
+        the operator onto the whole mixed expansion space is corrected n times
+        with FP64 products of the current Ritz vectors (solver.refine_fp64,
+        2 nstates FP64 product columns per round); the exact FP64 residual of
+        the vectors entering each round is in stats["refine_residuals"].
         guess_model (not in DFTBaby): a learned.GuessNet whose pair scores choose
         the initial Davidson vectors and whose shifts correct the diagonal
         preconditioner when no warm start is available; the solve runs to the
@@ -438,8 +437,21 @@ class LR_TDDFTB:
         learned = {}
         if guess_model is not None and XpY0 is None and nstates is not None:
             from . import learned as _learned
-            learned["guess_key"], learned["precond_diag"] = _learned.guess_inputs(guess_model, self)
+            # the frontier orbitals and those the network weights most form a block; the exact problem on
+            # that block gives the start vectors (DFTBaby's warm-start path, Solver.py:461-478, 707-748)
+            frontier = getattr(guess_model, "frontier", False)
+            if getattr(guess_model, "use_shift", False):
+                # the learned preconditioner correction (off by default: on held-out flakes, outside the
+                # polyene training set, it slowed convergence)
+                _, learned["precond_diag"] = _learned.guess_inputs(guess_model, self)
+            learned["XmYguess"], learned["XpYguess"], learned["w_guess"] = _learned.dense_start(
+                guess_model, self, nstates, frontier=frontier)
         self.stats["learned_start"] = bool(learned)
+
+        def guesses(extra, keys=("XmYguess", "XpYguess", "w_guess")):
+            kw = {k: v for k, v in dict(XmYguess=XmY0, XpYguess=XpY0, w_guess=Om0).items() if k in keys}
+            kw.update({k: v for k, v in extra.items() if k in keys or k == "precond_diag"})
+            return kw
         if verbose:
             print("construct and diagonalize full TD-DFTB matrix with dimension %d" % (self.nocc * self.nvirt)
                   if nstates is None else "solve eigenvalue problem iteratively")
@@ -460,8 +472,8 @@ class LR_TDDFTB:
 
             def run(extra):
                 return hermitian_davidson(rv, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
-                                          maxiter=diag_maxiter, XpYguess=XpY0, Oia=self.Oia,
-                                          L2_thresh=diag_L2threshold, stats=self.stats, **extra)
+                                          maxiter=diag_maxiter, Oia=self.Oia, L2_thresh=diag_L2threshold,
+                                          stats=self.stats, **guesses(extra, keys=("XpYguess",)))
 
             Om, C, XmY, XpY = self._with_fallback(run, learned)
         else:
@@ -475,8 +487,8 @@ class LR_TDDFTB:
                 mstats = {}
                 keep_basis = refine_fp64 and refine_iterations is not None
                 res = nonhermitian_davidson(mixed, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
-                                            maxiter=diag_maxiter, XmYguess=XmY0, XpYguess=XpY0, w_guess=Om0,
-                                            stats=mstats, symmetrize=True, return_basis=keep_basis, **learned)
+                                            maxiter=diag_maxiter, stats=mstats, symmetrize=True,
+                                            return_basis=keep_basis, **guesses(learned))
                 Om, C, XmY, XpY = res[:4]
                 mixed_basis = res[4] if keep_basis else None
                 tcgemm.check_errors(dev)
@@ -496,9 +508,9 @@ class LR_TDDFTB:
             elif precision != "mixed" or refine_fp64:
                 def run(extra):
                     return nonhermitian_davidson(prod, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
-                                                 maxiter=diag_maxiter, XmYguess=XmY0, XpYguess=XpY0, w_guess=Om0,
-                                                 stats=self.stats, accept_guess=(precision == "mixed"),
-                                                 Cguess=C0 if precision == "mixed" else None, **extra)
+                                                 maxiter=diag_maxiter, stats=self.stats,
+                                                 accept_guess=(precision == "mixed"),
+                                                 Cguess=C0 if precision == "mixed" else None, **guesses(extra))
 
                 Om, C, XmY, XpY = self._with_fallback(run, learned if XpY0 is None else {})
             self.stats["products"] = prod.products_applied
@@ -525,8 +537,12 @@ class LR_TDDFTB:
     def _casida(self, multiplicity):
         """Full diagonalisation, Solver.Casida (Solver.py:98-181), on the device."""
         q_oo, q_vv, q_ov = self.getTransitionCharges()
+        return self._casida_block(q_oo, q_vv, q_ov, self.omega, multiplicity)
+
+    def _casida_block(self, q_oo, q_vv, q_ov, omega, multiplicity="S"):
+        """Solver.Casida on the pairs of the given transition charges and orbital energy differences."""
         d = self.dftb2
-        no, nv = self.nocc, self.nvirt
+        no, nv = omega.shape
         n = no * nv
         g = d.gamma
         glr = d.gamma_lr if d.long_range_correction == 1 else torch.zeros_like(g)
@@ -535,7 +551,7 @@ class LR_TDDFTB:
         if multiplicity == "S":
             Ks = 2.0 * torch.einsum("Aia,AB,Bjb->iajb", q_ov, g, q_ov).reshape(n, n)
             KA, KB = KA + Ks, KB + Ks
-        om = self.omega.reshape(-1)
+        om = omega.reshape(-1)
         dfh = torch.ones_like(om)  # df/2 = 1 for a closed shell
         A = torch.diag(dfh * om) + dfh[:, None] * KA * dfh[None, :]
         B = dfh[:, None] * KB * dfh[None, :]

@@ -102,3 +102,29 @@ def test_learned_start_reaches_the_plain_solution():
         assert lrn.stats["learned_start"]
         assert np.abs(Ol - Op).max() * 27.211396132 < 1e-6
         print("Davidson iterations plain %d, learned start %d" % (plain.stats["iterations"], lrn.stats["iterations"]))
+
+
+def test_shipped_network_saves_iterations_on_held_out_molecules():
+    """What the start gains (the C4 configuration): the shipped GuessNet (trained on 20k converged
+    eigenvectors of seeded polyenes C10-C60) picks orbitals beyond the frontier block of the dense start, and
+    the long-range-corrected Davidson solves of held-out molecules it never saw -- hexagonal flakes and a
+    longer polyene -- converge to the plain solver's states in fewer iterations than from DFTBaby's
+    unit-vector start.  The untrained start on the frontier block alone is reported beside it."""
+    from dftbaby_b200 import LR_TDDFTB, learned
+    net = learned.GuessNet.load(learned.DEFAULT_MODEL)
+    opts = dict(nstates=10, diag_conv=1e-6, diag_maxiter=200)
+    mols = [geometry.hexagonal_flake(4, sigma=0.01, seed=504), geometry.hexagonal_flake(6, sigma=0.01, seed=506),
+            geometry.polyene(40, sigma=0.03, seed=940)]
+    for al in mols:
+        runs = {}
+        for tag, model in (("plain", None), ("learned", net), ("frontier", learned.FrontierStart())):
+            td = LR_TDDFTB(al, long_range_correction=1)
+            td.setGeometry(al)
+            Om, _ = td.getEnergies(guess_model=model, **opts)
+            runs[tag] = (Om, td.stats["iterations"], td.phase_ms()["excited_states"], td.stats["learned_start"])
+        (Op, ip, tp, _), (Ol, il, tl, used) = runs["plain"], runs["learned"]
+        print("%s: Davidson iterations plain %d, learned %d, frontier %d; excited-state ms plain %.1f, learned %.1f, "
+              "frontier %.1f" % (geometry.formula(al), ip, il, runs["frontier"][1], tp, tl, runs["frontier"][2]))
+        assert used
+        assert np.abs(Ol - Op).max() * 27.211396132 < 1e-5
+        assert il < ip
