@@ -96,6 +96,9 @@ def build_geometry(w, seed):
     return geometry.polyene(w["n"], sigma=w["sigma"], seed=seed)
 
 
+_ARGS = None
+
+
 def workload_config(name, w, n_gpus, precision="fp64"):
     from dftbaby_b200 import geometry
     if w["kind"] == "trajectories":
@@ -132,6 +135,9 @@ def workload_config(name, w, n_gpus, precision="fp64"):
            "atoms": nat, "orbitals": norb, "long_range_correction": w["lc"], "nstates": o["nstates"],
            "active_window": [o.get("nr_active_occ"), o.get("nr_active_virt")],
            "davidson_residual": o["diag_conv"], "scf_conv": 1e-10,
+           "start": "learned dense start (frontier orbital block plus GuessNet choices, exact Tamm-Dancoff "
+                    "block solve)" if precision == "mixed" and w["lc"] and getattr(_ARGS, "learned", False)
+                    else "DFTBaby's unit vectors",
            "precision": ("mixed: Davidson exchange products on tensor cores (bf16x3, f32 accumulate) to the "
                          "residual, then FP64 refinement (the projection onto the whole mixed expansion space "
                          "corrected with FP64 products of the Ritz vectors); Coulomb term, SCC (occupied-space "
@@ -472,6 +478,9 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="mixed: tensor-core exchange + FP64 refinement (default); fp64: the plain path")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison solve")
+    ap.add_argument("--learned", action="store_true",
+                    help="start the Davidson solve from the learned dense start instead of DFTBaby's unit vectors "
+                         "(on the 1104-atom flake it saves no iteration and costs the start)")
     ap.add_argument("--refine-iterations", type=int, default=1,
                     help="rounds of FP64 corrections of the mixed-precision projection (2 nstates FP64 product "
                          "columns each)")
@@ -480,6 +489,8 @@ def main():
                     help="after the timed region, profile one extra solve (CUDA activity records) and write its "
                          "per-kernel launches, device time and share to PATH (markdown)")
     args = ap.parse_args()
+    global _ARGS
+    _ARGS = args
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -503,7 +514,11 @@ def main():
         # (FP64 products of the Ritz vectors, refine_iterations rounds); SCC with occupied-space tracking
         # instead of a dense eigensolve in every iteration
         opts.update(precision="mixed", refine_fp64=True, refine_iterations=args.refine_iterations,
-                    eigensolver="subspace")
+                    eigensolver="subspace", subspace_tol=1.0e-4)
+        if args.learned and w["kind"] in ("armchair", "flake"):
+            # the learned dense start: frontier orbital block plus the network's choices (learned.dense_start)
+            from dftbaby_b200 import learned
+            opts["guess_model"] = learned.GuessNet.load(args.model or learned.DEFAULT_MODEL)
     mixed = opts.get("precision") == "mixed"
 
     def barrier():
@@ -571,7 +586,8 @@ def main():
                       "scc_dense_eigensolves": td.dftb2.scc_iterations - getattr(td.dftb2, "subspace_iterations", 0),
                       "davidson_iterations": td.stats.get("iterations"), "subspace": td.stats.get("subspace"),
                       "fp64_products": td.stats.get("products"), "mixed": td.stats.get("mixed"),
-                      "mixed_products": td.stats.get("mixed_products")})
+                      "mixed_products": td.stats.get("mixed_products"),
+                      "learned_start": td.stats.get("learned_start")})
         if td.stats.get("refine_residual") is not None:
             refine_res.append(td.stats["refine_residual"])
         if compare:

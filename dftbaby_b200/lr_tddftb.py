@@ -495,7 +495,6 @@ class LR_TDDFTB:
                 self.stats["mixed"] = {k: v for k, v in mstats.items() if k != "residual_norms"}
                 self.stats["mixed_products"] = mixed.products_applied
                 XmY0, XpY0, Om0, C0 = XmY, XpY, Om, C
-                del mixed
             if precision == "mixed" and refine_fp64 and refine_iterations is not None:
                 # FP64 corrections of the mixed-precision projection (refine_fp64 in solver.py)
                 rstats = {}
@@ -505,6 +504,8 @@ class LR_TDDFTB:
                 self.stats["refine_rounds"] = rstats["refine_rounds"]
                 self.stats["refine_residuals"] = rstats["refine_residuals"]
                 self.stats["refine_residual"] = rstats["refine_residuals"][-1]
+            if precision == "mixed":
+                del mixed
             elif precision != "mixed" or refine_fp64:
                 def run(extra):
                     return nonhermitian_davidson(prod, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
