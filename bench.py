@@ -332,7 +332,10 @@ def run_ensemble(args, w, rank, world, barrier):
             "gpu_launches": native.counters.launches, "clocks": clocks, "roofline": None,
             "solver": {"scc_iterations_max_per_group": [max(x) for x in stats["scc_iterations"]],
                        "davidson_iterations_max_per_group": [max(x) for x in stats["davidson_iterations"]],
-                       "phase_ms_per_group": stats.get("phase_ms")},
+                       "phase_ms_per_group": stats.get("phase_ms"),
+                       "autotuned_groups_size_x_orbitals": (stats.get("autotune") or {}).get("groups"),
+                       "autotune_fit_ms": (stats.get("autotune") or {}).get("fit_ms"),
+                       "davidson_products": "replayed from CUDA graphs captured per block shape"},
             "plain_fp64": {"value": nstates_total / (plain_ms / 1e3), "ms_per_step": plain_ms,
                            "how": "one-molecule FP64 path on %d seeded members, extrapolated" % len(sub),
                            "max_dOmega_meV": dmax, "max_df": fmax},
@@ -514,7 +517,7 @@ def main():
         # (FP64 products of the Ritz vectors, refine_iterations rounds); SCC with occupied-space tracking
         # instead of a dense eigensolve in every iteration
         opts.update(precision="mixed", refine_fp64=True, refine_iterations=args.refine_iterations,
-                    eigensolver="subspace", subspace_tol=1.0e-4)
+                    eigensolver="subspace")
         if args.learned and w["kind"] in ("armchair", "flake"):
             # the learned dense start: frontier orbital block plus the network's choices (learned.dense_start)
             from dftbaby_b200 import learned

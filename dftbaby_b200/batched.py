@@ -128,9 +128,78 @@ class _Mol:
     pass
 
 
+# ------------------------------------------------------------ autotuned grouping
+def _probe_ms(dev, B, N, reps=2):
+    """Device time (ms) of the work every lockstep SCC iteration does once per group of B padded molecules
+    of N orbitals: one batched symmetric eigensolve and three batched N x N products (Fock exchange and
+    density), on random symmetric data."""
+    g = torch.Generator(device="cpu").manual_seed(B * 1000 + N)
+    A = torch.randn((B, N, N), generator=g, dtype=torch.float64).to(dev)
+    A = A + A.transpose(1, 2)
+    batched_eigh(A)
+    torch.bmm(A, A)
+    best = None
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batched_eigh(A)
+        for _ in range(3):
+            torch.bmm(A, A)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    return best
+
+
+def autotune_groups(norbs, dev, max_group=256, probes=((8, 64), (8, 320), (64, 64), (64, 192), (64, 320),
+                                                        (256, 64), (256, 192), (256, 320))):
+    """Group the molecules for the lockstep solver (no counterpart in DFTBaby, which solves one molecule
+    at a time).  Molecules sorted by orbital count are cut into consecutive groups, each padded to its
+    largest member; the cut points minimise the predicted total time.  The prediction is measured on the
+    device: per-iteration costs of a few (group size B, padded size N) probes (``_probe_ms``) are fitted by
+    t(B, N) = c0 + c1 B N^2 + c2 B N^3 (non-negative least squares), and a dynamic programme over the
+    sorted list finds the cheapest partition into groups of at most max_group molecules.
+
+    Returns (groups, record): groups is a list of index lists into norbs; record holds the probes, the
+    fitted coefficients and the chosen (size, padded orbitals) of every group."""
+    norbs = np.asarray(norbs)
+    order = np.argsort(norbs, kind="stable")
+    ns = norbs[order]
+    rows, ts = [], []
+    for B, N in probes:
+        rows.append([1.0, B * N ** 2 / 1e6, B * N ** 3 / 1e9])
+        ts.append(_probe_ms(dev, B, N))
+    from scipy.optimize import nnls
+    coef, _ = nnls(np.array(rows), np.array(ts))
+    cost = lambda B, N: coef[0] + coef[1] * B * N ** 2 / 1e6 + coef[2] * B * N ** 3 / 1e9
+    n = len(ns)
+    best = np.full(n + 1, np.inf)
+    cut = np.zeros(n + 1, int)
+    best[0] = 0.0
+    for j in range(1, n + 1):
+        for i in range(max(0, j - max_group), j):
+            c = best[i] + cost(j - i, int(ns[j - 1]))
+            if c < best[j]:
+                best[j], cut[j] = c, i
+    bounds, j = [], n
+    while j > 0:
+        bounds.append((cut[j], j))
+        j = cut[j]
+    bounds.reverse()
+    groups = [[int(k) for k in order[a:b]] for a, b in bounds]
+    record = {"probes_ms": {"%dx%d" % bn: round(t, 3) for bn, t in zip(probes, ts)},
+              "fit_ms": [float(c) for c in coef], "predicted_ms_per_iteration": float(best[n]),
+              "groups": [[b - a, int(ns[b - 1])] for a, b in bounds]}
+    return groups, record
+
+
 class BatchedLR_TDDFTB:
     def __init__(self, atomlists, long_range_correction=1, long_range_radius=3.03, distance_cutoff=30.0,
-                 device=None, group_size=128, **opts):
+                 device=None, group_size="auto", graphs=True, **opts):
+        """group_size: molecules per lockstep group, or "auto" (autotune_groups: cut points of the
+        size-sorted list from measured costs).  graphs: replay the Davidson products of each group from
+        CUDA graphs captured at their first use."""
         native.load()
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.lc = long_range_correction
@@ -140,6 +209,7 @@ class BatchedLR_TDDFTB:
         self.par = Parametrization(Zs)
         self.atomlists = [[(int(Z), tuple(float(c) for c in p)) for Z, p in al] for al in atomlists]
         self.group_size = group_size
+        self.graphs = graphs
 
     # ------------------------------------------------------------ per-molecule setup (native kernels)
     def _setup_molecule(self, al):
@@ -198,16 +268,21 @@ class BatchedLR_TDDFTB:
         """Returns (Omega list, oscillator strength list) in the order of the atomlists.
 
         The SCC keywords have DFTB2.runSCC's names and defaults."""
-        order = np.argsort([sum(4 if Z > 2 else 1 for Z, _ in al) for al in self.atomlists], kind="stable")
+        norbs = [sum(len(self.par.valorbs[Z]) for Z, _ in al) for al in self.atomlists]
+        self.stats = {"groups": [], "scc_iterations": [], "davidson_iterations": []}
+        if self.group_size == "auto":
+            groups, self.stats["autotune"] = autotune_groups(norbs, self.device)
+        else:
+            order = np.argsort(norbs, kind="stable")
+            groups = [[int(i) for i in order[g0:g0 + self.group_size]]
+                      for g0 in range(0, len(order), self.group_size)]
         self.Omega = [None] * len(self.atomlists)
         self.oscillator_strength = [None] * len(self.atomlists)
-        self.stats = {"groups": [], "scc_iterations": [], "davidson_iterations": []}
-        for g0 in range(0, len(order), self.group_size):
-            idx = [int(i) for i in order[g0:g0 + self.group_size]]
+        for idx in groups:
             mols = [self._setup_molecule(self.atomlists[i]) for i in idx]
             Om, f, it_scc, it_dav = solve_group(mols, self.lc, self.device, nstates, diag_conv, diag_maxiter,
                                                 scf_conv, maxiter, mixing_threshold, linear_mixing_coefficient,
-                                                diis_m, level_shift, HOMO_LUMO_tol)
+                                                diis_m, level_shift, HOMO_LUMO_tol, graphs=self.graphs)
             for j, i in enumerate(idx):
                 self.Omega[i] = Om[j]
                 self.oscillator_strength[i] = f[j]
@@ -377,7 +452,7 @@ def _lockstep_scc(G, lc, scf_conv=1.0e-10, maxiter=1000, mix_thr=1.0e-3, alpha=0
     return dict(P=P, dq=dq, orbs=orbs, orbe=orbe, rel=rel, gap=gap), scc_it
 
 
-def _excited(G, lc, scc, nstates, conv, dmaxiter, guess=None):
+def _excited(G, lc, scc, nstates, conv, dmaxiter, guess=None, graphs=False):
     """Excited states of every molecule in the full active space: transition charges, the lockstep
     Davidson and C.  guess = (XmY, XpY, Co, Cv) of a previous solve of the same group starts the
     Davidson from those vectors, projected onto the current orbitals through the orbital overlap."""
@@ -416,6 +491,8 @@ def _excited(G, lc, scc, nstates, conv, dmaxiter, guess=None):
                                       Pv[:, None]).reshape(B, -1, nov)
         start = (proj(XmY0), proj(XpY0))
     prod = _BatchedProducts(G.gat, G.Glr if lc else None, qov, om, Co, Cv, SCo, SCv, no_max, nv_max)
+    if graphs and dev.type == "cuda":
+        prod = _GraphedProducts(prod)
     if lc:
         Om, C, XmY, XpY, dav_it = _batched_nonhermitian(prod, om, nstates, conv, dmaxiter, kmax, start)
     else:
@@ -433,7 +510,7 @@ def _oscillator_strengths(G, exc):
 
 
 def solve_group(mols, lc, dev, nstates, conv, dmaxiter, scf_conv=1.0e-10, maxiter=1000, mix_thr=1.0e-3,
-                alpha=0.33, diis_m=5, level_shift=0.1, homo_lumo_tol=0.05):
+                alpha=0.33, diis_m=5, level_shift=0.1, homo_lumo_tol=0.05, graphs=False):
     """Lockstep SCC + Davidson for one group of molecules.
 
     ``mols`` hold per-molecule tensors on ``dev``: S, H0 (norb, norb), D (3, norb, norb), g, glr
@@ -448,7 +525,7 @@ def solve_group(mols, lc, dev, nstates, conv, dmaxiter, scf_conv=1.0e-10, maxite
     scc, scc_it = _lockstep_scc(G, lc, scf_conv, maxiter, mix_thr, alpha, diis_m, level_shift, homo_lumo_tol)
     if ev:
         ev[2].record()
-    exc = _excited(G, lc, scc, nstates, conv, dmaxiter)
+    exc = _excited(G, lc, scc, nstates, conv, dmaxiter, graphs=graphs)
     fosc = _oscillator_strengths(G, exc)
     if ev:
         ev[3].record()
@@ -569,6 +646,38 @@ class _BatchedProducts:
         K1 = 0.25 * k1.reshape(B, m, nov).permute(0, 2, 1)
         K2 = 0.25 * k2.reshape(B, m, nov).permute(0, 2, 1)
         return coul - K1 - K2, omv + K2 - K1
+
+
+class _GraphedProducts:
+    """The batch's (A+B).V, (A-B).V replayed from CUDA graphs.  The lockstep Davidson multiplies a block of
+    the same shape (every molecule's 2 k new columns, dead ones zero) in every iteration, so the whole
+    product -- about twenty batched GEMM and element-wise launches -- is captured once per block shape on
+    first use and replayed as one graph launch thereafter.  Inputs are copied into the graph's static
+    buffer and the outputs copied out, since the next replay overwrites them."""
+
+    def __init__(self, prod):
+        self.prod = prod
+        self.graphs = {}
+        self.replays = 0
+
+    def __call__(self, V):
+        key = tuple(V.shape)
+        if key not in self.graphs:
+            static = V.clone()
+            side = torch.cuda.Stream(device=V.device)
+            side.wait_stream(torch.cuda.current_stream(V.device))
+            with torch.cuda.stream(side):
+                self.prod(static)  # warm-up outside capture (library handles, workspaces)
+            torch.cuda.current_stream(V.device).wait_stream(side)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                out = self.prod(static)
+            self.graphs[key] = (g, static, out)
+        g, static, out = self.graphs[key]
+        static.copy_(V)
+        g.replay()
+        self.replays += 1
+        return tuple(o.clone() for o in out)
 
 
 # diagonal given to unused (all-zero) columns of a projected matrix, in Hartree (Mp, Mm) and

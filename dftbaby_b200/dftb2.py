@@ -313,8 +313,9 @@ class DFTB2(object):
         and energies handed on are exact eigenpairs.  The density of a T = 0 closed shell depends on the
         occupied space only, so the mixing schedule, the convergence test and the fixed point are
         DFTBaby's; iterates differ by the rotations' residual (below subspace_tol times the last relative
-        change; 1e-4 moves the converged energy of the 1104-atom benchmark flake by 5e-9 Ha and its orbital
-        energies by 8e-8 Ha)."""
+        change; with 1e-4 the converged orbital energies of the 1104-atom benchmark flake move by 8e-8 Ha
+        from the dense path's, enough to move X+Y oscillator strengths by 1.6e-4, so the default is 1e-6:
+        3e-9 Ha)."""
         if fock_interpolator is not None:
             raise ValueError("Fock interpolation is not implemented")
         if isinstance(density_mixer, str):

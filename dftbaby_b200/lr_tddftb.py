@@ -97,13 +97,13 @@ class ExchangeAO:
 class ExchangeMixed(ExchangeAO):
     """(A+B).V and (A-B).V with the exchange contractions on the tensor cores.
 
-    Same AO-factorised algebra as ExchangeAO, evaluated per column with six
-    split-precision BF16 GEMMs (three BF16 passes each, FP32 accumulation,
-    ~2^-16 relative accuracy; tcgemm.py):
+    Same AO-factorised algebra as ExchangeAO, evaluated per column with four
+    split-precision BF16 GEMM launches (three BF16 passes each, FP32
+    accumulation, ~2^-16 relative accuracy; tcgemm.py):
         W^T  = [C_v; S~_v] v^T                        (2 Norb x nocc)
-        N_xy = Gamma o (X_o W_y), stored and transposed (fused epilogue)
-        P1^T = Ybar^T N,  P2^T = Ybar^T N^T            (K = 2 Norb)
-        K1^T = P1^T Xbar_o / 4,  K2^T = P2^T Xbar_o / 4
+        N_xy = Gamma o (X_o W_y), both y, stored and transposed (fused epilogue)
+        [P1^T | P2^T] = Ybar^T [N | N^T]              (K = 2 Norb)
+        [K1^T ; K2^T] = [P1^T ; P2^T] Xbar_o / 4      (rows interleaved)
     with Ybar = [S~_v; C_v] and Xbar = [S~_o; C_o].
 
     The Coulomb term 4 q_ov^T gamma q_ov V stays FP64 (native q_ov products)
@@ -128,14 +128,23 @@ class ExchangeMixed(ExchangeAO):
         self.XO = T.split(torch.cat([Co, So], dim=0))                      # (2 Norb, no), K = no
         self.YbarT = T.split(torch.cat([Sv, Cv], dim=0), transpose=True)   # (nv, 2 Norb), K = 2 Norb
         self.XbarT = T.split(torch.cat([So, Co], dim=0), transpose=True)   # (no, 2 Norb), K = 2 Norb
-        self.G2 = torch.cat([G_lr, G_lr], dim=0).to(torch.float32).contiguous()  # (2 Norb, Norb)
+        g = G_lr.to(torch.float32)
+        self.G4 = torch.cat([torch.cat([g, g], dim=1)] * 2, dim=0).contiguous()    # (2 Norb, 2 Norb)
         self.W = T.Pair(2 * norb, nocc, dev)
-        self.NN = T.Pair(2 * norb, 2 * norb, dev)
-        self.NT = T.Pair(2 * norb, 2 * norb, dev)
-        self.P1 = T.Pair(nvirt, 2 * norb, dev)
-        self.P2 = T.Pair(nvirt, 2 * norb, dev)
-        self.K1t = torch.empty((nvirt, nocc), dtype=torch.float32, device=dev)
-        self.K2t = torch.empty((nvirt, nocc), dtype=torch.float32, device=dev)
+        # N and N^T as the two halves of one operand, the second starting at a 64-row boundary, so that one
+        # launch forms P1 and P2 side by side: P = Ybar^T [N; N^T]^T (nv x 2 h), h = padded(2 Norb)
+        h = T.padded(2 * norb)
+        self.h = h
+        self.NB = T.Pair(2 * h, 2 * norb, dev)
+        self.NN = self._rows(self.NB, 0, 2 * norb)
+        self.NT = self._rows(self.NB, h, 2 * norb)
+        self.P12 = T.Pair(nvirt, 2 * h, dev)
+        # P12 read as 2 nv rows of length h: rows 2i and 2i + 1 are row i of P1 and of P2, so one launch
+        # forms K1^T and K2^T interleaved
+        self.Pint = T.Pair.__new__(T.Pair)
+        self.Pint.rows, self.Pint.cols, self.Pint.ld = 2 * nvirt, 2 * norb, h
+        self.Pint.hi, self.Pint.lo = self.P12.hi.view(2 * nvirt, h), self.P12.lo.view(2 * nvirt, h)
+        self.K12t = torch.empty((2 * nvirt, nocc), dtype=torch.float32, device=dev)
         self.Vp = T.Pair(nocc, nvirt, dev)
         self.coulomb_on_tensor_cores = coulomb_on_tensor_cores
         if coulomb_on_tensor_cores:
@@ -144,21 +153,15 @@ class ExchangeMixed(ExchangeAO):
             self.QOV = T.split(q2)                     # (Nat, nov), K = nov
             self.QOVT = T.split(q2, transpose=True)    # (nov, Nat), K = Nat
             self._colpairs = {}
-        # views for the per-y blocks (y = C, S~)
-        self.Wy, self.outN, self.outT = [], [], []
-        for y in range(2):
-            w = T.Pair.__new__(T.Pair)
-            w.rows, w.cols, w.ld = norb, nocc, self.W.ld
-            w.hi, w.lo = self.W.hi[y * norb:(y + 1) * norb], self.W.lo[y * norb:(y + 1) * norb]
-            self.Wy.append(w)
-            o = T.Pair.__new__(T.Pair)
-            o.rows, o.cols, o.ld = 2 * norb, norb, self.NN.ld
-            o.hi, o.lo = self.NN.hi[:, y * norb:], self.NN.lo[:, y * norb:]
-            self.outN.append(o)
-            t = T.Pair.__new__(T.Pair)
-            t.rows, t.cols, t.ld = norb, 2 * norb, self.NT.ld
-            t.hi, t.lo = self.NT.hi[y * norb:], self.NT.lo[y * norb:]
-            self.outT.append(t)
+
+
+    @staticmethod
+    def _rows(pair, r0, nrows):
+        """A Pair view of rows r0 .. r0 + nrows of another Pair."""
+        v = pair.__class__.__new__(pair.__class__)
+        v.rows, v.cols, v.ld = nrows, pair.cols, pair.ld
+        v.hi, v.lo = pair.hi[r0:r0 + nrows], pair.lo[r0:r0 + nrows]
+        return v
 
     def _pairs(self, m):
         """Column-block operands padded to at least 128 rows (one tensor-core tile)."""
@@ -195,16 +198,15 @@ class ExchangeMixed(ExchangeAO):
         for c in range(m):
             T.split(Vt[c].reshape(no, nv), out=self.Vp)
             T.gemm(self.YV, self.Vp, K=nv, out_pair=self.W)
-            for y in range(2):
-                T.gemm(self.XO, self.Wy[y], K=no, G=self.G2, out_pair=self.outN[y], out_pair_t=self.outT[y])
-            # (the Wy views carry both hi and lo parts, so all products use the shared-split kernel)
-            T.gemm(self.YbarT, self.NN, K=2 * norb, out_pair=self.P1)
-            T.gemm(self.YbarT, self.NT, K=2 * norb, out_pair=self.P2)
-            T.gemm(self.P1, self.XbarT, K=2 * norb, alpha=0.25, out=self.K1t)
-            T.gemm(self.P2, self.XbarT, K=2 * norb, alpha=0.25, out=self.K2t)
-            # transpose, widen to FP64 and scatter into column c in one copy
-            K1[:, c].view(no, nv).copy_(self.K1t.T)
-            K2[:, c].view(no, nv).copy_(self.K2t.T)
+            # N = Gamma o (X_o W^T) for both y at once, stored row-major and transposed
+            T.gemm(self.XO, self.W, K=no, G=self.G4, out_pair=self.NN, out_pair_t=self.NT)
+            # [P1 | P2] in one launch (the rows between the halves of NB are zero)
+            T.gemm(self.YbarT, self.NB, K=2 * norb, out_pair=self.P12)
+            # K1^T and K2^T interleaved by rows, in one launch
+            T.gemm(self.Pint, self.XbarT, K=2 * norb, alpha=0.25, out=self.K12t)
+            # transpose, widen to FP64 and scatter into column c in one copy each
+            K1[:, c].view(no, nv).copy_(self.K12t[0::2].T)
+            K2[:, c].view(no, nv).copy_(self.K12t[1::2].T)
         return K1, K2
 
 
@@ -494,7 +496,7 @@ class LR_TDDFTB:
                 tcgemm.check_errors(dev)
                 self.stats["mixed"] = {k: v for k, v in mstats.items() if k != "residual_norms"}
                 self.stats["mixed_products"] = mixed.products_applied
-                XmY0, XpY0, Om0, C0 = XmY, XpY, Om, C
+                XmY0, XpY0, Om0 = XmY, XpY, Om
             if precision == "mixed" and refine_fp64 and refine_iterations is not None:
                 # FP64 corrections of the mixed-precision projection (refine_fp64 in solver.py)
                 rstats = {}
@@ -504,16 +506,17 @@ class LR_TDDFTB:
                 self.stats["refine_rounds"] = rstats["refine_rounds"]
                 self.stats["refine_residuals"] = rstats["refine_residuals"]
                 self.stats["refine_residual"] = rstats["refine_residuals"][-1]
-            if precision == "mixed":
-                del mixed
             elif precision != "mixed" or refine_fp64:
                 def run(extra):
+                    # after a mixed-precision solve the first iteration already projects the FP64 operator
+                    # onto the mixed solution (Rayleigh-Ritz), and stops there if its residuals pass
                     return nonhermitian_davidson(prod, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
                                                  maxiter=diag_maxiter, stats=self.stats,
-                                                 accept_guess=(precision == "mixed"),
-                                                 Cguess=C0 if precision == "mixed" else None, **guesses(extra))
+                                                 ritz_on_guess=(precision == "mixed"), **guesses(extra))
 
                 Om, C, XmY, XpY = self._with_fallback(run, learned if XpY0 is None else {})
+            if precision == "mixed":
+                del mixed
             self.stats["products"] = prod.products_applied
         self._Omega_dev = Om
         self.Omega = Om.cpu().numpy()

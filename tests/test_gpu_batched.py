@@ -67,3 +67,23 @@ def test_batched_eigh_matches_torch(n):
     assert resid < 1e-11 * scale * n
     orth = (V.transpose(1, 2) @ V - torch.eye(n, dtype=A.dtype, device=A.device)).abs().max().item()
     assert orth < 1e-11
+
+
+def test_autotuned_groups_and_graph_replayed_products():
+    """group_size="auto": the molecules are partitioned by measured costs (batched.autotune_groups) into
+    size-sorted groups, and the lockstep Davidson's products are replayed from CUDA graphs; every molecule
+    still equals its one-molecule solve."""
+    from dftbaby_b200.batched import BatchedLR_TDDFTB
+    native.load()
+    mols = [geometry.polyene(n, 0.03, 200 + n) for n in (6, 20, 8, 30, 10)] + \\
+           [geometry.acene(r, 0.03, 300 + r) for r in (2, 4, 3)]
+    opts = dict(nstates=4, diag_conv=1e-7, diag_maxiter=100)
+    bt = BatchedLR_TDDFTB(mols, long_range_correction=1, group_size="auto")
+    Om_b, f_b = bt.getEnergies(**opts)
+    rec = bt.stats["autotune"]
+    assert sum(n for n, _ in rec["groups"]) == len(mols) and sum(bt.stats["groups"]) == len(mols)
+    assert all(t > 0 for t in rec["probes_ms"].values()) and min(rec["fit_ms"]) >= 0.0
+    for j in (0, 3, 5, 7):
+        Os, fs = _single(mols[j], 1, opts)
+        assert np.abs(Om_b[j] - Os).max() * HARTREE_TO_EV < 1e-7
+        assert np.abs(f_b[j] - fs).max() < 1e-7
