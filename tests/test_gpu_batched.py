@@ -75,7 +75,7 @@ def test_autotuned_groups_and_graph_replayed_products():
     still equals its one-molecule solve."""
     from dftbaby_b200.batched import BatchedLR_TDDFTB
     native.load()
-    mols = [geometry.polyene(n, 0.03, 200 + n) for n in (6, 20, 8, 30, 10)] + \\
+    mols = [geometry.polyene(n, 0.03, 200 + n) for n in (6, 20, 8, 30, 10)] + \
            [geometry.acene(r, 0.03, 300 + r) for r in (2, 4, 3)]
     opts = dict(nstates=4, diag_conv=1e-7, diag_maxiter=100)
     bt = BatchedLR_TDDFTB(mols, long_range_correction=1, group_size="auto")
