@@ -129,22 +129,13 @@ class _Mol:
 
 
 # ------------------------------------------------------------ autotuned grouping
-def _probe_ms(dev, B, N, reps=2):
-    """Device time (ms) of the work every lockstep SCC iteration does once per group of B padded molecules
-    of N orbitals: one batched symmetric eigensolve and three batched N x N products (Fock exchange and
-    density), on random symmetric data."""
-    g = torch.Generator(device="cpu").manual_seed(B * 1000 + N)
-    A = torch.randn((B, N, N), generator=g, dtype=torch.float64).to(dev)
-    A = A + A.transpose(1, 2)
-    batched_eigh(A)
-    torch.bmm(A, A)
+def _timed(fn, reps=1):
+    fn()
     best = None
     for _ in range(reps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        batched_eigh(A)
-        for _ in range(3):
-            torch.bmm(A, A)
+        fn()
         e1.record()
         e1.synchronize()
         ms = e0.elapsed_time(e1)
@@ -152,27 +143,70 @@ def _probe_ms(dev, B, N, reps=2):
     return best
 
 
-def autotune_groups(norbs, dev, max_group=256, probes=((8, 64), (8, 320), (64, 64), (64, 192), (64, 320),
-                                                        (256, 64), (256, 192), (256, 320))):
+def _probe_ms(dev, B, N, sub=256, cols=16):
+    """Device times (ms) of the per-iteration work of a group of B padded molecules of N orbitals, on random
+    data: an SCC iteration (one batched N x N eigensolve and three batched N^3 products) and a Davidson
+    iteration (two batched eigensolves of sub x sub subspace matrices and the products of `cols` new
+    columns, eight batched N^3 products per column)."""
+    g = torch.Generator(device="cpu").manual_seed(B * 1000 + N)
+    A = torch.randn((B, N, N), generator=g, dtype=torch.float64).to(dev)
+    A = A + A.transpose(1, 2)
+
+    def scc():
+        batched_eigh(A)
+        for _ in range(3):
+            torch.bmm(A, A)
+
+    M = torch.randn((B, sub, sub), generator=g, dtype=torch.float64).to(dev)
+    M = M + M.transpose(1, 2)
+    X = A[:, None].expand(B, cols, N, N)
+
+    def dav():
+        batched_eigh(M)
+        batched_eigh(M)
+        for _ in range(8):
+            torch.matmul(X, A[:, None])
+
+    return _timed(scc), _timed(dav)
+
+
+_FITS = {}
+
+
+def autotune_groups(norbs, dev, max_group=256, scc_iterations=45, davidson_iterations=25,
+                    probes=((8, 64), (8, 320), (64, 64), (64, 192), (64, 320), (256, 64), (256, 192), (256, 320))):
     """Group the molecules for the lockstep solver (no counterpart in DFTBaby, which solves one molecule
     at a time).  Molecules sorted by orbital count are cut into consecutive groups, each padded to its
     largest member; the cut points minimise the predicted total time.  The prediction is measured on the
-    device: per-iteration costs of a few (group size B, padded size N) probes (``_probe_ms``) are fitted by
-    t(B, N) = c0 + c1 B N^2 + c2 B N^3 (non-negative least squares), and a dynamic programme over the
-    sorted list finds the cheapest partition into groups of at most max_group molecules.
+    device, once per device: per-iteration times of SCC and Davidson iterations at a few (group size B,
+    padded size N) probes (``_probe_ms``) are fitted by t(B, N) = c0 + c1 B + c2 B N^2 + c3 B N^3
+    (non-negative least squares), a group costs scc_iterations t_scc + davidson_iterations t_dav, and a
+    dynamic programme over the sorted list finds the cheapest partition into groups of at most max_group
+    molecules.
 
     Returns (groups, record): groups is a list of index lists into norbs; record holds the probes, the
     fitted coefficients and the chosen (size, padded orbitals) of every group."""
+    from scipy.optimize import nnls
     norbs = np.asarray(norbs)
     order = np.argsort(norbs, kind="stable")
     ns = norbs[order]
-    rows, ts = [], []
-    for B, N in probes:
-        rows.append([1.0, B * N ** 2 / 1e6, B * N ** 3 / 1e9])
-        ts.append(_probe_ms(dev, B, N))
-    from scipy.optimize import nnls
-    coef, _ = nnls(np.array(rows), np.array(ts))
-    cost = lambda B, N: coef[0] + coef[1] * B * N ** 2 / 1e6 + coef[2] * B * N ** 3 / 1e9
+    key = str(dev)
+    if key not in _FITS:
+        rows, ts, td = [], [], []
+        for B, N in probes:
+            rows.append([1.0, B / 1e2, B * N ** 2 / 1e6, B * N ** 3 / 1e9])
+            a, b = _probe_ms(dev, B, N)
+            ts.append(a)
+            td.append(b)
+        X = np.array(rows)
+        _FITS[key] = (nnls(X, np.array(ts))[0], nnls(X, np.array(td))[0],
+                      {"%dx%d" % bn: [round(a, 3), round(b, 3)] for bn, a, b in zip(probes, ts, td)})
+    cs, cd, probe_rec = _FITS[key]
+
+    def cost(B, N):
+        f = np.array([1.0, B / 1e2, B * N ** 2 / 1e6, B * N ** 3 / 1e9])
+        return scc_iterations * float(f @ cs) + davidson_iterations * float(f @ cd)
+
     n = len(ns)
     best = np.full(n + 1, np.inf)
     cut = np.zeros(n + 1, int)
@@ -184,22 +218,24 @@ def autotune_groups(norbs, dev, max_group=256, probes=((8, 64), (8, 320), (64, 6
                 best[j], cut[j] = c, i
     bounds, j = [], n
     while j > 0:
-        bounds.append((cut[j], j))
-        j = cut[j]
+        bounds.append((int(cut[j]), j))
+        j = int(cut[j])
     bounds.reverse()
     groups = [[int(k) for k in order[a:b]] for a, b in bounds]
-    record = {"probes_ms": {"%dx%d" % bn: round(t, 3) for bn, t in zip(probes, ts)},
-              "fit_ms": [float(c) for c in coef], "predicted_ms_per_iteration": float(best[n]),
-              "groups": [[b - a, int(ns[b - 1])] for a, b in bounds]}
+    record = {"probes_ms_scc_dav": probe_rec, "fit_scc_ms": [float(c) for c in cs],
+              "fit_davidson_ms": [float(c) for c in cd], "predicted_ms": float(best[n]),
+              "groups": [[int(b - a), int(ns[b - 1])] for a, b in bounds]}
     return groups, record
 
 
 class BatchedLR_TDDFTB:
     def __init__(self, atomlists, long_range_correction=1, long_range_radius=3.03, distance_cutoff=30.0,
-                 device=None, group_size="auto", graphs=True, **opts):
+                 device=None, group_size="auto", graphs=False, **opts):
         """group_size: molecules per lockstep group, or "auto" (autotune_groups: cut points of the
         size-sorted list from measured costs).  graphs: replay the Davidson products of each group from
-        CUDA graphs captured at their first use."""
+        CUDA graphs captured at their first use (off by default: on the 512-molecule ensemble it measured
+        15.3 s against 9.3 s without, since every group captures its own graphs and the captured
+        products' intermediates stay allocated)."""
         native.load()
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.lc = long_range_correction

@@ -78,11 +78,12 @@ def test_autotuned_groups_and_graph_replayed_products():
     mols = [geometry.polyene(n, 0.03, 200 + n) for n in (6, 20, 8, 30, 10)] + \
            [geometry.acene(r, 0.03, 300 + r) for r in (2, 4, 3)]
     opts = dict(nstates=4, diag_conv=1e-7, diag_maxiter=100)
-    bt = BatchedLR_TDDFTB(mols, long_range_correction=1, group_size="auto")
+    bt = BatchedLR_TDDFTB(mols, long_range_correction=1, group_size="auto", graphs=True)
     Om_b, f_b = bt.getEnergies(**opts)
     rec = bt.stats["autotune"]
     assert sum(n for n, _ in rec["groups"]) == len(mols) and sum(bt.stats["groups"]) == len(mols)
-    assert all(t > 0 for t in rec["probes_ms"].values()) and min(rec["fit_ms"]) >= 0.0
+    assert all(min(t) > 0 for t in rec["probes_ms_scc_dav"].values())
+    assert min(rec["fit_scc_ms"]) >= 0.0 and min(rec["fit_davidson_ms"]) >= 0.0
     for j in (0, 3, 5, 7):
         Os, fs = _single(mols[j], 1, opts)
         assert np.abs(Om_b[j] - Os).max() * HARTREE_TO_EV < 1e-7
