@@ -251,6 +251,49 @@ class DFTB2(object):
         Hx += S @ (dP * G) @ S
         return Hx * (-1.0 / 8.0)
 
+    def _lc_exchange_tc(self, D):
+        """H^x(D) of a symmetric D (the form of lc_exact_exchange, linear in dP) with its five Norb^3
+        products on the tensor cores (split-precision BF16, FP32 accumulation, ~1e-5 relative):
+            A1 = S D,  t1 = (G o A1) S,  X = G o (A1 S),  Z = (D o G) S,  Y = S Z,
+            H^x = -1/8 (t1 + t1^T + X + Y)."""
+        from . import tcgemm as T
+        n = self.dim
+        c = getattr(self, "_lc_tc", None)
+        if c is None or c["n"] != n or c["S"] is not self.S or c["Glr"] is not self.G_lr:
+            dev = self.S.device
+            ld = T.padded(n, 4)
+            c = dict(n=n, S=self.S, Glr=self.G_lr, Sp=T.split(self.S), G=self.G_lr.to(torch.float32).contiguous(),
+                     Dp=T.Pair(n, n, dev), Ap=T.Pair(n, n, dev), Zt=T.Pair(n, n, dev),
+                     f32=[torch.empty((n, ld), dtype=torch.float32, device=dev)[:, :n] for _ in range(4)])
+            self._lc_tc = c
+        Sp, G = c["Sp"], c["G"]
+        A1, t1, X, Y = c["f32"]
+        T.split(D, out=c["Dp"])
+        T.gemm(Sp, c["Dp"], out=A1)                     # A1 = S D (D symmetric: its rows are its columns)
+        T.split(G * A1, out=c["Ap"])
+        T.gemm(c["Ap"], Sp, out=t1)                     # (G o A1) S
+        T.split(A1, out=c["Ap"])
+        T.gemm(c["Ap"], Sp, G=G, out=X)                 # G o (A1 S)
+        T.split(D * self.G_lr, out=c["Dp"])
+        T.gemm(c["Dp"], Sp, out_pair_t=c["Zt"])        # Z^T = S (D o G)
+        T.gemm(Sp, c["Zt"], out=Y)                      # S Z
+        Hx = (t1 + t1.T) + X + Y
+        return Hx.to(torch.float64) * (-1.0 / 8.0)
+
+    def _lc_exchange_anchored(self, lcs, exact):
+        """H^x(P - P0) as H^x of an anchor density P_a, formed in FP64, plus the tensor-core H^x of P - P_a.
+
+        H^x is linear in P, so the split-precision error is relative to |P - P_a| only: it shrinks as the
+        SCC converges, and a new FP64 anchor is formed whenever |P - P_a| has grown large against the
+        current density change (or exact=True)."""
+        if exact or lcs.get("P") is None:
+            lcs["Hx"] = self.lc_exact_exchange()
+            lcs["P"] = self.P.clone()
+            lcs["anchors"] = lcs.get("anchors", 0) + 1
+            return lcs["Hx"]
+        lcs["tc"] = lcs.get("tc", 0) + 1
+        return lcs["Hx"] + self._lc_exchange_tc(self.P - lcs["P"])
+
     def lc_exchange_energy(self):
         dP = self.P - self.P0
         S, G = self.S, self.G_lr
@@ -302,7 +345,8 @@ class DFTB2(object):
 
     def runSCC(self, maxiter=1000, scf_conv=1.0e-10, start_from_previous=1, mixing_threshold=1.0e-3,
                density_mixer="default", fock_interpolator=None, level_shift=0.1, HOMO_LUMO_tol=0.05,
-               linear_mixing_coefficient=0.33, eigensolver="full", subspace_start=0.1, subspace_tol=1.0e-6):
+               linear_mixing_coefficient=0.33, eigensolver="full", subspace_start=0.1, subspace_tol=1.0e-6,
+               lc_products="fp64", lc_anchor_ratio=100.0):
         """Self-consistent charges (DFTB2.runSCC, DFTB2.py:940-1160), T = 0.
 
         eigensolver (not in DFTBaby): "full" solves H C = S C e in every iteration, as DFTBaby does.
@@ -315,7 +359,15 @@ class DFTB2(object):
         DFTBaby's; iterates differ by the rotations' residual (below subspace_tol times the last relative
         change; with 1e-4 the converged orbital energies of the 1104-atom benchmark flake move by 8e-8 Ha
         from the dense path's, enough to move X+Y oscillator strengths by 1.6e-4, so the default is 1e-6:
-        3e-9 Ha)."""
+        3e-9 Ha).
+
+        lc_products (not in DFTBaby): "fp64" forms the long-range exchange H^x(P - P0) in FP64 in every
+        iteration, as DFTBaby does.  "mixed" forms it in FP64 at anchor densities only and adds the tensor-
+        core H^x of the difference to the last anchor (``_lc_exchange_anchored``); a new anchor is formed
+        when the distance |P - P_a| / |P| exceeds lc_anchor_ratio times the last relative change, and in the
+        converged (last) iteration, so the orbitals and energies handed on are those of the FP64 operator."""
+        if lc_products not in ("fp64", "mixed"):
+            raise ValueError("lc_products must be 'fp64' or 'mixed'")
         if fock_interpolator is not None:
             raise ValueError("Fock interpolation is not implemented")
         if isinstance(density_mixer, str):
@@ -359,11 +411,17 @@ class DFTB2(object):
         track = eigensolver == "subspace" and self.Nelec_val == 2 * nfull and 0 < nfull < norb
         self.subspace_iterations = 0
         tracked = None
+        lc_mixed = lc_products == "mixed" and self.long_range_correction == 1
+        lcs = {}
+        anchor_dist = float("inf")
         for self.i in range(maxiter):
             native.call("dftb_scc_hamiltonian", norb, nat, P(self._ind), P(self.H0), P(self.S), P(self.gamma),
                         P(self.dq), P(estat), P(H), st)
             Hk = H
-            if self.long_range_correction == 1:
+            if lc_mixed:
+                exact = converged or anchor_dist > lc_anchor_ratio * max(self.relative_change, scf_conv)
+                Hk = H + self._lc_exchange_anchored(lcs, exact)
+            elif self.long_range_correction == 1:
                 Hk = H + self.lc_exact_exchange()
             b = level_shift
             if have_orbe and self.HLgap < HOMO_LUMO_tol and not mixing_flag:
@@ -437,8 +495,13 @@ class DFTB2(object):
                 gap = self.orbe[HOMO + 1] - self.orbe[HOMO]
             else:
                 gap = torch.zeros((), device=dev, dtype=torch.float64)
-            host = torch.stack([rel.reshape(()), self.dq.sum(), gap.reshape(())]).cpu().numpy()
+            vals = [rel.reshape(()), self.dq.sum(), gap.reshape(())]
+            if lc_mixed:
+                vals.append(torch.linalg.norm(self.P - lcs["P"]) / torch.linalg.norm(self.P))
+            host = torch.stack(vals).cpu().numpy()
             self.relative_change, sum_dq, self.HLgap = float(host[0]), float(host[1]), float(host[2])
+            if lc_mixed:
+                anchor_dist = float(host[3])
             if abs(sum_dq + self.charge) > 1.0e-5:
                 raise SCFChargeInconsistency("Mulliken charges do not add up to total charge, sum dq = %s" % -sum_dq)
             if self.verbose > 0:
@@ -457,6 +520,10 @@ class DFTB2(object):
         else:
             raise SCFNotConverged("SCF calculation did not converge after %s iterations!!!" % (self.i + 1))
         self.scc_iterations = self.i + 1
+        self.lc_anchor_counts = (lcs.get("anchors", 0), lcs.get("tc", 0)) if lc_mixed else None
+        if lc_mixed and lcs.get("tc", 0):
+            from . import tcgemm
+            tcgemm.check_errors(self.S.device)
         if getattr(self, "save_converged_charges", None) is not None:
             np.savetxt(os.path.expandvars(os.path.expanduser(self.save_converged_charges)), self.dq.cpu().numpy())
 
