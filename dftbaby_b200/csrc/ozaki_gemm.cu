@@ -1,0 +1,657 @@
+// FP64 matrix products emulated exactly on the int8 tensor cores of B200 (tcgen05 kind::i8), after the
+// "Ozaki scheme II" of Ozaki, Uchino and Imamura (integer modular GEMMs plus the Chinese remainder theorem):
+//
+//   C = alpha * op(A) op(B) + beta * C            (row-major FP64; op = transpose when trans != 0)
+//
+// 1. Row m of op(A) is scaled by 2^sa[m] and column n of op(B) by 2^sb[n] and rounded to integers A', B'
+//    of at most `bits` bits, chosen so that every entry of A'B' (K terms) stays below P/2 in magnitude,
+//    P = p_1 ... p_N the product of N pairwise coprime moduli p_i <= 256.
+// 2. For each modulus the symmetric residues A' mod p_i and B' mod p_i (|r| <= 128, int8) are multiplied on
+//    the tensor cores with exact int32 accumulation (K < 2^17), and the epilogue keeps the product's residue
+//    mod p_i as int8.
+// 3. Per element, Garner's algorithm turns the N residues into mixed-radix digits (int32 arithmetic), whose
+//    Horner sum in FP64 is A'B' to within FP64 rounding, and C = 2^-(sa[m] + sb[n]) A'B'.
+//
+// The only approximation is step 1: each entry of op(A) (op(B)) is carried with `bits` bits relative to
+// the largest entry of its row (column); with N = 16 moduli and K <= 2^17 that is the full 53-bit FP64
+// mantissa.  The tensor-core work is N int8 GEMMs (B200: 4.5 dense int8 POPS against ~35 TFLOP/s of FP64
+// DGEMM).
+//
+// Kernels: ozaki_rowscale_kernel (exponents), ozaki_residue_kernel (int8 residue planes, K-major,
+// zero-padded), ozaki_mma_kernel (persistent tcgen05 GEMM over (M tile, N tile, modulus), TMA operand ring,
+// double-buffered TMEM accumulators, residue epilogue), ozaki_crt_kernel (Garner + Horner + scaling).
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+
+#include "dftbaby_b200.h"
+#include "tcgen05.cuh"
+
+namespace ozk {
+
+using namespace tc5;
+
+constexpr int MAXMOD = 16;
+// pairwise coprime: 2^8, 3*5*17, 11*23, 13*19 and primes
+constexpr int kModuli[MAXMOD] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 211, 199, 197, 193, 191};
+constexpr int KMAX = 131071;                // 128 * 128 * K < 2^31: exact int32 accumulation
+constexpr int SCALE_NONFINITE = -(1 << 20);  // row/column exponent marking an Inf or NaN entry
+
+struct Tables {
+    int p[MAXMOD];
+    float invpf[MAXMOD];
+    double invp[MAXMOD];
+    int D[MAXMOD][MAXMOD];  // D[j][i] = (p_0 ... p_{i-1}) mod p_j, i < j
+    int Binv[MAXMOD];       // (p_0 ... p_{j-1})^-1 mod p_j
+};
+
+// symmetric residue of an integer-valued t (|t| < 2^27) modulo p: range [-(p/2), (p-1)/2]
+__device__ __forceinline__ int symmod_i(int t, int p, float invpf) {
+    const int q = __float2int_rn(__int2float_rn(t) * invpf);
+    int r = t - q * p;
+    const int lo = -(p >> 1), hi = (p - 1) >> 1;
+    if (r > hi) r -= p;
+    if (r > hi) r -= p;
+    if (r < lo) r += p;
+    if (r < lo) r += p;
+    return r;
+}
+
+// ---------------------------------------------------------------------------- scaling and residues
+
+// Y(r, k) = trans ? X[k * ldx + r] : X[r * ldx + k]; s[r] = bits - 1 - ilogb(max_k |Y(r, k)|) so that
+// |Y(r, k)| 2^s[r] < 2^bits (0 for a zero row, SCALE_NONFINITE for a row holding Inf or NaN); rows in
+// [rows, rpad) get 0.
+__global__ void ozaki_rowscale_kernel(int rows, int rpad, int K, const double *X, long long ldx, int trans, int bits,
+                                      int *s) {
+    if (!trans) {
+        const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+        if (warp >= rpad) return;
+        double m = 0.0;
+        bool bad = false;
+        if (warp < rows) {
+            const double *x = X + (long long)warp * ldx;
+            for (int k = lane; k < K; k += 32) {
+                const double a = fabs(x[k]);
+                bad |= !(a <= 1.7976931348623157e308);
+                m = fmax(m, a);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+            bad |= __shfl_xor_sync(0xffffffffu, (int)bad, o) != 0;
+        }
+        if (lane == 0) s[warp] = bad ? SCALE_NONFINITE : (m > 0.0 ? bits - 1 - ilogb(m) : 0);
+    } else {
+        // 32 rows per block (threadIdx.x, consecutive in memory), 8 phases of k (threadIdx.y)
+        __shared__ double sm[8][32];
+        __shared__ int sbad[8][32];
+        const int r = blockIdx.x * 32 + threadIdx.x;
+        double m = 0.0;
+        int bad = 0;
+        if (r < rows) {
+            for (int k = threadIdx.y; k < K; k += 8) {
+                const double a = fabs(X[(long long)k * ldx + r]);
+                bad |= !(a <= 1.7976931348623157e308);
+                m = fmax(m, a);
+            }
+        }
+        sm[threadIdx.y][threadIdx.x] = m;
+        sbad[threadIdx.y][threadIdx.x] = bad;
+        __syncthreads();
+        if (threadIdx.y == 0 && r < rpad) {
+            for (int y = 1; y < 8; ++y) {
+                m = fmax(m, sm[y][threadIdx.x]);
+                bad |= sbad[y][threadIdx.x];
+            }
+            s[r] = bad ? SCALE_NONFINITE : (m > 0.0 ? bits - 1 - ilogb(m) : 0);
+        }
+    }
+}
+
+constexpr int RT_ROWS = 32, RT_K = 128;
+
+// Residue planes R[i][r][k] (i < nmod, r < rpad, k < kpad; zero outside rows x K) of the scaled, rounded
+// Y(r, k) 2^s[r].  One block per 32 x 128 tile of Y, staged through shared memory so that both the FP64
+// reads (along k, or along r when transposed) and the int8 writes (4 consecutive k per thread) coalesce.
+__global__ void __launch_bounds__(256) ozaki_residue_kernel(int rows, int K, const double *X, long long ldx, int trans,
+                                                            const int *s, int nmod,
+                                                            const __grid_constant__ Tables tb, int8_t *R,
+                                                            long long plane, int kpad) {
+    __shared__ double tile[RT_ROWS][RT_K + 1];
+    const int r0 = blockIdx.y * RT_ROWS, k0 = blockIdx.x * RT_K;
+    for (int idx = threadIdx.x; idx < RT_ROWS * RT_K; idx += blockDim.x) {
+        int rr, kk;
+        if (trans) {
+            rr = idx % RT_ROWS;
+            kk = idx / RT_ROWS;
+        } else {
+            rr = idx / RT_K;
+            kk = idx % RT_K;
+        }
+        const int r = r0 + rr, k = k0 + kk;
+        double v = 0.0;
+        if (r < rows && k < K) v = trans ? X[(long long)k * ldx + r] : X[(long long)r * ldx + k];
+        tile[rr][kk] = v;
+    }
+    __syncthreads();
+    for (int item = threadIdx.x; item < RT_ROWS * (RT_K / 4); item += blockDim.x) {
+        const int rr = item / (RT_K / 4), kq = (item % (RT_K / 4)) * 4;
+        const int r = r0 + rr, k = k0 + kq;
+        if (k >= kpad) continue;
+        const int sr = (r < rows) ? s[r] : 0;
+        double a[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            a[e] = (sr == SCALE_NONFINITE || r >= rows) ? 0.0 : rint(ldexp(tile[rr][kq + e], sr));
+        for (int i = 0; i < nmod; ++i) {
+            const double p = (double)tb.p[i];
+            uint32_t w = 0;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                // a is an integer of at most 53 bits: q within one of round(a / p), fma exact
+                const double q = rint(a[e] * tb.invp[i]);
+                double rd = fma(-q, p, a[e]);
+                const double lo = -(double)(tb.p[i] >> 1), hi = (double)((tb.p[i] - 1) >> 1);
+                if (rd > hi) rd -= p;
+                if (rd < lo) rd += p;
+                w |= ((uint32_t)(uint8_t)(int8_t)(int)rd) << (8 * e);
+            }
+            *reinterpret_cast<uint32_t *>(R + i * plane + (long long)r * kpad + k) = w;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------- int8 tensor-core GEMM
+
+// 128 x 256 output tiles: per 128-byte K block a stage holds 16 KiB of A and 32 KiB of B for four
+// 128 x 256 x 32 MMAs, a third fewer operand bytes per MMA than 128 x 128 tiles
+constexpr int BM = 128, BN = 256, BKB = 128;  // tile rows, tile columns, K bytes (= int8 elements) per stage
+constexpr int TILE_BYTES = BM * BKB;          // 16 KiB (A)
+constexpr int TILE_B_BYTES = BN * BKB;        // 32 KiB (B)
+constexpr int STAGES = 4;
+constexpr int STAGE_BYTES = TILE_BYTES + TILE_B_BYTES;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /* alignment slack */ + 256 /* barriers */;
+constexpr int EPI_THREADS = 128;
+// instruction descriptor: D = S32 (bits 4-5 = 2), A = B = signed int8 (bits 7-9, 10-12 = 1), both K-major,
+// N >> 3 at bit 17, M >> 4 at bit 24
+constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                              ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem_c, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_c),
+        "l"(da), "l"(db), "r"(kIdescI8), "r"(accumulate));
+}
+
+struct Maps {
+    CUtensorMap a;  // residue planes of op(A): (nmod * mpad) rows x kpad int8
+    CUtensorMap b;  // residue planes of op(B)^T: (nmod * npad) rows x kpad int8
+};
+
+struct MmaParams {
+    int M, N, kpad, mpad, npad, nmod;
+    int8_t *RC;  // product residues: plane i at RC + i * planeC, row-major with ldr (multiple of 32)
+    long long planeC;
+    int ldr;
+    int *err;
+};
+
+// Persistent kernel, one CTA per SM over the tiles t = (m tile, n tile, modulus), M fastest:
+//   warp 0 lane 0 : TMA producer over a 4-stage ring of 128-byte-wide A (128 rows) and B (256 rows) tiles
+//                   (128-byte swizzle);
+//   warp 1 lane 0 : tcgen05.mma kind::i8 issuer (M = 128, N = 256, K = 32 per instruction) into one of two
+//                   256-column int32 TMEM accumulators (tile j uses accumulator j % 2);
+//   warps 2..5    : epilogue of tile j under the MMAs of tile j + 1: int32 -> residue mod p -> int8.
+// Every wait is bounded; on timeout the kernel records an error code, stops issuing, drains its copies
+// and releases TMEM.
+__global__ void __launch_bounds__(192, 1) ozaki_mma_kernel(const __grid_constant__ Maps maps, const MmaParams p,
+                                                           const __grid_constant__ Tables tb) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    uint64_t *tfull = empty + STAGES;
+    uint64_t *tempty = tfull + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
+    int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int mt = p.mpad / BM, nt = p.npad / BN;
+    const int ntiles = mt * nt * p.nmod;
+    const int kblocks = p.kpad / BKB;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&tfull[a], 1);
+            mbar_init(&tempty[a], EPI_THREADS);
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncwarp();
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(2 * BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer
+            int it = 0;
+            bool stop = false;
+            for (int t = blockIdx.x; t < ntiles && !stop; t += gridDim.x) {
+                const int mi = t % mt, ni = (t / mt) % nt, mod = t / (mt * nt);
+                const int ya = mod * p.mpad + mi * BM, yb = mod * p.npad + ni * BN;
+                for (int kb = 0; kb < kblocks; ++kb) {
+                    const int s = it % STAGES;
+                    if (it >= STAGES && !mbar_wait(&empty[s], ((it / STAGES) - 1) & 1)) {
+                        atomicExch(p.err, 1);
+                        *(volatile int *)abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    if (*(volatile int *)abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    uint8_t *sa = smem + s * STAGE_BYTES;
+                    mbar_expect_tx(&full[s], STAGE_BYTES);
+                    tma_load_2d(sa, &maps.a, &full[s], kb * BKB, ya);
+                    tma_load_2d(sa + TILE_BYTES, &maps.b, &full[s], kb * BKB, yb);
+                    ++it;
+                }
+            }
+            // drain: wait (bounded) until every copy that was started has landed
+            for (int j = max(0, it - STAGES); j < it; ++j) mbar_wait(&full[j % STAGES], (j / STAGES) & 1);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer
+            int it = 0, j = 0;
+            bool stop = false;
+            for (int t = blockIdx.x; t < ntiles && !stop; t += gridDim.x, ++j) {
+                const int acc = j & 1;
+                const uint32_t tacc = tmem + (uint32_t)(acc * BN);
+                if (j >= 2 && !mbar_wait(&tempty[acc], ((j >> 1) - 1) & 1)) {
+                    atomicExch(p.err, 4);
+                    *(volatile int *)abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                for (int kb = 0; kb < kblocks; ++kb) {
+                    const int s = it % STAGES;
+                    if (!mbar_wait(&full[s], (it / STAGES) & 1)) {
+                        atomicExch(p.err, 2);
+                        *(volatile int *)abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    if (*(volatile int *)abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t sa = smem_u32(smem + s * STAGE_BYTES), sb = sa + TILE_BYTES;
+#pragma unroll
+                    for (int k = 0; k < BKB / 32; ++k) {
+                        // 32 int8 = 32 bytes along K per instruction, inside the 128-byte swizzle atom
+                        umma_i8(tacc, smem_desc_k128(sa + k * 32), smem_desc_k128(sb + k * 32),
+                                (kb > 0 || k > 0) ? 1u : 0u);
+                    }
+                    umma_commit(&empty[s]);
+                    ++it;
+                }
+                umma_commit(&tfull[acc]);
+            }
+        }
+    } else {
+        // ---------------- epilogue (warps 2..5): TMEM lanes 32 (warp % 4) .. + 31 are this warp's rows
+        const int rq = warp & 3;
+        const int rloc = rq * 32 + lane;
+        int j = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++j) {
+            const int mi = t % mt, ni = (t / mt) % nt, mod = t / (mt * nt);
+            const int acc = j & 1;
+            const int row = mi * BM + rloc, n0 = ni * BN;
+            const int pm = tb.p[mod];
+            const double invpd = tb.invp[mod];
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(&tfull[acc], (j >> 1) & 1) ? 1 : 0) != 0;
+            if (!ok && lane == 0) atomicExch(p.err, 3);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const bool live = ok && !*(volatile int *)abort_flag && kblocks > 0;  // warp-uniform
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+                uint32_t v[32];
+                tmem_ld32_raw(tmem + ((uint32_t)(rq * 32) << 16) + (uint32_t)(acc * BN + c0), v);
+                const int col0 = n0 + c0;
+                if (live && row < p.M && col0 < p.N) {
+                    uint32_t w[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        uint32_t word = 0;
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            // |a| < 2^31 is exact in FP64, so q is round(a / p) or one off near a tie
+                            const int a = (int)v[4 * q + e];
+                            const long long qq = (long long)rint((double)a * invpd);
+                            int r = (int)((long long)a - qq * pm);
+                            if (r > ((pm - 1) >> 1)) r -= pm;
+                            if (r < -(pm >> 1)) r += pm;
+                            word |= ((uint32_t)(uint8_t)(int8_t)r) << (8 * e);
+                        }
+                        w[q] = word;
+                    }
+                    uint4 *dst = reinterpret_cast<uint4 *>(p.RC + mod * p.planeC + (long long)row * p.ldr + col0);
+                    dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                    dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(&tempty[acc]);
+            if (!ok) break;
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN));
+    }
+}
+
+// ---------------------------------------------------------------------------- reconstruction
+
+// C[m][n] = alpha * 2^-(sa[m] + sb[n]) X + beta * C[m][n], X the integer with residues RC[i][m][n] (Garner's
+// mixed-radix digits v_j, symmetric, X = v_0 + p_0 (v_1 + p_1 (v_2 + ...)) evaluated in FP64).  Four
+// consecutive columns per thread (one 32-bit word per residue plane); NM moduli.
+template <int NM>
+__global__ void __launch_bounds__(256) ozaki_crt_kernel(int M, int N, const int8_t *RC, long long planeC, int ldr,
+                                                        const int *sa, const int *sb, double alpha, double beta,
+                                                        double *C, long long ldc, const __grid_constant__ Tables tb) {
+    const int nq = (N + 3) / 4;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)M * nq) return;
+    const int m = (int)(idx / nq), n0 = (int)(idx % nq) * 4;
+    uint32_t wd[NM];
+#pragma unroll
+    for (int i = 0; i < NM; ++i)
+        wd[i] = *reinterpret_cast<const uint32_t *>(RC + i * planeC + (long long)m * ldr + n0);
+    const int sm = sa[m];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int n = n0 + e;
+        if (n >= N) break;
+        int v[NM];
+        v[0] = (int)(int8_t)(uint8_t)(wd[0] >> (8 * e));
+#pragma unroll
+        for (int jj = 1; jj < NM; ++jj) {
+            // |r - sum_i v_i D| <= 128 + 15 * 128 * 255 < 2^19 and Binv <= 255: the product stays below 2^27
+            int acc = (int)(int8_t)(uint8_t)(wd[jj] >> (8 * e));
+#pragma unroll
+            for (int i = 0; i < jj; ++i) acc -= v[i] * tb.D[jj][i];
+            v[jj] = symmod_i(acc * tb.Binv[jj], tb.p[jj], tb.invpf[jj]);
+        }
+        double x = (double)v[NM - 1];
+#pragma unroll
+        for (int jj = NM - 2; jj >= 0; --jj) x = fma(x, (double)tb.p[jj], (double)v[jj]);
+        const int sn = sb[n];
+        double out;
+        if (sm == SCALE_NONFINITE || sn == SCALE_NONFINITE)
+            out = __longlong_as_double(0x7ff8000000000000ll);  // NaN
+        else
+            out = alpha * ldexp(x, -(sm + sn));
+        double *c = C + (long long)m * ldc + n;
+        *c = beta == 0.0 ? out : out + beta * *c;
+    }
+}
+
+template <int NM>
+void launch_crt(int M, int N, const int8_t *RC, long long planeC, int ldr, const int *sa, const int *sb, double alpha,
+                double beta, double *C, long long ldc, const Tables &tb, cudaStream_t st) {
+    const long long nthreads = (long long)M * ((N + 3) / 4);
+    ozaki_crt_kernel<NM><<<(unsigned)((nthreads + 255) / 256), 256, 0, st>>>(M, N, RC, planeC, ldr, sa, sb, alpha,
+                                                                             beta, C, ldc, tb);
+}
+
+// ---------------------------------------------------------------------------- host side
+thread_local char g_err[256] = "";
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::mutex g_mutex;
+Tables g_tables;
+bool g_tables_ready = false;
+
+int init_host() {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!g_encode) {
+        cudaDriverEntryPointQueryResult q;
+        void *fn = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            snprintf(g_err, sizeof(g_err), "cuTensorMapEncodeTiled unavailable");
+            return -1;
+        }
+        g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    if (!g_tables_ready) {
+        Tables &t = g_tables;
+        for (int i = 0; i < MAXMOD; ++i) {
+            t.p[i] = kModuli[i];
+            t.invpf[i] = 1.0f / (float)kModuli[i];
+            t.invp[i] = 1.0 / (double)kModuli[i];
+        }
+        for (int j = 0; j < MAXMOD; ++j) {
+            const int pj = kModuli[j];
+            long long prod = 1;  // p_0 ... p_{i-1} mod p_j
+            for (int i = 0; i < MAXMOD; ++i) {
+                t.D[j][i] = (i < j) ? (int)prod : 0;
+                if (i < j) prod = (prod * kModuli[i]) % pj;
+            }
+            // prod = p_0 ... p_{j-1} mod p_j; its inverse by search (p_j <= 256)
+            int inv = 0;
+            for (int x = 1; x < pj && j > 0; ++x)
+                if ((prod * x) % pj == 1) {
+                    inv = x;
+                    break;
+                }
+            t.Binv[j] = (j == 0) ? 1 : inv;
+        }
+        g_tables_ready = true;
+    }
+    return 0;
+}
+
+int make_map_i8(CUtensorMap *map, const void *base, long long rows, int kpad, int box_rows) {
+    cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)kpad};
+    cuuint32_t box[2] = {(cuuint32_t)BKB, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        snprintf(g_err, sizeof(g_err), "cuTensorMapEncodeTiled (int8) failed (%d): rows %lld kpad %d", (int)r, rows,
+                 kpad);
+        return -1;
+    }
+    return 0;
+}
+
+inline long long up(long long x, long long q) { return (x + q - 1) / q * q; }
+
+struct Layout {
+    long long mpad, npad, kpad, ldr, planeA, planeB, planeC;
+    size_t off_sa, off_sb, off_ra, off_rb, off_rc, total;
+};
+
+Layout layout(int m, int n, int k, int nmod) {
+    Layout L;
+    L.mpad = up(m, BM);
+    L.npad = up(n, BN);
+    L.kpad = up(k, BKB);
+    L.ldr = up(n, 32);
+    L.planeA = L.mpad * L.kpad;
+    L.planeB = L.npad * L.kpad;
+    L.planeC = (long long)m * L.ldr;
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = o;
+        o = (size_t)up((long long)(o + bytes), 256);
+        return at;
+    };
+    L.off_sa = take(sizeof(int) * L.mpad);
+    L.off_sb = take(sizeof(int) * L.npad);
+    L.off_ra = take((size_t)nmod * L.planeA);
+    L.off_rb = take((size_t)nmod * L.planeB);
+    L.off_rc = take((size_t)nmod * L.planeC);
+    L.total = o;
+    return L;
+}
+
+// largest bit count b with K 2^(2b) < P/2 (P the product of the first nmod moduli), at most 53
+int scale_bits(int k, int nmod) {
+    double log2P = 0.0;
+    for (int i = 0; i < nmod; ++i) log2P += log2((double)kModuli[i]);
+    const int b = (int)floor((log2P - 1.0 - log2((double)k) - 1e-6) / 2.0);
+    return b < 53 ? b : 53;
+}
+
+}  // namespace ozk
+
+extern "C" {
+
+const char *dftb_ozaki_last_error(void) { return ozk::g_err; }
+
+size_t dftb_ozaki_workspace_size(int m, int n, int k, int nmod) {
+    if (m <= 0 || n <= 0 || k <= 0 || nmod < 1 || nmod > ozk::MAXMOD) return 0;
+    return ozk::layout(m, n, k, nmod).total;
+}
+
+int dftb_ozaki_dgemm(int transa, int transb, int m, int n, int k, double alpha, const double *A, int lda,
+                     const double *B, int ldb, double beta, double *C, int ldc, int nmod, void *work,
+                     size_t work_bytes, int *err, void *stream) {
+    using namespace ozk;
+    if (m <= 0 || n <= 0 || k <= 0 || k > KMAX || nmod < 8 || nmod > MAXMOD) {
+        snprintf(g_err, sizeof(g_err), "ozaki_dgemm: m, n > 0, 0 < k <= %d and 8 <= nmod <= %d required", KMAX,
+                 MAXMOD);
+        return DFTB_ERR_BAD_SIZE;
+    }
+    if (!A || !B || !C || !work || !err) return DFTB_ERR_NULL;
+    if (lda < (transa ? m : k) || ldb < (transb ? k : n) || ldc < n) {
+        snprintf(g_err, sizeof(g_err), "ozaki_dgemm: leading dimension too small");
+        return DFTB_ERR_BAD_SIZE;
+    }
+    const int bits = scale_bits(k, nmod);
+    if (bits < 16) {
+        snprintf(g_err, sizeof(g_err), "ozaki_dgemm: %d moduli leave %d bits at k = %d", nmod, bits, k);
+        return DFTB_ERR_BAD_SIZE;
+    }
+    const Layout L = layout(m, n, k, nmod);
+    if (work_bytes < L.total || (reinterpret_cast<uintptr_t>(work) & 255)) {
+        snprintf(g_err, sizeof(g_err), "ozaki_dgemm: workspace of %zu bytes (256-byte aligned) needed", L.total);
+        return DFTB_ERR_WORKSPACE;
+    }
+    if ((long long)(L.mpad / BM) * (L.npad / BN) * nmod > (1LL << 30)) return DFTB_ERR_BAD_SIZE;
+    if (init_host()) return DFTB_ERR_CUDA;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    uint8_t *w = reinterpret_cast<uint8_t *>(work);
+    int *sa = reinterpret_cast<int *>(w + L.off_sa), *sb = reinterpret_cast<int *>(w + L.off_sb);
+    int8_t *RA = reinterpret_cast<int8_t *>(w + L.off_ra), *RB = reinterpret_cast<int8_t *>(w + L.off_rb);
+    int8_t *RC = reinterpret_cast<int8_t *>(w + L.off_rc);
+
+    // op(A)(r, k) = transa ? A[k][r] : A[r][k];  op(B)^T(r, k) = op(B)(k, r) = transb ? B[r][k] : B[k][r]
+    const int ta = transa ? 1 : 0, tb = transb ? 0 : 1;
+    auto scale = [&](int rows, long long rpad, const double *X, int ldx, int trans, int *s) {
+        if (!trans) {
+            const long long threads = rpad * 32;
+            ozaki_rowscale_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(rows, (int)rpad, k, X, ldx, 0,
+                                                                                     bits, s);
+        } else {
+            ozaki_rowscale_kernel<<<(unsigned)(rpad / 32), dim3(32, 8), 0, st>>>(rows, (int)rpad, k, X, ldx, 1, bits,
+                                                                               s);
+        }
+    };
+    scale(m, L.mpad, A, lda, ta, sa);
+    scale(n, L.npad, B, ldb, tb, sb);
+    {
+        dim3 ga((unsigned)(L.kpad / RT_K), (unsigned)(L.mpad / RT_ROWS));
+        ozaki_residue_kernel<<<ga, 256, 0, st>>>(m, k, A, lda, ta, sa, nmod, g_tables, RA, L.planeA, (int)L.kpad);
+        dim3 gb((unsigned)(L.kpad / RT_K), (unsigned)(L.npad / RT_ROWS));
+        ozaki_residue_kernel<<<gb, 256, 0, st>>>(n, k, B, ldb, tb, sb, nmod, g_tables, RB, L.planeB, (int)L.kpad);
+    }
+    Maps maps;
+    memset(&maps, 0, sizeof(maps));
+    if (make_map_i8(&maps.a, RA, (long long)nmod * L.mpad, (int)L.kpad, BM) ||
+        make_map_i8(&maps.b, RB, (long long)nmod * L.npad, (int)L.kpad, BN))
+        return DFTB_ERR_CUDA;
+    MmaParams p;
+    p.M = m;
+    p.N = n;
+    p.kpad = (int)L.kpad;
+    p.mpad = (int)L.mpad;
+    p.npad = (int)L.npad;
+    p.nmod = nmod;
+    p.RC = RC;
+    p.planeC = L.planeC;
+    p.ldr = (int)L.ldr;
+    p.err = err;
+    static bool attr_set[64] = {false};
+    static int sm_count[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        if (cudaFuncSetAttribute(ozaki_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) !=
+            cudaSuccess) {
+            snprintf(g_err, sizeof(g_err), "ozaki_dgemm: cannot reserve %d bytes of shared memory", SMEM_BYTES);
+            return DFTB_ERR_CUDA;
+        }
+        int nsm = 0;
+        if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0) nsm = 148;
+        sm_count[dev] = nsm;
+        attr_set[dev] = true;
+    }
+    const int sms = (dev >= 0 && dev < 64) ? sm_count[dev] : 148;
+    const long long ntiles = (L.mpad / BM) * (L.npad / BN) * nmod;
+    ozaki_mma_kernel<<<(unsigned)(ntiles < sms ? ntiles : sms), 192, SMEM_BYTES, st>>>(maps, p, g_tables);
+    switch (nmod) {
+#define OZK_CRT(NMV)                                                                                  \
+    case NMV:                                                                                         \
+        launch_crt<NMV>(m, n, RC, L.planeC, (int)L.ldr, sa, sb, alpha, beta, C, ldc, g_tables, st); \
+        break;
+        OZK_CRT(8)
+        OZK_CRT(9)
+        OZK_CRT(10)
+        OZK_CRT(11)
+        OZK_CRT(12)
+        OZK_CRT(13)
+        OZK_CRT(14)
+        OZK_CRT(15)
+        OZK_CRT(16)
+#undef OZK_CRT
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        snprintf(g_err, sizeof(g_err), "ozaki_dgemm: %s", cudaGetErrorString(e));
+        return DFTB_ERR_CUDA;
+    }
+    return DFTB_OK;
+}
+
+}  // extern "C"

@@ -89,6 +89,9 @@ _SIGNATURES = {
     "dftb_solver_reset": (_I, [_P]),
     "dftb_solver_destroy": (_I, [_P]),
     "dftb_solver_last_error": (ctypes.c_char_p, []),
+    "dftb_ozaki_workspace_size": (_Z, [_I, _I, _I, _I]),
+    "dftb_ozaki_dgemm": (_I, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _I, _P, _Z, _P, _P]),
+    "dftb_ozaki_last_error": (ctypes.c_char_p, []),
 }
 
 
@@ -130,7 +133,7 @@ def check(rc, what):
         if _lib is not None:
             msg = (_lib.dftb_last_error().decode() or _lib.dftb_grad_last_error().decode()
                    or _lib.dftb_mlp_last_error().decode() or _lib.dftb_eigh_last_error().decode()
-                   or _lib.dftb_solver_last_error().decode())
+                   or _lib.dftb_solver_last_error().decode() or _lib.dftb_ozaki_last_error().decode())
         raise NativeError("%s failed (%s): %s" % (what, _ERRORS.get(rc, rc), msg))
 
 
@@ -142,7 +145,7 @@ KERNELS_PER_CALL = {
     "dftb_davidson_precondition": 1, "dftb_davidson_residual": 2, "dftb_dgemm": 1,
     "dftb_gradients_h0_and_s": 3, "dftb_sk_gradient_contract": 1, "dftb_pair_gradients": 1,
     "dftb_repulsive_energy": 1, "dftb_mlp_bias_relu": 1, "dftb_mlp_relu_backward": 1, "dftb_mlp_output": 1,
-    "dftb_mlp_adam": 1,
+    "dftb_mlp_adam": 1, "dftb_ozaki_dgemm": 6,
 }
 
 

@@ -234,6 +234,26 @@ int dftb_split_bf16_f64(int rows, int cols, const double *X, int ldx, int transp
                         void *lo, int ld, void *stream);
 const char *dftb_tc_last_error(void);
 
+/* FP64 product C = alpha * op(A) . op(B) + beta * C (row-major, op = transpose
+ * when trans != 0) emulated on the int8 tensor cores (no counterpart in
+ * DFTBaby; it carries the FP64 contractions of the SCC, DFTB2.py:1086-1266,
+ * and of the FP64 exchange products, Solver.py:583-635).  Ozaki scheme II:
+ * rows of op(A) and columns of op(B) are scaled by powers of two and rounded
+ * to integers of b bits, b the largest with k 2^(2b) < P/2 (at most 53; P the
+ * product of the first nmod of 16 coprime moduli <= 256), the integer product
+ * is formed exactly from nmod int8 GEMMs of residues (int32 accumulation) and
+ * recovered by the Chinese remainder theorem.  Each entry enters with b bits
+ * relative to the largest magnitude of its row (column); nmod = 16 gives
+ * b = 53 for every k <= 131071.  A row or column holding Inf or NaN gives NaN
+ * in its row (column) of C.  work: dftb_ozaki_workspace_size bytes, 256-byte
+ * aligned; err: device int set non-zero if an internal wait timed out.
+ * Returns DFTB_ERR_BAD_SIZE for k > 131071 or nmod outside 8..16. */
+size_t dftb_ozaki_workspace_size(int m, int n, int k, int nmod);
+int dftb_ozaki_dgemm(int transa, int transb, int m, int n, int k, double alpha, const double *A, int lda,
+                     const double *B, int ldb, double beta, double *C, int ldc, int nmod, void *work,
+                     size_t work_bytes, int *err, void *stream);
+const char *dftb_ozaki_last_error(void);
+
 /* General FP64 product C = alpha * op(A) . op(B) + beta * C on row-major
  * matrices (op = transpose when trans != 0), the contraction engine behind the
  * entry points above, exported for the host-side solver. */
