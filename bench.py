@@ -143,8 +143,9 @@ def workload_config(name, w, n_gpus, precision="fp64"):
                          "residual, then FP64 refinement (the projection onto the whole mixed expansion space "
                          "corrected with FP64 products of the Ritz vectors); SCC with occupied-space tracking "
                          "between dense eigensolves and its long-range exchange on the tensor cores between FP64 "
-                         "anchor densities (the converged iteration in FP64); Coulomb term, Gram-Schmidt and "
-                         "subspace eigenproblems f64; "
+                         "anchor densities (the converged iteration in FP64), its FP64 products emulated on the "
+                         "int8 tensor cores (Ozaki scheme II, 53-bit operands, exact integer products); Coulomb "
+                         "term, Gram-Schmidt and subspace eigenproblems f64; "
                          "accuracy vs the plain f64 path on the same geometries reported per run")
            if precision == "mixed" and w["lc"] else "fp64",
            "geometry": "seeded jitter per step and rank",
@@ -517,10 +518,10 @@ def main():
     if args.precision == "mixed" and w["lc"]:
         # tensor-core exchange, then FP64 corrections of the projection onto the whole mixed expansion space
         # (FP64 products of the Ritz vectors, refine_iterations rounds); SCC with occupied-space tracking
-        # instead of a dense eigensolve in every iteration, and its long-range exchange formed on the tensor
-        # cores relative to FP64 anchor densities
+        # instead of a dense eigensolve in every iteration, its long-range exchange formed on the tensor
+        # cores relative to FP64 anchor densities, and its FP64 products on the int8 tensor cores
         opts.update(precision="mixed", refine_fp64=True, refine_iterations=args.refine_iterations,
-                    eigensolver="subspace", lc_products="mixed")
+                    eigensolver="subspace", lc_products="mixed", fp64_products="ozaki")
         if args.learned and w["kind"] in ("armchair", "flake"):
             # the learned dense start: frontier orbital block plus the network's choices (learned.dense_start)
             from dftbaby_b200 import learned

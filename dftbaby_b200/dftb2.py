@@ -244,11 +244,12 @@ class DFTB2(object):
         fourth term is the transpose of the first."""
         dP = self.P - self.P0
         S, G = self.S, self.G_lr
-        A1 = S @ dP
-        t1 = (G * A1) @ S
+        mm = self._mm
+        A1 = mm(S, dP)
+        t1 = mm(G * A1, S)
         Hx = t1 + t1.T
-        Hx += G * (A1 @ S)
-        Hx += S @ (dP * G) @ S
+        Hx += G * mm(A1, S)
+        Hx += mm(S, mm(dP * G, S))
         return Hx * (-1.0 / 8.0)
 
     def _lc_exchange_tc(self, D):
@@ -293,6 +294,12 @@ class DFTB2(object):
             return lcs["Hx"]
         lcs["tc"] = lcs.get("tc", 0) + 1
         return lcs["Hx"] + self._lc_exchange_tc(self.P - lcs["P"])
+
+    @property
+    def _mm(self):
+        """The FP64 matrix product of the SCC: cuBLAS DGEMM, or the int8 tensor-core emulation
+        (runSCC(fp64_products="ozaki"))."""
+        return getattr(self, "_mm_fn", None) or torch.matmul
 
     def lc_exchange_energy(self):
         dP = self.P - self.P0
@@ -346,7 +353,7 @@ class DFTB2(object):
     def runSCC(self, maxiter=1000, scf_conv=1.0e-10, start_from_previous=1, mixing_threshold=1.0e-3,
                density_mixer="default", fock_interpolator=None, level_shift=0.1, HOMO_LUMO_tol=0.05,
                linear_mixing_coefficient=0.33, eigensolver="full", subspace_start=0.1, subspace_tol=1.0e-6,
-               lc_products="fp64", lc_anchor_ratio=100.0):
+               lc_products="fp64", lc_anchor_ratio=100.0, fp64_products="cublas"):
         """Self-consistent charges (DFTB2.runSCC, DFTB2.py:940-1160), T = 0.
 
         eigensolver (not in DFTBaby): "full" solves H C = S C e in every iteration, as DFTBaby does.
@@ -365,9 +372,21 @@ class DFTB2(object):
         iteration, as DFTBaby does.  "mixed" forms it in FP64 at anchor densities only and adds the tensor-
         core H^x of the difference to the last anchor (``_lc_exchange_anchored``); a new anchor is formed
         when the distance |P - P_a| / |P| exceeds lc_anchor_ratio times the last relative change, and in the
-        converged (last) iteration, so the orbitals and energies handed on are those of the FP64 operator."""
+        converged (last) iteration, so the orbitals and energies handed on are those of the FP64 operator.
+
+        fp64_products (not in DFTBaby): "cublas" forms the FP64 matrix products of the iteration (exchange,
+        tracking rotations, densities, level-shift projections) with cuBLAS DGEMM; "ozaki" with the int8
+        tensor-core emulation of FP64 products (ozaki.matmul: every operand entry keeps its 53-bit mantissa
+        relative to the largest entry of its row or column, the integer products are exact)."""
         if lc_products not in ("fp64", "mixed"):
             raise ValueError("lc_products must be 'fp64' or 'mixed'")
+        if fp64_products not in ("cublas", "ozaki"):
+            raise ValueError("fp64_products must be 'cublas' or 'ozaki'")
+        if fp64_products == "ozaki":
+            from . import ozaki
+            self._mm_fn = ozaki.matmul
+        else:
+            self._mm_fn = None
         if fock_interpolator is not None:
             raise ValueError("Fock interpolation is not implemented")
         if isinstance(density_mixer, str):
@@ -410,6 +429,7 @@ class DFTB2(object):
         # occupied-space tracking needs a closed shell with at least one empty orbital
         track = eigensolver == "subspace" and self.Nelec_val == 2 * nfull and 0 < nfull < norb
         self.subspace_iterations = 0
+        self.rotation_steps = 0
         tracked = None
         lc_mixed = lc_products == "mixed" and self.long_range_correction == 1
         lcs = {}
@@ -439,20 +459,21 @@ class DFTB2(object):
                                              shift=b if (shift_flag and b > 0.0) else 0.0, tol_rel=subspace_tol)
                 if moved is not None:
                     tracked, step_tracked = moved, True
+            mm = self._mm
             if step_tracked:
                 Co = tracked[0]
-                Pnew = 2.0 * (Co @ Co.T)
+                Pnew = 2.0 * mm(Co, Co.T)
                 self.subspace_iterations += 1
             else:
                 if shift_flag and b > 0.0:
                     # level shift of the virtual block in the basis of the last MOs (DFTB2.py:1059-1081); after
                     # tracked iterations those are the tracked occupied and virtual spaces
                     B = self.orbs if tracked is None else torch.cat([tracked[0], tracked[1]], dim=1)
-                    Hm = B.T @ Hk @ B
+                    Hm = mm(mm(B.T, Hk), B)
                     virt = torch.nonzero(self.f == 0.0).flatten()
                     Hm[virt, virt] += b
                     self.orbe, Cp = torch.linalg.eigh(Hm)
-                    self.orbs = B @ Cp
+                    self.orbs = mm(B, Cp)
                 else:
                     # L^-1 Hk L^-T and L^-T C' by triangular solves (n^3 FLOPs each instead of the
                     # 2 n^3 of a product with an explicit inverse); eigh reads the lower triangle
@@ -464,7 +485,7 @@ class DFTB2(object):
                 self.f = self._occupation(self.orbe)
                 occ = self.f > 0.0
                 Cocc = self.orbs[:, occ]
-                Pnew = (Cocc * self.f[occ]) @ Cocc.T
+                Pnew = mm(Cocc * self.f[occ], Cocc.T)
                 if track:
                     # eigh returns ascending energies: the occupied space is the first nfull columns; the
                     # virtual levels are kept without the level shift this solve may have added
@@ -533,37 +554,52 @@ class DFTB2(object):
         Each step forms the coupling block F = Cv^T H Co and rotates the two spaces by the first-order
         (Jacobi) correction Y_ai = F_ai / (e_i - e_a), with e_i = diag(Co^T H Co) and e_a the virtual
         levels of the last full solve: Co + Cv Y and Cv - Co Y^T stay exactly S-orthogonal to each other,
-        and their Gram matrices I + Y^T Y and I + Y Y^T renormalise them (Cholesky).  Steps repeat until
-        max |F| < max(1e-13, tol_rel rel), rel being the last relative density change.  A level shift b > 0
-        is DFTBaby's (DFTB2.py:1059-1081): b added to the virtual block in the basis of the previous
-        orbitals, i.e. H + b S Cv0 Cv0^T S with Cv0 the virtual space on entry.  Returns the new
-        (Co, Cv, e_o, e_v), or None when an occupied level is not below every virtual one or the rotations
-        have not converged after max_steps; the caller then solves the full eigenproblem."""
+        and their Gram matrices I + Y^T Y and I + Y Y^T renormalise them -- by the symmetric (Lowdin)
+        inverse square root I - G/2 + 3 G^2/8 when |Y|_F^2 <= 3e-6 (the omitted terms are below
+        5/16 |Y|_F^6 < 1e-17), by Cholesky otherwise.  Steps repeat until max |F| < max(1e-13, tol_rel rel),
+        rel being the last relative density change.  A level shift b > 0 is DFTBaby's (DFTB2.py:1059-1081):
+        b added to the virtual block in the basis of the previous orbitals, i.e. H + b S Cv0 Cv0^T S with
+        Cv0 the virtual space on entry.  Returns the new (Co, Cv, e_o, e_v), or None when an occupied level
+        is not below every virtual one or the rotations have not converged after max_steps; the caller then
+        solves the full eigenproblem."""
         Co, Cv, eo, ev = tracked
+        mm = self._mm
         tol = max(1.0e-13, tol_rel * rel)
-        no, nv = Co.shape[1], Cv.shape[1]
-        SCv0 = self.S @ Cv if shift > 0.0 else None
+        SCv0 = mm(self.S, Cv) if shift > 0.0 else None
         for step in range(max_steps + 1):
-            HCo = H @ Co
+            HCo = mm(H, Co)
             if SCv0 is not None:
-                HCo = torch.addmm(HCo, SCv0, SCv0.T @ Co, alpha=shift)
-            F = Cv.T @ HCo
+                HCo = HCo + shift * mm(SCv0, mm(SCv0.T, Co))
+            F = mm(Cv.T, HCo)
             eo = torch.sum(Co * HCo, dim=0)
             den = eo[None, :] - (ev[:, None] + shift)
-            fmax, dmax = torch.stack([torch.max(torch.abs(F)), torch.max(den)]).cpu().numpy()
+            Y = F / den
+            fmax, dmax, y2 = torch.stack([torch.max(torch.abs(F)), torch.max(den), torch.sum(Y * Y)]).cpu().numpy()
             if not np.isfinite(fmax) or dmax >= 0.0:
                 return None
             if fmax < tol:
                 return Co, Cv, eo, ev
             if step == max_steps:
                 return None
-            Y = F / den
-            Con = torch.addmm(Co, Cv, Y)
-            Cvn = torch.addmm(Cv, Co, Y.T, alpha=-1.0)
-            Lo, io = torch.linalg.cholesky_ex(torch.addmm(torch.eye(no, dtype=Y.dtype, device=Y.device), Y.T, Y))
-            Lv, iv = torch.linalg.cholesky_ex(torch.addmm(torch.eye(nv, dtype=Y.dtype, device=Y.device), Y, Y.T))
-            Co = torch.linalg.solve_triangular(Lo.mT, Con, upper=True, left=False)
-            Cv = torch.linalg.solve_triangular(Lv.mT, Cvn, upper=True, left=False)
+            self.rotation_steps += 1
+            Con = Co + mm(Cv, Y)
+            Cvn = Cv - mm(Co, Y.T)
+            Go = mm(Y.T, Y)
+            Gv = mm(Y, Y.T)
+            if y2 <= 3.0e-6:
+                # (I + G)^(-1/2) = I - G/2 + 3/8 G^2 - 5/16 G^3 + ...,  |G|_2 <= |Y|_F^2
+                Mo = 0.375 * mm(Go, Go) - 0.5 * Go
+                Mo.diagonal().add_(1.0)
+                Mv = 0.375 * mm(Gv, Gv) - 0.5 * Gv
+                Mv.diagonal().add_(1.0)
+                Co, Cv = mm(Con, Mo), mm(Cvn, Mv)
+            else:
+                Go.diagonal().add_(1.0)
+                Gv.diagonal().add_(1.0)
+                Lo, _ = torch.linalg.cholesky_ex(Go)
+                Lv, _ = torch.linalg.cholesky_ex(Gv)
+                Co = torch.linalg.solve_triangular(Lo.mT, Con, upper=True, left=False)
+                Cv = torch.linalg.solve_triangular(Lv.mT, Cvn, upper=True, left=False)
         return None
 
     def setCharge(self, charge):

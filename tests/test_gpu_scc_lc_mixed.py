@@ -10,9 +10,15 @@ from dftbaby_b200 import geometry, native
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name,eigensolver", [("polyene20_lc", "full"), ("armchair2_lc", "full"),
-                                              ("armchair3_lc", "subspace"), ("polyene20_lc", "subspace")])
-def test_anchored_lc_exchange_matches_oracle(name, eigensolver):
+@pytest.mark.parametrize("name,eigensolver,products", [("polyene20_lc", "full", "cublas"),
+                                                       ("armchair2_lc", "full", "cublas"),
+                                                       ("armchair3_lc", "subspace", "cublas"),
+                                                       ("polyene20_lc", "subspace", "cublas"),
+                                                       ("armchair3_lc", "subspace", "ozaki"),
+                                                       ("armchair2_lc", "full", "ozaki")])
+def test_anchored_lc_exchange_matches_oracle(name, eigensolver, products):
+    """products="ozaki": the FP64 products of the iteration (anchors, tracking, densities) on the int8
+    tensor cores."""
     native.load()
     from dftbaby_b200.dftb2 import DFTB2
     from oracle import dftb_oracle as O
@@ -24,7 +30,7 @@ def test_anchored_lc_exchange_matches_oracle(name, eigensolver):
     E_o = o.getEnergy()
     d = DFTB2(al, long_range_correction=1)
     d.setGeometry(al)
-    E = d.getEnergy(lc_products="mixed", eigensolver=eigensolver)
+    E = d.getEnergy(lc_products="mixed", eigensolver=eigensolver, fp64_products=products)
     anchors, tc = d.lc_anchor_counts
     assert tc > anchors  # most iterations used the tensor-core exchange
     assert abs(d.scc_iterations - o.scc_iterations) <= 1
