@@ -118,10 +118,11 @@ __global__ void ozaki_rowscale_kernel(int rows, int rpad, int K, const double *X
 
 constexpr int RT_ROWS = 32, RT_K = 128;
 
-// Residue planes R[i][r][k] (i < nmod, r < rpad, k < kpad; zero outside rows x K) of the scaled, rounded
-// Y(r, k) 2^s[r].  One block per 32 x 128 tile of Y, staged through shared memory so that both the FP64
-// reads (along k, or along r when transposed) and the int8 writes (4 consecutive k per thread) coalesce.
-__global__ void __launch_bounds__(256) ozaki_residue_kernel(int rows, int K, const double *X, long long ldx, int trans,
+// Residue planes R[i][r][k] (i < nmod, r < rows_write, k < kpad; zero outside rows x K) of the scaled,
+// rounded Y(r, k) 2^s[r].  One block per 32 x 128 tile of Y, staged through shared memory so that both the
+// FP64 reads (along k, or along r when transposed) and the int8 writes (4 consecutive k per thread) coalesce.
+__global__ void __launch_bounds__(256) ozaki_residue_kernel(int rows, int rows_write, int K, const double *X,
+                                                            long long ldx, int trans,
                                                             const int *s, int nmod,
                                                             const __grid_constant__ Tables tb, int8_t *R,
                                                             long long plane, int kpad) {
@@ -145,7 +146,7 @@ __global__ void __launch_bounds__(256) ozaki_residue_kernel(int rows, int K, con
     for (int item = threadIdx.x; item < RT_ROWS * (RT_K / 4); item += blockDim.x) {
         const int rr = item / (RT_K / 4), kq = (item % (RT_K / 4)) * 4;
         const int r = r0 + rr, k = k0 + kq;
-        if (k >= kpad) continue;
+        if (k >= kpad || r >= rows_write) continue;
         const int sr = (r < rows) ? s[r] : 0;
         double a[4];
 #pragma unroll
@@ -194,12 +195,13 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem_c, uint64_t da, uint64_t d
 }
 
 struct Maps {
-    CUtensorMap a;  // residue planes of op(A): (nmod * mpad) rows x kpad int8
-    CUtensorMap b;  // residue planes of op(B)^T: (nmod * npad) rows x kpad int8
+    CUtensorMap a;  // residue planes of the A operand: nmod * arows rows x kpad int8
+    CUtensorMap b;  // residue planes of the B operand: nmod * brows rows x kpad int8
 };
 
 struct MmaParams {
-    int M, N, kpad, mpad, npad, nmod;
+    int M, N, kpad, nmod;
+    int arows, brows;  // rows per residue plane of the A and B operands (multiples of 256)
     int8_t *RC;  // product residues: plane i at RC + i * planeC, row-major with ldr (multiple of 32)
     long long planeC;
     int ldr;
@@ -226,7 +228,7 @@ __global__ void __launch_bounds__(192, 1) ozaki_mma_kernel(const __grid_constant
     int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const int mt = p.mpad / BM, nt = p.npad / BN;
+    const int mt = (p.M + BM - 1) / BM, nt = (p.N + BN - 1) / BN;
     const int ntiles = mt * nt * p.nmod;
     const int kblocks = p.kpad / BKB;
 
@@ -260,7 +262,7 @@ __global__ void __launch_bounds__(192, 1) ozaki_mma_kernel(const __grid_constant
             bool stop = false;
             for (int t = blockIdx.x; t < ntiles && !stop; t += gridDim.x) {
                 const int mi = t % mt, ni = (t / mt) % nt, mod = t / (mt * nt);
-                const int ya = mod * p.mpad + mi * BM, yb = mod * p.npad + ni * BN;
+                const int ya = mod * p.arows + mi * BM, yb = mod * p.brows + ni * BN;
                 for (int kb = 0; kb < kblocks; ++kb) {
                     const int s = it % STAGES;
                     if (it >= STAGES && !mbar_wait(&empty[s], ((it / STAGES) - 1) & 1)) {
@@ -378,13 +380,14 @@ __global__ void __launch_bounds__(192, 1) ozaki_mma_kernel(const __grid_constant
 
 // ---------------------------------------------------------------------------- reconstruction
 
-// C[m][n] = alpha * 2^-(sa[m] + sb[n]) X + beta * C[m][n], X the integer with residues RC[i][m][n] (Garner's
+// C[m][n] = alpha G[m][n] 2^-(sa[m] + sb[n]) X + beta C[m][n] (G optional), X the integer with residues RC[i][m][n] (Garner's
 // mixed-radix digits v_j, symmetric, X = v_0 + p_0 (v_1 + p_1 (v_2 + ...)) evaluated in FP64).  Four
 // consecutive columns per thread (one 32-bit word per residue plane); NM moduli.
 template <int NM>
 __global__ void __launch_bounds__(256) ozaki_crt_kernel(int M, int N, const int8_t *RC, long long planeC, int ldr,
-                                                        const int *sa, const int *sb, double alpha, double beta,
-                                                        double *C, long long ldc, const __grid_constant__ Tables tb) {
+                                                        const int *sa, const int *sb, double alpha, const double *G,
+                                                        long long ldg, double beta, double *C, long long ldc,
+                                                        const __grid_constant__ Tables tb) {
     const int nq = (N + 3) / 4;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)M * nq) return;
@@ -417,6 +420,7 @@ __global__ void __launch_bounds__(256) ozaki_crt_kernel(int M, int N, const int8
             out = __longlong_as_double(0x7ff8000000000000ll);  // NaN
         else
             out = alpha * ldexp(x, -(sm + sn));
+        if (G) out *= G[(long long)m * ldg + n];
         double *c = C + (long long)m * ldc + n;
         *c = beta == 0.0 ? out : out + beta * *c;
     }
@@ -424,10 +428,11 @@ __global__ void __launch_bounds__(256) ozaki_crt_kernel(int M, int N, const int8
 
 template <int NM>
 void launch_crt(int M, int N, const int8_t *RC, long long planeC, int ldr, const int *sa, const int *sb, double alpha,
-                double beta, double *C, long long ldc, const Tables &tb, cudaStream_t st) {
+                const double *G, long long ldg, double beta, double *C, long long ldc, const Tables &tb,
+                cudaStream_t st) {
     const long long nthreads = (long long)M * ((N + 3) / 4);
     ozaki_crt_kernel<NM><<<(unsigned)((nthreads + 255) / 256), 256, 0, st>>>(M, N, RC, planeC, ldr, sa, sb, alpha,
-                                                                             beta, C, ldc, tb);
+                                                                             G, ldg, beta, C, ldc, tb);
 }
 
 // ---------------------------------------------------------------------------- host side
@@ -496,34 +501,26 @@ int make_map_i8(CUtensorMap *map, const void *base, long long rows, int kpad, in
 
 inline long long up(long long x, long long q) { return (x + q - 1) / q * q; }
 
-struct Layout {
-    long long mpad, npad, kpad, ldr, planeA, planeB, planeC;
-    size_t off_sa, off_sb, off_ra, off_rb, off_rc, total;
+// An operand in residue form: rows_total rows (padded to 256) of a K-major matrix, k columns (padded to 128):
+//   int32 exponent per row | nmod int8 residue planes of rpad x kpad
+struct OperandLayout {
+    long long rpad, kpad, plane;
+    size_t off_res, total;
 };
 
-Layout layout(int m, int n, int k, int nmod) {
-    Layout L;
-    L.mpad = up(m, BM);
-    L.npad = up(n, BN);
+OperandLayout operand_layout(int rows_total, int k, int nmod) {
+    OperandLayout L;
+    L.rpad = up(rows_total, 256);
     L.kpad = up(k, BKB);
-    L.ldr = up(n, 32);
-    L.planeA = L.mpad * L.kpad;
-    L.planeB = L.npad * L.kpad;
-    L.planeC = (long long)m * L.ldr;
-    size_t o = 0;
-    auto take = [&](size_t bytes) {
-        const size_t at = o;
-        o = (size_t)up((long long)(o + bytes), 256);
-        return at;
-    };
-    L.off_sa = take(sizeof(int) * L.mpad);
-    L.off_sb = take(sizeof(int) * L.npad);
-    L.off_ra = take((size_t)nmod * L.planeA);
-    L.off_rb = take((size_t)nmod * L.planeB);
-    L.off_rc = take((size_t)nmod * L.planeC);
-    L.total = o;
+    L.plane = L.rpad * L.kpad;
+    L.off_res = (size_t)up(4 * L.rpad, 256);
+    L.total = L.off_res + (size_t)nmod * L.plane;
     return L;
 }
+
+// product residues: nmod planes of m x ldr int8
+inline long long product_ldr(int n) { return up(n, 32); }
+inline size_t product_bytes(int m, int n, int nmod) { return (size_t)up((long long)nmod * m * product_ldr(n), 256); }
 
 // largest bit count b with K 2^(2b) < P/2 (P the product of the first nmod moduli), at most 53
 int scale_bits(int k, int nmod) {
@@ -533,84 +530,60 @@ int scale_bits(int k, int nmod) {
     return b < 53 ? b : 53;
 }
 
-}  // namespace ozk
-
-extern "C" {
-
-const char *dftb_ozaki_last_error(void) { return ozk::g_err; }
-
-size_t dftb_ozaki_workspace_size(int m, int n, int k, int nmod) {
-    if (m <= 0 || n <= 0 || k <= 0 || nmod < 1 || nmod > ozk::MAXMOD) return 0;
-    return ozk::layout(m, n, k, nmod).total;
+int check_shape(int k, int nmod) {
+    if (k <= 0 || k > KMAX || nmod < 8 || nmod > MAXMOD) {
+        snprintf(g_err, sizeof(g_err), "ozaki: 0 < k <= %d and 8 <= nmod <= %d required", KMAX, MAXMOD);
+        return DFTB_ERR_BAD_SIZE;
+    }
+    if (scale_bits(k, nmod) < 16) {
+        snprintf(g_err, sizeof(g_err), "ozaki: %d moduli leave too few bits at k = %d", nmod, k);
+        return DFTB_ERR_BAD_SIZE;
+    }
+    return DFTB_OK;
 }
 
-int dftb_ozaki_dgemm(int transa, int transb, int m, int n, int k, double alpha, const double *A, int lda,
-                     const double *B, int ldb, double beta, double *C, int ldc, int nmod, void *work,
-                     size_t work_bytes, int *err, void *stream) {
-    using namespace ozk;
-    if (m <= 0 || n <= 0 || k <= 0 || k > KMAX || nmod < 8 || nmod > MAXMOD) {
-        snprintf(g_err, sizeof(g_err), "ozaki_dgemm: m, n > 0, 0 < k <= %d and 8 <= nmod <= %d required", KMAX,
-                 MAXMOD);
-        return DFTB_ERR_BAD_SIZE;
-    }
-    if (!A || !B || !C || !work || !err) return DFTB_ERR_NULL;
-    if (lda < (transa ? m : k) || ldb < (transb ? k : n) || ldc < n) {
-        snprintf(g_err, sizeof(g_err), "ozaki_dgemm: leading dimension too small");
-        return DFTB_ERR_BAD_SIZE;
-    }
+// rows [row0, row0 + rows) of the operand from Y(r, k) = trans ? X[k][r] : X[r][k]; when they are the last
+// rows (row0 + rows == rows_total) the padding rows up to 256 are written as zeros too
+int prepare(int trans, int rows, int k, const double *X, long long ldx, int nmod, uint8_t *op, int rows_total,
+            int row0, cudaStream_t st) {
+    const OperandLayout L = operand_layout(rows_total, k, nmod);
     const int bits = scale_bits(k, nmod);
-    if (bits < 16) {
-        snprintf(g_err, sizeof(g_err), "ozaki_dgemm: %d moduli leave %d bits at k = %d", nmod, bits, k);
-        return DFTB_ERR_BAD_SIZE;
+    const int rows_write = (row0 + rows == rows_total) ? (int)(L.rpad - row0) : rows;
+    int *s = reinterpret_cast<int *>(op) + row0;
+    int8_t *R = reinterpret_cast<int8_t *>(op + L.off_res) + (long long)row0 * L.kpad;
+    if (!trans) {
+        const long long threads = (long long)rows_write * 32;
+        ozaki_rowscale_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(rows, rows_write, k, X, ldx, 0, bits,
+                                                                                 s);
+    } else {
+        ozaki_rowscale_kernel<<<(unsigned)((rows_write + 31) / 32), dim3(32, 8), 0, st>>>(rows, rows_write, k, X, ldx,
+                                                                                        1, bits, s);
     }
-    const Layout L = layout(m, n, k, nmod);
-    if (work_bytes < L.total || (reinterpret_cast<uintptr_t>(work) & 255)) {
-        snprintf(g_err, sizeof(g_err), "ozaki_dgemm: workspace of %zu bytes (256-byte aligned) needed", L.total);
-        return DFTB_ERR_WORKSPACE;
-    }
-    if ((long long)(L.mpad / BM) * (L.npad / BN) * nmod > (1LL << 30)) return DFTB_ERR_BAD_SIZE;
-    if (init_host()) return DFTB_ERR_CUDA;
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    uint8_t *w = reinterpret_cast<uint8_t *>(work);
-    int *sa = reinterpret_cast<int *>(w + L.off_sa), *sb = reinterpret_cast<int *>(w + L.off_sb);
-    int8_t *RA = reinterpret_cast<int8_t *>(w + L.off_ra), *RB = reinterpret_cast<int8_t *>(w + L.off_rb);
-    int8_t *RC = reinterpret_cast<int8_t *>(w + L.off_rc);
+    dim3 g((unsigned)(L.kpad / RT_K), (unsigned)((rows_write + RT_ROWS - 1) / RT_ROWS));
+    ozaki_residue_kernel<<<g, 256, 0, st>>>(rows, rows_write, k, X, ldx, trans, s, nmod, g_tables, R, L.plane,
+                                            (int)L.kpad);
+    return cudaGetLastError() == cudaSuccess ? DFTB_OK : DFTB_ERR_CUDA;
+}
 
-    // op(A)(r, k) = transa ? A[k][r] : A[r][k];  op(B)^T(r, k) = op(B)(k, r) = transb ? B[r][k] : B[k][r]
-    const int ta = transa ? 1 : 0, tb = transb ? 0 : 1;
-    auto scale = [&](int rows, long long rpad, const double *X, int ldx, int trans, int *s) {
-        if (!trans) {
-            const long long threads = rpad * 32;
-            ozaki_rowscale_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(rows, (int)rpad, k, X, ldx, 0,
-                                                                                     bits, s);
-        } else {
-            ozaki_rowscale_kernel<<<(unsigned)(rpad / 32), dim3(32, 8), 0, st>>>(rows, (int)rpad, k, X, ldx, 1, bits,
-                                                                               s);
-        }
-    };
-    scale(m, L.mpad, A, lda, ta, sa);
-    scale(n, L.npad, B, ldb, tb, sb);
-    {
-        dim3 ga((unsigned)(L.kpad / RT_K), (unsigned)(L.mpad / RT_ROWS));
-        ozaki_residue_kernel<<<ga, 256, 0, st>>>(m, k, A, lda, ta, sa, nmod, g_tables, RA, L.planeA, (int)L.kpad);
-        dim3 gb((unsigned)(L.kpad / RT_K), (unsigned)(L.npad / RT_ROWS));
-        ozaki_residue_kernel<<<gb, 256, 0, st>>>(n, k, B, ldb, tb, sb, nmod, g_tables, RB, L.planeB, (int)L.kpad);
-    }
+int product(int m, int n, int k, int nmod, const uint8_t *A, int rows_a, const uint8_t *B, int rows_b, double alpha,
+            const double *G, long long ldg, double beta, double *C, long long ldc, int8_t *RC, int *err,
+            cudaStream_t st) {
+    const OperandLayout LA = operand_layout(rows_a, k, nmod), LB = operand_layout(rows_b, k, nmod);
     Maps maps;
     memset(&maps, 0, sizeof(maps));
-    if (make_map_i8(&maps.a, RA, (long long)nmod * L.mpad, (int)L.kpad, BM) ||
-        make_map_i8(&maps.b, RB, (long long)nmod * L.npad, (int)L.kpad, BN))
+    if (make_map_i8(&maps.a, A + LA.off_res, (long long)nmod * LA.rpad, (int)LA.kpad, BM) ||
+        make_map_i8(&maps.b, B + LB.off_res, (long long)nmod * LB.rpad, (int)LB.kpad, BN))
         return DFTB_ERR_CUDA;
     MmaParams p;
     p.M = m;
     p.N = n;
-    p.kpad = (int)L.kpad;
-    p.mpad = (int)L.mpad;
-    p.npad = (int)L.npad;
+    p.kpad = (int)LA.kpad;
     p.nmod = nmod;
+    p.arows = (int)LA.rpad;
+    p.brows = (int)LB.rpad;
     p.RC = RC;
-    p.planeC = L.planeC;
-    p.ldr = (int)L.ldr;
+    p.ldr = (int)product_ldr(n);
+    p.planeC = (long long)m * p.ldr;
     p.err = err;
     static bool attr_set[64] = {false};
     static int sm_count[64] = {0};
@@ -619,7 +592,7 @@ int dftb_ozaki_dgemm(int transa, int transb, int m, int n, int k, double alpha, 
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
         if (cudaFuncSetAttribute(ozaki_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) !=
             cudaSuccess) {
-            snprintf(g_err, sizeof(g_err), "ozaki_dgemm: cannot reserve %d bytes of shared memory", SMEM_BYTES);
+            snprintf(g_err, sizeof(g_err), "ozaki: cannot reserve %d bytes of shared memory", SMEM_BYTES);
             return DFTB_ERR_CUDA;
         }
         int nsm = 0;
@@ -628,12 +601,14 @@ int dftb_ozaki_dgemm(int transa, int transb, int m, int n, int k, double alpha, 
         attr_set[dev] = true;
     }
     const int sms = (dev >= 0 && dev < 64) ? sm_count[dev] : 148;
-    const long long ntiles = (L.mpad / BM) * (L.npad / BN) * nmod;
+    const long long ntiles = (long long)((m + BM - 1) / BM) * ((n + BN - 1) / BN) * nmod;
+    if (ntiles > (1LL << 30)) return DFTB_ERR_BAD_SIZE;
     ozaki_mma_kernel<<<(unsigned)(ntiles < sms ? ntiles : sms), 192, SMEM_BYTES, st>>>(maps, p, g_tables);
+    const int *sa = reinterpret_cast<const int *>(A), *sb = reinterpret_cast<const int *>(B);
     switch (nmod) {
-#define OZK_CRT(NMV)                                                                                  \
-    case NMV:                                                                                         \
-        launch_crt<NMV>(m, n, RC, L.planeC, (int)L.ldr, sa, sb, alpha, beta, C, ldc, g_tables, st); \
+#define OZK_CRT(NMV)                                                                                              \
+    case NMV:                                                                                                     \
+        launch_crt<NMV>(m, n, RC, p.planeC, p.ldr, sa, sb, alpha, G, ldg, beta, C, ldc, g_tables, st); \
         break;
         OZK_CRT(8)
         OZK_CRT(9)
@@ -648,10 +623,102 @@ int dftb_ozaki_dgemm(int transa, int transb, int m, int n, int k, double alpha, 
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
-        snprintf(g_err, sizeof(g_err), "ozaki_dgemm: %s", cudaGetErrorString(e));
+        snprintf(g_err, sizeof(g_err), "ozaki: %s", cudaGetErrorString(e));
         return DFTB_ERR_CUDA;
     }
     return DFTB_OK;
+}
+
+}  // namespace ozk
+
+extern "C" {
+
+const char *dftb_ozaki_last_error(void) { return ozk::g_err; }
+
+size_t dftb_ozaki_operand_size(int rows, int k, int nmod) {
+    if (rows <= 0 || ozk::check_shape(k, nmod) != DFTB_OK) return 0;
+    return ozk::operand_layout(rows, k, nmod).total;
+}
+
+int dftb_ozaki_prepare(int trans, int rows, int k, const double *X, int ldx, int nmod, void *operand, int rows_total,
+                       int row0, void *stream) {
+    using namespace ozk;
+    if (int rc = check_shape(k, nmod)) return rc;
+    if (rows <= 0 || row0 < 0 || row0 + rows > rows_total || ldx < (trans ? rows : k)) {
+        snprintf(g_err, sizeof(g_err), "ozaki_prepare: rows %d at %d of %d, ldx %d", rows, row0, rows_total, ldx);
+        return DFTB_ERR_BAD_SIZE;
+    }
+    if (!X || !operand) return DFTB_ERR_NULL;
+    if (reinterpret_cast<uintptr_t>(operand) & 255) {
+        snprintf(g_err, sizeof(g_err), "ozaki_prepare: the operand must be 256-byte aligned");
+        return DFTB_ERR_BAD_SIZE;
+    }
+    if (init_host()) return DFTB_ERR_CUDA;
+    return prepare(trans, rows, k, X, ldx, nmod, reinterpret_cast<uint8_t *>(operand), rows_total, row0,
+                   reinterpret_cast<cudaStream_t>(stream));
+}
+
+size_t dftb_ozaki_product_workspace_size(int m, int n, int nmod) {
+    if (m <= 0 || n <= 0 || nmod < 1 || nmod > ozk::MAXMOD) return 0;
+    return ozk::product_bytes(m, n, nmod);
+}
+
+int dftb_ozaki_product(int m, int n, int k, int nmod, const void *A, int rows_a, const void *B, int rows_b,
+                       double alpha, const double *G, int ldg, double beta, double *C, int ldc, void *work,
+                       size_t work_bytes, int *err, void *stream) {
+    using namespace ozk;
+    if (int rc = check_shape(k, nmod)) return rc;
+    if (m <= 0 || n <= 0 || m > rows_a || n > rows_b || ldc < n || (G && ldg < n)) {
+        snprintf(g_err, sizeof(g_err), "ozaki_product: m %d of %d rows, n %d of %d rows, ldc %d", m, rows_a, n, rows_b,
+                 ldc);
+        return DFTB_ERR_BAD_SIZE;
+    }
+    if (!A || !B || !C || !work || !err) return DFTB_ERR_NULL;
+    if (work_bytes < product_bytes(m, n, nmod) || ((reinterpret_cast<uintptr_t>(work) |
+                                                    reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) &
+                                                   255)) {
+        snprintf(g_err, sizeof(g_err), "ozaki_product: workspace of %zu bytes and 256-byte aligned operands needed",
+                 product_bytes(m, n, nmod));
+        return DFTB_ERR_WORKSPACE;
+    }
+    if (init_host()) return DFTB_ERR_CUDA;
+    return product(m, n, k, nmod, reinterpret_cast<const uint8_t *>(A), rows_a, reinterpret_cast<const uint8_t *>(B),
+                   rows_b, alpha, G, ldg, beta, C, ldc, reinterpret_cast<int8_t *>(work), err,
+                   reinterpret_cast<cudaStream_t>(stream));
+}
+
+size_t dftb_ozaki_workspace_size(int m, int n, int k, int nmod) {
+    if (m <= 0 || n <= 0 || ozk::check_shape(k, nmod) != DFTB_OK) return 0;
+    return ozk::operand_layout(m, k, nmod).total + ozk::operand_layout(n, k, nmod).total +
+           ozk::product_bytes(m, n, nmod);
+}
+
+int dftb_ozaki_dgemm(int transa, int transb, int m, int n, int k, double alpha, const double *A, int lda,
+                     const double *B, int ldb, double beta, double *C, int ldc, int nmod, void *work,
+                     size_t work_bytes, int *err, void *stream) {
+    using namespace ozk;
+    if (int rc = check_shape(k, nmod)) return rc;
+    if (m <= 0 || n <= 0) return DFTB_ERR_BAD_SIZE;
+    if (!A || !B || !C || !work || !err) return DFTB_ERR_NULL;
+    if (lda < (transa ? m : k) || ldb < (transb ? k : n) || ldc < n) {
+        snprintf(g_err, sizeof(g_err), "ozaki_dgemm: leading dimension too small");
+        return DFTB_ERR_BAD_SIZE;
+    }
+    const size_t need = dftb_ozaki_workspace_size(m, n, k, nmod);
+    if (work_bytes < need || (reinterpret_cast<uintptr_t>(work) & 255)) {
+        snprintf(g_err, sizeof(g_err), "ozaki_dgemm: workspace of %zu bytes (256-byte aligned) needed", need);
+        return DFTB_ERR_WORKSPACE;
+    }
+    if (init_host()) return DFTB_ERR_CUDA;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    uint8_t *w = reinterpret_cast<uint8_t *>(work);
+    uint8_t *opA = w, *opB = w + operand_layout(m, k, nmod).total;
+    int8_t *RC = reinterpret_cast<int8_t *>(opB + operand_layout(n, k, nmod).total);
+    // op(A)(r, k) = transa ? A[k][r] : A[r][k];  op(B)^T(r, k) = op(B)(k, r) = transb ? B[r][k] : B[k][r]
+    int rc = prepare(transa ? 1 : 0, m, k, A, lda, nmod, opA, m, 0, st);
+    if (rc == DFTB_OK) rc = prepare(transb ? 0 : 1, n, k, B, ldb, nmod, opB, n, 0, st);
+    if (rc == DFTB_OK) rc = product(m, n, k, nmod, opA, m, opB, n, alpha, nullptr, 0, beta, C, ldc, RC, err, st);
+    return rc;
 }
 
 }  // extern "C"

@@ -210,6 +210,63 @@ class ExchangeMixed(ExchangeAO):
         return K1, K2
 
 
+class ExchangeOzaki(ExchangeAO):
+    """(A+B).V and (A-B).V with the exchange in FP64, its products on the int8 tensor cores.
+
+    The merged AO-factorised algebra of ExchangeMixed in FP64, each product an ozaki.product (every operand
+    entry with its 53-bit mantissa relative to its row's largest, exact integer products):
+        W^T  = [C_v; S~_v] v^T                        (2 Norb x nocc, K = nvirt)
+        N    = Gamma o ([C_o; S~_o] W)                (2 Norb x 2 Norb, K = nocc)
+        [P1 | P2] = Ybar^T [N; N^T]^T                 (nvirt x 4 Norb, K = 2 Norb)
+        [K1^T ; K2^T] = [P1^T ; P2^T] Xbar_o / 4      (rows interleaved, K = 2 Norb)
+    with Ybar = [S~_v; C_v] and Xbar = [S~_o; C_o]; the four constant operands are converted once.  The
+    Coulomb term is ExchangeAO's (native FP64 q_ov products)."""
+
+    def __init__(self, gamma, G_lr, q_ov, omega_flat, Co, Cv, S, nat, nocc, nvirt, workspace, lc=1):
+        from . import ozaki as O
+        super().__init__(gamma, G_lr, q_ov, omega_flat, Co, Cv, S, nat, nocc, nvirt, workspace, lc=lc,
+                         max_bytes=1)
+        self.O = O
+        dev = Co.device
+        norb = Co.shape[0]
+        self.norb = norb
+        So, Sv = S @ Co, S @ Cv
+        self.opYV = O.Operand(2 * norb, nvirt, dev).set(torch.cat([Cv, Sv], dim=0))
+        self.opXO = O.Operand(2 * norb, nocc, dev).set(torch.cat([Co, So], dim=0))
+        self.opYbarT = O.Operand(nvirt, 2 * norb, dev).set(torch.cat([Sv, Cv], dim=0).T)
+        self.opXbarT = O.Operand(nocc, 2 * norb, dev).set(torch.cat([So, Co], dim=0).T)
+        self.G4 = torch.cat([torch.cat([G_lr, G_lr], dim=1)] * 2, dim=0).contiguous()
+        self.opV = O.Operand(nocc, nvirt, dev)
+        self.opW = O.Operand(2 * norb, nocc, dev)
+        self.opNB = O.Operand(4 * norb, 2 * norb, dev)
+        self.opP = O.Operand(2 * nvirt, 2 * norb, dev)
+        self.WT = torch.empty((2 * norb, nocc), dtype=torch.float64, device=dev)
+        self.N = torch.empty((2 * norb, 2 * norb), dtype=torch.float64, device=dev)
+        self.P12 = torch.empty((nvirt, 4 * norb), dtype=torch.float64, device=dev)
+        self.K12t = torch.empty((2 * nvirt, nocc), dtype=torch.float64, device=dev)
+
+    def exchange(self, V):
+        O = self.O
+        nov, m = V.shape
+        no, nv, norb = self.nocc, self.nvirt, self.norb
+        K1 = torch.empty_like(V)
+        K2 = torch.empty_like(V)
+        Vt = V.T.contiguous()
+        for c in range(m):
+            self.opV.set(Vt[c].view(no, nv))
+            O.product(self.opYV, self.opV, out=self.WT)
+            self.opW.set(self.WT)
+            O.product(self.opXO, self.opW, out=self.N, G=self.G4)
+            self.opNB.set(self.N, row0=0)
+            self.opNB.set(self.N.T, row0=2 * norb)
+            O.product(self.opYbarT, self.opNB, out=self.P12)
+            self.opP.set(self.P12.view(2 * nv, 2 * norb))
+            O.product(self.opP, self.opXbarT, out=self.K12t, alpha=0.25)
+            K1[:, c].view(no, nv).copy_(self.K12t[0::2].T)
+            K2[:, c].view(no, nv).copy_(self.K12t[1::2].T)
+        return K1, K2
+
+
 class LR_TDDFTB:
     XpY = None
     XmY = None
@@ -352,6 +409,8 @@ class LR_TDDFTB:
         if ct_correction or stability:
             raise ValueError("ct_correction and stability analysis are not implemented")
         d = self.dftb2
+        # "ozaki" also moves the FP64 exchange products of the refinement stage onto the int8 tensor cores
+        self._fp64_products = scf_opts.get("fp64_products", "cublas")
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         ev[0].record()
         self.en0 = d.getEnergy(**scf_opts)
@@ -480,8 +539,9 @@ class LR_TDDFTB:
             Om, C, XmY, XpY = self._with_fallback(run, learned)
         else:
             Co, Cv = self._active_coefficients()
-            prod = ExchangeAO(d.gamma, d.G_lr, self.qtrans_ov, self.omega.reshape(-1), Co, Cv, d.S,
-                              len(d.atomlist), self.nocc, self.nvirt, d.workspace, lc=1)
+            fp64_cls = ExchangeOzaki if getattr(self, "_fp64_products", "cublas") == "ozaki" else ExchangeAO
+            prod = fp64_cls(d.gamma, d.G_lr, self.qtrans_ov, self.omega.reshape(-1), Co, Cv, d.S,
+                            len(d.atomlist), self.nocc, self.nvirt, d.workspace, lc=1)
             if precision == "mixed":
                 from . import tcgemm
                 mixed = ExchangeMixed(d.gamma, d.G_lr, self.qtrans_ov, self.omega.reshape(-1), Co, Cv, d.S,

@@ -91,6 +91,10 @@ _SIGNATURES = {
     "dftb_solver_last_error": (ctypes.c_char_p, []),
     "dftb_ozaki_workspace_size": (_Z, [_I, _I, _I, _I]),
     "dftb_ozaki_dgemm": (_I, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _I, _P, _Z, _P, _P]),
+    "dftb_ozaki_operand_size": (_Z, [_I, _I, _I]),
+    "dftb_ozaki_prepare": (_I, [_I, _I, _I, _P, _I, _I, _P, _I, _I, _P]),
+    "dftb_ozaki_product_workspace_size": (_Z, [_I, _I, _I]),
+    "dftb_ozaki_product": (_I, [_I, _I, _I, _I, _P, _I, _P, _I, _D, _P, _I, _D, _P, _I, _P, _Z, _P, _P]),
     "dftb_ozaki_last_error": (ctypes.c_char_p, []),
 }
 
@@ -145,7 +149,7 @@ KERNELS_PER_CALL = {
     "dftb_davidson_precondition": 1, "dftb_davidson_residual": 2, "dftb_dgemm": 1,
     "dftb_gradients_h0_and_s": 3, "dftb_sk_gradient_contract": 1, "dftb_pair_gradients": 1,
     "dftb_repulsive_energy": 1, "dftb_mlp_bias_relu": 1, "dftb_mlp_relu_backward": 1, "dftb_mlp_output": 1,
-    "dftb_mlp_adam": 1, "dftb_ozaki_dgemm": 6,
+    "dftb_mlp_adam": 1, "dftb_ozaki_dgemm": 6, "dftb_ozaki_prepare": 2, "dftb_ozaki_product": 2,
 }
 
 

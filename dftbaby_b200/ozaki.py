@@ -79,6 +79,52 @@ def matmul(A, B, out=None, alpha=1.0, beta=0.0, nmod=16):
     return out
 
 
+class Operand:
+    """A K-major matrix (rows x k) in residue form, reusable across products (dftb_ozaki_prepare).
+
+    ``set(X, row0)`` fills rows row0 .. row0 + X.shape[0] from an FP64 matrix X (rows of X along K; any
+    strides).  An operand stacked from several blocks is complete once every block is set."""
+
+    def __init__(self, rows, k, device, nmod=16):
+        self.rows, self.k, self.nmod = int(rows), int(k), int(nmod)
+        if self.k > KMAX:
+            raise ValueError("an operand holds k <= %d columns" % KMAX)
+        nbytes = native.load().dftb_ozaki_operand_size(self.rows, self.k, self.nmod)
+        if nbytes == 0:
+            raise ValueError("bad operand shape (%d, %d) or nmod %d" % (rows, k, nmod))
+        self.buf = torch.zeros(nbytes, dtype=torch.uint8, device=device)
+
+    def set(self, X, row0=0):
+        if X.dtype != torch.float64 or X.shape[1] != self.k:
+            raise ValueError("an FP64 block with %d columns is required" % self.k)
+        X, trans, ld = _rowmajor(X)
+        native.call("dftb_ozaki_prepare", trans, X.shape[0], self.k, native.ptr(X), ld, self.nmod,
+                    native.ptr(self.buf), self.rows, int(row0), native.stream())
+        return self
+
+
+def product(A, B, out=None, alpha=1.0, beta=0.0, G=None, m=None, n=None):
+    """alpha * G o (A B^T) + beta * out for Operands A (first m rows) and B (first n rows) of the same k."""
+    if A.k != B.k or A.nmod != B.nmod:
+        raise ValueError("operands of different k or nmod")
+    m = A.rows if m is None else m
+    n = B.rows if n is None else n
+    dev = A.buf.device
+    if out is None:
+        out = torch.empty((m, n), dtype=torch.float64, device=dev)
+        beta = 0.0
+    elif out.shape != (m, n) or out.stride(1) != 1:
+        raise ValueError("out must be a row-major (m, n) matrix")
+    if G is not None and (G.shape != (m, n) or G.stride(1) != 1 or G.dtype != torch.float64):
+        raise ValueError("G must be a row-major FP64 (m, n) matrix")
+    L = native.load()
+    ws = _workspace(dev, L.dftb_ozaki_product_workspace_size(m, n, A.nmod))
+    native.call("dftb_ozaki_product", m, n, A.k, A.nmod, native.ptr(A.buf), A.rows, native.ptr(B.buf), B.rows,
+                float(alpha), native.ptr(G), G.stride(0) if G is not None else 0, float(beta), native.ptr(out),
+                out.stride(0), native.ptr(ws), ws.numel(), native.ptr(_errword(dev)), native.stream())
+    return out
+
+
 def check_errors(device):
     e = int(_errword(device).item())
     if e:

@@ -252,6 +252,24 @@ size_t dftb_ozaki_workspace_size(int m, int n, int k, int nmod);
 int dftb_ozaki_dgemm(int transa, int transb, int m, int n, int k, double alpha, const double *A, int lda,
                      const double *B, int ldb, double beta, double *C, int ldc, int nmod, void *work,
                      size_t work_bytes, int *err, void *stream);
+/* The same product in two stages, for operands used in several products.
+ * An operand is a K-major matrix Y (rows_total x k) in residue form (per-row
+ * exponents and nmod int8 residue planes; dftb_ozaki_operand_size bytes,
+ * 256-byte aligned).  dftb_ozaki_prepare fills rows [row0, row0 + rows) of
+ * it from Y(r, c) = trans ? X[c][r] : X[r][c] (X row-major, ldx); the call
+ * that fills the last rows also zeroes the padding rows, so an operand built
+ * from several row blocks (a stacked matrix) is complete once every block is
+ * prepared.  dftb_ozaki_product then forms
+ *   C(i, j) = alpha * G(i, j) * sum_c A(i, c) B(j, c) + beta * C(i, j)
+ * for i < m, j < n from two operands of the same k and nmod (G optional,
+ * row-major ldg; work: dftb_ozaki_product_workspace_size bytes). */
+size_t dftb_ozaki_operand_size(int rows, int k, int nmod);
+int dftb_ozaki_prepare(int trans, int rows, int k, const double *X, int ldx, int nmod, void *operand, int rows_total,
+                       int row0, void *stream);
+size_t dftb_ozaki_product_workspace_size(int m, int n, int nmod);
+int dftb_ozaki_product(int m, int n, int k, int nmod, const void *A, int rows_a, const void *B, int rows_b,
+                       double alpha, const double *G, int ldg, double beta, double *C, int ldc, void *work,
+                       size_t work_bytes, int *err, void *stream);
 const char *dftb_ozaki_last_error(void);
 
 /* General FP64 product C = alpha * op(A) . op(B) + beta * C on row-major

@@ -69,8 +69,27 @@ def test_mixed_solve_within_1meV_and_refined_solve_matches_fp64():
     assert np.abs(Or - O64).max() * HARTREE_TO_EV < 1e-6
 
 
-@pytest.mark.parametrize("rounds", [1, 2])
-def test_mixed_with_fp64_corrections_meets_the_accuracy_gate_on_a_flake(rounds):
+def test_ozaki_exchange_products_match_fp64():
+    """The FP64 exchange with its products on the int8 tensor cores (ExchangeOzaki) against cuBLAS
+    (ExchangeAO): the same algebra at FP64 accuracy."""
+    from dftbaby_b200.lr_tddftb import ExchangeAO, ExchangeOzaki
+    native.load()
+    al = geometry.armchair_flake(2, sigma=0.01, seed=7)
+    td, omega = _setup(al)
+    d = td.dftb2
+    Co, Cv = td._active_coefficients()
+    args = (d.gamma, d.G_lr, td.qtrans_ov, omega.reshape(-1), Co, Cv, d.S, len(al), td.nocc, td.nvirt, d.workspace)
+    ref = ExchangeAO(*args, lc=1)
+    oz = ExchangeOzaki(*args, lc=1)
+    g = torch.Generator(device="cpu").manual_seed(1)
+    V = torch.randn(td.nocc * td.nvirt, 3, generator=g, dtype=torch.float64).to(d.device)
+    for a, b in zip(oz(V), ref(V)):
+        rel = (a - b).abs().max().item() / b.abs().max().item()
+        assert rel < 1e-12, rel
+
+
+@pytest.mark.parametrize("rounds,products", [(1, "cublas"), (2, "cublas"), (1, "ozaki")])
+def test_mixed_with_fp64_corrections_meets_the_accuracy_gate_on_a_flake(rounds, products):
     """The benchmark's accuracy gate on a mid-size long-range-corrected flake (armchair C114H30, 60 x 60
     window, 12 states): the tensor-core solve followed by FP64 corrections of its projection (refine_fp64 in
     solver.py) against the plain FP64 path run to a residual of 1e-10.  Energies within 1 meV and X+Y
@@ -87,7 +106,7 @@ def test_mixed_with_fp64_corrections_meets_the_accuracy_gate_on_a_flake(rounds):
     tm = LR_TDDFTB(al, long_range_correction=1)
     tm.setGeometry(al)
     Om, _ = tm.getEnergies(diag_conv=1e-6, precision="mixed", refine_fp64=True, refine_iterations=rounds,
-                           eigensolver="subspace", **win)
+                           eigensolver="subspace", fp64_products=products, **win)
     fxy = tm.oscillatorStrengthsXpY()
     assert np.abs(Om - O64).max() * HARTREE_TO_EV < 1e-3
     worst, i, tol = 0.0, 0, 1e-3 / HARTREE_TO_EV
