@@ -101,7 +101,8 @@ class Basis:
         self._grow(capacity)
 
     def _grow(self, need):
-        cap = max(need, 2 * self.cap, 16)
+        # growth by half: a grow copies every column held so far and briefly holds old and new blocks
+        cap = max(need, self.cap + self.cap // 2, 16)
         def grow(old):
             new = torch.empty((self.nov, cap), dtype=torch.float64, device=self.device)
             if old is not None and self.l > 0:
@@ -140,6 +141,18 @@ class Basis:
 
     def prod(self, i):
         return self.P[i][:, :self.l]
+
+
+def initial_capacity(nov, nprod, lmin, lmax, device, fraction=0.35):
+    """Columns to reserve for an expansion space: every column it can reach (lmax) if that fits in
+    `fraction` of the memory the device has left (free plus the allocator's unused cache), else as many as
+    do, but at least lmin.  Reserving up front avoids growing (copying) blocks of many GB mid-solve."""
+    if device.type != "cuda":
+        return max(lmin, min(lmax, 64))
+    free, _ = torch.cuda.mem_get_info(device)
+    free += torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
+    fit = int(fraction * free // (8 * nov * (1 + nprod)))
+    return max(lmin, min(lmax, fit))
 
 
 def _residuals(AV, X, lam):
@@ -244,6 +257,24 @@ def _sqrtm_spd(M):
     return (V * torch.sqrt(lam)) @ V.T
 
 
+def _ssf_cholesky(Mp, Mm):
+    """Ritz pairs of the projected SSF problem through the Cholesky factor Mm = L L^T: (A-B)(A+B) is similar
+    to L^T (A+B) L, so its eigenpairs (w^2, T') give R = L T' / sqrt(w) and L_vec = (A+B) R / w -- the pairs
+    of the (A-B)^1/2 (A+B) (A-B)^1/2 form (Solver.py:757-798) with one Cholesky factorisation in place of a
+    second eigendecomposition.  Returns (w, Rb, Lb, Lc, T', asym) or None when Mm is not positive definite;
+    asym = sum |Mh - Mh^T| is DFTBaby's hermiticity check of the transformed matrix."""
+    Lc, info = torch.linalg.cholesky_ex(0.5 * (Mm + Mm.T))
+    if int(info.item()) != 0:
+        return None
+    Mh = Lc.T @ Mp @ Lc
+    asym = torch.sum(torch.abs(Mh - Mh.T)).item()
+    w2, Tp = torch.linalg.eigh(0.5 * (Mh + Mh.T))
+    w = torch.sqrt(w2)
+    Rb = (Lc @ Tp) / torch.sqrt(w)
+    Lb = (Mp @ Rb) / w
+    return w, Rb, Lb, Lc, Tp, asym
+
+
 def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxiter=10, XmYguess=None,
                           XpYguess=None, w_guess=None, stats=None, symmetrize=False, accept_guess=False,
                           Cguess=None, guess_key=None, precond_diag=None, ritz_on_guess=False,
@@ -286,9 +317,11 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
         lmax = lmaxp + lmaxm
         cols = torch.cat([XmYguess.reshape(nstates, -1), XpYguess.reshape(nstates, -1)[:lmaxm]], dim=0).T
         bs = orthonormal_columns(cols / torch.linalg.norm(cols, dim=0)).contiguous()
-    B = Basis(om.numel(), 2, dev, capacity=lmax + 8 * k, mirror=not symmetrize)
+    cap = initial_capacity(om.numel(), 2, lmax + 8 * k, min(kmax, lmax + maxiter * 2 * k), dev)
+    B = Basis(om.numel(), 2, dev, capacity=cap, mirror=not symmetrize)
     B.append(bs, list(products(bs)))
     l = lmax
+    chol = None  # (Mm, L, T') of the last Cholesky-form Ritz step, for the C vectors
     for it in range(maxiter):
         bs, AP, AM = B.bs, B.prod(0), B.prod(1)
         if XpYguess is None or it > 0 or ritz_on_guess:
@@ -297,14 +330,21 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
             if symmetrize:
                 Mp = 0.5 * (Mp + Mp.T)
                 Mm = 0.5 * (Mm + Mm.T)
-            Mmsq = _sqrtm_spd(Mm)
-            Mh = Mmsq @ Mp @ Mmsq
-            if torch.sum(torch.abs(Mh - Mh.T)).item() > 1.0e-10:
+            ritz = _ssf_cholesky(Mp, Mm)
+            if ritz is not None:
+                w, Rb, Lb, Lc, Tp, asym = ritz
+                chol, Tb = (Mm, Lc, Tp), None
+            else:
+                Mmsq = _sqrtm_spd(Mm)
+                Mh = Mmsq @ Mp @ Mmsq
+                asym = torch.sum(torch.abs(Mh - Mh.T)).item()
+                w2, Tb = torch.linalg.eigh(Mh)
+                w = torch.sqrt(w2)
+                Rb = (Mmsq @ Tb) / torch.sqrt(w)
+                Lb = (Mp @ Rb) / w
+                chol = None
+            if asym > 1.0e-10:
                 raise ExcitedStatesError("Mh is not hermitian!")
-            w2, Tb = torch.linalg.eigh(Mh)
-            w = torch.sqrt(w2)
-            Rb = (Mmsq @ Tb) / torch.sqrt(w)
-            Lb = (Mp @ Rb) / w
             err = torch.sum(torch.abs(Lb.T @ Rb - torch.eye(len(w), dtype=torch.float64, device=dev))).item()
             if err > 1.0e-3:
                 raise ExcitedStatesError("(X+Y) and (X-Y) vectors not orthonormal! error = %s" % err)
@@ -367,6 +407,11 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
             raise ExcitedStatesError("a guess was accepted without its C vectors")
         C = Cguess.reshape(k, -1).T
     else:
+        if Tb is None:
+            # eigenvectors of the (A-B)^1/2 (A+B) (A-B)^1/2 form, DFTBaby's C: Tb = (Mm)^-1/2 L T'
+            Mm_last, Lc, Tp = chol
+            lam, U = torch.linalg.eigh(0.5 * (Mm_last + Mm_last.T))
+            Tb = (U / torch.sqrt(lam)) @ (U.T @ (Lc @ Tp[:, :k]))
         C = bs @ Tb[:, :k]
     shape = (k, nocc, nvirt)
     out = (Omega, C.T.reshape(shape), Lk.T.reshape(shape), Rk.T.reshape(shape))
