@@ -381,7 +381,7 @@ class LR_TDDFTB:
                     response_method="Casida", multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5,
                     diag_maxiter=50, diag_check=0, diag_L2threshold=0.0, diag_selected_irreps=None,
                     ct_correction=0, stability=0, precision="fp64", refine_fp64=True, refine_iterations=None,
-                    guess_model=None, **scf_opts):
+                    guess_model=None, mixed_coulomb=False, mixed_conv=None, **scf_opts):
         """LR_TDDFTB.getEnergies (LR_TDDFTB.py:37-114); returns (Omega, f) in Hartree.
 
         precision="mixed" (not in DFTBaby) evaluates the long-range exchange of
@@ -393,6 +393,13 @@ class LR_TDDFTB:
         with FP64 products of the current Ritz vectors (solver.refine_fp64,
         2 nstates FP64 product columns per round); the exact FP64 residual of
         the vectors entering each round is in stats["refine_residuals"].
+        mixed_conv (not in DFTBaby): residual threshold of the reduced-precision
+        stage when FP64 refinement rounds follow (default diag_conv); the
+        refined result's accuracy is set by the reduced-precision operator's
+        error more than by this threshold.
+        mixed_coulomb (not in DFTBaby): with precision="mixed", the Coulomb term of the
+        reduced-precision products on the tensor cores too (its error is corrected
+        with the exchange's by the FP64 refinement rounds).
         guess_model (not in DFTBaby): a learned.GuessNet whose pair scores choose
         the initial Davidson vectors and whose shifts correct the diagonal
         preconditioner when no warm start is available; the solve runs to the
@@ -427,7 +434,8 @@ class LR_TDDFTB:
         self._solve_lr_equations(multiplicity=multiplicity, nstates=nstates, diag_ifact=diag_ifact,
                                  diag_conv=diag_conv, diag_maxiter=diag_maxiter, diag_check=diag_check,
                                  diag_L2threshold=diag_L2threshold, precision=precision, refine_fp64=refine_fp64,
-                                 refine_iterations=refine_iterations, guess_model=guess_model)
+                                 refine_iterations=refine_iterations, guess_model=guess_model,
+                                 mixed_coulomb=mixed_coulomb, mixed_conv=mixed_conv)
         ev[2].record()
         verbose = getattr(d, "verbose", 0) > 0
         if oszis == "Dipoles":
@@ -464,7 +472,7 @@ class LR_TDDFTB:
 
     def _solve_lr_equations(self, multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5, diag_maxiter=50,
                             diag_check=0, diag_L2threshold=0.0, precision="fp64", refine_fp64=True,
-                            refine_iterations=None, guess_model=None):
+                            refine_iterations=None, guess_model=None, mixed_coulomb=False, mixed_conv=None):
         """LR_TDDFTB._solve_lr_equations (LR_TDDFTB.py:403-527)."""
         d = self.dftb2
         dev = d.device
@@ -545,10 +553,12 @@ class LR_TDDFTB:
             if precision == "mixed":
                 from . import tcgemm
                 mixed = ExchangeMixed(d.gamma, d.G_lr, self.qtrans_ov, self.omega.reshape(-1), Co, Cv, d.S,
-                                      len(d.atomlist), self.nocc, self.nvirt, d.workspace, lc=1)
+                                      len(d.atomlist), self.nocc, self.nvirt, d.workspace, lc=1,
+                                      coulomb_on_tensor_cores=mixed_coulomb)
                 mstats = {}
                 keep_basis = refine_fp64 and refine_iterations is not None
-                res = nonhermitian_davidson(mixed, self.omega, nstates, ifact=diag_ifact, conv=diag_conv,
+                mconv = mixed_conv if (keep_basis and mixed_conv is not None) else diag_conv
+                res = nonhermitian_davidson(mixed, self.omega, nstates, ifact=diag_ifact, conv=mconv,
                                             maxiter=diag_maxiter, stats=mstats, symmetrize=True,
                                             return_basis=keep_basis, **guesses(learned))
                 Om, C, XmY, XpY = res[:4]

@@ -108,8 +108,10 @@ class Basis:
             if old is not None and self.l > 0:
                 new[:, :self.l] = old[:, :self.l]
             return new
+        # one block at a time: each old block is released before the next new one is allocated
         self.V = grow(self.V)
-        self.P = [grow(p) for p in self.P]
+        for i in range(self.nprod):
+            self.P[i] = grow(self.P[i])
         self.cap = cap
 
     def append(self, Q, prods):
