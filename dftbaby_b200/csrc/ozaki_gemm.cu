@@ -46,21 +46,24 @@ constexpr int SCALE_NONFINITE = -(1 << 20);  // row/column exponent marking an I
 
 struct Tables {
     int p[MAXMOD];
-    float invpf[MAXMOD];
     double invp[MAXMOD];
     int D[MAXMOD][MAXMOD];  // D[j][i] = (p_0 ... p_{i-1}) mod p_j, i < j
     int Binv[MAXMOD];       // (p_0 ... p_{j-1})^-1 mod p_j
+    uint32_t mb[MAXMOD];    // Barrett multiplier floor(2^32 / p) + 1
+    int bias[MAXMOD];       // p 2^20, a multiple of p above 2^27
+    double q3[MAXMOD / 3 + 1];  // p_3k p_3k+1 p_3k+2, the radix of digit triple k
+    int c18[MAXMOD], c36[MAXMOD];  // 2^18 and 2^36 modulo p
 };
 
-// symmetric residue of an integer-valued t (|t| < 2^27) modulo p: range [-(p/2), (p-1)/2]
-__device__ __forceinline__ int symmod_i(int t, int p, float invpf) {
-    const int q = __float2int_rn(__int2float_rn(t) * invpf);
-    int r = t - q * p;
-    const int lo = -(p >> 1), hi = (p - 1) >> 1;
-    if (r > hi) r -= p;
-    if (r > hi) r -= p;
-    if (r < lo) r += p;
-    if (r < lo) r += p;
+// symmetric residue of t (|t| < 2^27) modulo p without float conversions: u = t + p 2^20 is in
+// [0, 2^29), floor(u mb / 2^32) is floor(u / p) or one more (the multiplier's excess over 2^32 / p is
+// below 1, so u mb / 2^32 exceeds u / p by less than 1/8), and the remainder is corrected once.
+__device__ __forceinline__ int symmod_b(int t, int p, uint32_t mb, int bias) {
+    const uint32_t u = (uint32_t)(t + bias);
+    const uint32_t q = __umulhi(u, mb);
+    int r = (int)(u - q * (uint32_t)p);
+    if (r < 0) r += p;
+    if (r > ((p - 1) >> 1)) r -= p;
     return r;
 }
 
@@ -78,7 +81,15 @@ __global__ void ozaki_rowscale_kernel(int rows, int rpad, int K, const double *X
         bool bad = false;
         if (warp < rows) {
             const double *x = X + (long long)warp * ldx;
-            for (int k = lane; k < K; k += 32) {
+            int k = lane;
+            for (; k + 96 < K; k += 128) {
+                // four independent loads in flight per lane
+                const double a0 = fabs(x[k]), a1 = fabs(x[k + 32]), a2 = fabs(x[k + 64]), a3 = fabs(x[k + 96]);
+                bad |= !(a0 <= 1.7976931348623157e308 && a1 <= 1.7976931348623157e308 &&
+                         a2 <= 1.7976931348623157e308 && a3 <= 1.7976931348623157e308);
+                m = fmax(fmax(m, fmax(a0, a1)), fmax(a2, a3));
+            }
+            for (; k < K; k += 32) {
                 const double a = fabs(x[k]);
                 bad |= !(a <= 1.7976931348623157e308);
                 m = fmax(m, a);
@@ -121,9 +132,9 @@ constexpr int RT_ROWS = 32, RT_K = 128;
 // Residue planes R[i][r][k] (i < nmod, r < rows_write, k < kpad; zero outside rows x K) of the scaled,
 // rounded Y(r, k) 2^s[r].  One block per 32 x 128 tile of Y, staged through shared memory so that both the
 // FP64 reads (along k, or along r when transposed) and the int8 writes (4 consecutive k per thread) coalesce.
+template <int NM>
 __global__ void __launch_bounds__(256) ozaki_residue_kernel(int rows, int rows_write, int K, const double *X,
-                                                            long long ldx, int trans,
-                                                            const int *s, int nmod,
+                                                            long long ldx, int trans, const int *s,
                                                             const __grid_constant__ Tables tb, int8_t *R,
                                                             long long plane, int kpad) {
     __shared__ double tile[RT_ROWS][RT_K + 1];
@@ -148,22 +159,25 @@ __global__ void __launch_bounds__(256) ozaki_residue_kernel(int rows, int rows_w
         const int r = r0 + rr, k = k0 + kq;
         if (k >= kpad || r >= rows_write) continue;
         const int sr = (r < rows) ? s[r] : 0;
-        double a[4];
+        // the scaled, rounded entries (at most 53 bits) as h 2^36 + m 2^18 + l, |h| <= 2^17, 0 <= m, l < 2^18
+        int h[4], md[4], l[4];
 #pragma unroll
-        for (int e = 0; e < 4; ++e)
-            a[e] = (sr == SCALE_NONFINITE || r >= rows) ? 0.0 : rint(ldexp(tile[rr][kq + e], sr));
-        for (int i = 0; i < nmod; ++i) {
-            const double p = (double)tb.p[i];
+        for (int e = 0; e < 4; ++e) {
+            const long long ai =
+                (sr == SCALE_NONFINITE || r >= rows) ? 0ll : __double2ll_rn(ldexp(tile[rr][kq + e], sr));
+            h[e] = (int)(ai >> 36);
+            md[e] = (int)((ai >> 18) & 0x3FFFF);
+            l[e] = (int)(ai & 0x3FFFF);
+        }
+#pragma unroll
+        for (int i = 0; i < NM; ++i) {
             uint32_t w = 0;
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-                // a is an integer of at most 53 bits: q within one of round(a / p), fma exact
-                const double q = rint(a[e] * tb.invp[i]);
-                double rd = fma(-q, p, a[e]);
-                const double lo = -(double)(tb.p[i] >> 1), hi = (double)((tb.p[i] - 1) >> 1);
-                if (rd > hi) rd -= p;
-                if (rd < lo) rd += p;
-                w |= ((uint32_t)(uint8_t)(int8_t)(int)rd) << (8 * e);
+                // |h c36 + m c18 + l| < 2^25 + 2^26 + 2^18 < 2^27
+                const int t = h[e] * tb.c36[i] + md[e] * tb.c18[i] + l[e];
+                const int rd = symmod_b(t, tb.p[i], tb.mb[i], tb.bias[i]);
+                w |= ((uint32_t)(uint8_t)(int8_t)rd) << (8 * e);
             }
             *reinterpret_cast<uint32_t *>(R + i * plane + (long long)r * kpad + k) = w;
         }
@@ -409,11 +423,21 @@ __global__ void __launch_bounds__(256) ozaki_crt_kernel(int M, int N, const int8
             int acc = (int)(int8_t)(uint8_t)(wd[jj] >> (8 * e));
 #pragma unroll
             for (int i = 0; i < jj; ++i) acc -= v[i] * tb.D[jj][i];
-            v[jj] = symmod_i(acc * tb.Binv[jj], tb.p[jj], tb.invpf[jj]);
+            v[jj] = symmod_b(acc * tb.Binv[jj], tb.p[jj], tb.mb[jj], tb.bias[jj]);
         }
-        double x = (double)v[NM - 1];
+        // Horner over digit triples: each triple v_a + p_a (v_b + p_b v_c) is an exact int32 (< 2^24)
+        constexpr int NG = (NM + 2) / 3;
+        double x = 0.0;
 #pragma unroll
-        for (int jj = NM - 2; jj >= 0; --jj) x = fma(x, (double)tb.p[jj], (double)v[jj]);
+        for (int g = NG - 1; g >= 0; --g) {
+            const int a = 3 * g;
+            int t = v[a];
+            if (a + 2 < NM)
+                t += tb.p[a] * (v[a + 1] + tb.p[a + 1] * v[a + 2]);
+            else if (a + 1 < NM)
+                t += tb.p[a] * v[a + 1];
+            x = (g == NG - 1) ? (double)t : fma(x, tb.q3[g], (double)t);
+        }
         const int sn = sb[n];
         double out;
         if (sm == SCALE_NONFINITE || sn == SCALE_NONFINITE)
@@ -459,7 +483,6 @@ int init_host() {
         Tables &t = g_tables;
         for (int i = 0; i < MAXMOD; ++i) {
             t.p[i] = kModuli[i];
-            t.invpf[i] = 1.0f / (float)kModuli[i];
             t.invp[i] = 1.0 / (double)kModuli[i];
         }
         for (int j = 0; j < MAXMOD; ++j) {
@@ -477,6 +500,15 @@ int init_host() {
                     break;
                 }
             t.Binv[j] = (j == 0) ? 1 : inv;
+            t.mb[j] = (uint32_t)((1ull << 32) / (unsigned long long)pj + 1ull);
+            t.bias[j] = pj << 20;
+            t.c18[j] = (int)((1ull << 18) % (unsigned long long)pj);
+            t.c36[j] = (int)((1ull << 36) % (unsigned long long)pj);
+        }
+        for (int g = 0; 3 * g < MAXMOD; ++g) {
+            double q = 1.0;
+            for (int i = 3 * g; i < 3 * g + 3 && i < MAXMOD; ++i) q *= (double)kModuli[i];
+            t.q3[g] = q;
         }
         g_tables_ready = true;
     }
@@ -560,8 +592,23 @@ int prepare(int trans, int rows, int k, const double *X, long long ldx, int nmod
                                                                                         1, bits, s);
     }
     dim3 g((unsigned)(L.kpad / RT_K), (unsigned)((rows_write + RT_ROWS - 1) / RT_ROWS));
-    ozaki_residue_kernel<<<g, 256, 0, st>>>(rows, rows_write, k, X, ldx, trans, s, nmod, g_tables, R, L.plane,
-                                            (int)L.kpad);
+    switch (nmod) {
+#define OZK_RES(NMV)                                                                                            \
+    case NMV:                                                                                                   \
+        ozaki_residue_kernel<NMV><<<g, 256, 0, st>>>(rows, rows_write, k, X, ldx, trans, s, g_tables, R, L.plane, \
+                                                     (int)L.kpad);                                              \
+        break;
+        OZK_RES(8)
+        OZK_RES(9)
+        OZK_RES(10)
+        OZK_RES(11)
+        OZK_RES(12)
+        OZK_RES(13)
+        OZK_RES(14)
+        OZK_RES(15)
+        OZK_RES(16)
+#undef OZK_RES
+    }
     return cudaGetLastError() == cudaSuccess ? DFTB_OK : DFTB_ERR_CUDA;
 }
 
