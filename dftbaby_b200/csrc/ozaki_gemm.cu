@@ -101,14 +101,14 @@ __global__ void ozaki_rowscale_kernel(int rows, int rpad, int K, const double *X
         }
         if (lane == 0) s[warp] = bad ? SCALE_NONFINITE : (m > 0.0 ? bits - 1 - ilogb(m) : 0);
     } else {
-        // 32 rows per block (threadIdx.x, consecutive in memory), 8 phases of k (threadIdx.y)
-        __shared__ double sm[8][32];
-        __shared__ int sbad[8][32];
+        // 32 rows per block (threadIdx.x, consecutive in memory), 32 phases of k (threadIdx.y)
+        __shared__ double sm[32][32];
+        __shared__ int sbad[32][32];
         const int r = blockIdx.x * 32 + threadIdx.x;
         double m = 0.0;
         int bad = 0;
         if (r < rows) {
-            for (int k = threadIdx.y; k < K; k += 8) {
+            for (int k = threadIdx.y; k < K; k += 32) {
                 const double a = fabs(X[(long long)k * ldx + r]);
                 bad |= !(a <= 1.7976931348623157e308);
                 m = fmax(m, a);
@@ -118,7 +118,7 @@ __global__ void ozaki_rowscale_kernel(int rows, int rpad, int K, const double *X
         sbad[threadIdx.y][threadIdx.x] = bad;
         __syncthreads();
         if (threadIdx.y == 0 && r < rpad) {
-            for (int y = 1; y < 8; ++y) {
+            for (int y = 1; y < 32; ++y) {
                 m = fmax(m, sm[y][threadIdx.x]);
                 bad |= sbad[y][threadIdx.x];
             }
@@ -588,8 +588,8 @@ int prepare(int trans, int rows, int k, const double *X, long long ldx, int nmod
         ozaki_rowscale_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(rows, rows_write, k, X, ldx, 0, bits,
                                                                                  s);
     } else {
-        ozaki_rowscale_kernel<<<(unsigned)((rows_write + 31) / 32), dim3(32, 8), 0, st>>>(rows, rows_write, k, X, ldx,
-                                                                                        1, bits, s);
+        ozaki_rowscale_kernel<<<(unsigned)((rows_write + 31) / 32), dim3(32, 32), 0, st>>>(rows, rows_write, k, X, ldx,
+                                                                                         1, bits, s);
     }
     dim3 g((unsigned)(L.kpad / RT_K), (unsigned)((rows_write + RT_ROWS - 1) / RT_ROWS));
     switch (nmod) {
