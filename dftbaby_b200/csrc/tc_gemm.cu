@@ -42,7 +42,6 @@ namespace tcg {
 using namespace tc5;
 
 constexpr int BM = 128, BN = 128, BK = 64;
-constexpr int TILE_A_BYTES = BM * BK * 2;  // 16 KiB
 // segment mode: one (A, B) tile pair per stage, 4 stages;
 // shared-split mode: A_hi, A_lo, B_hi, B_lo per stage (three MMAs reuse them), 3 stages
 // Row-chunk moves of the epilogue: 16 consecutive elements of one row, as 16- or 8-byte words
@@ -119,13 +118,17 @@ constexpr int EPI_THREADS = 128;
 constexpr int TPITCH = 40;
 constexpr int TSTAGE_BYTES = 4 * 2 * 32 * TPITCH * 2;
 
-template <bool SPLIT> struct Cfg {
-    // 128 x 128 output tiles in both modes (128 x 256 tiles with two stages measured slower in the
-    // solver: the mainloop is bound by copy latency, not by operand bytes)
-    static constexpr int BNX = 128;
-    static constexpr int TILE_BX = BNX * BK * 2;
-    static constexpr int STAGES = SPLIT ? 3 : 4;
-    static constexpr int STAGE_BYTES = SPLIT ? 2 * (TILE_A_BYTES + TILE_BX) : TILE_A_BYTES + TILE_BX;
+template <bool SPLIT, bool WIDE = false> struct Cfg {
+    // 128 x 128 output tiles with 64-element K blocks (128-byte swizzle); WIDE (split mode only): 128 x 256
+    // tiles with 32-element K blocks (64-byte swizzle), so four stages of A_hi, A_lo, B_hi, B_lo fit and a
+    // stage carries the same MMA work with a quarter fewer operand bytes.  (128 x 256 tiles with 64-element
+    // blocks leave room for two stages only, which measured slower.)
+    static constexpr int BNX = WIDE ? 256 : 128;
+    static constexpr int BKX = WIDE ? 32 : BK;
+    static constexpr int TILE_AX = BM * BKX * 2;
+    static constexpr int TILE_BX = BNX * BKX * 2;
+    static constexpr int STAGES = WIDE ? 4 : (SPLIT ? 3 : 4);
+    static constexpr int STAGE_BYTES = SPLIT ? 2 * (TILE_AX + TILE_BX) : TILE_AX + TILE_BX;
     static constexpr int SMEM_BYTES =
         STAGES * STAGE_BYTES + TSTAGE_BYTES + 1024 /* alignment slack */ + 256 /* barriers */;
     static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BNX >> 3) << 17) |
@@ -151,6 +154,22 @@ struct Params {
     long long ldt;
     int *err;  // device error word (0 = ok)
 };
+
+// UMMA shared-memory descriptor for K-major rows of 64 B with 64-byte swizzle: 8-row groups 512 B apart
+__device__ __forceinline__ uint64_t smem_desc_k64(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFF) >> 4);  // start address
+    d |= (uint64_t)1 << 16;                    // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(512 >> 4) << 32;           // stride byte offset
+    d |= (uint64_t)1 << 46;                    // descriptor version
+    d |= (uint64_t)4 << 61;                    // SWIZZLE_64B
+    return d;
+}
+
+template <bool WIDE>
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+    return WIDE ? smem_desc_k64(saddr) : smem_desc_k128(saddr);
+}
 
 // instruction descriptor: D = F32, A = B = BF16, both K-major, M = 128, N = 128
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
@@ -209,12 +228,13 @@ __device__ __forceinline__ TileCoords tile_coords(int t, int mt, int nt, int bnx
 //                   lanes 32 (w % 4) .. 32 (w % 4) + 31.
 // Barriers: full/empty per ring slot, tfull (MMA -> epilogue, tcgen05.commit) and tempty
 // (epilogue -> MMA, 128 arrivals) per accumulator.  Every wait is bounded.
-template <bool SPLIT>
+template <bool SPLIT, bool WIDE>
 __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Maps maps, const Params p) {
-    constexpr int STAGES = Cfg<SPLIT>::STAGES, STAGE_BYTES = Cfg<SPLIT>::STAGE_BYTES;
-    constexpr int BNX = Cfg<SPLIT>::BNX, TILE_BX = Cfg<SPLIT>::TILE_BX;
-    constexpr uint32_t IDESC = Cfg<SPLIT>::IDESC;
-    static_assert(BNX == 128, "epilogue assumes 128 tile columns");
+    using C = Cfg<SPLIT, WIDE>;
+    constexpr int STAGES = C::STAGES, STAGE_BYTES = C::STAGE_BYTES;
+    constexpr int BNX = C::BNX, TILE_BX = C::TILE_BX, TILE_AX = C::TILE_AX, BKX = C::BKX;
+    constexpr uint32_t IDESC = C::IDESC;
+    static_assert(BNX % 32 == 0 && (!WIDE || SPLIT), "tile columns come in 32-column chunks; WIDE is split-only");
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     __nv_bfloat16 *tstage = reinterpret_cast<__nv_bfloat16 *>(smem + STAGES * STAGE_BYTES);
@@ -228,7 +248,7 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ma
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int mt = (p.M + BM - 1) / BM, nt = (p.N + BNX - 1) / BNX;
     const int ntiles = mt * nt * p.ksplit;
-    const int kblocks_all = (p.K + BK - 1) / BK;
+    const int kblocks_all = (p.K + BKX - 1) / BKX;
     const int kper = (kblocks_all + p.ksplit - 1) / p.ksplit;
 
     if (threadIdx.x == 0) {
@@ -279,15 +299,15 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ma
                     mbar_expect_tx(&full[s], STAGE_BYTES);
                     if (SPLIT) {
                         // stage layout: A_hi | A_lo | B_hi | B_lo
-                        const int kx = (tc.kb0 + i) * BK;
+                        const int kx = (tc.kb0 + i) * BKX;
                         tma_load_2d(sa, &maps.a[0], &full[s], kx, tc.m0);
-                        tma_load_2d(sa + TILE_A_BYTES, &maps.a[1], &full[s], kx, tc.m0);
-                        tma_load_2d(sa + 2 * TILE_A_BYTES, &maps.b[0], &full[s], kx, tc.n0);
-                        tma_load_2d(sa + 2 * TILE_A_BYTES + TILE_BX, &maps.b[1], &full[s], kx, tc.n0);
+                        tma_load_2d(sa + TILE_AX, &maps.a[1], &full[s], kx, tc.m0);
+                        tma_load_2d(sa + 2 * TILE_AX, &maps.b[0], &full[s], kx, tc.n0);
+                        tma_load_2d(sa + 2 * TILE_AX + TILE_BX, &maps.b[1], &full[s], kx, tc.n0);
                     } else {
                         const int seg = i / tc.kblocks, kb = tc.kb0 + i % tc.kblocks;
-                        tma_load_2d(sa, &maps.a[seg], &full[s], kb * BK, tc.m0);
-                        tma_load_2d(sa + TILE_A_BYTES, &maps.b[seg], &full[s], kb * BK, tc.n0);
+                        tma_load_2d(sa, &maps.a[seg], &full[s], kb * BKX, tc.m0);
+                        tma_load_2d(sa + TILE_AX, &maps.b[seg], &full[s], kb * BKX, tc.n0);
                     }
                     ++it;
                 }
@@ -326,19 +346,20 @@ __global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ Ma
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
                     if (SPLIT) {
-                        const uint32_t sal = sa + TILE_A_BYTES, sb = sa + 2 * TILE_A_BYTES, sbl = sb + TILE_BX;
+                        const uint32_t sal = sa + TILE_AX, sb = sa + 2 * TILE_AX, sbl = sb + TILE_BX;
 #pragma unroll
-                        for (int k = 0; k < BK / 16; ++k) {
+                        for (int k = 0; k < BKX / 16; ++k) {
+                            // 16 BF16 = 32 bytes along K per instruction, inside the swizzle atom
                             const uint32_t o = k * 32;
-                            umma_bf16(tacc, smem_desc_k128(sa + o), smem_desc_k128(sb + o),
+                            umma_bf16(tacc, smem_desc<WIDE>(sa + o), smem_desc<WIDE>(sb + o),
                                       (i > 0 || k > 0) ? 1u : 0u, IDESC);
-                            umma_bf16(tacc, smem_desc_k128(sa + o), smem_desc_k128(sbl + o), 1u, IDESC);
-                            umma_bf16(tacc, smem_desc_k128(sal + o), smem_desc_k128(sb + o), 1u, IDESC);
+                            umma_bf16(tacc, smem_desc<WIDE>(sa + o), smem_desc<WIDE>(sbl + o), 1u, IDESC);
+                            umma_bf16(tacc, smem_desc<WIDE>(sal + o), smem_desc<WIDE>(sb + o), 1u, IDESC);
                         }
                     } else {
-                        const uint32_t sb = sa + TILE_A_BYTES;
+                        const uint32_t sb = sa + TILE_AX;
 #pragma unroll
-                        for (int k = 0; k < BK / 16; ++k) {
+                        for (int k = 0; k < BKX / 16; ++k) {
                             // advance 16 BF16 = 32 bytes along K inside the 128-byte swizzle atom
                             umma_bf16(tacc, smem_desc_k128(sa + k * 32), smem_desc_k128(sb + k * 32),
                                       (i > 0 || k > 0) ? 1u : 0u);
@@ -521,14 +542,17 @@ int get_encode() {
     return 0;
 }
 
-int make_map(CUtensorMap *map, const void *base, int rows, int cols, long long ld, int box_rows = BM) {
-    // 2D BF16 tensor: innermost dimension = columns (K), box 64 x box_rows, 128-byte swizzle, zero fill
+int make_map(CUtensorMap *map, const void *base, int rows, int cols, long long ld, int box_rows = BM,
+             int box_cols = BK) {
+    // 2D BF16 tensor: innermost dimension = columns (K), box box_cols x box_rows, zero fill; rows of 64
+    // elements (128 B) use the 128-byte swizzle, rows of 32 elements the 64-byte swizzle
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
-    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
+    const CUtensorMapSwizzle sw = box_cols == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
     CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         snprintf(g_err, sizeof(g_err), "cuTensorMapEncodeTiled failed (%d): rows %d cols %d ld %lld", (int)r, rows,
@@ -560,8 +584,9 @@ int dftb_bf16x3_gemm_ex(int M, int N, int K, int nseg, int shared_split, int ksp
                         void *Ohi, void *Olo, int ldo, void *Thi, void *Tlo, int ldt, int *err, void *stream) {
     using namespace tcg;
     if (M <= 0 || N <= 0 || K <= 0 || nseg < 1 || nseg > 3 || ksplit < 1 || ksplit > 64) return DFTB_ERR_BAD_SIZE;
-    if (shared_split && nseg != 2) {
-        snprintf(g_err, sizeof(g_err), "bf16x3_gemm: shared-split mode takes the pairs (A_hi, A_lo), (B_hi, B_lo)");
+    if (shared_split < 0 || shared_split > 2 || (shared_split && nseg != 2)) {
+        snprintf(g_err, sizeof(g_err), "bf16x3_gemm: shared-split mode (1, or 2 for 128 x 256 tiles) takes the pairs "
+                 "(A_hi, A_lo), (B_hi, B_lo)");
         return DFTB_ERR_BAD_SIZE;
     }
     if (ksplit > 1 && (!C || G || Ohi || Thi)) {
@@ -584,8 +609,10 @@ int dftb_bf16x3_gemm_ex(int M, int N, int K, int nseg, int shared_split, int ksp
             snprintf(g_err, sizeof(g_err), "bf16x3_gemm: operands must be 16-byte aligned");
             return DFTB_ERR_BAD_SIZE;
         }
-        if (make_map(&maps.a[s], A[s], M, K, lda) ||
-            make_map(&maps.b[s], B[s], N, K, ldb, shared_split ? Cfg<true>::BNX : Cfg<false>::BNX))
+        const bool wide = shared_split == 2;
+        const int bkx = wide ? Cfg<true, true>::BKX : BK;
+        const int bnx = wide ? Cfg<true, true>::BNX : (shared_split ? Cfg<true>::BNX : Cfg<false>::BNX);
+        if (make_map(&maps.a[s], A[s], M, K, lda, BM, bkx) || make_map(&maps.b[s], B[s], N, K, ldb, bnx, bkx))
             return DFTB_ERR_CUDA;
     }
     Params p;
@@ -606,23 +633,24 @@ int dftb_bf16x3_gemm_ex(int M, int N, int K, int nseg, int shared_split, int ksp
     p.Tlo = reinterpret_cast<__nv_bfloat16 *>(Tlo);
     p.ldt = ldt;
     p.err = err;
-    static bool attr_set[2][64] = {{false}};
+    static bool attr_set[3][64] = {{false}};
     int dev = 0;
     cudaGetDevice(&dev);
-    const int mode = shared_split ? 1 : 0;
-    const int smem = shared_split ? Cfg<true>::SMEM_BYTES : Cfg<false>::SMEM_BYTES;
+    const int mode = shared_split;  // 0 segments, 1 split, 2 split with 128 x 256 tiles
+    const int smem = mode == 2 ? Cfg<true, true>::SMEM_BYTES : (mode ? Cfg<true>::SMEM_BYTES : Cfg<false>::SMEM_BYTES);
     if (dev >= 0 && dev < 64 && !attr_set[mode][dev]) {
-        cudaError_t e = shared_split ? cudaFuncSetAttribute(gemm_kernel<true>,
-                                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
-                                     : cudaFuncSetAttribute(gemm_kernel<false>,
-                                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaError_t e =
+            mode == 2 ? cudaFuncSetAttribute(gemm_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+            : mode    ? cudaFuncSetAttribute(gemm_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+                      : cudaFuncSetAttribute(gemm_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             smem);
         if (e != cudaSuccess) {
             snprintf(g_err, sizeof(g_err), "bf16x3_gemm: cannot reserve %d bytes of shared memory", smem);
             return DFTB_ERR_CUDA;
         }
         attr_set[mode][dev] = true;
     }
-    const int bnx = shared_split ? Cfg<true>::BNX : Cfg<false>::BNX;
+    const int bnx = mode == 2 ? Cfg<true, true>::BNX : (mode ? Cfg<true>::BNX : Cfg<false>::BNX);
     // persistent launch: one CTA per SM (the shared-memory footprint admits one), each walking tiles
     const long long ntiles = (long long)((M + BM - 1) / BM) * ((N + bnx - 1) / bnx) * ksplit;
     if (ntiles > (1LL << 30)) return DFTB_ERR_BAD_SIZE;
@@ -634,10 +662,13 @@ int dftb_bf16x3_gemm_ex(int M, int N, int K, int nseg, int shared_split, int ksp
     }
     const int sms = (dev >= 0 && dev < 64) ? sm_count[dev] : 148;
     dim3 grid((unsigned)(ntiles < sms ? ntiles : sms));
-    if (shared_split)
-        gemm_kernel<true><<<grid, 192, smem, reinterpret_cast<cudaStream_t>(stream)>>>(maps, p);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (mode == 2)
+        gemm_kernel<true, true><<<grid, 192, smem, st>>>(maps, p);
+    else if (mode == 1)
+        gemm_kernel<true, false><<<grid, 192, smem, st>>>(maps, p);
     else
-        gemm_kernel<false><<<grid, 192, smem, reinterpret_cast<cudaStream_t>(stream)>>>(maps, p);
+        gemm_kernel<false, false><<<grid, 192, smem, st>>>(maps, p);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         snprintf(g_err, sizeof(g_err), "gemm_kernel: %s", cudaGetErrorString(e));

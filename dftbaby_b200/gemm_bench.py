@@ -34,6 +34,7 @@ def main():
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--epilogue", choices=["pair", "gpt", "f32"], default="pair")
+    ap.add_argument("--wide", action="store_true", help="split mode on 128 x 256 tiles")
     ap.add_argument("--ozaki", action="store_true")
     ap.add_argument("--nmod", type=int, default=16)
     ap.add_argument("--phases", action="store_true", help="with --ozaki: per-kernel device time (CUPTI)")
@@ -47,10 +48,10 @@ def main():
     B = torch.randn(a.n, a.k, generator=g, dtype=torch.float32).to(dev)
     pa, pb = tcgemm.split(A), tcgemm.split(B)
     C = tcgemm.Pair(a.m, a.n, dev)
-    kw = dict(K=a.k, out_pair=C)
+    kw = dict(K=a.k, out_pair=C, wide=a.wide)
     if a.epilogue == "f32":
         # FP32 output, K split over several CTAs when the output has fewer tiles than SMs
-        kw = dict(K=a.k, alpha=0.25, out=torch.empty((a.m, a.n), dtype=torch.float32, device=dev))
+        kw = dict(K=a.k, alpha=0.25, out=torch.empty((a.m, a.n), dtype=torch.float32, device=dev), wide=a.wide)
     if a.epilogue == "gpt":
         kw.update(G=torch.rand(a.m, a.n, generator=g, dtype=torch.float32).to(dev),
                   out_pair_t=tcgemm.Pair(a.n, a.m, dev))
@@ -69,7 +70,8 @@ def main():
     peak_file = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
     peak = json.load(open(peak_file)).get("bf16_tflops", 1637.5) if os.path.exists(peak_file) else 1590.0
     tf = flops / (ms / 1e3) / 1e12
-    print(json.dumps({"shape": [a.m, a.n, a.k], "epilogue": a.epilogue, "segments": 3, "ms": ms, "tflops": tf, "peak_bf16_tflops": peak,
+    print(json.dumps({"shape": [a.m, a.n, a.k], "epilogue": a.epilogue, "segments": 3, "wide": a.wide, "ms": ms,
+                      "tflops": tf, "peak_bf16_tflops": peak,
                       "frac": tf / peak}))
 
 

@@ -115,7 +115,7 @@ class ExchangeMixed(ExchangeAO):
     """
 
     def __init__(self, gamma, G_lr, q_ov, omega_flat, Co, Cv, S, nat, nocc, nvirt, workspace, lc=1,
-                 coulomb_on_tensor_cores=False):
+                 coulomb_on_tensor_cores=False, segments=3):
         from . import tcgemm as T
         super().__init__(gamma, G_lr, q_ov, omega_flat, Co, Cv, S, nat, nocc, nvirt, workspace, lc=lc,
                          max_bytes=1)
@@ -147,6 +147,8 @@ class ExchangeMixed(ExchangeAO):
         self.K12t = torch.empty((2 * nvirt, nocc), dtype=torch.float32, device=dev)
         self.Vp = T.Pair(nocc, nvirt, dev)
         self.coulomb_on_tensor_cores = coulomb_on_tensor_cores
+        # 3: hi.hi + hi.lo + lo.hi (~2^-16); 1: hi.hi only (BF16, ~2^-8)
+        self.refine = segments == 3
         if coulomb_on_tensor_cores:
             # Coulomb operands: q_ov and its transpose as BF16 hi/lo pairs
             q2 = q_ov.reshape(nat, -1)
@@ -196,14 +198,15 @@ class ExchangeMixed(ExchangeAO):
         K2 = torch.empty_like(V)
         Vt = V.T.contiguous()  # one contiguous (nocc, nvirt) block per column
         for c in range(m):
+            rf = self.refine
             T.split(Vt[c].reshape(no, nv), out=self.Vp)
-            T.gemm(self.YV, self.Vp, K=nv, out_pair=self.W)
+            T.gemm(self.YV, self.Vp, K=nv, out_pair=self.W, refine=rf)
             # N = Gamma o (X_o W^T) for both y at once, stored row-major and transposed
-            T.gemm(self.XO, self.W, K=no, G=self.G4, out_pair=self.NN, out_pair_t=self.NT)
+            T.gemm(self.XO, self.W, K=no, G=self.G4, out_pair=self.NN, out_pair_t=self.NT, refine=rf)
             # [P1 | P2] in one launch (the rows between the halves of NB are zero)
-            T.gemm(self.YbarT, self.NB, K=2 * norb, out_pair=self.P12)
+            T.gemm(self.YbarT, self.NB, K=2 * norb, out_pair=self.P12, refine=rf)
             # K1^T and K2^T interleaved by rows, in one launch
-            T.gemm(self.Pint, self.XbarT, K=2 * norb, alpha=0.25, out=self.K12t)
+            T.gemm(self.Pint, self.XbarT, K=2 * norb, alpha=0.25, out=self.K12t, refine=rf)
             # transpose, widen to FP64 and scatter into column c in one copy each
             K1[:, c].view(no, nv).copy_(self.K12t[0::2].T)
             K2[:, c].view(no, nv).copy_(self.K12t[1::2].T)
@@ -381,7 +384,7 @@ class LR_TDDFTB:
                     response_method="Casida", multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5,
                     diag_maxiter=50, diag_check=0, diag_L2threshold=0.0, diag_selected_irreps=None,
                     ct_correction=0, stability=0, precision="fp64", refine_fp64=True, refine_iterations=None,
-                    guess_model=None, mixed_coulomb=False, mixed_conv=None, **scf_opts):
+                    guess_model=None, mixed_coulomb=False, mixed_conv=None, mixed_segments=3, **scf_opts):
         """LR_TDDFTB.getEnergies (LR_TDDFTB.py:37-114); returns (Omega, f) in Hartree.
 
         precision="mixed" (not in DFTBaby) evaluates the long-range exchange of
@@ -435,7 +438,8 @@ class LR_TDDFTB:
                                  diag_conv=diag_conv, diag_maxiter=diag_maxiter, diag_check=diag_check,
                                  diag_L2threshold=diag_L2threshold, precision=precision, refine_fp64=refine_fp64,
                                  refine_iterations=refine_iterations, guess_model=guess_model,
-                                 mixed_coulomb=mixed_coulomb, mixed_conv=mixed_conv)
+                                 mixed_coulomb=mixed_coulomb, mixed_conv=mixed_conv,
+                                 mixed_segments=mixed_segments)
         ev[2].record()
         verbose = getattr(d, "verbose", 0) > 0
         if oszis == "Dipoles":
@@ -472,7 +476,8 @@ class LR_TDDFTB:
 
     def _solve_lr_equations(self, multiplicity="S", nstates=None, diag_ifact=1, diag_conv=1.0e-5, diag_maxiter=50,
                             diag_check=0, diag_L2threshold=0.0, precision="fp64", refine_fp64=True,
-                            refine_iterations=None, guess_model=None, mixed_coulomb=False, mixed_conv=None):
+                            refine_iterations=None, guess_model=None, mixed_coulomb=False, mixed_conv=None,
+                            mixed_segments=3):
         """LR_TDDFTB._solve_lr_equations (LR_TDDFTB.py:403-527)."""
         d = self.dftb2
         dev = d.device
@@ -554,7 +559,7 @@ class LR_TDDFTB:
                 from . import tcgemm
                 mixed = ExchangeMixed(d.gamma, d.G_lr, self.qtrans_ov, self.omega.reshape(-1), Co, Cv, d.S,
                                       len(d.atomlist), self.nocc, self.nvirt, d.workspace, lc=1,
-                                      coulomb_on_tensor_cores=mixed_coulomb)
+                                      coulomb_on_tensor_cores=mixed_coulomb, segments=mixed_segments)
                 mstats = {}
                 keep_basis = refine_fp64 and refine_iterations is not None
                 mconv = mixed_conv if (keep_basis and mixed_conv is not None) else diag_conv

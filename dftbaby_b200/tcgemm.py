@@ -81,10 +81,13 @@ def _errword(device):
 
 
 SMS = 148
+# split-mode products on 128 x 256 tiles with 32-element K blocks (four stages) instead of 128 x 128 tiles
+# with 64-element blocks (three stages)
+WIDE = True
 
 
 def gemm(A, B, K=None, refine=True, alpha=1.0, G=None, out=None, out_pair=None, out_pair_t=None, segments=None,
-         ksplit=None):
+         ksplit=None, wide=None):
     """alpha * A B^T on the tensor cores.  A, B: Pair (K-major); K defaults to A.cols.
 
     G (FP32, M x N) multiplies the result elementwise; results go to ``out``
@@ -93,12 +96,14 @@ def gemm(A, B, K=None, refine=True, alpha=1.0, G=None, out=None, out_pair=None, 
     K-block and accumulates hi.hi + hi.lo + lo.hi.  ``segments`` overrides the
     operand list with explicit (A_bf16, B_bf16) pairs.  When the output alone
     has too few 128x128 tiles to fill the GPU and only ``out`` is requested,
-    the K range is split over several CTAs that add into ``out``.
+    the K range is split over several CTAs that add into ``out``.  ``wide``
+    (default: the module's WIDE) runs the split mode on 128 x 256 tiles.
     """
     L = _lib()
     M, N = A.rows, B.rows
     K = K or A.cols
     shared = segments is None and refine
+    wide = (WIDE if wide is None else wide) and shared
     if segments is None:
         segments = [(A.hi, B.hi)] + ([(A.hi, B.lo), (A.lo, B.hi)] if refine else [])
     if shared:
@@ -109,7 +114,8 @@ def gemm(A, B, K=None, refine=True, alpha=1.0, G=None, out=None, out_pair=None, 
     Aptrs = (ctypes.c_void_p * 3)(*ptrA + [0] * (3 - nseg))
     Bptrs = (ctypes.c_void_p * 3)(*ptrB + [0] * (3 - nseg))
     lda, ldb = segments[0][0].stride(0), segments[0][1].stride(0)
-    tiles = ((M + 127) // 128) * ((N + 127) // 128)
+    bn = 256 if wide else 128
+    tiles = ((M + 127) // 128) * ((N + bn - 1) // bn)
     if ksplit is None:
         ksplit = 1
         if out is not None and G is None and out_pair is None and out_pair_t is None and tiles < SMS:
@@ -122,7 +128,8 @@ def gemm(A, B, K=None, refine=True, alpha=1.0, G=None, out=None, out_pair=None, 
     if timed:
         ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
         ev[0].record()
-    rc = L.dftb_bf16x3_gemm_ex(M, N, K, nseg, int(shared), int(ksplit), Aptrs, lda, Bptrs, ldb, float(alpha), P(G),
+    mode = (2 if wide else 1) if shared else 0
+    rc = L.dftb_bf16x3_gemm_ex(M, N, K, nseg, mode, int(ksplit), Aptrs, lda, Bptrs, ldb, float(alpha), P(G),
                                G.stride(0) if G is not None
                             else 0, P(out), out.stride(0) if out is not None else 0,
                             P(out_pair.hi) if out_pair else None, P(out_pair.lo) if out_pair else None,

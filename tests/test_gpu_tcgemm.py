@@ -115,3 +115,36 @@ def test_gemm_split_k_with_an_empty_range():
     torch.cuda.synchronize()
     tcgemm.check_errors(dev)
     assert (C.double() - ref).abs().max().item() / ref.abs().max().item() < 5e-5
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 256, 64), (300, 200, 150), (1000, 513, 777), (2000, 1500, 300),
+                                   (1225, 1225, 8292)])
+def test_wide_tiles_match_the_segment_mode(M, N, K):
+    """Split mode on 128 x 256 tiles with 32-element K blocks (64-byte swizzle): FP64 accuracy of the three
+    products, the G epilogue and all three outputs on ragged edges, against the segment mode."""
+    native.load()
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device="cpu").manual_seed(M * 3 + K)
+    A = torch.randn(M, K, generator=g, dtype=torch.float64).to(dev)
+    B = torch.randn(N, K, generator=g, dtype=torch.float64).to(dev)
+    G = torch.rand(M, N, generator=g, dtype=torch.float32).to(dev)
+    ref = (A @ B.T) * G.double()
+    pa, pb = tcgemm.split(A), tcgemm.split(B)
+    C = torch.empty((M, N), dtype=torch.float32, device=dev)
+    O = tcgemm.Pair(M, N, dev)
+    T = tcgemm.Pair(N, M, dev)
+    tcgemm.gemm(pa, pb, K=K, G=G, out=C, out_pair=O, out_pair_t=T, wide=True)
+    C_seg = torch.empty((M, N), dtype=torch.float32, device=dev)
+    tcgemm.gemm(pa, pb, K=K, G=G, out=C_seg, segments=[(pa.hi, pb.hi), (pa.hi, pb.lo), (pa.lo, pb.hi)])
+    C_k = torch.empty((M, N), dtype=torch.float32, device=dev)
+    tcgemm.gemm(pa, pb, K=K, out=C_k, wide=True, ksplit=3)
+    torch.cuda.synchronize()
+    tcgemm.check_errors(dev)
+    scale = ref.abs().max().item()
+    assert (C.double() - ref).abs().max().item() / scale < 5e-5
+    # the two modes accumulate in FP32 in different K blocks (32 and 64 elements): both within the bound
+    assert (C_seg.double() - ref).abs().max().item() / scale < 5e-5
+    assert (O.hi[:, :N].double() + O.lo[:, :N].double() - C.double()).abs().max().item() / scale < 1e-5
+    assert (T.hi[:, :M].double() + T.lo[:, :M].double() - C.double().T).abs().max().item() / scale < 1e-5
+    refk = A @ B.T
+    assert (C_k.double() - refk).abs().max().item() / refk.abs().max().item() < 5e-5
