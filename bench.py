@@ -64,10 +64,10 @@ WORKLOADS = {
 # DRAM bytes (read + write) per tensor-core GEMM launch, from single-launch ncu captures of the four
 # exchange shapes of one product column (W, N for both y, P1|P2, K1;K2): their sum over the 4 launches / 4.
 GEMM_TRAFFIC_PER_LAUNCH = {
-    "armchair7": (6.47e8, "ncu dram__bytes_read.sum + dram__bytes_write.sum of the shapes 8292x1225x1225 (W), "
+    "armchair7": (6.36e8, "ncu dram__bytes_read.sum + dram__bytes_write.sum of the shapes 8292x1225x1225 (W), "
                           "8292x8292x1225 (N with G, pair + transposed pair), 1225x16640x8292 (P1|P2) and "
-                          "2450x1225x8292 (K1;K2) run alone through gemm_bench, averaged over the 4 launches of one "
-                          "product column"),
+                          "2450x1225x8292 (K1;K2) run alone through gemm_bench --wide (128 x 256 tiles), averaged "
+                          "over the 4 launches of one product column"),
 }
 
 
