@@ -144,7 +144,6 @@ class ExchangeMixed(ExchangeAO):
         self.Pint = T.Pair.__new__(T.Pair)
         self.Pint.rows, self.Pint.cols, self.Pint.ld = 2 * nvirt, 2 * norb, h
         self.Pint.hi, self.Pint.lo = self.P12.hi.view(2 * nvirt, h), self.P12.lo.view(2 * nvirt, h)
-        self.K12t = torch.empty((2 * nvirt, nocc), dtype=torch.float32, device=dev)
         self.Vp = T.Pair(nocc, nvirt, dev)
         self.coulomb_on_tensor_cores = coulomb_on_tensor_cores
         # 3: hi.hi + hi.lo + lo.hi (~2^-16); 1: hi.hi only (BF16, ~2^-8)
@@ -194,8 +193,9 @@ class ExchangeMixed(ExchangeAO):
         T = self.T
         nov, m = V.shape
         no, nv, norb = self.nocc, self.nvirt, self.norb
-        K1 = torch.empty_like(V)
-        K2 = torch.empty_like(V)
+        # K1^T and K2^T of every column, interleaved by rows as the K launch writes them; one transposing copy
+        # per block afterwards instead of two strided copies per column
+        Kall = torch.empty((m, 2 * nv, no), dtype=torch.float32, device=V.device)
         Vt = V.T.contiguous()  # one contiguous (nocc, nvirt) block per column
         for c in range(m):
             rf = self.refine
@@ -206,10 +206,10 @@ class ExchangeMixed(ExchangeAO):
             # [P1 | P2] in one launch (the rows between the halves of NB are zero)
             T.gemm(self.YbarT, self.NB, K=2 * norb, out_pair=self.P12, refine=rf)
             # K1^T and K2^T interleaved by rows, in one launch
-            T.gemm(self.Pint, self.XbarT, K=2 * norb, alpha=0.25, out=self.K12t, refine=rf)
-            # transpose, widen to FP64 and scatter into column c in one copy each
-            K1[:, c].view(no, nv).copy_(self.K12t[0::2].T)
-            K2[:, c].view(no, nv).copy_(self.K12t[1::2].T)
+            T.gemm(self.Pint, self.XbarT, K=2 * norb, alpha=0.25, out=Kall[c], refine=rf)
+        # (m, nv, no) -> (no, nv, m) = the (nov, m) column block, widened to FP64
+        K1 = Kall[:, 0::2, :].permute(2, 1, 0).to(torch.float64).reshape(no * nv, m)
+        K2 = Kall[:, 1::2, :].permute(2, 1, 0).to(torch.float64).reshape(no * nv, m)
         return K1, K2
 
 
@@ -223,9 +223,11 @@ class ExchangeOzaki(ExchangeAO):
         [P1 | P2] = Ybar^T [N; N^T]^T                 (nvirt x 4 Norb, K = 2 Norb)
         [K1^T ; K2^T] = [P1^T ; P2^T] Xbar_o / 4      (rows interleaved, K = 2 Norb)
     with Ybar = [S~_v; C_v] and Xbar = [S~_o; C_o]; the four constant operands are converted once.  The
-    Coulomb term is ExchangeAO's (native FP64 q_ov products)."""
+    Coulomb term is ExchangeAO's (native FP64 q_ov products).  nmod = 14 moduli carry 47 bits per operand
+    entry at K = 8292 (49 at K = 1225): ~1e-14 relative, far below the 2^-16 error of the tensor-core
+    products these FP64 products correct."""
 
-    def __init__(self, gamma, G_lr, q_ov, omega_flat, Co, Cv, S, nat, nocc, nvirt, workspace, lc=1):
+    def __init__(self, gamma, G_lr, q_ov, omega_flat, Co, Cv, S, nat, nocc, nvirt, workspace, lc=1, nmod=14):
         from . import ozaki as O
         super().__init__(gamma, G_lr, q_ov, omega_flat, Co, Cv, S, nat, nocc, nvirt, workspace, lc=lc,
                          max_bytes=1)
@@ -234,15 +236,15 @@ class ExchangeOzaki(ExchangeAO):
         norb = Co.shape[0]
         self.norb = norb
         So, Sv = S @ Co, S @ Cv
-        self.opYV = O.Operand(2 * norb, nvirt, dev).set(torch.cat([Cv, Sv], dim=0))
-        self.opXO = O.Operand(2 * norb, nocc, dev).set(torch.cat([Co, So], dim=0))
-        self.opYbarT = O.Operand(nvirt, 2 * norb, dev).set(torch.cat([Sv, Cv], dim=0).T)
-        self.opXbarT = O.Operand(nocc, 2 * norb, dev).set(torch.cat([So, Co], dim=0).T)
+        self.opYV = O.Operand(2 * norb, nvirt, dev, nmod).set(torch.cat([Cv, Sv], dim=0))
+        self.opXO = O.Operand(2 * norb, nocc, dev, nmod).set(torch.cat([Co, So], dim=0))
+        self.opYbarT = O.Operand(nvirt, 2 * norb, dev, nmod).set(torch.cat([Sv, Cv], dim=0).T)
+        self.opXbarT = O.Operand(nocc, 2 * norb, dev, nmod).set(torch.cat([So, Co], dim=0).T)
         self.G4 = torch.cat([torch.cat([G_lr, G_lr], dim=1)] * 2, dim=0).contiguous()
-        self.opV = O.Operand(nocc, nvirt, dev)
-        self.opW = O.Operand(2 * norb, nocc, dev)
-        self.opNB = O.Operand(4 * norb, 2 * norb, dev)
-        self.opP = O.Operand(2 * nvirt, 2 * norb, dev)
+        self.opV = O.Operand(nocc, nvirt, dev, nmod)
+        self.opW = O.Operand(2 * norb, nocc, dev, nmod)
+        self.opNB = O.Operand(4 * norb, 2 * norb, dev, nmod)
+        self.opP = O.Operand(2 * nvirt, 2 * norb, dev, nmod)
         self.WT = torch.empty((2 * norb, nocc), dtype=torch.float64, device=dev)
         self.N = torch.empty((2 * norb, 2 * norb), dtype=torch.float64, device=dev)
         self.P12 = torch.empty((nvirt, 4 * norb), dtype=torch.float64, device=dev)
