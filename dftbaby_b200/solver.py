@@ -69,14 +69,17 @@ def orthonormal_columns(Q):
 
 
 def orthonormalize_new(bs, Q):
-    """Orthonormalise the columns of Q against bs (CGS2) and among themselves (Cholesky QR2)."""
+    """Orthonormalise the columns of Q against bs (CGS2) and among themselves (Cholesky QR2).  A third
+    projection follows when the normalisation has left components along bs above 1e-14 (it rarely does;
+    measuring them costs one of the pass's two products)."""
     if bs is not None and bs.shape[1] > 0:
         for _ in range(2):
             Q = Q - bs @ (bs.T @ Q)
     Q = orthonormal_columns(Q)
     if bs is not None and bs.shape[1] > 0:
-        Q = Q - bs @ (bs.T @ Q)
-        Q = orthonormal_columns(Q)
+        X = bs.T @ Q
+        if float(torch.max(torch.abs(X)).item()) > 1.0e-14:
+            Q = orthonormal_columns(Q - bs @ X)
     return Q
 
 
