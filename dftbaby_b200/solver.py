@@ -78,7 +78,7 @@ def orthonormalize_new(bs, Q):
     Q = orthonormal_columns(Q)
     if bs is not None and bs.shape[1] > 0:
         X = bs.T @ Q
-        if float(torch.max(torch.abs(X)).item()) > 1.0e-14:
+        if X.numel() > 0 and float(torch.max(torch.abs(X)).item()) > 1.0e-14:
             Q = orthonormal_columns(Q - bs @ X)
     return Q
 
@@ -397,6 +397,13 @@ def nonhermitian_davidson(products, omega, nstates, ifact=1, conv=1.0e-14, maxit
         assert len(src) == dk
         Q = _precondition(torch.cat([WL, WR], dim=1), src, state, w, pdiag)
         Q = orthonormalize_new(bs, Q)
+        if Q.shape[1] == 0:
+            # the expansion space holds the whole problem (or nothing new survives orthogonalisation): its Ritz
+            # pairs are final.  With FP64 products that happens only once they are exact; with reduced-
+            # precision products (residuals above conv from the operator's own noise) it ends the stage here.
+            if stats is not None:
+                stats["space_exhausted"] = True
+            break
         B.append(Q, list(products(Q)))
         l = B.l
     else:

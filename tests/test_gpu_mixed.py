@@ -121,3 +121,21 @@ def test_mixed_with_fp64_corrections_meets_the_accuracy_gate_on_a_flake(rounds, 
     assert len(res) == rounds and all(np.isfinite(res))
     if rounds > 1:
         assert res[-1] < res[0]
+
+
+def test_tensor_core_stage_that_fills_the_whole_space():
+    """A molecule small enough for the tensor-core stage to fill the whole (A+B, A-B) space before its
+    operator noise lets the residuals reach the threshold: the stage stops there, and one round of FP64
+    corrections over the full space gives the FP64 energies."""
+    from dftbaby_b200 import LR_TDDFTB
+    native.load()
+    al = geometry.polyene(6, sigma=0.02, seed=2)
+    opts = dict(nstates=4, diag_conv=1e-8, diag_maxiter=100)
+    tp = LR_TDDFTB(al, long_range_correction=1)
+    tp.setGeometry(al)
+    O64, _ = tp.getEnergies(**opts)
+    tm = LR_TDDFTB(al, long_range_correction=1)
+    tm.setGeometry(al)
+    Om, _ = tm.getEnergies(precision="mixed", refine_fp64=True, refine_iterations=1, **opts)
+    assert tm.stats["mixed"].get("space_exhausted") or tm.stats["mixed"]["subspace"] < tm.nocc * tm.nvirt
+    assert np.abs(Om - O64).max() * HARTREE_TO_EV < 1e-6
