@@ -662,6 +662,17 @@ class _BatchedProducts:
             self.Xo_bar = torch.stack([SCo, Co], 1)
             self.Yv_bar = torch.stack([SCv, Cv], 1)
 
+    def subset(self, idx):
+        """The products of the molecules idx (a device index tensor) only."""
+        sub = _BatchedProducts.__new__(_BatchedProducts)
+        sub.gat, sub.qov, sub.om = self.gat[idx], self.qov[idx], self.om[idx]
+        sub.Glr = self.Glr[idx] if self.Glr is not None else None
+        sub.no, sub.nv = self.no, self.nv
+        if self.Glr is not None:
+            sub.Xo, sub.Yv = self.Xo[idx], self.Yv[idx]
+            sub.Xo_bar, sub.Yv_bar = self.Xo_bar[idx], self.Yv_bar[idx]
+        return sub
+
     def __call__(self, V):
         """V: (B, nov, m) -> (ApB V, AmB V)."""
         B, nov, m = V.shape
@@ -891,11 +902,15 @@ def _batched_hermitian(prod, om, k, conv, maxiter, kmax, guess=None):
     return Om, C, XmY, XpY, iters.tolist()
 
 
-def _batched_nonhermitian(prod, om, k, conv, maxiter, kmax, guess=None):
+def _batched_nonhermitian(prod, om, k, conv, maxiter, kmax, guess=None, compact=0.75):
     """Lockstep Stratmann-Scuseria-Frisch Davidson over a batch (Solver.nonHermitianDavidson):
     every molecule adds exactly the correction vectors DFTBaby would add, so its search space,
-    and with it the subspace-dependent C = bs Tb behind the oscillator strengths, is DFTBaby's."""
-    B, nov = om.shape
+    and with it the subspace-dependent C = bs Tb behind the oscillator strengths, is DFTBaby's.
+    Once the molecules still iterating are at most `compact` of the working batch, the converged
+    ones leave it (their results are final), so the later, costlier iterations run on the
+    unconverged molecules only."""
+    B_all, nov = om.shape
+    B = B_all
     dev = om.device
     f64 = torch.float64
     if guess is not None:
@@ -915,7 +930,18 @@ def _batched_nonhermitian(prod, om, k, conv, maxiter, kmax, guess=None):
     C = torch.zeros((B, k, nov), dtype=f64, device=dev)
     XmY = torch.zeros_like(C)
     XpY = torch.zeros_like(C)
-    iters = np.zeros(B, int)
+    iters = np.zeros(B_all, int)
+    # results of the whole batch; gidx maps the working batch's rows to it
+    res = [torch.zeros_like(Om), torch.zeros_like(C), torch.zeros_like(C), torch.zeros_like(C)]
+    gidx = np.arange(B_all)
+    kmax = list(kmax)
+
+    def store(rows):
+        g = torch.as_tensor(gidx[rows], device=dev)
+        r = torch.as_tensor(rows, device=dev)
+        for dst, src in zip(res, (Om, C, XmY, XpY)):
+            dst[g] = src[r]
+
     for it in range(maxiter):
         Mp = _pad_dead(Mp0, live)
         Mm = _pad_dead(Mm0, live)
@@ -943,10 +969,24 @@ def _batched_nonhermitian(prod, om, k, conv, maxiter, kmax, guess=None):
         XmY = torch.where(act_t[:, None, None], Lv.transpose(1, 2), XmY)
         XpY = torch.where(act_t[:, None, None], R.transpose(1, 2), XpY)
         newly = active & (norms < conv).all(1) & (it > 0)
-        iters[active] = it + 1
+        iters[gidx[active]] = it + 1
         active = active & ~newly
         if not active.any():
             break
+        n_act = int(active.sum())
+        if n_act <= compact * B and hasattr(prod, "subset"):
+            # the converged molecules leave the working batch with their final results
+            store(np.nonzero(~active)[0])
+            keep_np = np.nonzero(active)[0]
+            keep = torch.as_tensor(keep_np, device=dev)
+            bs, AP, AM, Mp0, Mm0, live = bs[keep], AP[keep], AM[keep], Mp0[keep], Mm0[keep], live[keep]
+            Om, C, XmY, XpY, om, w = Om[keep], C[keep], XmY[keep], XpY[keep], om[keep], w[keep]
+            WL, WR = WL[keep], WR[keep]
+            normsL, normsR, l_live = normsL[keep_np], normsR[keep_np], l_live[keep_np]
+            kmax = [kmax[i] for i in keep_np]
+            gidx, active = gidx[keep_np], active[keep_np]
+            prod = prod.subset(keep)
+            B = n_act
         sel = _select_new(normsL, normsR, k, l_live, kmax, conv, True) & active[:, None]
         # correction vectors: L residuals, then R residuals, (w - omega)^-1 preconditioner
         wk = w[:, None, :k]
@@ -963,7 +1003,8 @@ def _batched_nonhermitian(prod, om, k, conv, maxiter, kmax, guess=None):
         AM = torch.cat([AM, am], 2)
     else:
         raise ExcitedStatesNotConverged("batched Davidson: %d molecules did not converge" % int(active.sum()))
-    return Om, C, XmY, XpY, iters.tolist()
+    store(np.arange(B))
+    return res[0], res[1], res[2], res[3], iters.tolist()
 
 
 def main(argv=None):
