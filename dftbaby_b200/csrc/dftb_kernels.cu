@@ -517,12 +517,30 @@ __global__ void __launch_bounds__(TC_THREADS) tc_tile_kernel(int nat, int n1, in
             }
 #pragma unroll
             for (int r = 0; r < TC_ROWS; ++r) {
-                const int p = p0 + pl0 + r;
-                if (p >= n1 || qg >= n2) continue;
+                const int p = p0 + pl0 + r;  // the same for the whole warp
+                if (p >= n1) continue;
                 double *row = q + ((size_t)A * n1 + p) * n2;
-                if (VEC && qg + 1 < n2) {
-                    *reinterpret_cast<double2 *>(row + qg) = make_double2(0.5 * acc0[r], 0.5 * acc1[r]);
+                if (VEC) {
+                    // 16-byte stores on every row: a row whose tile segment starts on an odd element (odd n2)
+                    // stores the pairs (qg + 1, qg + 2), the second value taken from the next lane; lane 0
+                    // stores its first column and lane 31 its second as single elements
+                    const int lane = tid & 31;
+                    const double nxt = __shfl_down_sync(0xffffffffu, acc0[r], 1);
+                    const bool odd = (reinterpret_cast<uintptr_t>(row + q0) & 15) != 0;  // warp-uniform
+                    if (!odd) {
+                        if (qg + 1 < n2)
+                            *reinterpret_cast<double2 *>(row + qg) = make_double2(0.5 * acc0[r], 0.5 * acc1[r]);
+                        else if (qg < n2)
+                            row[qg] = 0.5 * acc0[r];
+                    } else {
+                        if (lane == 0 && qg < n2) row[qg] = 0.5 * acc0[r];
+                        if (lane < 31 && qg + 2 < n2)
+                            *reinterpret_cast<double2 *>(row + qg + 1) = make_double2(0.5 * acc1[r], 0.5 * nxt);
+                        else if (qg + 1 < n2)
+                            row[qg + 1] = 0.5 * acc1[r];
+                    }
                 } else {
+                    if (qg >= n2) continue;
                     row[qg] = 0.5 * acc0[r];
                     if (qg + 1 < n2) row[qg + 1] = 0.5 * acc1[r];
                 }
@@ -536,8 +554,8 @@ int launch_tc(int nat, int n1, int n2, const int *first, const double *C1, const
               const double *Sc2, double *out, cudaStream_t st, const char *where) {
     dim3 grid(cdiv(n2, TC_TQ), cdiv(n1, TC_TP), cdiv(nat, TC_ATOMS));
     if (grid.y > 65535u || grid.z > 65535u) return fail(DFTB_ERR_BAD_SIZE, "trans_charges: grid too large");
-    // 16-byte stores need every row of the output to start on an even index (and an aligned base)
-    if (n2 % 2 == 0 && ((uintptr_t)out & 15) == 0)
+    // 16-byte stores need an aligned base; rows that start on an odd element shift their pairs by one
+    if (((uintptr_t)out & 15) == 0)
         tc_tile_kernel<true><<<grid, TC_THREADS, 0, st>>>(nat, n1, n2, first, C1, Sc1, C2, Sc2, out);
     else
         tc_tile_kernel<false><<<grid, TC_THREADS, 0, st>>>(nat, n1, n2, first, C1, Sc1, C2, Sc2, out);
@@ -555,11 +573,59 @@ __global__ void tc_diag_kernel(int n, const int *first, const double *C, const d
     q[(size_t)A * n + p] = 0.5 * acc;
 }
 
+// cuBLAS for plain FP64 GEMMs (the Coulomb product's two, the transition charges' S.C).  The library is resolved at run
+// time (dlopen / dlsym, reusing the copy the process has already loaded), so the shared library
+// loads without it and the product falls back to dgemm_kernel.
+using blas_create_t = cublasStatus_t (*)(cublasHandle_t *);
+using blas_stream_t = cublasStatus_t (*)(cublasHandle_t, cudaStream_t);
+using blas_dgemm_t = cublasStatus_t (*)(cublasHandle_t, cublasOperation_t, cublasOperation_t, int, int, int,
+                                        const double *, const double *, int, const double *, int, const double *,
+                                        double *, int);
+struct Blas {
+    blas_create_t create = nullptr;
+    blas_stream_t set_stream = nullptr;
+    blas_dgemm_t dgemm = nullptr;
+    bool ok = false;
+};
+
+Blas &blas() {
+    static Blas b;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *h = dlopen("libcublas.so.12", RTLD_NOW | RTLD_NOLOAD);
+        if (!h) h = dlopen("libcublas.so.12", RTLD_NOW | RTLD_GLOBAL);
+        if (!h) h = dlopen("libcublas.so", RTLD_NOW | RTLD_GLOBAL);
+        if (!h) return;
+        b.create = reinterpret_cast<blas_create_t>(dlsym(h, "cublasCreate_v2"));
+        b.set_stream = reinterpret_cast<blas_stream_t>(dlsym(h, "cublasSetStream_v2"));
+        b.dgemm = reinterpret_cast<blas_dgemm_t>(dlsym(h, "cublasDgemm_v2"));
+        b.ok = b.create && b.set_stream && b.dgemm;
+    });
+    return b;
+}
+
+// one handle per host thread and device, bound to the caller's stream; nullptr if unavailable
+cublasHandle_t blas_handle(cudaStream_t st) {
+    Blas &b = blas();
+    if (!b.ok) return nullptr;
+    thread_local cublasHandle_t handles[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (!handles[dev] && b.create(&handles[dev]) != CUBLAS_STATUS_SUCCESS) {
+        handles[dev] = nullptr;
+        return nullptr;
+    }
+    if (b.set_stream(handles[dev], st) != CUBLAS_STATUS_SUCCESS) return nullptr;
+    return handles[dev];
+}
+
 size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
+// use_blas: S.C by cuBLAS when it resolves (the entry points that may allocate; the allocation-free one
+// keeps the library's own dgemm_kernel)
 int trans_charges_common(int norb, int nat, int nocc, int nvirt, const double *co, const double *cv,
                          const double *Smat, const int *opa, void *work, size_t work_bytes, cudaStream_t st,
-                         double **sco, double **scv, int **first) {
+                         double **sco, double **scv, int **first, bool use_blas = true) {
     if (norb <= 0 || nat <= 0 || nocc < 0 || nvirt < 0) return fail(DFTB_ERR_BAD_SIZE, "trans_charges: sizes");
     if (!Smat || !opa || (nocc > 0 && !co) || (nvirt > 0 && !cv)) return fail(DFTB_ERR_NULL, "trans_charges: null");
     if (!work || work_bytes < dftb_trans_charges_workspace_size(norb, nocc, nvirt))
@@ -574,9 +640,18 @@ int trans_charges_common(int norb, int nat, int nocc, int nvirt, const double *c
     int rc = check_launch("prefix_kernel");
     if (rc) return rc;
     // Sc = S . C (S is symmetric)
+    cublasHandle_t bh = use_blas ? blas_handle(st) : nullptr;
     for (int b = 0; b < 2; ++b) {
         const int n = b == 0 ? nocc : nvirt;
         if (n == 0) continue;
+        if (bh) {
+            // row-major Sc (norb x n) is the column-major Sc^T = C^T S^T = C^T S
+            const double one = 1.0, zero = 0.0;
+            if (blas().dgemm(bh, CUBLAS_OP_N, CUBLAS_OP_N, n, norb, norb, &one, b == 0 ? co : cv, n, Smat, norb, &zero,
+                             b == 0 ? *sco : *scv, n) != CUBLAS_STATUS_SUCCESS)
+                return fail(DFTB_ERR_CUDA, "trans_charges: cublasDgemm (S C) failed");
+            continue;
+        }
         GemmP p = gemm_defaults();
         p.M = norb;
         p.N = n;
@@ -671,53 +746,7 @@ __global__ void omega_scale_kernel(long long nov, int nvec, const double *omega,
     us[idx] = omega[idx / nvec] * vs[idx];
 }
 
-// Coulomb part shared by the Hermitian and (A+B) products:
-// cuBLAS for the two plain FP64 GEMMs of the Coulomb product.  The library is resolved at run
-// time (dlopen / dlsym, reusing the copy the process has already loaded), so the shared library
-// loads without it and the product falls back to dgemm_kernel.
-using blas_create_t = cublasStatus_t (*)(cublasHandle_t *);
-using blas_stream_t = cublasStatus_t (*)(cublasHandle_t, cudaStream_t);
-using blas_dgemm_t = cublasStatus_t (*)(cublasHandle_t, cublasOperation_t, cublasOperation_t, int, int, int,
-                                        const double *, const double *, int, const double *, int, const double *,
-                                        double *, int);
-struct Blas {
-    blas_create_t create = nullptr;
-    blas_stream_t set_stream = nullptr;
-    blas_dgemm_t dgemm = nullptr;
-    bool ok = false;
-};
-
-Blas &blas() {
-    static Blas b;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void *h = dlopen("libcublas.so.12", RTLD_NOW | RTLD_NOLOAD);
-        if (!h) h = dlopen("libcublas.so.12", RTLD_NOW | RTLD_GLOBAL);
-        if (!h) h = dlopen("libcublas.so", RTLD_NOW | RTLD_GLOBAL);
-        if (!h) return;
-        b.create = reinterpret_cast<blas_create_t>(dlsym(h, "cublasCreate_v2"));
-        b.set_stream = reinterpret_cast<blas_stream_t>(dlsym(h, "cublasSetStream_v2"));
-        b.dgemm = reinterpret_cast<blas_dgemm_t>(dlsym(h, "cublasDgemm_v2"));
-        b.ok = b.create && b.set_stream && b.dgemm;
-    });
-    return b;
-}
-
-// one handle per host thread and device, bound to the caller's stream; nullptr if unavailable
-cublasHandle_t blas_handle(cudaStream_t st) {
-    Blas &b = blas();
-    if (!b.ok) return nullptr;
-    thread_local cublasHandle_t handles[64] = {nullptr};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-    if (!handles[dev] && b.create(&handles[dev]) != CUBLAS_STATUS_SUCCESS) {
-        handles[dev] = nullptr;
-        return nullptr;
-    }
-    if (b.set_stream(handles[dev], st) != CUBLAS_STATUS_SUCCESS) return nullptr;
-    return handles[dev];
-}
-
+// Coulomb part shared by the Hermitian and (A+B) products (cuBLAS handle: blas() above).
 // us(ia, n) = omega_ia v(ia, n) + fac us(ia, n)   (in place; the non-Hermitian Coulomb epilogue)
 __global__ void rv_inplace_kernel(long long total, int nvec, const double *omega, const double *vs, double *us,
                                   double fac) {
@@ -1284,7 +1313,7 @@ extern "C" int dftb_trans_charges_noalloc(int norb, int nat, int nocc, int nvirt
     double *sco, *scv;
     int *first;
     rc = trans_charges_common(norb, nat, nocc, nvirt, co, cv, Sm, opa, scratch, kNoAllocScratchBytes, st, &sco, &scv,
-                              &first);
+                              &first, false);
     if (rc) return rc;
     struct Blk {
         double *out;

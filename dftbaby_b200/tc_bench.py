@@ -5,7 +5,8 @@
 Calls dftb_trans_charges for the occupied-virtual block only on random coefficients and overlap (a quarter
 of the atoms hydrogen with one orbital, the rest carbon with four), times REPS calls with CUDA events after
 one warm-up call and prints the q_ov bytes written per second of the whole call (the two S.C products
-included).  ``1104 1225 1225`` is the size of the 1104-atom benchmark's window; ``600 300 300 1`` is the
+included), then the device time of each kernel of one more call (CUDA activity records) with the tile
+kernel's own rate.  ``1104 1225 1225`` is the size of the 1104-atom benchmark's window; ``600 300 300 1`` is the
 small case profiled under ncu.
 """
 import sys
@@ -53,6 +54,17 @@ def main(argv=None):
     gb = 8.0 * nat * no * nv / 1e9
     print("nat %d norb %d window %dx%d: q_ov %.2f GB, whole call %.3f ms (min %.3f) -> %.0f GB/s of q_ov writes" % (
         nat, norb, no, nv, gb, float(np.median(ts)), min(ts), gb / (min(ts) / 1e3)))
+    # device time per kernel of one call (CUDA activity records): the tile kernel alone against the q_ov bytes
+    from torch.profiler import ProfilerActivity, profile
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        call()
+        torch.cuda.synchronize()
+    for k in prof.key_averages():
+        if k.device_type.name == "CUDA" and k.device_time_total > 0:
+            ms = k.device_time_total / 1e3
+            extra = " -> %.0f GB/s of q_ov writes" % (gb / (ms / 1e3)) if "tc_tile" in k.key else ""
+            name = k.key.replace("(anonymous namespace)::", "").split("(")[0] or k.key
+            print("  %-60s %8.3f ms%s" % (name[:60], ms, extra))
 
 
 if __name__ == "__main__":

@@ -116,7 +116,8 @@ def test_trans_charges_and_monopoles_match_oracle(dev):
 @pytest.mark.parametrize("nocc,nvirt", [(130, 258), (67, 257), (1, 3)])
 def test_trans_charges_ragged_tiles_match_oracle(dev, nocc, nvirt):
     """Shapes that cut every tile of the transition-charge kernel (64 rows p x 128 columns q x 8 atoms):
-    partial tiles in both directions, even and odd row lengths (16-byte and scalar stores), 19 atoms (a
+    partial tiles in both directions, even and odd row lengths (aligned and shifted 16-byte stores; NaN-filled
+    outputs catch a column stored by no lane), 19 atoms (a
     partial atom run) with 1, 4, 9 and 10 orbitals (the last one above the staged limit, read from global
     memory).  Random coefficients and overlap: the kernel is plain algebra on them."""
     rng = np.random.default_rng(nocc + nvirt)
