@@ -973,6 +973,52 @@ int check_products(int nat, int nocc, int nvirt, int nvec, int lc, const double 
     return DFTB_OK;
 }
 
+// ---------------------------------------------------------------------------- layout changes of column blocks
+
+// Y (cols x rows) = X^T through a 32 x 32 shared-memory tile: reads and writes run along rows of 256 bytes
+// (a strided element copy moves a whole 32-byte sector per 8-byte element on one side)
+__global__ void __launch_bounds__(256) transpose_f64_kernel(int rows, int cols, const double *__restrict__ X,
+                                                            long long ldx, double *__restrict__ Y, long long ldy) {
+    __shared__ double t[32][33];
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int k = ty; k < 32; k += 8) {
+        const int r = r0 + k, c = c0 + tx;
+        if (r < rows && c < cols) t[k][tx] = X[(long long)r * ldx + c];
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int c = c0 + k, r = r0 + tx;
+        if (c < cols && r < rows) Y[(long long)c * ldy + r] = t[tx][k];
+    }
+}
+
+// K_y[(i nvirt + a) m + c] = Kall[c][2a + y][i] (FP32 -> FP64): the exchange's last launch writes, for each
+// product column c, K1^T and K2^T with their rows interleaved.  A CTA takes one a and a run of 32 i for
+// every c: it reads 128-byte pieces of Kall rows and writes whole m-long rows of K1 and K2.
+__global__ void __launch_bounds__(256) exchange_unpack_kernel(int m, int nv, int no, const float *__restrict__ Kall,
+                                                              double *__restrict__ K1, double *__restrict__ K2) {
+    __shared__ float t[2][64][33];
+    const int a = blockIdx.y, i0 = blockIdx.x * 32;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int c0 = 0; c0 < m; c0 += 64) {
+        const int mc = min(64, m - c0);
+        for (int row = wid; row < 2 * mc; row += 8) {
+            const int c = row >> 1, y = row & 1, i = i0 + lane;
+            t[y][c][lane] = i < no ? Kall[((long long)(c0 + c) * 2 * nv + 2 * a + y) * no + i] : 0.0f;
+        }
+        __syncthreads();
+        for (int row = wid; row < 64; row += 8) {
+            const int il = row >> 1, y = row & 1, i = i0 + il;
+            if (i < no) {
+                double *dst = (y ? K2 : K1) + ((long long)i * nv + a) * m + c0;
+                for (int c = lane; c < mc; c += 32) dst[c] = (double)t[y][c][il];
+            }
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 // ============================================================================
@@ -1203,6 +1249,24 @@ int dftb_davidson_residual(int nov, int ncol, const double *AV, int ldav, const 
     if (rc) return rc;
     sqrt_kernel<<<cdiv(ncol, 128), 128, 0, st>>>(ncol, norms);
     return check_launch("sqrt_kernel");
+}
+
+int dftb_transpose_f64(int rows, int cols, const double *X, int ldx, double *Y, int ldy, void *stream) {
+    if (rows < 0 || cols < 0 || ldx < cols || ldy < rows) return fail(DFTB_ERR_BAD_SIZE, "transpose_f64: sizes");
+    if (rows == 0 || cols == 0) return DFTB_OK;
+    if (!X || !Y) return fail(DFTB_ERR_NULL, "transpose_f64: null");
+    if (cdiv(cols, 32) > 65535) return fail(DFTB_ERR_BAD_SIZE, "transpose_f64: more than 2097120 columns");
+    transpose_f64_kernel<<<dim3(cdiv(rows, 32), cdiv(cols, 32)), 256, 0, S(stream)>>>(rows, cols, X, ldx, Y, ldy);
+    return check_launch("transpose_f64_kernel");
+}
+
+int dftb_exchange_unpack(int m, int nvirt, int nocc, const float *Kall, double *K1, double *K2, void *stream) {
+    if (m < 0 || nvirt < 0 || nocc < 0) return fail(DFTB_ERR_BAD_SIZE, "exchange_unpack: sizes");
+    if (m == 0 || nvirt == 0 || nocc == 0) return DFTB_OK;
+    if (!Kall || !K1 || !K2) return fail(DFTB_ERR_NULL, "exchange_unpack: null");
+    if (nvirt > 65535) return fail(DFTB_ERR_BAD_SIZE, "exchange_unpack: more than 65535 virtual orbitals");
+    exchange_unpack_kernel<<<dim3(cdiv(nocc, 32), nvirt), 256, 0, S(stream)>>>(m, nvirt, nocc, Kall, K1, K2);
+    return check_launch("exchange_unpack_kernel");
 }
 
 int dftb_dgemm(int transa, int transb, int m, int n, int k, double alpha, const double *A, int lda, const double *B,

@@ -51,8 +51,14 @@ class DIIS_80:
         self._add(flat)
         if self.start_flag:
             n = len(self.resid)
-            R = torch.stack(self.resid[:n])
-            gram = (R @ R.T).cpu().numpy()
+            # the Gram matrix of the Norb^2-long residuals as separate dot products: a product with a tiny
+            # n x n output and K = Norb^2 leaves most of the GPU idle
+            dots = [torch.dot(self.resid[i], self.resid[j]) for i in range(n) for j in range(i, n)]
+            upper = iter(torch.stack(dots).cpu().numpy())
+            gram = np.zeros((n, n))
+            for i in range(n):
+                for j in range(i, n):
+                    gram[i, j] = gram[j, i] = next(upper)
             A = np.zeros((n + 1, n + 1))
             A[:n, :n] = gram
             A[:n, n] = A[n, :n] = -1.0
@@ -384,11 +390,10 @@ class DFTB2(object):
         Jacobi-type rotations (``_track_occupied``, a handful of Norb^2 Nocc GEMMs instead of a dense
         eigensolve), and the last, converged iteration solves the full problem again, so the orbitals
         and energies handed on are exact eigenpairs.  The density of a T = 0 closed shell depends on the
-        occupied space only, so the mixing schedule, the convergence test and the fixed point are
-        DFTBaby's; iterates differ by the rotations' residual (below subspace_tol times the last relative
-        change; with 1e-4 the converged orbital energies of the 1104-atom benchmark flake move by 8e-8 Ha
-        from the dense path's, enough to move X+Y oscillator strengths by 1.6e-4, so the default is 1e-6:
-        3e-9 Ha).
+        occupied space only, so the mixing schedule, the convergence test and the fixed point are DFTBaby's;
+        iterates differ by the rotations' residual (below subspace_tol times the last relative change; with
+        1e-4 the converged orbital energies of the 1104-atom benchmark flake move by 8e-8 Ha from the dense
+        path's, enough to move X+Y oscillator strengths by 1.6e-4, so the default is 1e-6: 3e-10 Ha).
 
         lc_products (not in DFTBaby): "fp64" forms the long-range exchange H^x(P - P0) in FP64 in every
         iteration, as DFTBaby does.  "mixed" forms it in FP64 at anchor densities only and adds the tensor-
@@ -578,19 +583,23 @@ class DFTB2(object):
         """Move an S-orthonormal occupied/virtual split (Co, Cv) onto the invariant subspaces of H.
 
         Each step forms the coupling block F = Cv^T H Co and rotates the two spaces by the first-order
-        (Jacobi) correction Y_ai = F_ai / (e_i - e_a), with e_i = diag(Co^T H Co) and e_a the virtual
-        levels of the last full solve: Co + Cv Y and Cv - Co Y^T stay exactly S-orthogonal to each other,
-        and their Gram matrices I + Y^T Y and I + Y Y^T renormalise them -- by the symmetric (Lowdin)
-        inverse square root I - G/2 + 3 G^2/8 when |Y|_F^2 <= 3e-6 (the omitted terms are below
-        5/16 |Y|_F^6 < 1e-17), by Cholesky otherwise.  Steps repeat until max |F| < max(1e-13, tol_rel rel),
-        rel being the last relative density change.  A level shift b > 0 is DFTBaby's (DFTB2.py:1059-1081):
-        b added to the virtual block in the basis of the previous orbitals, i.e. H + b S Cv0 Cv0^T S with
-        Cv0 the virtual space on entry.  Returns the new (Co, Cv, e_o, e_v), or None when an occupied level
-        is not below every virtual one or the rotations have not converged after max_steps; the caller then
-        solves the full eigenproblem."""
+        (Jacobi) correction Y_ai = F_ai / (e_i - e_a), with e_i = diag(Co^T H Co) and e_a = diag(Cv^T H Cv)
+        on entry (one Norb^2 Nvirt product per call; with the virtual levels of the last full solve, which
+        the SCC has moved since, the 1104-atom benchmark flake took 14 % more steps and converged to orbital
+        energies ten times further from the full solve's): Co + Cv Y and Cv - Co Y^T stay exactly
+        S-orthogonal to each other, and their Gram matrices I + Y^T Y and I + Y Y^T renormalise them -- by
+        the symmetric (Lowdin) inverse square root I - G/2 + 3 G^2/8 when |Y|_F^2 <= 3e-6 (the omitted terms
+        are below 5/16 |Y|_F^6 < 1e-17), without its G^2 term once 3/8 |Y|_F^4 < 1e-17 and not at all once
+        |Y|_F^2 / 2 < 1e-17 (the late steps of a converging SCC), by Cholesky otherwise.  Steps repeat
+        until max |F| < max(1e-13, tol_rel rel), rel being the last relative density change.  A level shift
+        b > 0 is DFTBaby's (DFTB2.py:1059-1081): b added to the virtual block in the basis of the previous
+        orbitals, i.e. H + b S Cv0 Cv0^T S with Cv0 the virtual space on entry.  Returns the new
+        (Co, Cv, e_o, e_v), or None when an occupied level is not below every virtual one or the rotations
+        have not converged after max_steps; the caller then solves the full eigenproblem."""
         Co, Cv, eo, ev = tracked
         mm = self._mm
         tol = max(1.0e-13, tol_rel * rel)
+        ev = torch.sum(Cv * mm(H, Cv), dim=0)
         SCv0 = mm(self.S, Cv) if shift > 0.0 else None
         for step in range(max_steps + 1):
             HCo = mm(H, Co)
@@ -610,13 +619,21 @@ class DFTB2(object):
             self.rotation_steps += 1
             Con = Co + mm(Cv, Y)
             Cvn = Cv - mm(Co, Y.T)
+            if y2 <= 2.0e-17:
+                # the renormalisation would change the columns by |G|_2 / 2 <= |Y|_F^2 / 2 < 1e-17
+                Co, Cv = Con, Cvn
+                continue
             Go = mm(Y.T, Y)
             Gv = mm(Y, Y.T)
             if y2 <= 3.0e-6:
-                # (I + G)^(-1/2) = I - G/2 + 3/8 G^2 - 5/16 G^3 + ...,  |G|_2 <= |Y|_F^2
-                Mo = 0.375 * mm(Go, Go) - 0.5 * Go
+                # (I + G)^(-1/2) = I - G/2 + 3/8 G^2 - 5/16 G^3 + ...,  |G|_2 <= |Y|_F^2; the G^2 term only
+                # while 3/8 |Y|_F^4 exceeds 1e-17
+                if y2 > 5.0e-9:
+                    Mo = 0.375 * mm(Go, Go) - 0.5 * Go
+                    Mv = 0.375 * mm(Gv, Gv) - 0.5 * Gv
+                else:
+                    Mo, Mv = -0.5 * Go, -0.5 * Gv
                 Mo.diagonal().add_(1.0)
-                Mv = 0.375 * mm(Gv, Gv) - 0.5 * Gv
                 Mv.diagonal().add_(1.0)
                 Co, Cv = mm(Con, Mo), mm(Cvn, Mv)
             else:

@@ -196,7 +196,7 @@ class ExchangeMixed(ExchangeAO):
         # K1^T and K2^T of every column, interleaved by rows as the K launch writes them; one transposing copy
         # per block afterwards instead of two strided copies per column
         Kall = torch.empty((m, 2 * nv, no), dtype=torch.float32, device=V.device)
-        Vt = V.T.contiguous()  # one contiguous (nocc, nvirt) block per column
+        Vt = native.transpose(V)  # one contiguous (nocc, nvirt) block per column
         for c in range(m):
             rf = self.refine
             T.split(Vt[c].reshape(no, nv), out=self.Vp)
@@ -208,8 +208,10 @@ class ExchangeMixed(ExchangeAO):
             # K1^T and K2^T interleaved by rows, in one launch
             T.gemm(self.Pint, self.XbarT, K=2 * norb, alpha=0.25, out=Kall[c], refine=rf)
         # (m, nv, no) -> (no, nv, m) = the (nov, m) column block, widened to FP64
-        K1 = Kall[:, 0::2, :].permute(2, 1, 0).to(torch.float64).reshape(no * nv, m)
-        K2 = Kall[:, 1::2, :].permute(2, 1, 0).to(torch.float64).reshape(no * nv, m)
+        K1 = torch.empty((no * nv, m), dtype=torch.float64, device=V.device)
+        K2 = torch.empty_like(K1)
+        native.call("dftb_exchange_unpack", m, nv, no, native.ptr(Kall), native.ptr(K1), native.ptr(K2),
+                    native.stream())
         return K1, K2
 
 
@@ -256,7 +258,7 @@ class ExchangeOzaki(ExchangeAO):
         no, nv, norb = self.nocc, self.nvirt, self.norb
         K1 = torch.empty_like(V)
         K2 = torch.empty_like(V)
-        Vt = V.T.contiguous()
+        Vt = native.transpose(V)
         for c in range(m):
             self.opV.set(Vt[c].view(no, nv))
             O.product(self.opYV, self.opV, out=self.WT)

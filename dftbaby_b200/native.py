@@ -59,6 +59,8 @@ _SIGNATURES = {
     "dftb_ambv": (_I, [_I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _Z, _P]),
     "dftb_davidson_precondition": (_I, [_I, _I, _P, _I, _P, _P, _P, _P, _P, _I, _P]),
     "dftb_davidson_residual": (_I, [_I, _I, _P, _I, _P, _I, _P, _P, _I, _P, _P]),
+    "dftb_transpose_f64": (_I, [_I, _I, _P, _I, _P, _I, _P]),
+    "dftb_exchange_unpack": (_I, [_I, _I, _I, _P, _P, _P, _P]),
     "dftb_dgemm": (_I, [_I, _I, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I, _P]),
     "dftb_bf16x3_gemm": (_I, [_I, _I, _I, _I, ctypes.POINTER(_P), _I, ctypes.POINTER(_P), _I, ctypes.c_float, _P, _I,
                               _P, _I, _P, _P, _I, _P, _P, _I, _P, _P]),
@@ -131,6 +133,17 @@ def stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
+def transpose(X):
+    """X^T of an FP64 CUDA matrix as a new contiguous tensor (dftb_transpose_f64: shared-memory tiles, where
+    torch's strided copy reads or writes one 32-byte sector per element)."""
+    if X.stride(1) != 1 or X.stride(0) < X.shape[1]:
+        X = X.contiguous()
+    rows, cols = X.shape
+    Y = torch.empty((cols, rows), dtype=torch.float64, device=X.device)
+    call("dftb_transpose_f64", rows, cols, ptr(X), max(1, X.stride(0)), ptr(Y), max(1, rows), stream())
+    return Y
+
+
 def check(rc, what):
     if rc != DFTB_OK:
         msg = ""
@@ -144,8 +157,8 @@ def check(rc, what):
 # kernels launched per entry point (dgemm-backed entry points launch several)
 KERNELS_PER_CALL = {
     "dftb_directional_cosines": 1, "dftb_h0_and_s": 1, "dftb_dipole_matrix": 1, "dftb_gamma_matrices": 1,
-    "dftb_ao_expand": 1, "dftb_scc_hamiltonian": 2, "dftb_monopoles": 1, "dftb_trans_charges": 6,
-    "dftb_trans_charges_diag": 5, "dftb_trans_charges_noalloc": 6, "dftb_hermitian_rv": 3, "dftb_apbv": 2, "dftb_ambv": 1,
+    "dftb_ao_expand": 1, "dftb_scc_hamiltonian": 2, "dftb_monopoles": 1, "dftb_trans_charges": 4,
+    "dftb_trans_charges_diag": 3, "dftb_trans_charges_noalloc": 6, "dftb_hermitian_rv": 3, "dftb_apbv": 2, "dftb_ambv": 1,
     "dftb_davidson_precondition": 1, "dftb_davidson_residual": 2, "dftb_dgemm": 1,
     "dftb_gradients_h0_and_s": 3, "dftb_sk_gradient_contract": 1, "dftb_pair_gradients": 1,
     "dftb_repulsive_energy": 1, "dftb_mlp_bias_relu": 1, "dftb_mlp_relu_backward": 1, "dftb_mlp_output": 1,

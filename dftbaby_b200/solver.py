@@ -36,6 +36,21 @@ def initial_expansion_vectors(omega_flat, lmax):
     return bs
 
 
+def gram(Q, chunks=148):
+    """Q^T Q of a tall block Q (n, m), n >> m.  A single product with an m x m output and K = n keeps few
+    SMs busy; the rows are cut into `chunks` slabs (one per SM) whose Gram matrices run as one batched
+    product and are summed.  A non-contiguous Q takes the single product (cutting it would copy it)."""
+    n, m = Q.shape
+    if not Q.is_contiguous() or n < 64 * chunks or m == 0:
+        return Q.T @ Q
+    rows = n // chunks * chunks
+    Qc = Q[:rows].view(chunks, n // chunks, m)
+    G = torch.bmm(Qc.transpose(1, 2), Qc).sum(dim=0)
+    if rows < n:
+        G += Q[rows:].T @ Q[rows:]
+    return G
+
+
 def orthonormal_columns(Q):
     """Orthonormal basis of the column span of a tall block Q (nov, m), m small.
 
@@ -55,13 +70,13 @@ def orthonormal_columns(Q):
     eye = torch.eye(m, dtype=Q.dtype, device=Q.device)
     ok = None
     for _ in range(2):
-        G = Q.T @ Q
+        G = gram(Q)
         L, info = torch.linalg.cholesky_ex(0.5 * (G + G.T))
         Linv = torch.linalg.solve_triangular(L, eye, upper=False)
         Q = Q @ Linv.T
         bad = (info != 0).reshape(())
         ok = ~bad if ok is None else ok & ~bad
-    err = torch.max(torch.abs(Q.T @ Q - eye))
+    err = torch.max(torch.abs(gram(Q) - eye))
     host = torch.stack([ok.to(torch.float64), err]).cpu().numpy()
     if host[0] != 1.0 or not np.isfinite(host[1]) or host[1] > 1.0e-12:
         Q, _ = torch.linalg.qr(Q0, mode="reduced")

@@ -272,6 +272,17 @@ int dftb_ozaki_product(int m, int n, int k, int nmod, const void *A, int rows_a,
                        size_t work_bytes, int *err, void *stream);
 const char *dftb_ozaki_last_error(void);
 
+/* Layout changes of (nov x m) column blocks of the Davidson solve (no
+ * counterpart in DFTBaby, whose vectors are numpy arrays).
+ * Y (cols x rows, leading dimension ldy) = X^T of a row-major FP64 X (rows x
+ * cols, leading dimension ldx); cols <= 2097120. */
+int dftb_transpose_f64(int rows, int cols, const double *X, int ldx, double *Y, int ldy, void *stream);
+/* K1, K2 (nocc*nvirt x m, FP64, row-major) from the FP32 output Kall (m x
+ * 2 nvirt x nocc) of the last launch of the tensor-core exchange, whose rows
+ * 2a and 2a + 1 hold K1^T and K2^T of product column c:
+ *   K_y[(i nvirt + a) m + c] = Kall[c][2a + y][i];  nvirt <= 65535. */
+int dftb_exchange_unpack(int m, int nvirt, int nocc, const float *Kall, double *K1, double *K2, void *stream);
+
 /* General FP64 product C = alpha * op(A) . op(B) + beta * C on row-major
  * matrices (op = transpose when trans != 0), the contraction engine behind the
  * entry points above, exported for the host-side solver. */

@@ -10,8 +10,11 @@ from dftbaby_b200 import geometry, native
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name", ["polyene20_lc", "armchair2_lc", "polyene12_nolc"])
-def test_subspace_scc_matches_oracle(name):
+@pytest.mark.parametrize("name,start", [("polyene20_lc", 0.1), ("armchair2_lc", 0.1), ("polyene12_nolc", 0.1),
+                                        ("polyene20_lc", 0.3), ("armchair2_lc", 0.3)])
+def test_subspace_scc_matches_oracle(name, start):
+    """start: the relative density change below which tracking replaces the dense eigensolve (0.1, the
+    default, and 0.3, the benchmark's)."""
     native.load()
     from dftbaby_b200.lr_tddftb import LR_TDDFTB
     from oracle import dftb_oracle as O
@@ -23,7 +26,7 @@ def test_subspace_scc_matches_oracle(name):
     E_o = o.getEnergy()
     td = LR_TDDFTB(al, long_range_correction=lc)
     td.setGeometry(al)
-    Om_s, f_s = td.getEnergies(nstates=6, diag_conv=1e-8, eigensolver="subspace")
+    Om_s, f_s = td.getEnergies(nstates=6, diag_conv=1e-8, eigensolver="subspace", subspace_start=start)
     d = td.dftb2
     assert d.subspace_iterations > 0.5 * d.scc_iterations  # most iterations skipped the dense eigensolve
     assert d.scc_iterations == o.scc_iterations
@@ -59,6 +62,9 @@ def test_subspace_scc_with_level_shift_follows_the_dense_path():
     (Ef, nf, _, dqf, ef), (Es, ns, nsub, dqs, es) = runs["full"], runs["subspace"]
     assert nsub > 0.9 * ns
     assert ns == nf
-    # both stop on DFTBaby's DIIS-change criterion, within ~1e-7 of the fixed point
-    assert abs(Es - Ef) < 1e-9
+    # both stop on DFTBaby's DIIS-change criterion, within ~1e-7 of the fixed point.  Over 230 DIIS iterations
+    # between exactly degenerate levels the iterate that meets it moves with the tracking's residual: the
+    # two paths agree to 3e-10 Ha when tracking divides by the virtual levels of the last full solve and to
+    # 3e-9 Ha with the current levels (which bring the benchmark flake's orbital energies ten times closer)
+    assert abs(Es - Ef) < 1e-8
     assert np.abs(dqs - dqf).max() < 1e-6 and np.abs(es - ef).max() < 1e-6
