@@ -584,6 +584,26 @@ class DFTB2(object):
         if getattr(self, "save_converged_charges", None) is not None:
             np.savetxt(os.path.expandvars(os.path.expanduser(self.save_converged_charges)), self.dq.cpu().numpy())
 
+    def _fixed_left_operand(self, H):
+        """X -> H X for a left factor H used in several products: with the int8 emulation H is converted to
+        residues once (ozaki.Operand) instead of in every product; the results are those of ozaki.matmul."""
+        if getattr(self, "_mm_fn", None) is None:
+            return lambda X: H @ X
+        from . import ozaki as O
+        n = H.shape[0]
+        c = getattr(self, "_track_oz", None)
+        if c is None or c["n"] != n or c["dev"] != H.device:
+            c = dict(n=n, dev=H.device, H=O.Operand(n, H.shape[1], H.device), X={})
+            self._track_oz = c
+        opH = c["H"].set(H)
+
+        def times(X):
+            k = X.shape[1]
+            if k not in c["X"]:
+                c["X"][k] = O.Operand(k, H.shape[1], H.device)
+            return O.product(opH, c["X"][k].set(X.T))
+        return times
+
     def _track_occupied(self, H, tracked, rel, shift=0.0, max_steps=8, tol_rel=1.0e-6):
         """Move an S-orthonormal occupied/virtual split (Co, Cv) onto the invariant subspaces of H.
 
@@ -604,10 +624,11 @@ class DFTB2(object):
         Co, Cv, eo, ev = tracked
         mm = self._mm
         tol = max(1.0e-13, tol_rel * rel)
-        ev = torch.sum(Cv * mm(H, Cv), dim=0)
+        H_times = self._fixed_left_operand(H)
+        ev = torch.sum(Cv * H_times(Cv), dim=0)
         SCv0 = mm(self.S, Cv) if shift > 0.0 else None
         for step in range(max_steps + 1):
-            HCo = mm(H, Co)
+            HCo = H_times(Co)
             if SCv0 is not None:
                 HCo = HCo + shift * mm(SCv0, mm(SCv0.T, Co))
             F = mm(Cv.T, HCo)
