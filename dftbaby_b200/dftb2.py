@@ -590,6 +590,8 @@ class DFTB2(object):
         if getattr(self, "_mm_fn", None) is None:
             return lambda X: H @ X
         from . import ozaki as O
+        if H.shape[1] > O.KMAX:
+            return lambda X: O.matmul(H, X)  # K beyond one operand's exact range: matmul splits it
         n = H.shape[0]
         c = getattr(self, "_track_oz", None)
         if c is None or c["n"] != n or c["dev"] != H.device:
