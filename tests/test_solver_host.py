@@ -69,3 +69,65 @@ def test_basis_projected_matrices_match_full_projection(mirror):
     if mirror:
         l0 = 10
         assert torch.equal(B.M[0][l0:, :l0], B.M[0][:l0, l0:].T)
+
+
+@pytest.mark.parametrize("n,m,sliced", [(20000, 1, False), (20000, 7, False), (9473, 60, False), (30001, 24, True)])
+def test_gram_slabs_match_the_single_product(n, m, sliced):
+    """solver.gram cuts tall blocks into one slab per SM for a batched product: the same Q^T Q as one
+    product, up to the rounding of a different summation order; rows left over after the slabs and
+    non-contiguous blocks (which take the single product) included."""
+    from dftbaby_b200.solver import gram
+    g = torch.Generator().manual_seed(n + m)
+    Q = torch.randn(n, m + 5 if sliced else m, generator=g, dtype=torch.float64)
+    Q = Q[:, :m] if sliced else Q
+    G, ref = gram(Q), Q.T @ Q
+    assert G.shape == (m, m)
+    assert (G - ref).abs().max().item() < 1e-13 * n
+
+
+def test_orthonormal_columns_through_slabs():
+    """A block tall enough for the slab Gram products still comes out orthonormal and spanning the input."""
+    A = _block(12000, 20, 1e6, seed=7)
+    Q = orthonormal_columns(A)
+    eye = torch.eye(20, dtype=torch.float64)
+    assert (Q.T @ Q - eye).abs().max().item() < 1e-12
+    Qh, _ = torch.linalg.qr(A)
+    assert (Q - Qh @ (Qh.T @ Q)).abs().max().item() < 1e-10
+
+
+def test_diis_gram_by_dot_products_matches_the_stacked_product():
+    """DIIS_80 forms the Gram matrix of long (>= 2^20 entries) residuals by dot products instead of one
+    product of the stacked residuals; the extrapolated densities are the same to rounding."""
+    from dftbaby_b200.dftb2 import DIIS_80
+    g = torch.Generator().manual_seed(11)
+    base = torch.randn(1024, 1024, generator=g, dtype=torch.float64)
+    seq = [base + 0.5 ** k * torch.randn(1024, 1024, generator=g, dtype=torch.float64) for k in range(9)]
+    d = DIIS_80(5)
+    trial, resid, outs, refs = [], [], [], []
+    for k, P in enumerate(seq):
+        d.start_flag = k >= 4
+        outs.append(d.next_approximation(P.clone()).reshape(-1))
+        # the same bookkeeping with the Gram matrix of the stacked residuals
+        trial.append(P.reshape(-1).clone())
+        if len(trial) >= 2:
+            resid.append(trial[-1] - trial[-2])
+        if len(trial) > 5:
+            trial.pop(0)
+            resid.pop(0)
+        if k < 4:
+            refs.append(P.reshape(-1))
+            continue
+        n = len(resid)
+        R = torch.stack(resid)
+        A = np.zeros((n + 1, n + 1))
+        A[:n, :n] = (R @ R.T).numpy()
+        A[:n, n] = A[n, :n] = -1.0
+        b = np.zeros(n + 1)
+        b[-1] = -1.0
+        c = np.linalg.solve(A, b)
+        p = sum(float(c[i]) * trial[i] for i in range(n))
+        trial[-1] = p
+        resid[-1] = p - trial[-2]
+        refs.append(p)
+    for o, r in zip(outs, refs):
+        assert (o - r).abs().max().item() < 1e-10 * r.abs().max().item()
