@@ -11,10 +11,12 @@
  *   - the return value is a status code (DFTB_OK or a negative DFTB_ERR_*);
  *     no entry point allocates device memory -- where scratch space is needed
  *     the caller passes a workspace whose size the *_workspace_size query
- *     returns.  The one exception is library state: dftb_apbv (cuBLAS) and
+ *     returns.  The one exception is library state: dftb_apbv and
+ *     dftb_trans_charges / dftb_trans_charges_diag (cuBLAS) and
  *     dftb_batched_eigh (cuSOLVER) create one handle per calling thread and
  *     device on first use, and those handles hold the libraries' own device
- *     memory until the process exits.
+ *     memory until the process exits.  dftb_trans_charges_noalloc uses no
+ *     library handle.
  *
  * Each function cites the DFTBaby interface it replaces (file:line inside the
  * DFTBaby project).
@@ -117,7 +119,9 @@ int dftb_monopoles(int norb, int nat, const double *P, const double *P0, const d
  *   orbs_occ: (norb, nocc), orbs_virt: (norb, nvirt), S: (norb, norb);
  *   q_oo: (nat, nocc, nocc), q_ov: (nat, nocc, nvirt), q_vv: (nat, nvirt, nvirt);
  *   any of the three outputs may be NULL to skip it;
- *   work: at least dftb_trans_charges_workspace_size() bytes. */
+ *   work: at least dftb_trans_charges_workspace_size() bytes.
+ * The two S.C products run in cuBLAS (cublasDgemm, resolved at run time) when
+ * libcublas can be loaded, otherwise in the library's own FP64 GEMM. */
 size_t dftb_trans_charges_workspace_size(int norb, int nocc, int nvirt);
 int dftb_trans_charges(int norb, int nat, int nocc, int nvirt, const double *orbs_occ, const double *orbs_virt,
                        const double *S, const int *orbs_per_atom, double *q_oo, double *q_ov, double *q_vv,
