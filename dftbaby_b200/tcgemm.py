@@ -119,7 +119,19 @@ def gemm(A, B, K=None, refine=True, alpha=1.0, G=None, out=None, out_pair=None, 
     if ksplit is None:
         ksplit = 1
         if out is not None and G is None and out_pair is None and out_pair_t is None and tiles < SMS:
-            ksplit = max(1, min(16, (2 * SMS) // tiles, (K + 63) // 64 // 8))
+            # K ranges per output tile: a persistent launch runs ceil(tiles ks / SMS) rounds of 1/ks of a tile's
+            # work, so take the ks with the fewest rounds per ks (2 % added per extra range for its atomics and
+            # pipeline refill; at least 32 K-blocks per range).  The exchange's 2450 x 1225 x 8292 launch (100
+            # wide tiles) gets ks = 4 instead of 2: 0.176 -> 0.170 ms, less than the rounds predict
+            kblocks = (K + (32 if wide else 64) - 1) // (32 if wide else 64)
+            best = (1.0, 1)
+            for ks in range(2, 17):
+                if kblocks // ks < 32:
+                    break
+                cost = -(-tiles * ks // SMS) / ks * (1.0 + 0.02 * (ks - 1))
+                if cost < best[0] - 1e-12:
+                    best = (cost, ks)
+            ksplit = best[1]
     if ksplit > 1:
         out.zero_()
     err = _errword(A.hi.device)
